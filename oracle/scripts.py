@@ -1,0 +1,408 @@
+"""Oracle drivers: CPU restatements of the reference scripts' solver functions.
+
+Each ``Case`` subclass mirrors one script of PTsolvers/PseudoTransientStokes.jl:
+
+  ``V2D``        scripts/Stokes2D.jl:72-169             (2D viscous, 4 role kernels)
+  ``VE2D``       scripts/Stokes2D_ve.jl:87-206          (2D Maxwell VE, 4 role kernels)
+  ``VE2DPerf``   scripts/Stokes2D_ve_perf.jl:80-197     (2D VE, fused explicit-index kernels)
+  ``VE3D``       scripts/stokes_3D/Stokes3D_ve_multixpu.jl:118-295 (3D VE, 1 rank)
+  ``VE3DPerf``   scripts/stokes_3D/Stokes3D_ve_perf.jl:116-255     (3D VE, fused kernels)
+  ``V3D``        3D viscous: no reference script; the 3D perf kernels with the elastic
+                 terms removed and the viscous iteration parameters of Stokes2D.jl:27-31.
+
+Arrays are Float64 column-major numpy arrays with the reference's own extents, so the
+oracle state can be compared field by field with the CUDA path (test infrastructure only).
+"""
+import ctypes
+import math
+
+import numpy as np
+
+from .binding import lib, arr, stats
+
+PI = math.pi
+
+
+def linrange(a, b, n):
+    """Julia ``LinRange(a, b, n)`` element values: (1-t)*a + t*b with t = (i-1)/(n-1)."""
+    out = np.empty(n)
+    d = n - 1
+    for j in range(n):
+        t = j / d if d > 0 else 0.0
+        out[j] = (1 - t) * a + t * b
+    return out
+
+
+def zeros(*shape):
+    return np.zeros(shape, dtype=np.float64, order="F")
+
+
+class Case:
+    """Common driver state. Subclasses set the per-script physics, numerics and kernels."""
+
+    ndim = 2
+    elastic = True
+    # numerics defaults (overridable through keyword arguments)
+    defaults = {}
+
+    def __init__(self, nx, ny, nz=None, **kw):
+        self.nx, self.ny, self.nz = nx, ny, nz
+        p = dict(lx=10.0, ly=10.0, lz=10.0, xi=1.0, mus0=1.0, musi=1e-3, G=1.0, ebg=1.0)
+        p.update(self.defaults)
+        p.update(kw)
+        self.p = p
+        for k, v in p.items():
+            setattr(self, k, v)
+        self.dt = self.mus0 / (self.G * self.xi)
+        self.L = lib()
+        self.f = {}
+        self.iters = []
+        self.err_hist = []
+
+    # ---------------------------------------------------------------- helpers
+    def A(self, name):
+        return arr(self.f[name])
+
+    def alloc(self, **shapes):
+        for k, s in shapes.items():
+            self.f[k] = zeros(*s)
+
+    # ---------------------------------------------------------------- driver
+    def run(self, nt=None, iter_max=None, nout=None, eps=None):
+        """The reference's time loop + PT loop (e.g. Stokes3D_ve_perf.jl:192-226)."""
+        nt = self.nt if nt is None else nt
+        iter_max = self.iterMax if iter_max is None else iter_max
+        nout = self.nout if nout is None else nout
+        eps = self.eps if eps is None else eps
+        self.ittot = 0
+        for it in range(1, nt + 1):
+            err = 2 * eps
+            it_ = 0
+            if self.elastic:
+                self.assign_tau()
+            while err > eps and it_ <= iter_max:
+                self.iteration()
+                it_ += 1
+                if it_ % nout == 0:
+                    err, norms = self.check()
+                    self.err_hist.append((it, it_, err, norms))
+                    if math.isnan(err):
+                        raise FloatingPointError("NaN")
+            self.iters.append(it_)
+            self.ittot += it_
+        return self
+
+    def norm_err(self, names_R, name_div, len_over=None):
+        """err = max(norm_R..., norm_∇V) as in Stokes3D_ve_perf.jl:211-218."""
+        _, vmin, vmax = stats(self.f["Vx"])
+        _, pmin, pmax = stats(self.f["Pt"])
+        norms = []
+        for n in names_R:
+            s, _, _ = stats(self.f[n])
+            norms.append(math.sqrt(s) / (pmax - pmin) * self.lx / math.sqrt(self.f[n].size))
+        s, _, _ = stats(self.f[name_div])
+        norms.append(math.sqrt(s) / (vmax - vmin) * self.lx / math.sqrt(self.f[name_div].size))
+        return max(norms), norms
+
+
+class _Case2D(Case):
+    ndim = 2
+
+    def setup(self):
+        """Allocations, initial conditions and iteration parameters (Stokes2D.jl:87-125)."""
+        nx, ny, L = self.nx, self.ny, self.L
+        self.dx, self.dy = self.lx / nx, self.ly / ny
+        self._dx, self._dy = 1.0 / self.dx, 1.0 / self.dy
+        self.max_lxy = max(self.lx, self.ly)
+        self.Vpdt = min(self.dx, self.dy) * self.CFL
+        self.xc = linrange(self.dx / 2, self.lx - self.dx / 2, nx)
+        self.yc = linrange(self.dy / 2, self.ly - self.dy / 2, ny)
+        self.alloc(Pt=(nx, ny), divV=(nx, ny), txx=(nx, ny), tyy=(nx, ny), txy=(nx - 1, ny - 1),
+                   Rx=(nx - 1, ny - 2), Ry=(nx - 2, ny - 1), dVx=(nx - 1, ny - 2), dVy=(nx - 2, ny - 1),
+                   Mus2=(nx, ny), Must=(nx, ny), Gdt=(nx, ny), dtRho=(nx, ny))
+        if self.elastic:
+            self.alloc(txx_o=(nx, ny), tyy_o=(nx, ny), txy_o=(nx - 1, ny - 1))
+        dx, dy, lx, ly = self.dx, self.dy, self.lx, self.ly
+        ix = np.arange(1, nx + 2, dtype=np.float64)
+        iy = np.arange(1, ny + 2, dtype=np.float64)
+        X = (ix[:nx] - 1) * dx + 0.5 * dx - 0.5 * lx
+        Y = (iy[:ny] - 1) * dy + 0.5 * dy - 0.5 * ly
+        Rad2 = np.asfortranarray(X[:, None] ** 2 + Y[None, :] ** 2)
+        self.f["Vx"] = np.asfortranarray(np.repeat((-self.ebg * ((ix - 1) * dx - 0.5 * lx))[:, None], ny, axis=1))
+        self.f["Vy"] = np.asfortranarray(np.repeat((self.ebg * ((iy - 1) * dy - 0.5 * ly))[None, :], nx, axis=0))
+        Mus = self.mus0 * np.ones((nx, ny), order="F")
+        Mus[Rad2 < 1.0] = self.musi
+        self.init_viscosity(Mus)
+        return self
+
+    def init_viscosity(self, Mus):
+        """Smoothing, local-max viscosity and iteration parameters (Stokes2D.jl:115-125)."""
+        L = self.L
+        Mus2 = self.f["Mus2"]
+        Mus2[...] = Mus
+        for _ in range(10):
+            L.ora2_smooth(arr(Mus2), arr(Mus), 1.0)
+            Mus, Mus2 = Mus2, Mus
+        self.f["Mus"], self.f["Mus2"] = Mus, Mus2
+        Must = self.f["Must"]
+        Must[...] = Mus
+        L.ora2_maxloc(arr(Must), arr(Mus))
+        L.ora2_bc_x(arr(Must))
+        L.ora2_bc_y(arr(Must))
+        self.iter_params()
+
+    def bc(self):
+        self.L.ora2_bc_y(self.A("Vx"))
+        self.L.ora2_bc_x(self.A("Vy"))
+
+    def assign_tau(self):
+        for n in ("txx", "tyy", "txy"):
+            self.L.ora_copy(self.A(n + "_o"), self.A(n))
+
+
+class V2D(_Case2D):
+    """scripts/Stokes2D.jl (2D viscous)."""
+
+    elastic = False
+    defaults = dict(nt=1, iterMax=1e5, nout=500, eps=1e-8, CFL=0.9 / math.sqrt(2), Re=5 * PI, r=1.0)
+
+    def iter_params(self):
+        self.L.ora_iter_params_v(self.A("dtRho"), self.A("Gdt"), self.A("Must"), self.Vpdt, self.Re, self.r,
+                                 self.max_lxy)
+
+    def iteration(self):
+        L, A = self.L, self.A
+        L.ora2_compute_P(A("divV"), A("Pt"), A("Vx"), A("Vy"), A("Gdt"), self.r, self.dx, self.dy)
+        L.ora2v_compute_tau(A("txx"), A("tyy"), A("txy"), A("Vx"), A("Vy"), A("Mus"), A("Gdt"), self.dx, self.dy)
+        L.ora2v_compute_dV(A("Rx"), A("Ry"), A("dVx"), A("dVy"), A("Pt"), A("txx"), A("tyy"), A("txy"),
+                           A("dtRho"), self.dx, self.dy)
+        L.ora2_compute_V(A("Vx"), A("Vy"), A("dVx"), A("dVy"))
+        self.bc()
+
+    def check(self):
+        # Rx, Ry come from compute_dV! of this iteration (Stokes2D.jl:136-143)
+        return self.norm_err(("Rx", "Ry"), "divV")
+
+
+class VE2D(_Case2D):
+    """scripts/Stokes2D_ve.jl (2D Maxwell visco-elastic, role kernels)."""
+
+    defaults = dict(nt=5, iterMax=2e5, nout=200, eps=1e-8, CFL=0.8 / math.sqrt(2), Re=5 * PI, r=1.0)
+
+    def iter_params(self):
+        self.L.ora_iter_params_ve(self.A("dtRho"), self.A("Gdt"), self.A("Must"), self.Vpdt, self.G, self.dt,
+                                  self.Re, self.r, self.max_lxy)
+
+    def iteration(self):
+        L, A = self.L, self.A
+        L.ora2_compute_P(A("divV"), A("Pt"), A("Vx"), A("Vy"), A("Gdt"), self.r, self.dx, self.dy)
+        L.ora2ve_compute_tau(A("txx"), A("tyy"), A("txy"), A("txx_o"), A("tyy_o"), A("txy_o"), A("Gdt"), A("Vx"),
+                             A("Vy"), A("Mus"), self.G, self.dt, self.dx, self.dy)
+        L.ora2ve_compute_dV(A("dVx"), A("dVy"), A("Pt"), A("txx"), A("tyy"), A("txy"), A("dtRho"), self.dx, self.dy)
+        L.ora2_compute_V(A("Vx"), A("Vy"), A("dVx"), A("dVy"))
+        self.bc()
+
+    def check(self):
+        A = self.A
+        self.L.ora2ve_compute_Res(A("Rx"), A("Ry"), A("Pt"), A("txx"), A("tyy"), A("txy"), self.dx, self.dy)
+        return self.norm_err(("Rx", "Ry"), "divV")
+
+
+class VE2DPerf(VE2D):
+    """scripts/Stokes2D_ve_perf.jl (2D VE, fused explicit-index kernels)."""
+
+    defaults = dict(nt=1, iterMax=100, nout=2000, eps=1e-8, CFL=0.8 / math.sqrt(2), Re=5 * PI, r=1.0)
+
+    def iteration(self):
+        L, A = self.L, self.A
+        L.ora2p_compute_Pt_tau(A("Pt"), A("txx"), A("tyy"), A("txy"), A("txx_o"), A("tyy_o"), A("txy_o"), A("Gdt"),
+                               A("Vx"), A("Vy"), A("Mus"), self.r, self.G, self.dt, self._dx, self._dy)
+        Vx, Vy = self.f["Vx"], self.f["Vy"]
+        L.ora2p_compute_V(A("Vx"), A("Vy"), A("Pt"), A("txx"), A("tyy"), A("txy"), A("dtRho"), self._dx, self._dy,
+                          Vx.shape[0] - 2, Vx.shape[1] - 2, Vy.shape[0] - 2, Vy.shape[1] - 2)
+        self.bc()
+
+    def check(self):
+        A = self.A
+        self.L.ora2p_compute_Res(A("divV"), A("Rx"), A("Ry"), A("Pt"), A("Vx"), A("Vy"), A("txx"), A("tyy"),
+                                 A("txy"), self._dx, self._dy)
+        return self.norm_err(("Rx", "Ry"), "divV")
+
+
+class _Case3D(Case):
+    ndim = 3
+    igg_coords = False  # Stokes3D_ve_multixpu.jl builds the ICs through ImplicitGlobalGrid's x_g
+
+    def setup(self):
+        """Allocations, initial conditions and iteration parameters (Stokes3D_ve_perf.jl:135-192)."""
+        nx, ny, nz = self.nx, self.ny, self.nz
+        self.dx, self.dy, self.dz = self.lx / nx, self.ly / ny, self.lz / nz
+        self._dx, self._dy, self._dz = 1.0 / self.dx, 1.0 / self.dy, 1.0 / self.dz
+        self.max_lxyz = max(self.lx, self.ly, self.lz)
+        self.Vpdt = min(self.dx, self.dy, self.dz) * self.CFL
+        self.xc = linrange(self.dx / 2, self.lx - self.dx / 2, nx)
+        self.yc = linrange(self.dy / 2, self.ly - self.dy / 2, ny)
+        self.zc = linrange(self.dz / 2, self.lz - self.dz / 2, nz)
+        self.alloc(Pt=(nx, ny, nz), dtRho=(nx, ny, nz), Gdt=(nx, ny, nz), divV=(nx, ny, nz), Vy=(nx, ny + 1, nz),
+                   txx=(nx, ny - 2, nz - 2), tyy=(nx - 2, ny, nz - 2), tzz=(nx - 2, ny - 2, nz),
+                   txy=(nx - 1, ny - 1, nz - 2), txz=(nx - 1, ny - 2, nz - 1), tyz=(nx - 2, ny - 1, nz - 1),
+                   Rx=(nx - 1, ny - 2, nz - 2), Ry=(nx - 2, ny - 1, nz - 2), Rz=(nx - 2, ny - 2, nz - 1),
+                   Mus2=(nx, ny, nz), Must=(nx, ny, nz))
+        if self.elastic:
+            for n in ("txx", "tyy", "tzz", "txy", "txz", "tyz"):
+                self.f[n + "_o"] = zeros(*self.f[n].shape)
+        if self.unfused:
+            self.alloc(dVx=(nx - 1, ny - 2, nz - 2), dVy=(nx - 2, ny - 1, nz - 2), dVz=(nx - 2, ny - 2, nz - 1))
+        dx, dy, dz, lx, ly, lz = self.dx, self.dy, self.dz, self.lx, self.ly, self.lz
+        ix = np.arange(1, nx + 2, dtype=np.float64)
+        iy = np.arange(1, ny + 1, dtype=np.float64)
+        iz = np.arange(1, nz + 2, dtype=np.float64)
+        X = (ix[:nx] - 1) * dx + 0.5 * dx - 0.5 * lx
+        Y = (iy - 1) * dy + 0.5 * dy - 0.5 * ly
+        Z = (iz[:nz] - 1) * dz + 0.5 * dz - 0.5 * lz
+        if self.igg_coords:
+            # x_g(ix,dx,A) = (ix-1)*dx + 0.5*(nx_g-size(A,1))*dx (ImplicitGlobalGrid, 1 rank);
+            # for the staggered Vx/Vz this is (ix-1)*dx - 0.5*dx (Stokes3D_ve_multixpu.jl:174-176).
+            xv = ((ix - 1) * dx + (-0.5 * dx)) + 0.5 * dx - 0.5 * lx
+            zv = ((iz - 1) * dz + (-0.5 * dz)) + 0.5 * dz - 0.5 * lz
+            X = ((ix[:nx] - 1) * dx + 0.0) + 0.5 * dx - 0.5 * lx
+            Y = ((iy - 1) * dy + 0.0) + 0.5 * dy - 0.5 * ly
+            Z = ((iz[:nz] - 1) * dz + 0.0) + 0.5 * dz - 0.5 * lz
+        else:
+            xv = (ix - 1) * dx - 0.5 * lx
+            zv = (iz - 1) * dz - 0.5 * lz
+        Rad2 = (X[:, None, None] ** 2 + Y[None, :, None] ** 2) + Z[None, None, :] ** 2
+        self.f["Vx"] = np.asfortranarray(np.broadcast_to((-self.ebg * xv)[:, None, None], (nx + 1, ny, nz)))
+        self.f["Vz"] = np.asfortranarray(np.broadcast_to((self.ebg * zv)[None, None, :], (nx, ny, nz + 1)))
+        Mus = self.mus0 * np.ones((nx, ny, nz), order="F")
+        Mus[Rad2 < 1.0] = self.musi
+        self.init_viscosity(Mus)
+        return self
+
+    def init_viscosity(self, Mus):
+        """Smoothing, local-max viscosity and iteration parameters (Stokes3D_ve_perf.jl:173-192)."""
+        L = self.L
+        Mus = np.asfortranarray(Mus, dtype=np.float64)
+        Mus2 = self.f["Mus2"]
+        Mus2[...] = Mus
+        for _ in range(10):
+            L.ora3_smooth(arr(Mus2), arr(Mus), 1.0)
+            Mus, Mus2 = Mus2, Mus
+        self.f["Mus"], self.f["Mus2"] = Mus, Mus2
+        Must = self.f["Must"]
+        Must[...] = Mus
+        L.ora3_maxloc(arr(Must), arr(Mus))
+        L.ora3_bc_x(arr(Must))
+        L.ora3_bc_y(arr(Must))
+        L.ora3_bc_z(arr(Must))
+        self.iter_params()
+
+    def iter_params(self):
+        if self.elastic:
+            self.L.ora_iter_params_ve(self.A("dtRho"), self.A("Gdt"), self.A("Must"), self.Vpdt, self.G, self.dt,
+                                      self.Re, self.r, self.max_lxyz)
+        else:
+            self.L.ora_iter_params_v(self.A("dtRho"), self.A("Gdt"), self.A("Must"), self.Vpdt, self.Re, self.r,
+                                     self.max_lxyz)
+
+    def bc(self):
+        """The six free-slip copies, in the reference's order (Stokes3D_ve_perf.jl:202-207)."""
+        L, A = self.L, self.A
+        L.ora3_bc_x(A("Vy"))
+        L.ora3_bc_x(A("Vz"))
+        L.ora3_bc_y(A("Vx"))
+        L.ora3_bc_y(A("Vz"))
+        L.ora3_bc_z(A("Vx"))
+        L.ora3_bc_z(A("Vy"))
+
+    def assign_tau(self):
+        for n in ("txx", "tyy", "tzz", "txy", "txz", "tyz"):
+            self.L.ora_copy(self.A(n + "_o"), self.A(n))
+
+    def _tau_o(self):
+        if self.elastic:
+            return [self.A(n + "_o") for n in ("txx", "tyy", "tzz", "txy", "txz", "tyz")]
+        return [arr(None)] * 6
+
+    def _tau(self):
+        return [self.A(n) for n in ("txx", "tyy", "tzz", "txy", "txz", "tyz")]
+
+
+class VE3D(_Case3D):
+    """scripts/stokes_3D/Stokes3D_ve_multixpu.jl on one rank (role kernels, /dx form)."""
+
+    unfused = True
+    igg_coords = True
+    defaults = dict(nt=5, iterMax=2e5, nout=200, eps=1e-8, CFL=0.8 / math.sqrt(3), Re=6 * PI, r=1.0)
+
+    def iteration(self):
+        L, A = self.L, self.A
+        L.ora3m_compute_P(A("divV"), A("Pt"), A("Vx"), A("Vy"), A("Vz"), A("Gdt"), self.r, self.dx, self.dy, self.dz)
+        L.ora3m_compute_tau(*self._tau(), *self._tau_o(), A("Vx"), A("Vy"), A("Vz"), A("Mus"), A("Gdt"), self.G,
+                            self.dt, self.dx, self.dy, self.dz, int(self.elastic))
+        L.ora3m_compute_dV(A("dVx"), A("dVy"), A("dVz"), A("Pt"), *self._tau(), A("dtRho"), self.dx, self.dy,
+                           self.dz, 0)
+        L.ora3_compute_V(A("Vx"), A("Vy"), A("Vz"), A("dVx"), A("dVy"), A("dVz"))
+        self.bc()
+
+    def check(self):
+        A = self.A
+        self.L.ora3m_compute_dV(A("Rx"), A("Ry"), A("Rz"), A("Pt"), *self._tau(), arr(None), self.dx, self.dy,
+                                self.dz, 1)
+        return self.norm_err(("Rx", "Ry", "Rz"), "divV")
+
+
+class VE3DPerf(_Case3D):
+    """scripts/stokes_3D/Stokes3D_ve_perf.jl (fused explicit-index kernels, _dx form)."""
+
+    unfused = False
+    defaults = dict(nt=1, iterMax=200, nout=2000, eps=1e-8, CFL=0.8 / math.sqrt(3), Re=6 * PI, r=1.0)
+
+    def iteration(self):
+        L, A = self.L, self.A
+        L.ora3p_compute_Pt_tau(A("Pt"), *self._tau(), *self._tau_o(), A("Vx"), A("Vy"), A("Vz"), A("Mus"), A("Gdt"),
+                               self.r, self.G, self.dt, self._dx, self._dy, self._dz, int(self.elastic))
+        L.ora3p_compute_V(A("Vx"), A("Vy"), A("Vz"), A("Pt"), *self._tau(), A("dtRho"), self._dx, self._dy,
+                          self._dz)
+        self.bc()
+
+    def check(self):
+        A = self.A
+        self.L.ora3p_compute_Res(A("divV"), A("Rx"), A("Ry"), A("Rz"), A("Vx"), A("Vy"), A("Vz"), A("Pt"),
+                                 *self._tau(), self._dx, self._dy, self._dz)
+        return self.norm_err(("Rx", "Ry", "Rz"), "divV")
+
+
+class V3D(VE3DPerf):
+    """3D viscous Stokes: the fused 3D kernels without elastic terms (no reference script)."""
+
+    elastic = False
+    defaults = dict(nt=1, iterMax=2e5, nout=200, eps=1e-8, CFL=0.8 / math.sqrt(3), Re=6 * PI, r=1.0)
+
+
+VARIANTS = {
+    "2d_v": V2D,
+    "2d_ve": VE2D,
+    "2d_ve_perf": VE2DPerf,
+    "3d_ve": VE3D,
+    "3d_ve_perf": VE3DPerf,
+    "3d_v": V3D,
+}
+
+
+def make(variant, nx, ny, nz=None, **kw):
+    return VARIANTS[variant](nx, ny, nz, **kw).setup()
+
+
+def fixture_sample(case):
+    """The reference test's sample: 12 indices per dimension (test/test_2D.jl:19-21)."""
+    def inds(n):
+        return (np.ceil(linrange(1.0, float(n), 12)).astype(np.int64) - 1)
+    ix = inds(case.nx)
+    iy = inds(case.ny)
+    if case.ndim == 2:
+        P = case.f["Pt"][np.ix_(ix, iy)]
+    else:
+        iz = inds(case.nz)
+        P = case.f["Pt"][np.ix_(ix, iy, iz)]
+    return case.xc[ix], P
