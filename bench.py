@@ -1,0 +1,345 @@
+"""Benchmark: T_eff of the 3D Maxwell visco-elastic PT iteration at 511^3 (FP64) on B200.
+
+A step is one check block of the reference's PT loop: `nout` PT iterations
+(compute_Pt_τ! + compute_V! + the free-slip copies) followed by one convergence check
+(compute_Res! + norms), for the Stokes3D_ve_perf.jl problem (spherical inclusion,
+pure shear) at nx = ny = nz = 511. T_eff = A_eff / t_it with the reference's
+A_eff = 29 * nx*ny*nz * 8 bytes per PT iteration (Stokes3D_ve_perf.jl:229).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank runs an independent replica (the path is single-GPU; there is
+no data-path collective): value = sum over ranks of the work / max-over-ranks time.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "pseudotransientstokes.jl_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "T_eff GB/s & time-to-tol 1e-8, 3D VE 511³: FP32+FP64 refine vs plain FP64, 1 B200"
+A_EFF_ARRAYS = 29  # Stokes3D_ve_perf.jl:229: (10*2 + 6*1 + 3) arrays per PT iteration
+
+
+def a_eff(n, itemsize=8):
+    return A_EFF_ARRAYS * n * n * n * itemsize
+
+
+def hbm_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        sm.sort()
+        med = sm[len(sm) // 2] if sm else None
+        return {"sm_mhz": med, "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return ws, rank, local, pg
+
+
+def max_over_ranks(x, pg):
+    if pg is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+# ------------------------------------------------------------------------------ CPU arm
+def cpu_sample(n, iters):
+    """The oracle's OpenMP FP64 restatement of Stokes3D_ve_perf.jl on the host cores."""
+    from oracle import scripts as S
+    from oracle.binding import lib
+
+    nthreads = lib().ora_num_threads()
+    c = S.make("3d_ve_perf", n, n, n)
+    c.assign_tau()
+    c.iteration()  # warm the pages
+    t0 = time.perf_counter()
+    for _ in range(iters):
+        c.iteration()
+    dt = time.perf_counter() - t0
+    return a_eff(n) * iters / dt / 1e9, nthreads, dt
+
+
+def run_reference(args, ws, rank, pg):
+    if rank != 0:
+        return
+    n = args.cpu_n
+    vals = []
+    for s in range(args.warmup + args.steps):
+        v, thr, dt = cpu_sample(n, args.cpu_iters)
+        if s >= args.warmup:
+            vals.append(v)
+    val = sum(vals) / len(vals)
+    sample = f"Stokes3D_ve_perf.jl kernels at {n}^3, {args.cpu_iters} PT iterations per step (OpenMP FP64 restatement)"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(val, 3), "unit": "GB/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (the reference's own inclusion problem)",
+        "config": {"workload": "3D VE Stokes (Stokes3D_ve_perf.jl), FP64, 511^3 box 10^3, inclusion r=1 mu=1e-3",
+                   "cpu_grid": n},
+        "cpu_baseline": {"value": round(val, 3), "unit": "GB/s", "cores": thr, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": round(val, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference's own CPU path (Julia ParallelStencil Threads) cannot run here: no Julia runtime; "
+                "timed instead: the oracle port of the same kernels",
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------------------ GPU arm
+def run_ours(args, ws, rank, local, pg):
+    import numpy as np
+    import torch
+
+    import ptstokes
+
+    torch.cuda.set_device(local)
+    n = args.n
+    nout = args.iters_per_step
+    variant = "3d_ve_perf"
+    s = ptstokes.Solver(variant, n, n, n, nout=nout, eps=0.0, iter_max=nout - 1)
+    s.setup_inclusion()
+    s.assign_tau()
+    stream = torch.cuda.ExternalStream(s.stream_handle())
+
+    def step():
+        s.solve()  # one graph launch: nout PT iterations + residual check; err readback
+
+    for _ in range(args.warmup):
+        step()
+    s.sync()
+    torch.cuda.synchronize()
+    barrier(pg)
+    clk = ClockSampler(local)
+    clk.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    barrier(pg)
+    clocks = clk.stop()
+    t_ms = max_over_ranks(e0.elapsed_time(e1), pg)
+    iters = args.steps * nout
+    t_it = t_ms / 1e3 / iters
+    value = ws * a_eff(n) / t_it / 1e9
+
+    # dominant kernel alone: compute_Pt_τ! (25 arrays/launch) and compute_V!+bc (14)
+    def time_kernel(fn, reps=10):
+        for _ in range(2):
+            fn()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        b.record(stream)
+        b.synchronize()
+        return a.elapsed_time(b) / reps
+
+    ms_A = time_kernel(s.compute_Pt_tau)
+    ms_B = time_kernel(s.compute_V_bc)
+    peak, peak_kind = hbm_peak()
+    bytes_A = 25 * n ** 3 * 8
+    achieved = bytes_A / (ms_A / 1e3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        try:
+            tj = json.load(open(tp)).get("k3_Pt_tau")
+            if tj:
+                traffic = tj["bytes_per_cell"] * n ** 3
+        except Exception:
+            traffic = None
+
+    # e2e through the public API with host buffers: per step upload the initial fields
+    # (Mus, Vx, Vy, Vz) from pinned host memory, set up, iterate, read Pt back.
+    e2e = None
+    if not args.no_e2e:
+        host = {}
+        # ICs exactly as the script builds them (Stokes3D_ve_perf.jl:164-172), in pinned memory
+        shapes = {"Vx": (n + 1, n, n), "Vy": (n, n + 1, n), "Vz": (n, n, n + 1), "Mus": (n, n, n)}
+        dx = 10.0 / n
+        for name, shp in shapes.items():
+            t = torch.empty(int(np.prod(shp)), dtype=torch.float64, pin_memory=True)
+            host[name] = t.numpy().reshape(shp, order="F")
+        ix = np.arange(n + 1, dtype=np.float64)
+        host["Vx"][...] = (-1.0 * (ix * dx - 0.5 * 10.0))[:, None, None]
+        host["Vy"][...] = 0.0
+        host["Vz"][...] = (1.0 * (ix * dx - 0.5 * 10.0))[None, None, :]
+        X = (ix[:n] * dx + 0.5 * dx) - 0.5 * 10.0
+        rad2 = (X[:, None, None] ** 2 + X[None, :, None] ** 2) + X[None, None, :] ** 2
+        host["Mus"][...] = np.where(rad2 < 1.0, 1e-3, 1.0)
+        out = torch.empty(n * n * n, dtype=torch.float64, pin_memory=True).numpy().reshape((n, n, n), order="F")
+        h2d = sum(a.nbytes for a in host.values())
+        d2h = out.nbytes
+
+        def e2e_step():
+            for name, a in host.items():
+                s._ck(s.lib.pts_set_field(s.ctx, ptstokes._abi.FIELD_ID[name], a.ctypes.data, a.size))
+            s.smooth(10, 1.0)
+            s.compute_maxloc()
+            s.compute_iter_params()
+            s.assign_tau()
+            s.solve()
+            s._ck(s.lib.pts_get_field(s.ctx, ptstokes._abi.FIELD_ID["Pt"], out.ctypes.data, out.size))
+
+        e2e_step()
+        s.sync()
+        barrier(pg)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(args.steps):
+            e2e_step()
+        b.record(stream)
+        b.synchronize()
+        t_e2e = max_over_ranks(a.elapsed_time(b), pg)
+        e2e = {"value": round(ws * a_eff(n) * nout * args.steps / (t_e2e / 1e3) / 1e9, 3), "unit": "GB/s",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "ms_per_step": round(t_e2e / args.steps, 3),
+               "includes": "pinned H2D of Mus,Vx,Vy,Vz; set-up kernels; nout PT iterations + check; D2H of Pt"}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        v, thr, dt = cpu_sample(args.cpu_n, args.cpu_iters)
+        cpu = {"value": round(v, 3), "unit": "GB/s", "cores": thr, "kind": "port",
+               "sample": f"oracle (C++/OpenMP FP64 restatement of Stokes3D_ve_perf.jl) at {args.cpu_n}^3, "
+                         f"{args.cpu_iters} PT iterations, {dt:.1f} s"}
+
+    launches = args.steps * (2 * nout + 2)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(t_ms / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (the reference's own "
+            "inclusion problem: spherical inclusion r=1 mu=1e-3, pure shear, G=1, dt=1)",
+            "config": {"workload": "3D VE Stokes (Stokes3D_ve_perf.jl kernels), FP64, 511^3, box 10^3",
+                       "nx": n, "ny": n, "nz": n, "iters_per_step": nout, "t_it_ms": round(t_it * 1e3, 4),
+                       "path": "2 kernels per PT iteration, CUDA graph per check block",
+                       "parallelism": f"replicas x{ws}", "l2": "inputs larger than L2 (1.07 GB per field)"},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": traffic, "kernel": "k3_Pt_tau",
+                         "peak_kind": peak_kind, "kernel_ms": round(ms_A, 4), "algorithmic_bytes": bytes_A,
+                         "other_kernel": {"name": "k3_V_bc", "ms": round(ms_B, 4),
+                                          "achieved": round(14 * n ** 3 * 8 / (ms_B / 1e3) / 1e9, 1)}},
+            "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    s.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=511)
+    ap.add_argument("--iters-per-step", type=int, default=200)
+    ap.add_argument("--cpu-n", type=int, default=255)
+    ap.add_argument("--cpu-iters", type=int, default=8)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    ws, rank, local, pg = dist_setup()
+    try:
+        if args.impl == "reference":
+            run_reference(args, ws, rank, pg)
+        else:
+            run_ours(args, ws, rank, local, pg)
+    finally:
+        if pg is not None:
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

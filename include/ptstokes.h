@@ -1,0 +1,171 @@
+/*
+ * ptstokes.h -- C ABI of libptstokes.so, the B200 (sm_100a) pseudo-transient Stokes
+ * solver. Drop-in for the hot path of PTsolvers/PseudoTransientStokes.jl: the PT
+ * iteration of 2D/3D viscous and Maxwell visco-elastic Stokes flow on a staggered grid.
+ *
+ * The reference has no library boundary: each script defines its stencil kernels with
+ * ParallelStencil and calls them positionally, e.g.
+ *   @parallel compute_Pt_τ!(Pt, τxx, ..., Vx, Vy, Vz, Mus, Gdτ, r, G, dt, _dx, _dy, _dz)
+ *   (scripts/stokes_3D/Stokes3D_ve_perf.jl:200-201).
+ * Each entry point below replaces one such kernel call (cited per function); a Julia
+ * `ccall` shim, a Python `ctypes` binding or C code calls them with plain pointers.
+ *
+ * Conventions
+ *  - A context owns every device field of one problem. Host arrays passed in are
+ *    Float64, column-major (x fastest), with the reference's own extents for that
+ *    field (pts_field_shape); they are borrowed for the duration of the call.
+ *  - Every call returns PTS_OK (0) or a negative PTS_E_* code; pts_last_error()
+ *    gives the message. Nothing throws or exits across the ABI.
+ *  - One context = one CUDA stream. Calls on different contexts are independent;
+ *    a single context is not thread-safe. Calls are asynchronous on the context's
+ *    stream unless documented as synchronous.
+ */
+#ifndef PTSTOKES_H
+#define PTSTOKES_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PTS_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define PTS_API __attribute__((visibility("default")))
+#else
+#define PTS_API
+#endif
+
+/* ---- status codes ---- */
+#define PTS_OK 0
+#define PTS_E_INVAL (-1)    /* bad argument (size, field id, variant, pointer) */
+#define PTS_E_CUDA (-2)     /* CUDA runtime error */
+#define PTS_E_NOMEM (-3)    /* device allocation failed */
+#define PTS_E_NAN (-4)      /* residual check found NaN/Inf: `isnan(err) && error("NaN")`
+                               (scripts/Stokes2D_ve.jl:171) */
+#define PTS_E_STATE (-5)    /* call not valid for this context's variant / state */
+
+/* ---- solver variants: which reference script's kernels and expression order ---- */
+enum pts_variant {
+    PTS_2D_V = 0,        /* scripts/Stokes2D.jl             2D viscous, roles P/τ/dV/V, /dx form   */
+    PTS_2D_VE = 1,       /* scripts/Stokes2D_ve.jl          2D Maxwell VE, roles P/τ/dV/V          */
+    PTS_2D_VE_PERF = 2,  /* scripts/Stokes2D_ve_perf.jl     2D VE, fused Pt_τ + V, _dx form        */
+    PTS_3D_VE = 3,       /* scripts/stokes_3D/Stokes3D_ve_multixpu.jl (one rank), roles P/τ/dV/V */
+    PTS_3D_VE_PERF = 4,  /* scripts/stokes_3D/Stokes3D_ve_perf.jl, fused Pt_τ + V             */
+    PTS_3D_V = 5         /* 3D viscous: the 3D fused kernels without elastic terms (no script) */
+};
+
+enum pts_precision {
+    PTS_FP64 = 0,  /* plain FP64: the reference's arithmetic, bit for bit */
+    PTS_MIXED = 1  /* FP32 inner PT sweeps on a correction, FP64 defect correction outside */
+};
+
+/* Problem description (physics + numerics of the script's Stokes2D_()/Stokes3D_()). */
+typedef struct pts_desc {
+    int32_t variant;    /* enum pts_variant */
+    int32_t precision;  /* enum pts_precision */
+    int32_t nx, ny, nz; /* cells (nz ignored in 2D); each >= 3 */
+    int32_t nout;       /* error-check cadence `nout` (e.g. Stokes3D_ve_multixpu.jl:130) */
+    double lx, ly, lz;  /* domain extents */
+    double G, dt;       /* shear modulus and physical step (VE); ignored for viscous */
+    double r, Re, CFL;  /* iteration parameters r, Re, CFL (Stokes3D_ve_perf.jl:129-131) */
+    double max_l;       /* length in dτ_Rho = Vpdτ*max_l/Re/μ_eff; 0 => max(lx,ly[,lz]) */
+    double eps;         /* tolerance ε on err (Stokes3D_ve_perf.jl:132) */
+    double iter_max;    /* `while err > ε && iter <= iterMax` */
+    int32_t mixed_inner;    /* MIXED: FP32 sweeps between FP64 corrections; 0 => nout */
+    int32_t reserved[7];
+} pts_desc;
+
+/* Fields, by the reference's names. Extents are the reference's (pts_field_shape). */
+enum pts_field {
+    PTS_F_PT = 0,
+    PTS_F_VX, PTS_F_VY, PTS_F_VZ,
+    PTS_F_TXX, PTS_F_TYY, PTS_F_TZZ, PTS_F_TXY, PTS_F_TXZ, PTS_F_TYZ,
+    PTS_F_TXX_O, PTS_F_TYY_O, PTS_F_TZZ_O, PTS_F_TXY_O, PTS_F_TXZ_O, PTS_F_TYZ_O,
+    PTS_F_MUS,      /* Mus (smoothed viscosity)            */
+    PTS_F_MUS_TAU,  /* Musτ (local-max viscosity)          */
+    PTS_F_GDTAU,    /* Gdτ                                 */
+    PTS_F_DTAU_RHO, /* dτ_Rho                              */
+    PTS_F_DIVV,     /* ∇V                                  */
+    PTS_F_RX, PTS_F_RY, PTS_F_RZ,
+    PTS_F_DVX, PTS_F_DVY, PTS_F_DVZ,
+    PTS_F_COUNT
+};
+
+/* Result of one convergence check (Stokes3D_ve_perf.jl:210-218). */
+typedef struct pts_check {
+    double err;                                       /* max of the four norms      */
+    double norm_Rx, norm_Ry, norm_Rz, norm_divV;      /* norm_Rz = 0 in 2D          */
+    double Vmin, Vmax, Pmin, Pmax;                    /* over Vx and Pt             */
+} pts_check;
+
+/* Outcome of one physical step's PT loop. */
+typedef struct pts_solve_info {
+    int64_t iters;       /* PT iterations done (`iter` at loop exit)          */
+    int32_t converged;   /* 1 if the loop ended on err <= eps, 0 on iter_max  */
+    int32_t nchecks;     /* residual checks done                              */
+    pts_check last;      /* last check (err = 2*eps if none was done)         */
+} pts_solve_info;
+
+typedef struct pts_ctx pts_ctx;
+
+/* ---- lifetime ---- */
+PTS_API int pts_create(const pts_desc* desc, pts_ctx** out);   /* allocates + zeroes all fields (@zeros) */
+PTS_API int pts_destroy(pts_ctx* ctx);
+PTS_API const char* pts_last_error(const pts_ctx* ctx);        /* ctx may be NULL (creation errors) */
+PTS_API int pts_abi_version(void);
+PTS_API int pts_sync(pts_ctx* ctx);                            /* wait for the context's stream */
+/* The context's cudaStream_t (as void*), to order or time the caller's own work with it. */
+PTS_API int pts_stream(pts_ctx* ctx, void** stream);
+
+/* ---- fields (Data.Array arguments of the kernels) ---- */
+PTS_API int pts_field_shape(const pts_ctx* ctx, int32_t field, int64_t shape[3]);
+PTS_API int pts_set_field(pts_ctx* ctx, int32_t field, const double* host, int64_t n);   /* synchronous */
+PTS_API int pts_get_field(pts_ctx* ctx, int32_t field, double* host, int64_t n);         /* synchronous */
+/* Same, with a device pointer to a dense column-major array (a CuArray's pointer). */
+PTS_API int pts_set_field_device(pts_ctx* ctx, int32_t field, const double* dev, int64_t n);
+PTS_API int pts_get_field_device(pts_ctx* ctx, int32_t field, double* dev, int64_t n);
+
+/* ---- problem set-up on the device ---- */
+/* Initial conditions of the scripts: Mus = mus0, Mus = musi where the squared distance of
+ * the cell centre from the box centre is < radius2, pure-shear V with strain rate ebg,
+ * every other field zero (Stokes3D_ve_perf.jl:164-172, Stokes2D.jl:106-114). */
+PTS_API int pts_init_inclusion(pts_ctx* ctx, double mus0, double musi, double radius2, double ebg);
+/* smooth!(Mus2, Mus, fact) nsweeps times with the Mus/Mus2 swap (Stokes3D_ve_perf.jl:173-177). */
+PTS_API int pts_smooth(pts_ctx* ctx, int32_t nsweeps, double fact);
+/* Musτ .= Mus; compute_maxloc!(Musτ, Mus); bc_x!/bc_y!/bc_z!(Musτ) (Stokes3D_ve_perf.jl:178-182). */
+PTS_API int pts_compute_maxloc(pts_ctx* ctx);
+/* compute_iter_params! (Stokes3D_ve_perf.jl:34-39; viscous Stokes2D.jl:27-31). */
+PTS_API int pts_compute_iter_params(pts_ctx* ctx);
+
+/* ---- PT iteration roles ---- */
+PTS_API int pts_assign_tau(pts_ctx* ctx);        /* assign_τ!  (Stokes3D_ve_perf.jl:41-49)              */
+PTS_API int pts_compute_P(pts_ctx* ctx);         /* compute_P! (Stokes3D_ve_multixpu.jl:57-61): ∇V, Pt  */
+PTS_API int pts_compute_tau(pts_ctx* ctx);       /* compute_τ! (Stokes3D_ve_multixpu.jl:69-77)          */
+PTS_API int pts_compute_dV(pts_ctx* ctx);        /* compute_dV! (Stokes3D_ve_multixpu.jl:79-84)         */
+PTS_API int pts_compute_V(pts_ctx* ctx);         /* compute_V! (Stokes3D_ve_multixpu.jl:86-91)          */
+PTS_API int pts_apply_bc(pts_ctx* ctx);          /* the bc_x!/bc_y!/bc_z! calls on V (…_perf.jl:202-207) */
+PTS_API int pts_compute_Pt_tau(pts_ctx* ctx);    /* compute_Pt_τ! (Stokes3D_ve_perf.jl:69-78)           */
+PTS_API int pts_compute_V_bc(pts_ctx* ctx);      /* compute_V! + bc (Stokes3D_ve_perf.jl:83-88,202-207)  */
+/* compute_Res! + the norms of the check (Stokes3D_ve_perf.jl:209-219). Synchronous. */
+PTS_API int pts_compute_res(pts_ctx* ctx, pts_check* out);
+
+/* ---- drivers ---- */
+/* n PT iterations (roles + BCs) on the fast path, no checks. Asynchronous. */
+PTS_API int pts_iterate(pts_ctx* ctx, int64_t n);
+/* One physical step's PT loop: `while err > ε && iter <= iterMax` with a check every
+ * nout iterations (Stokes3D_ve_perf.jl:198-223). Synchronous. Returns PTS_OK whether
+ * the loop ended on the tolerance or on iter_max (info->converged tells which) and
+ * PTS_E_NAN when a check's err is NaN (`if isnan(err) error("NaN") end`, :219). */
+PTS_API int pts_solve(pts_ctx* ctx, pts_solve_info* info);
+/* nt physical steps: assign_τ! (VE) then pts_solve, as the time loop
+ * `for it = 1:nt` (Stokes3D_ve_perf.jl:194-226). iters_per_step (length nt) may be NULL;
+ * info (may be NULL) receives the last step's outcome with iters = ittot. */
+PTS_API int pts_run(pts_ctx* ctx, int32_t nt, int64_t* iters_per_step, pts_solve_info* info);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PTSTOKES_H */

@@ -1,0 +1,590 @@
+// pts_abi.cu -- the C ABI of libptstokes.so: contexts, fields, set-up, roles and the PT
+// loop driver. Host code only (plus launches of the kernels in pts_kernels64.cu).
+//
+// The PT loop runs on the context's stream. Between two convergence checks the nout
+// iterations (two kernels each) and the check are one CUDA graph, so the host wakes
+// once per check, reads a small pinned result block and decides whether to go on --
+// the `while err > ε && iter <= iterMax` loop of the scripts (Stokes3D_ve_perf.jl:198-223).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "pts_internal.h"
+
+using namespace pts;
+
+namespace {
+std::string g_create_err;
+}
+
+struct pts_ctx {
+    pts_desc d{};
+    int v = 0;
+    bool d3 = false, elastic = false, perf = false;
+    Geom g{};
+    Num n{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    Fields64 f{};
+    std::vector<double*> owned;  // every device allocation
+    double* partials = nullptr;
+    int partials_cap = 0;
+    CheckResult* d_result = nullptr;
+    CheckResult* h_result = nullptr;  // pinned
+    cudaGraphExec_t chunk = nullptr;  // nout iterations + check
+    std::string err;
+};
+
+namespace {
+
+int fail(pts_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    else g_create_err = msg;
+    return code;
+}
+
+#define CK(call)                                                                                  \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess) return fail(c, PTS_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+struct FInfo {
+    double** ptr;
+    int64_t e[3];  // the reference's extents
+    int s[3];      // unified start of the reference's element [1,1,1]
+};
+
+// Field table: reference extents (Stokes3D_ve_perf.jl:141-162, Stokes2D_ve_perf.jl:105-118)
+// and where each field's first element sits in the unified staggered layout.
+bool field_info(pts_ctx* c, int id, FInfo* o) {
+    const int nx = c->g.nx, ny = c->g.ny, nz = c->d3 ? c->g.nz : 1;
+    Fields64& f = c->f;
+    auto set = [&](double** p, int64_t a, int64_t b, int64_t cc, int s0, int s1, int s2) {
+        o->ptr = p;
+        o->e[0] = a; o->e[1] = b; o->e[2] = cc;
+        o->s[0] = s0; o->s[1] = s1; o->s[2] = s2;
+    };
+    const bool d3 = c->d3, el = c->elastic;
+    switch (id) {
+        case PTS_F_PT: set(&f.Pt, nx, ny, nz, 0, 0, 0); break;
+        case PTS_F_MUS: set(&f.Mus, nx, ny, nz, 0, 0, 0); break;
+        case PTS_F_MUS_TAU: set(&f.Must, nx, ny, nz, 0, 0, 0); break;
+        case PTS_F_GDTAU: set(&f.Gdt, nx, ny, nz, 0, 0, 0); break;
+        case PTS_F_DTAU_RHO: set(&f.dtRho, nx, ny, nz, 0, 0, 0); break;
+        case PTS_F_DIVV: set(&f.divV, nx, ny, nz, 0, 0, 0); break;
+        case PTS_F_VX: set(&f.Vx, nx + 1, ny, nz, 0, 0, 0); break;
+        case PTS_F_VY: set(&f.Vy, nx, ny + 1, nz, 0, 0, 0); break;
+        case PTS_F_VZ: if (!d3) return false; set(&f.Vz, nx, ny, nz + 1, 0, 0, 0); break;
+        case PTS_F_TXX: case PTS_F_TXX_O:
+            if (id == PTS_F_TXX_O && !el) return false;
+            if (d3) set(id == PTS_F_TXX ? &f.txx : &f.txx_o, nx, ny - 2, nz - 2, 0, 1, 1);
+            else set(id == PTS_F_TXX ? &f.txx : &f.txx_o, nx, ny, 1, 0, 0, 0);
+            break;
+        case PTS_F_TYY: case PTS_F_TYY_O:
+            if (id == PTS_F_TYY_O && !el) return false;
+            if (d3) set(id == PTS_F_TYY ? &f.tyy : &f.tyy_o, nx - 2, ny, nz - 2, 1, 0, 1);
+            else set(id == PTS_F_TYY ? &f.tyy : &f.tyy_o, nx, ny, 1, 0, 0, 0);
+            break;
+        case PTS_F_TZZ: case PTS_F_TZZ_O:
+            if (!d3 || (id == PTS_F_TZZ_O && !el)) return false;
+            set(id == PTS_F_TZZ ? &f.tzz : &f.tzz_o, nx - 2, ny - 2, nz, 1, 1, 0);
+            break;
+        case PTS_F_TXY: case PTS_F_TXY_O:
+            if (id == PTS_F_TXY_O && !el) return false;
+            if (d3) set(id == PTS_F_TXY ? &f.txy : &f.txy_o, nx - 1, ny - 1, nz - 2, 1, 1, 1);
+            else set(id == PTS_F_TXY ? &f.txy : &f.txy_o, nx - 1, ny - 1, 1, 1, 1, 0);
+            break;
+        case PTS_F_TXZ: case PTS_F_TXZ_O:
+            if (!d3 || (id == PTS_F_TXZ_O && !el)) return false;
+            set(id == PTS_F_TXZ ? &f.txz : &f.txz_o, nx - 1, ny - 2, nz - 1, 1, 1, 1);
+            break;
+        case PTS_F_TYZ: case PTS_F_TYZ_O:
+            if (!d3 || (id == PTS_F_TYZ_O && !el)) return false;
+            set(id == PTS_F_TYZ ? &f.tyz : &f.tyz_o, nx - 2, ny - 1, nz - 1, 1, 1, 1);
+            break;
+        case PTS_F_RX: case PTS_F_DVX:
+            set(id == PTS_F_RX ? &f.Rx : &f.dVx, nx - 1, ny - 2, d3 ? nz - 2 : 1, 1, 1, d3 ? 1 : 0);
+            break;
+        case PTS_F_RY: case PTS_F_DVY:
+            set(id == PTS_F_RY ? &f.Ry : &f.dVy, nx - 2, ny - 1, d3 ? nz - 2 : 1, 1, 1, d3 ? 1 : 0);
+            break;
+        case PTS_F_RZ: case PTS_F_DVZ:
+            if (!d3) return false;
+            set(id == PTS_F_RZ ? &f.Rz : &f.dVz, nx - 2, ny - 2, nz - 1, 1, 1, 1);
+            break;
+        default: return false;
+    }
+    return true;
+}
+
+int alloc_field(pts_ctx* c, double** p) {
+    if (*p) return PTS_OK;
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, (size_t)c->g.n * sizeof(double));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(c, PTS_E_NOMEM, std::string("cudaMalloc of a field failed: ") + cudaGetErrorString(e));
+    }
+    CK(cudaMemsetAsync(q, 0, (size_t)c->g.n * sizeof(double), c->stream));
+    *p = (double*)q;
+    c->owned.push_back(*p);
+    return PTS_OK;
+}
+
+void drop_graph(pts_ctx* c) {
+    if (c->chunk) {
+        cudaGraphExecDestroy(c->chunk);
+        c->chunk = nullptr;
+    }
+}
+
+int enter(pts_ctx* c) {
+    if (!c) return PTS_E_INVAL;
+    CK(cudaSetDevice(c->device));
+    return PTS_OK;
+}
+
+int copy3d(pts_ctx* c, int id, const double* src_dense, double* dst_dense, int64_t n, cudaMemcpyKind kind) {
+    FInfo fi;
+    if (!field_info(c, id, &fi)) return fail(c, PTS_E_INVAL, "field not present for this variant: " + std::to_string(id));
+    if (*fi.ptr == nullptr) return fail(c, PTS_E_STATE, "field not allocated: " + std::to_string(id));
+    const int64_t want = fi.e[0] * fi.e[1] * fi.e[2];
+    if (n != want)
+        return fail(c, PTS_E_INVAL, "field " + std::to_string(id) + " has " + std::to_string(want) + " elements, got " +
+                                        std::to_string(n));
+    cudaMemcpy3DParms p;
+    memset(&p, 0, sizeof(p));
+    cudaPitchedPtr dense = make_cudaPitchedPtr(src_dense ? (void*)src_dense : (void*)dst_dense,
+                                               (size_t)fi.e[0] * sizeof(double), (size_t)fi.e[0], (size_t)fi.e[1]);
+    cudaPitchedPtr pad = make_cudaPitchedPtr(*fi.ptr, (size_t)c->g.px * sizeof(double), (size_t)c->g.px,
+                                             (size_t)c->g.py);
+    cudaPos at = make_cudaPos((size_t)fi.s[0] * sizeof(double), (size_t)fi.s[1], (size_t)fi.s[2]);
+    if (src_dense) {
+        p.srcPtr = dense;
+        p.dstPtr = pad;
+        p.dstPos = at;
+    } else {
+        p.srcPtr = pad;
+        p.srcPos = at;
+        p.dstPtr = dense;
+    }
+    p.extent = make_cudaExtent((size_t)fi.e[0] * sizeof(double), (size_t)fi.e[1], (size_t)fi.e[2]);
+    p.kind = kind;
+    CK(cudaMemcpy3DAsync(&p, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return PTS_OK;
+}
+
+// One PT iteration on the fast path: compute_Pt_τ! then compute_V! + bc.
+int iteration(pts_ctx* c, bool store_divV) {
+    CK(launch_Pt_tau(c->v, c->g, c->f, c->n, ROLE_P | ROLE_TAU, store_divV && !c->perf, c->stream));
+    CK(launch_V_bc(c->v, c->g, c->f, c->n, true, c->stream));
+    return PTS_OK;
+}
+
+int enqueue_check(pts_ctx* c) {
+    CK(launch_check(c->v, c->g, c->f, c->n, c->partials, c->partials_cap, c->d_result, c->stream));
+    CK(cudaMemcpyAsync(c->h_result, c->d_result, sizeof(CheckResult), cudaMemcpyDeviceToHost, c->stream));
+    return PTS_OK;
+}
+
+int build_chunk(pts_ctx* c) {
+    if (c->chunk) return PTS_OK;
+    cudaGraph_t graph = nullptr;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = PTS_OK;
+    for (int q = 0; q < c->d.nout && rc == PTS_OK; ++q) rc = iteration(c, q == c->d.nout - 1);
+    if (rc == PTS_OK) rc = enqueue_check(c);
+    cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+    if (rc != PTS_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (e != cudaSuccess) return fail(c, PTS_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&c->chunk, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        c->chunk = nullptr;
+        return fail(c, PTS_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    }
+    return PTS_OK;
+}
+
+void to_check(const CheckResult& r, pts_check* o) {
+    o->err = r.err;
+    o->norm_Rx = r.nRx;
+    o->norm_Ry = r.nRy;
+    o->norm_Rz = r.nRz;
+    o->norm_divV = r.ndiv;
+    o->Vmin = r.vmin;
+    o->Vmax = r.vmax;
+    o->Pmin = r.pmin;
+    o->Pmax = r.pmax;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pts_abi_version(void) { return PTS_ABI_VERSION; }
+
+const char* pts_last_error(const pts_ctx* c) { return c ? c->err.c_str() : g_create_err.c_str(); }
+
+int pts_create(const pts_desc* d, pts_ctx** out) {
+    pts_ctx* c = nullptr;
+    if (!d || !out) return fail(nullptr, PTS_E_INVAL, "null argument");
+    *out = nullptr;
+    if (d->variant < PTS_2D_V || d->variant > PTS_3D_V) return fail(nullptr, PTS_E_INVAL, "unknown variant");
+    if (d->precision != PTS_FP64 && d->precision != PTS_MIXED) return fail(nullptr, PTS_E_INVAL, "unknown precision");
+    if (d->precision == PTS_MIXED) return fail(nullptr, PTS_E_INVAL, "mixed precision is not available in this build");
+    const bool d3 = variant_is3d(d->variant);
+    if (d->nx < 3 || d->ny < 3 || (d3 && d->nz < 3)) return fail(nullptr, PTS_E_INVAL, "each of nx, ny(, nz) must be >= 3");
+    if ((int64_t)d->nx + 1 > (1 << 20) || (int64_t)d->ny + 1 > (1 << 20) || (d3 && (int64_t)d->nz + 1 > (1 << 20)))
+        return fail(nullptr, PTS_E_INVAL, "grid extent too large");
+    if (d->nout < 1) return fail(nullptr, PTS_E_INVAL, "nout must be >= 1");
+    if (!(d->lx > 0) || !(d->ly > 0) || (d3 && !(d->lz > 0))) return fail(nullptr, PTS_E_INVAL, "domain extents must be > 0");
+    c = new pts_ctx();
+    c->d = *d;
+    c->v = d->variant;
+    c->d3 = d3;
+    c->elastic = variant_elastic(c->v);
+    c->perf = variant_perf(c->v);
+    Geom& g = c->g;
+    g.nx = d->nx;
+    g.ny = d->ny;
+    g.nz = d3 ? d->nz : 1;
+    g.px = ((d->nx + 1) + 15) / 16 * 16;
+    g.py = d->ny + 1;
+    g.pz = d3 ? d->nz + 1 : 1;
+    g.pxy = (int64_t)g.px * g.py;
+    g.n = g.pxy * g.pz;
+    Num& n = c->n;
+    n.lx = d->lx; n.ly = d->ly; n.lz = d3 ? d->lz : 1.0;
+    n.dx = d->lx / d->nx;
+    n.dy = d->ly / d->ny;
+    n.dz = d3 ? d->lz / d->nz : 1.0;
+    n._dx = 1.0 / n.dx;
+    n._dy = 1.0 / n.dy;
+    n._dz = 1.0 / n.dz;
+    n.r = d->r;
+    n.G = d->G;
+    n.dt = d->dt;
+    n.gdt = d->G * d->dt;
+    n.Re = d->Re;
+    n.Vpdt = (d3 ? std::min(std::min(n.dx, n.dy), n.dz) : std::min(n.dx, n.dy)) * d->CFL;
+    n.max_l = d->max_l > 0 ? d->max_l : (d3 ? std::max(std::max(d->lx, d->ly), d->lz) : std::max(d->lx, d->ly));
+    int rc = PTS_OK;
+    auto bail = [&](int code) {
+        g_create_err = c->err;
+        pts_destroy(c);
+        return code;
+    };
+    if (cudaGetDevice(&c->device) != cudaSuccess) {
+        cudaGetLastError();
+        c->err = "no CUDA device";
+        return bail(PTS_E_CUDA);
+    }
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        c->err = "cudaStreamCreate failed";
+        return bail(PTS_E_CUDA);
+    }
+    Fields64& f = c->f;
+    double** always[] = {&f.Pt, &f.Vx, &f.Vy, &f.txx, &f.tyy, &f.txy, &f.Mus, &f.Must, &f.Gdt, &f.dtRho, &f.divV,
+                         &f.Rx, &f.Ry, &f.Mus2};
+    for (double** p : always)
+        if ((rc = alloc_field(c, p)) != PTS_OK) return bail(rc);
+    if (d3) {
+        double** more[] = {&f.Vz, &f.tzz, &f.txz, &f.tyz, &f.Rz};
+        for (double** p : more)
+            if ((rc = alloc_field(c, p)) != PTS_OK) return bail(rc);
+    }
+    if (c->elastic) {
+        double** olds[] = {&f.txx_o, &f.tyy_o, &f.txy_o};
+        for (double** p : olds)
+            if ((rc = alloc_field(c, p)) != PTS_OK) return bail(rc);
+        if (d3) {
+            double** olds3[] = {&f.tzz_o, &f.txz_o, &f.tyz_o};
+            for (double** p : olds3)
+                if ((rc = alloc_field(c, p)) != PTS_OK) return bail(rc);
+        }
+    }
+    c->partials_cap = check_num_blocks(c->v, g);
+    if (cudaMalloc((void**)&c->partials, (size_t)c->partials_cap * kCheckSlots * sizeof(double)) != cudaSuccess ||
+        cudaMalloc((void**)&c->d_result, sizeof(CheckResult)) != cudaSuccess ||
+        cudaMallocHost((void**)&c->h_result, sizeof(CheckResult)) != cudaSuccess) {
+        cudaGetLastError();
+        c->err = "allocation of the check buffers failed";
+        return bail(PTS_E_NOMEM);
+    }
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
+        c->err = std::string("initialisation: ") + cudaGetErrorString(cudaGetLastError());
+        return bail(PTS_E_CUDA);
+    }
+    *out = c;
+    return PTS_OK;
+}
+
+int pts_destroy(pts_ctx* c) {
+    if (!c) return PTS_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    drop_graph(c);
+    for (double* p : c->owned) cudaFree(p);
+    if (c->partials) cudaFree(c->partials);
+    if (c->d_result) cudaFree(c->d_result);
+    if (c->h_result) cudaFreeHost(c->h_result);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return PTS_OK;
+}
+
+int pts_sync(pts_ctx* c) {
+    int rc = enter(c);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    return PTS_OK;
+}
+
+int pts_stream(pts_ctx* c, void** stream) {
+    if (!c || !stream) return PTS_E_INVAL;
+    *stream = (void*)c->stream;
+    return PTS_OK;
+}
+
+int pts_field_shape(const pts_ctx* cc, int32_t id, int64_t shape[3]) {
+    pts_ctx* c = const_cast<pts_ctx*>(cc);
+    if (!c || !shape) return PTS_E_INVAL;
+    FInfo fi;
+    if (!field_info(c, id, &fi)) return fail(c, PTS_E_INVAL, "field not present for this variant: " + std::to_string(id));
+    shape[0] = fi.e[0];
+    shape[1] = fi.e[1];
+    shape[2] = fi.e[2];
+    return PTS_OK;
+}
+
+int pts_set_field(pts_ctx* c, int32_t id, const double* host, int64_t n) {
+    int rc = enter(c);
+    if (rc) return rc;
+    if (!host) return fail(c, PTS_E_INVAL, "null host pointer");
+    FInfo fi;
+    if ((id == PTS_F_DVX || id == PTS_F_DVY || id == PTS_F_DVZ) && field_info(c, id, &fi) &&
+        (rc = alloc_field(c, fi.ptr)) != PTS_OK)
+        return rc;
+    return copy3d(c, id, host, nullptr, n, cudaMemcpyHostToDevice);
+}
+
+int pts_get_field(pts_ctx* c, int32_t id, double* host, int64_t n) {
+    int rc = enter(c);
+    if (rc) return rc;
+    if (!host) return fail(c, PTS_E_INVAL, "null host pointer");
+    return copy3d(c, id, nullptr, host, n, cudaMemcpyDeviceToHost);
+}
+
+int pts_set_field_device(pts_ctx* c, int32_t id, const double* dev, int64_t n) {
+    int rc = enter(c);
+    if (rc) return rc;
+    if (!dev) return fail(c, PTS_E_INVAL, "null device pointer");
+    return copy3d(c, id, dev, nullptr, n, cudaMemcpyDeviceToDevice);
+}
+
+int pts_get_field_device(pts_ctx* c, int32_t id, double* dev, int64_t n) {
+    int rc = enter(c);
+    if (rc) return rc;
+    if (!dev) return fail(c, PTS_E_INVAL, "null device pointer");
+    return copy3d(c, id, nullptr, dev, n, cudaMemcpyDeviceToDevice);
+}
+
+int pts_init_inclusion(pts_ctx* c, double mus0, double musi, double radius2, double ebg) {
+    int rc = enter(c);
+    if (rc) return rc;
+    for (double* p : c->owned) CK(cudaMemsetAsync(p, 0, (size_t)c->g.n * sizeof(double), c->stream));
+    CK(launch_init_inclusion(c->v, c->g, c->f, c->n, mus0, musi, radius2, ebg, c->stream));
+    return PTS_OK;
+}
+
+int pts_smooth(pts_ctx* c, int32_t nsweeps, double fact) {
+    int rc = enter(c);
+    if (rc) return rc;
+    if (nsweeps < 0) return fail(c, PTS_E_INVAL, "nsweeps < 0");
+    // Mus2 .= Mus, then ping-pong (the boundary cells of both stay the initial Mus)
+    CK(cudaMemcpyAsync(c->f.Mus2, c->f.Mus, (size_t)c->g.n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    for (int s = 0; s < nsweeps; ++s) {
+        CK(launch_smooth(c->v, c->g, c->f.Mus2, c->f.Mus, fact, c->stream));
+        std::swap(c->f.Mus, c->f.Mus2);
+    }
+    drop_graph(c);  // the graph captured the old Mus pointer
+    return PTS_OK;
+}
+
+int pts_compute_maxloc(pts_ctx* c) {
+    int rc = enter(c);
+    if (rc) return rc;
+    CK(launch_maxloc(c->v, c->g, c->f.Must, c->f.Mus, c->stream));
+    return PTS_OK;
+}
+
+int pts_compute_iter_params(pts_ctx* c) {
+    int rc = enter(c);
+    if (rc) return rc;
+    CK(launch_iter_params(c->v, c->g, c->f, c->n, c->stream));
+    return PTS_OK;
+}
+
+int pts_assign_tau(pts_ctx* c) {
+    int rc = enter(c);
+    if (rc) return rc;
+    if (!c->elastic) return PTS_OK;  // viscous scripts have no τ_o
+    Fields64& f = c->f;
+    std::pair<double*, double*> cp[] = {{f.txx_o, f.txx}, {f.tyy_o, f.tyy}, {f.txy_o, f.txy},
+                                        {f.tzz_o, f.tzz}, {f.txz_o, f.txz}, {f.tyz_o, f.tyz}};
+    for (auto& pr : cp)
+        if (pr.first) CK(cudaMemcpyAsync(pr.first, pr.second, (size_t)c->g.n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    return PTS_OK;
+}
+
+int pts_compute_P(pts_ctx* c) {
+    int rc = enter(c);
+    if (rc) return rc;
+    CK(launch_Pt_tau(c->v, c->g, c->f, c->n, ROLE_P, !c->perf, c->stream));
+    return PTS_OK;
+}
+
+int pts_compute_tau(pts_ctx* c) {
+    int rc = enter(c);
+    if (rc) return rc;
+    CK(launch_Pt_tau(c->v, c->g, c->f, c->n, ROLE_TAU, false, c->stream));
+    return PTS_OK;
+}
+
+int pts_compute_dV(pts_ctx* c) {
+    int rc = enter(c);
+    if (rc) return rc;
+    double** dv[] = {&c->f.dVx, &c->f.dVy, &c->f.dVz};
+    for (int q = 0; q < (c->d3 ? 3 : 2); ++q)
+        if ((rc = alloc_field(c, dv[q])) != PTS_OK) return rc;
+    CK(launch_dV(c->v, c->g, c->f, c->n, c->stream));
+    return PTS_OK;
+}
+
+int pts_compute_V(pts_ctx* c) {
+    int rc = enter(c);
+    if (rc) return rc;
+    if (!c->f.dVx) return fail(c, PTS_E_STATE, "compute_V needs dV: call pts_compute_dV first");
+    CK(launch_add_dV(c->v, c->g, c->f, c->stream));
+    return PTS_OK;
+}
+
+int pts_apply_bc(pts_ctx* c) {
+    int rc = enter(c);
+    if (rc) return rc;
+    CK(launch_V_bc(c->v, c->g, c->f, c->n, false, c->stream));
+    return PTS_OK;
+}
+
+int pts_compute_Pt_tau(pts_ctx* c) {
+    int rc = enter(c);
+    if (rc) return rc;
+    CK(launch_Pt_tau(c->v, c->g, c->f, c->n, ROLE_P | ROLE_TAU, !c->perf, c->stream));
+    return PTS_OK;
+}
+
+int pts_compute_V_bc(pts_ctx* c) {
+    int rc = enter(c);
+    if (rc) return rc;
+    CK(launch_V_bc(c->v, c->g, c->f, c->n, true, c->stream));
+    return PTS_OK;
+}
+
+int pts_compute_res(pts_ctx* c, pts_check* out) {
+    int rc = enter(c);
+    if (rc) return rc;
+    if ((rc = enqueue_check(c)) != PTS_OK) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    if (out) to_check(*c->h_result, out);
+    return c->h_result->flag_nan != 0.0 ? fail(c, PTS_E_NAN, "NaN in the residual check") : PTS_OK;
+}
+
+int pts_iterate(pts_ctx* c, int64_t niter) {
+    int rc = enter(c);
+    if (rc) return rc;
+    if (niter < 0) return fail(c, PTS_E_INVAL, "niter < 0");
+    for (int64_t q = 0; q < niter; ++q)
+        if ((rc = iteration(c, q == niter - 1)) != PTS_OK) return rc;
+    return PTS_OK;
+}
+
+int pts_solve(pts_ctx* c, pts_solve_info* info) {
+    int rc = enter(c);
+    if (rc) return rc;
+    const int64_t nout = c->d.nout;
+    const double eps = c->d.eps;
+    const int64_t last_iter = (int64_t)std::floor(c->d.iter_max);  // loop runs while iter <= iter_max
+    int64_t iter = 0;
+    double err = 2 * eps;
+    pts_solve_info res;
+    memset(&res, 0, sizeof(res));
+    res.last.err = err;
+    bool converged = false;
+    while (err > eps && iter <= last_iter) {
+        const int64_t till_check = nout - iter % nout;
+        const int64_t remaining = last_iter - iter + 1;
+        if (remaining >= till_check) {
+            if (till_check == nout) {
+                if ((rc = build_chunk(c)) != PTS_OK) return rc;
+                CK(cudaGraphLaunch(c->chunk, c->stream));
+            } else {
+                if ((rc = pts_iterate(c, till_check)) != PTS_OK) return rc;
+                if ((rc = enqueue_check(c)) != PTS_OK) return rc;
+            }
+            CK(cudaStreamSynchronize(c->stream));
+            iter += till_check;
+            to_check(*c->h_result, &res.last);
+            res.nchecks++;
+            err = c->h_result->err;
+            if (c->h_result->flag_nan != 0.0) {
+                res.iters = iter;
+                if (info) *info = res;
+                return fail(c, PTS_E_NAN, "NaN");
+            }
+            if (!(err > eps)) converged = true;
+        } else {
+            if ((rc = pts_iterate(c, remaining)) != PTS_OK) return rc;
+            iter += remaining;
+            CK(cudaStreamSynchronize(c->stream));
+        }
+    }
+    res.iters = iter;
+    res.converged = converged ? 1 : 0;
+    if (info) *info = res;
+    return PTS_OK;
+}
+
+int pts_run(pts_ctx* c, int32_t nt, int64_t* iters_per_step, pts_solve_info* info) {
+    int rc = enter(c);
+    if (rc) return rc;
+    if (nt < 0) return fail(c, PTS_E_INVAL, "nt < 0");
+    pts_solve_info step;
+    memset(&step, 0, sizeof(step));
+    int64_t ittot = 0;
+    for (int32_t it = 0; it < nt; ++it) {
+        if ((rc = pts_assign_tau(c)) != PTS_OK) return rc;
+        rc = pts_solve(c, &step);
+        ittot += step.iters;
+        if (iters_per_step) iters_per_step[it] = step.iters;
+        if (rc != PTS_OK) {
+            step.iters = ittot;
+            if (info) *info = step;
+            return rc;
+        }
+    }
+    step.iters = ittot;
+    if (info) *info = step;
+    return PTS_OK;
+}
+
+}  // extern "C"

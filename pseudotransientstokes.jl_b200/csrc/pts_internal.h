@@ -1,0 +1,94 @@
+// pts_internal.h -- shared layout, parameter and launch declarations of libptstokes.
+//
+// Data layout in HBM ("unified staggered layout"): every field of a problem is stored in
+// its own array of the same padded extent px x py x pz, px = round_up(nx+1, 16) (so each
+// x-row starts on a 128-byte boundary), py = ny+1, pz = nz+1 (pz = 1 in 2D). A field
+// element lives at the unified staggered coordinate (i,j,k) of the point it describes:
+//   cell centre (i,j,k)            Pt, Mus, Musτ, Gdτ, dτ_Rho, ∇V, τxx, τyy, τzz
+//   x-face i (between cells i-1,i) Vx, Rx, dVx;   y-face j: Vy ...;   z-face k: Vz ...
+//   x-face i, y-face j, cell k     τxy (edge);    τxz: x-face,cell,z-face;  τyz: cell,y-face,z-face
+// so a neighbour in x/y/z is always at offset +-1 / +-px / +-px*py whatever the field. The
+// reference's arrays (1-based, column-major, each with its own extent) map to this layout
+// with a per-field start offset (field_info() in pts_abi.cu); set/get convert once.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "ptstokes.h"
+
+namespace pts {
+
+enum Variant {
+    V2D = PTS_2D_V,
+    VE2D = PTS_2D_VE,
+    VE2D_PERF = PTS_2D_VE_PERF,
+    VE3D = PTS_3D_VE,
+    VE3D_PERF = PTS_3D_VE_PERF,
+    V3D = PTS_3D_V,
+};
+
+inline bool variant_is3d(int v) { return v == VE3D || v == VE3D_PERF || v == V3D; }
+inline bool variant_elastic(int v) { return v != V2D && v != V3D; }
+// "perf" variants multiply by _dx = 1/dx (explicit-index kernels); the others divide by dx.
+inline bool variant_perf(int v) { return v == VE2D_PERF || v == VE3D_PERF || v == V3D; }
+// ∇V of the check: from compute_P! before the V update (role variants), or recomputed
+// from the current V by compute_Res! (perf variants).
+inline bool variant_divV_from_P(int v) { return !variant_perf(v); }
+
+struct Geom {
+    int nx, ny, nz;   // cells (nz = 1 in 2D)
+    int px, py, pz;   // padded extents of every field array
+    int64_t pxy;      // px * py
+    int64_t n;        // px * py * pz elements per field
+};
+
+__host__ __device__ inline int64_t gidx(const Geom& g, int i, int j, int k) {
+    return (int64_t)i + (int64_t)g.px * ((int64_t)j + (int64_t)g.py * (int64_t)k);
+}
+
+// Scalars of the scripts' "Derived numerics" (Stokes3D_ve_perf.jl:135-138).
+struct Num {
+    double dx, dy, dz, _dx, _dy, _dz;
+    double r, G, dt, gdt;  // gdt = G*dt
+    double Vpdt, max_l, Re;
+    double lx, ly, lz;
+};
+
+template <typename T>
+struct FieldsT {
+    T *Pt, *Vx, *Vy, *Vz;
+    T *txx, *tyy, *tzz, *txy, *txz, *tyz;
+    T *txx_o, *tyy_o, *tzz_o, *txy_o, *txz_o, *tyz_o;
+    T *Mus, *Must, *Gdt, *dtRho, *divV;
+    T *Rx, *Ry, *Rz, *dVx, *dVy, *dVz;
+    T *Mus2;
+};
+using Fields64 = FieldsT<double>;
+
+// Per-block partials of the check reduction: sums of squares of Rx, Ry, Rz, ∇V and
+// min/max of Vx and Pt (Stokes3D_ve_perf.jl:211-216).
+constexpr int kCheckSlots = 8;
+// Device result block written by the check finaliser.
+struct CheckResult {
+    double err, nRx, nRy, nRz, ndiv, vmin, vmax, pmin, pmax;
+    double flag_nan;
+};
+
+// ---- launchers implemented in pts_kernels64.cu (FP64, no FMA contraction) ----
+enum RoleMask { ROLE_P = 1, ROLE_TAU = 2 };
+cudaError_t launch_Pt_tau(int variant, const Geom& g, const Fields64& f, const Num& n, int roles, bool store_divV,
+                          cudaStream_t s);
+cudaError_t launch_V_bc(int variant, const Geom& g, const Fields64& f, const Num& n, bool apply_update,
+                        cudaStream_t s);
+cudaError_t launch_dV(int variant, const Geom& g, const Fields64& f, const Num& n, cudaStream_t s);
+cudaError_t launch_add_dV(int variant, const Geom& g, const Fields64& f, cudaStream_t s);
+cudaError_t launch_check(int variant, const Geom& g, const Fields64& f, const Num& n, double* partials,
+                         int nblocks_cap, CheckResult* result, cudaStream_t s);
+int check_num_blocks(int variant, const Geom& g);
+cudaError_t launch_init_inclusion(int variant, const Geom& g, const Fields64& f, const Num& n, double mus0,
+                                  double musi, double radius2, double ebg, cudaStream_t s);
+cudaError_t launch_smooth(int variant, const Geom& g, double* dst, const double* src, double fact, cudaStream_t s);
+cudaError_t launch_maxloc(int variant, const Geom& g, double* must, const double* mus, cudaStream_t s);
+cudaError_t launch_iter_params(int variant, const Geom& g, const Fields64& f, const Num& n, cudaStream_t s);
+
+}  // namespace pts

@@ -1,0 +1,735 @@
+// pts_kernels64.cu -- FP64 stencil kernels of the PT iteration (all variants).
+//
+// Compiled with --fmad=false: no multiply-add is contracted, and every expression below
+// is written in the reference's left-to-right order, so each kernel reproduces the
+// reference's Float64 arithmetic bit for bit (the fixtures in tests/golden pin this).
+// IEEE division and sqrt are the CUDA defaults (-prec-div=true, -prec-sqrt=true).
+//
+// Kernels here are the straightforward one-thread-per-point forms (two launches per PT
+// iteration: compute_Pt_τ! and compute_V! + bc); the 3D visco-elastic hot path also has
+// the single-pass z-streaming kernel in pts_fused3d.cu.
+#include <cfloat>
+#include <cmath>
+
+#include "pts_internal.h"
+
+namespace pts {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+// ------------------------------------------------------------------ expression helpers
+
+// Normal stress update. Perf form (Stokes3D_ve_perf.jl:71-73):
+//   (τ + τ_o*Gr + 2.0*Gdτ*(_dx*d)) / (1.0 + Gdτ/Mus + Gr),  Gr = Gdτ/(G*dt)
+// Role form (Stokes3D_ve_multixpu.jl:70-72): the same with (d/dx).
+// Viscous: the τ_o and Gr terms are absent.
+template <bool EL, bool PERF>
+__device__ __forceinline__ double tau_n(double t, double to, double g, double m, double gdt, double h, double ih,
+                                        double d) {
+    const double e = PERF ? (ih * d) : (d / h);
+    if (EL) {
+        const double Gr = g / gdt;
+        return ((t + to * Gr) + (2.0 * g) * e) / ((1.0 + g / m) + Gr);
+    }
+    return (t + (2.0 * g) * e) / (1.0 + g / m);
+}
+
+// Shear stress update (Stokes3D_ve_perf.jl:74-76, Stokes3D_ve_multixpu.jl:73-75):
+//   (τ + τ_o*av_Gr + 2.0*av_Gdτ*(0.5*(_h1*d1 + _h2*d2))) / (1.0 + av_Gdτ/av_Mus + av_Gr)
+template <bool EL, bool PERF>
+__device__ __forceinline__ double tau_s(double t, double to, double ag, double am, double gdt, double h1, double ih1,
+                                        double d1, double h2, double ih2, double d2) {
+    const double s = PERF ? (ih1 * d1 + ih2 * d2) : (d1 / h1 + d2 / h2);
+    if (EL) {
+        const double Gr = ag / gdt;
+        return ((t + to * Gr) + (2.0 * ag) * (0.5 * s)) / ((1.0 + ag / am) + Gr);
+    }
+    return (t + (2.0 * ag) * (0.5 * s)) / (1.0 + ag / am);
+}
+
+template <bool PERF>
+__device__ __forceinline__ double dsc(double d, double h, double ih) {
+    return PERF ? (ih * d) : (d / h);
+}
+
+// ------------------------------------------------------------------ 3D kernels
+
+// compute_P! + compute_τ! (roles) == compute_Pt_τ! (perf), one thread per cell (i,j,k).
+template <bool EL, bool PERF>
+__global__ void __launch_bounds__(256) k3_Pt_tau(Geom g, Fields64 f, Num n, int roles, int store_divV) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    if (i >= nx || j >= ny) return;
+    const int64_t c = gidx(g, i, j, k);
+    const int64_t sx = 1, sy = g.px, sz = g.pxy;
+    const double dvx = f.Vx[c + sx] - f.Vx[c];
+    const double dvy = f.Vy[c + sy] - f.Vy[c];
+    const double dvz = f.Vz[c + sz] - f.Vz[c];
+    const double Gc = f.Gdt[c];
+    if (roles & ROLE_P) {
+        if (PERF) {
+            f.Pt[c] = f.Pt[c] - n.r * Gc * ((n._dx * dvx + n._dy * dvy) + n._dz * dvz);
+        } else {
+            const double dv = (dvx / n.dx + dvy / n.dy) + dvz / n.dz;
+            if (store_divV) f.divV[c] = dv;
+            f.Pt[c] = f.Pt[c] - n.r * Gc * dv;
+        }
+    }
+    if (!(roles & ROLE_TAU)) return;
+    const double Mc = f.Mus[c];
+    const double gdt = n.gdt;
+    if (j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2)
+        f.txx[c] = tau_n<EL, PERF>(f.txx[c], EL ? f.txx_o[c] : 0.0, Gc, Mc, gdt, n.dx, n._dx, dvx);
+    if (i >= 1 && i <= nx - 2 && k >= 1 && k <= nz - 2)
+        f.tyy[c] = tau_n<EL, PERF>(f.tyy[c], EL ? f.tyy_o[c] : 0.0, Gc, Mc, gdt, n.dy, n._dy, dvy);
+    if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2)
+        f.tzz[c] = tau_n<EL, PERF>(f.tzz[c], EL ? f.tzz_o[c] : 0.0, Gc, Mc, gdt, n.dz, n._dz, dvz);
+    // τxy on edge (x-face i, y-face j, cell k): i in [1,nx-1], j in [1,ny-1], k in [1,nz-2]
+    if (i >= 1 && j >= 1 && k >= 1 && k <= nz - 2) {
+        const double ag = (((f.Gdt[c - sx - sy] + f.Gdt[c - sy]) + f.Gdt[c - sx]) + Gc) * 0.25;
+        const double am = (((f.Mus[c - sx - sy] + f.Mus[c - sy]) + f.Mus[c - sx]) + Mc) * 0.25;
+        f.txy[c] = tau_s<EL, PERF>(f.txy[c], EL ? f.txy_o[c] : 0.0, ag, am, gdt, n.dy, n._dy, f.Vx[c] - f.Vx[c - sy],
+                                   n.dx, n._dx, f.Vy[c] - f.Vy[c - sx]);
+    }
+    // τxz on edge (x-face i, cell j, z-face k): i in [1,nx-1], j in [1,ny-2], k in [1,nz-1]
+    if (i >= 1 && j >= 1 && j <= ny - 2 && k >= 1) {
+        const double ag = (((f.Gdt[c - sx - sz] + f.Gdt[c - sz]) + f.Gdt[c - sx]) + Gc) * 0.25;
+        const double am = (((f.Mus[c - sx - sz] + f.Mus[c - sz]) + f.Mus[c - sx]) + Mc) * 0.25;
+        f.txz[c] = tau_s<EL, PERF>(f.txz[c], EL ? f.txz_o[c] : 0.0, ag, am, gdt, n.dz, n._dz, f.Vx[c] - f.Vx[c - sz],
+                                   n.dx, n._dx, f.Vz[c] - f.Vz[c - sx]);
+    }
+    // τyz on edge (cell i, y-face j, z-face k): i in [1,nx-2], j in [1,ny-1], k in [1,nz-1]
+    if (i >= 1 && i <= nx - 2 && j >= 1 && k >= 1) {
+        const double ag = (((f.Gdt[c - sy - sz] + f.Gdt[c - sz]) + f.Gdt[c - sy]) + Gc) * 0.25;
+        const double am = (((f.Mus[c - sy - sz] + f.Mus[c - sz]) + f.Mus[c - sy]) + Mc) * 0.25;
+        f.tyz[c] = tau_s<EL, PERF>(f.tyz[c], EL ? f.tyz_o[c] : 0.0, ag, am, gdt, n.dz, n._dz, f.Vy[c] - f.Vy[c - sz],
+                                   n.dy, n._dy, f.Vz[c] - f.Vz[c - sy]);
+    }
+}
+
+// Momentum residuals at interior faces (compute_Res!, Stokes3D_ve_perf.jl:92-94;
+// compute_dV!/compute_Res!, Stokes3D_ve_multixpu.jl:80-82,94-96).
+template <bool PERF>
+__device__ __forceinline__ double res3_x(const Fields64& f, const Num& n, int64_t c, int64_t sx, int64_t sy,
+                                         int64_t sz) {
+    return ((dsc<PERF>(f.txx[c] - f.txx[c - sx], n.dx, n._dx) + dsc<PERF>(f.txy[c + sy] - f.txy[c], n.dy, n._dy)) +
+            dsc<PERF>(f.txz[c + sz] - f.txz[c], n.dz, n._dz)) -
+           dsc<PERF>(f.Pt[c] - f.Pt[c - sx], n.dx, n._dx);
+}
+template <bool PERF>
+__device__ __forceinline__ double res3_y(const Fields64& f, const Num& n, int64_t c, int64_t sx, int64_t sy,
+                                         int64_t sz) {
+    return ((dsc<PERF>(f.tyy[c] - f.tyy[c - sy], n.dy, n._dy) + dsc<PERF>(f.txy[c + sx] - f.txy[c], n.dx, n._dx)) +
+            dsc<PERF>(f.tyz[c + sz] - f.tyz[c], n.dz, n._dz)) -
+           dsc<PERF>(f.Pt[c] - f.Pt[c - sy], n.dy, n._dy);
+}
+template <bool PERF>
+__device__ __forceinline__ double res3_z(const Fields64& f, const Num& n, int64_t c, int64_t sx, int64_t sy,
+                                         int64_t sz) {
+    return ((dsc<PERF>(f.tzz[c] - f.tzz[c - sz], n.dz, n._dz) + dsc<PERF>(f.txz[c + sx] - f.txz[c], n.dx, n._dx)) +
+            dsc<PERF>(f.tyz[c + sy] - f.tyz[c], n.dy, n._dy)) -
+           dsc<PERF>(f.Pt[c] - f.Pt[c - sz], n.dz, n._dz);
+}
+
+// Free-slip copies folded into the update: a face whose tangential indices are the first
+// or last interior ones also writes its value onto the adjacent boundary faces. The
+// reference's bc_x!/bc_y!/bc_z! calls copy whole planes in sequence
+// (Stokes3D_ve_perf.jl:202-207), which leaves every boundary face equal to the face at
+// its tangential indices clamped into the interior; writing from the source face gives
+// exactly that, with no face read after another thread wrote it.
+__device__ __forceinline__ void bc_copies(double* A, int64_t c, double v, int a, int alo, int ahi, int64_t sa, int b,
+                                          int blo, int bhi, int64_t sb) {
+    const int da = (a == alo) ? -1 : 0, ua = (a == ahi) ? 1 : 0;
+    const int db = (b == blo) ? -1 : 0, ub = (b == bhi) ? 1 : 0;
+    if (da) A[c - sa] = v;
+    if (ua) A[c + sa] = v;
+    if (db) A[c - sb] = v;
+    if (ub) A[c + sb] = v;
+    if (da && db) A[c - sa - sb] = v;
+    if (da && ub) A[c - sa + sb] = v;
+    if (ua && db) A[c + sa - sb] = v;
+    if (ua && ub) A[c + sa + sb] = v;
+}
+
+// compute_V! (perf: Stokes3D_ve_perf.jl:83-88; roles: compute_dV! + compute_V!,
+// Stokes3D_ve_multixpu.jl:79-91) with the six bc copies, one thread per face point.
+template <bool PERF>
+__global__ void __launch_bounds__(256) k3_V_bc(Geom g, Fields64 f, Num n, int update) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    if (i > nx || j > ny) return;
+    const int64_t c = gidx(g, i, j, k);
+    const int64_t sx = 1, sy = g.px, sz = g.pxy;
+    // Vx: source faces j in [1,ny-2], k in [1,nz-2]; updated for i in [1,nx-1]
+    if (j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2) {
+        double v = f.Vx[c];
+        if (update && i >= 1 && i <= nx - 1) {
+            v = v + res3_x<PERF>(f, n, c, sx, sy, sz) * ((f.dtRho[c - sx] + f.dtRho[c]) * 0.5);
+            f.Vx[c] = v;
+        }
+        bc_copies(f.Vx, c, v, j, 1, ny - 2, sy, k, 1, nz - 2, sz);
+    }
+    // Vy: source faces i in [1,nx-2], k in [1,nz-2]; updated for j in [1,ny-1]
+    if (i >= 1 && i <= nx - 2 && k >= 1 && k <= nz - 2) {
+        double v = f.Vy[c];
+        if (update && j >= 1 && j <= ny - 1) {
+            v = v + res3_y<PERF>(f, n, c, sx, sy, sz) * ((f.dtRho[c - sy] + f.dtRho[c]) * 0.5);
+            f.Vy[c] = v;
+        }
+        bc_copies(f.Vy, c, v, i, 1, nx - 2, sx, k, 1, nz - 2, sz);
+    }
+    // Vz: source faces i in [1,nx-2], j in [1,ny-2]; updated for k in [1,nz-1]
+    if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2) {
+        double v = f.Vz[c];
+        if (update && k >= 1 && k <= nz - 1) {
+            v = v + res3_z<PERF>(f, n, c, sx, sy, sz) * ((f.dtRho[c - sz] + f.dtRho[c]) * 0.5);
+            f.Vz[c] = v;
+        }
+        bc_copies(f.Vz, c, v, i, 1, nx - 2, sx, j, 1, ny - 2, sy);
+    }
+}
+
+// compute_dV! alone (Stokes3D_ve_multixpu.jl:79-84): dV = R*@av_xi(dτ_Rho) at interior faces.
+template <bool PERF>
+__global__ void k3_dV(Geom g, Fields64 f, Num n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    if (i > nx || j > ny) return;
+    const int64_t c = gidx(g, i, j, k);
+    const int64_t sx = 1, sy = g.px, sz = g.pxy;
+    if (i >= 1 && i <= nx - 1 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2)
+        f.dVx[c] = res3_x<PERF>(f, n, c, sx, sy, sz) * ((f.dtRho[c - sx] + f.dtRho[c]) * 0.5);
+    if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 1 && k >= 1 && k <= nz - 2)
+        f.dVy[c] = res3_y<PERF>(f, n, c, sx, sy, sz) * ((f.dtRho[c - sy] + f.dtRho[c]) * 0.5);
+    if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 1)
+        f.dVz[c] = res3_z<PERF>(f, n, c, sx, sy, sz) * ((f.dtRho[c - sz] + f.dtRho[c]) * 0.5);
+}
+
+// compute_V! alone (Stokes3D_ve_multixpu.jl:86-91): @inn(V) = @inn(V) + @all(dV).
+__global__ void k3_add_dV(Geom g, Fields64 f) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    if (i > nx || j > ny) return;
+    const int64_t c = gidx(g, i, j, k);
+    if (i >= 1 && i <= nx - 1 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2) f.Vx[c] = f.Vx[c] + f.dVx[c];
+    if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 1 && k >= 1 && k <= nz - 2) f.Vy[c] = f.Vy[c] + f.dVy[c];
+    if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 1) f.Vz[c] = f.Vz[c] + f.dVz[c];
+}
+
+// ------------------------------------------------------------------ 2D kernels
+
+// compute_P! + compute_τ! for the three 2D scripts:
+//   V2D        Stokes2D.jl:33-44      VE2D  Stokes2D_ve.jl:42-55     VE2D_PERF  Stokes2D_ve_perf.jl:47-53
+template <int VAR>
+__global__ void __launch_bounds__(256) k2_Pt_tau(Geom g, Fields64 f, Num n, int roles, int store_divV) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int nx = g.nx, ny = g.ny;
+    if (i >= nx || j >= ny) return;
+    const int64_t c = gidx(g, i, j, 0);
+    const int64_t sx = 1, sy = g.px;
+    const double dvx = f.Vx[c + sx] - f.Vx[c];
+    const double dvy = f.Vy[c + sy] - f.Vy[c];
+    const double Gc = f.Gdt[c];
+    if (roles & ROLE_P) {
+        if (VAR == VE2D_PERF) {
+            f.Pt[c] = f.Pt[c] - n.r * Gc * (n._dx * dvx + n._dy * dvy);
+        } else {
+            const double dv = dvx / n.dx + dvy / n.dy;
+            if (store_divV) f.divV[c] = dv;
+            f.Pt[c] = f.Pt[c] - n.r * Gc * dv;
+        }
+    }
+    if (!(roles & ROLE_TAU)) return;
+    const double Mc = f.Mus[c];
+    if (VAR == V2D) {
+        f.txx[c] = (f.txx[c] + ((2.0 * Gc) * dvx) / n.dx) / (Gc / Mc + 1.0);
+        f.tyy[c] = (f.tyy[c] + ((2.0 * Gc) * dvy) / n.dy) / (Gc / Mc + 1.0);
+    } else {
+        const double Gr = Gc / n.gdt;
+        const double ex = (VAR == VE2D_PERF) ? n._dx * dvx : dvx / n.dx;
+        const double ey = (VAR == VE2D_PERF) ? n._dy * dvy : dvy / n.dy;
+        f.txx[c] = ((f.txx[c] + f.txx_o[c] * Gr) + (2.0 * Gc) * ex) / ((1.0 + Gc / Mc) + Gr);
+        f.tyy[c] = ((f.tyy[c] + f.tyy_o[c] * Gr) + (2.0 * Gc) * ey) / ((1.0 + Gc / Mc) + Gr);
+    }
+    // τxy on the vertex (x-face i, y-face j): i in [1,nx-1], j in [1,ny-1]
+    if (i >= 1 && j >= 1) {
+        const double ag = (((f.Gdt[c - sx - sy] + f.Gdt[c - sy]) + f.Gdt[c - sx]) + Gc) * 0.25;
+        const double am = (((f.Mus[c - sx - sy] + f.Mus[c - sy]) + f.Mus[c - sx]) + Mc) * 0.25;
+        const double d1 = f.Vx[c] - f.Vx[c - sy];  // @d_yi(Vx)
+        const double d2 = f.Vy[c] - f.Vy[c - sx];  // @d_xi(Vy)
+        if (VAR == V2D) {
+            f.txy[c] = (f.txy[c] + (2.0 * ag) * (0.5 * (d1 / n.dy + d2 / n.dx))) / (ag / am + 1.0);
+        } else if (VAR == VE2D) {
+            const double Gr = ag / n.gdt;
+            f.txy[c] = ((f.txy[c] + f.txy_o[c] * Gr) + (2.0 * ag) * (0.5 * (d1 / n.dy + d2 / n.dx))) /
+                       ((1.0 + ag / am) + Gr);
+        } else {
+            const double Gr = ag / n.gdt;
+            f.txy[c] = ((f.txy[c] + f.txy_o[c] * Gr) + ((2.0 * ag) * 0.5) * (n._dy * d1 + n._dx * d2)) /
+                       ((1.0 + ag / am) + Gr);
+        }
+    }
+}
+
+template <bool PERF>
+__device__ __forceinline__ double res2_x(const Fields64& f, const Num& n, int64_t c, int64_t sx, int64_t sy) {
+    return (dsc<PERF>(f.txx[c] - f.txx[c - sx], n.dx, n._dx) + dsc<PERF>(f.txy[c + sy] - f.txy[c], n.dy, n._dy)) -
+           dsc<PERF>(f.Pt[c] - f.Pt[c - sx], n.dx, n._dx);
+}
+template <bool PERF>
+__device__ __forceinline__ double res2_y(const Fields64& f, const Num& n, int64_t c, int64_t sx, int64_t sy) {
+    return (dsc<PERF>(f.tyy[c] - f.tyy[c - sy], n.dy, n._dy) + dsc<PERF>(f.txy[c + sx] - f.txy[c], n.dx, n._dx)) -
+           dsc<PERF>(f.Pt[c] - f.Pt[c - sy], n.dy, n._dy);
+}
+
+// compute_V! (+ compute_dV!) with bc_y!(Vx), bc_x!(Vy) (Stokes2D.jl:46-58,133-134;
+// Stokes2D_ve_perf.jl:55-59,151-152).
+template <int VAR>
+__global__ void __launch_bounds__(256) k2_V_bc(Geom g, Fields64 f, Num n, int update) {
+    constexpr bool PERF = (VAR == VE2D_PERF);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int nx = g.nx, ny = g.ny;
+    if (i > nx || j > ny) return;
+    const int64_t c = gidx(g, i, j, 0);
+    const int64_t sx = 1, sy = g.px;
+    if (j >= 1 && j <= ny - 2) {  // Vx source faces (bc_y!)
+        double v = f.Vx[c];
+        if (update && i >= 1 && i <= nx - 1) {
+            v = v + res2_x<PERF>(f, n, c, sx, sy) * ((f.dtRho[c - sx] + f.dtRho[c]) * 0.5);
+            f.Vx[c] = v;
+        }
+        if (j == 1) f.Vx[c - sy] = v;
+        if (j == ny - 2) f.Vx[c + sy] = v;
+    }
+    if (i >= 1 && i <= nx - 2) {  // Vy source faces (bc_x!)
+        double v = f.Vy[c];
+        if (update && j >= 1 && j <= ny - 1) {
+            v = v + res2_y<PERF>(f, n, c, sx, sy) * ((f.dtRho[c - sy] + f.dtRho[c]) * 0.5);
+            f.Vy[c] = v;
+        }
+        if (i == 1) f.Vy[c - sx] = v;
+        if (i == nx - 2) f.Vy[c + sx] = v;
+    }
+}
+
+// compute_dV! alone; Stokes2D.jl:46-52 also stores Rx, Ry.
+template <int VAR>
+__global__ void k2_dV(Geom g, Fields64 f, Num n) {
+    constexpr bool PERF = (VAR == VE2D_PERF);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int nx = g.nx, ny = g.ny;
+    if (i > nx || j > ny) return;
+    const int64_t c = gidx(g, i, j, 0);
+    const int64_t sx = 1, sy = g.px;
+    if (i >= 1 && i <= nx - 1 && j >= 1 && j <= ny - 2) {
+        const double R = res2_x<PERF>(f, n, c, sx, sy);
+        if (VAR == V2D) f.Rx[c] = R;
+        f.dVx[c] = R * ((f.dtRho[c - sx] + f.dtRho[c]) * 0.5);
+    }
+    if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 1) {
+        const double R = res2_y<PERF>(f, n, c, sx, sy);
+        if (VAR == V2D) f.Ry[c] = R;
+        f.dVy[c] = R * ((f.dtRho[c - sy] + f.dtRho[c]) * 0.5);
+    }
+}
+
+__global__ void k2_add_dV(Geom g, Fields64 f) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int nx = g.nx, ny = g.ny;
+    if (i > nx || j > ny) return;
+    const int64_t c = gidx(g, i, j, 0);
+    if (i >= 1 && i <= nx - 1 && j >= 1 && j <= ny - 2) f.Vx[c] = f.Vx[c] + f.dVx[c];
+    if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 1) f.Vy[c] = f.Vy[c] + f.dVy[c];
+}
+
+// ------------------------------------------------------------------ convergence check
+
+struct Acc {
+    double s[4];   // Σ Rx², Σ Ry², Σ Rz², Σ ∇V²
+    double vmin, vmax, pmin, pmax;
+};
+
+__device__ __forceinline__ void acc_init(Acc& a) {
+    a.s[0] = a.s[1] = a.s[2] = a.s[3] = 0.0;
+    a.vmin = a.pmin = DBL_MAX;
+    a.vmax = a.pmax = -DBL_MAX;
+}
+
+// Deterministic block reduction (fixed shuffle tree, then fixed cross-warp order).
+__device__ void acc_block_store(Acc& a, double* out) {
+    for (int o = 16; o > 0; o >>= 1) {
+        for (int q = 0; q < 4; ++q) a.s[q] += __shfl_down_sync(kFull, a.s[q], o);
+        a.vmin = fmin(a.vmin, __shfl_down_sync(kFull, a.vmin, o));
+        a.vmax = fmax(a.vmax, __shfl_down_sync(kFull, a.vmax, o));
+        a.pmin = fmin(a.pmin, __shfl_down_sync(kFull, a.pmin, o));
+        a.pmax = fmax(a.pmax, __shfl_down_sync(kFull, a.pmax, o));
+    }
+    __shared__ double sm[32][kCheckSlots];
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const int nthr = blockDim.x * blockDim.y * blockDim.z;
+    const int lane = tid & 31, warp = tid >> 5, nw = (nthr + 31) >> 5;
+    if (lane == 0) {
+        sm[warp][0] = a.s[0]; sm[warp][1] = a.s[1]; sm[warp][2] = a.s[2]; sm[warp][3] = a.s[3];
+        sm[warp][4] = a.vmin; sm[warp][5] = a.vmax; sm[warp][6] = a.pmin; sm[warp][7] = a.pmax;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double r[kCheckSlots];
+        for (int q = 0; q < kCheckSlots; ++q) r[q] = sm[0][q];
+        for (int w = 1; w < nw; ++w) {
+            for (int q = 0; q < 4; ++q) r[q] += sm[w][q];
+            r[4] = fmin(r[4], sm[w][4]); r[5] = fmax(r[5], sm[w][5]);
+            r[6] = fmin(r[6], sm[w][6]); r[7] = fmax(r[7], sm[w][7]);
+        }
+        const int64_t b = blockIdx.x + (int64_t)gridDim.x * (blockIdx.y + (int64_t)gridDim.y * blockIdx.z);
+        for (int q = 0; q < kCheckSlots; ++q) out[b * kCheckSlots + q] = r[q];
+    }
+}
+
+// 3D check: compute_Res! (perf: ∇V from the current V) / stored ∇V (roles), the residual
+// arrays and the per-block partial norms and extrema. Blocks stride over z.
+template <bool PERF>
+__global__ void __launch_bounds__(256) k3_check(Geom g, Fields64 f, Num n, double* partials) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const int64_t sx = 1, sy = g.px, sz = g.pxy;
+    Acc a;
+    acc_init(a);
+    if (i <= nx && j < ny) {
+        for (int k = blockIdx.z; k < nz; k += gridDim.z) {
+            const int64_t c = gidx(g, i, j, k);
+            const double vx = f.Vx[c];
+            a.vmin = fmin(a.vmin, vx);
+            a.vmax = fmax(a.vmax, vx);
+            if (i < nx) {
+                const double p = f.Pt[c];
+                a.pmin = fmin(a.pmin, p);
+                a.pmax = fmax(a.pmax, p);
+                double dv;
+                if (PERF) {
+                    dv = (n._dx * (f.Vx[c + sx] - f.Vx[c]) + n._dy * (f.Vy[c + sy] - f.Vy[c])) +
+                         n._dz * (f.Vz[c + sz] - f.Vz[c]);
+                    f.divV[c] = dv;
+                } else {
+                    dv = f.divV[c];
+                }
+                a.s[3] += dv * dv;
+            }
+            if (i >= 1 && i <= nx - 1 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2) {
+                const double R = res3_x<PERF>(f, n, c, sx, sy, sz);
+                f.Rx[c] = R;
+                a.s[0] += R * R;
+            }
+            if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 1 && k >= 1 && k <= nz - 2) {
+                const double R = res3_y<PERF>(f, n, c, sx, sy, sz);
+                f.Ry[c] = R;
+                a.s[1] += R * R;
+            }
+            if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 1) {
+                const double R = res3_z<PERF>(f, n, c, sx, sy, sz);
+                f.Rz[c] = R;
+                a.s[2] += R * R;
+            }
+        }
+    }
+    acc_block_store(a, partials);
+}
+
+template <int VAR>
+__global__ void __launch_bounds__(256) k2_check(Geom g, Fields64 f, Num n, double* partials) {
+    constexpr bool PERF = (VAR == VE2D_PERF);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int nx = g.nx, ny = g.ny;
+    const int64_t sx = 1, sy = g.px;
+    Acc a;
+    acc_init(a);
+    if (i <= nx && j < ny) {
+        const int64_t c = gidx(g, i, j, 0);
+        const double vx = f.Vx[c];
+        a.vmin = vx;
+        a.vmax = vx;
+        if (i < nx) {
+            a.pmin = a.pmax = f.Pt[c];
+            double dv;
+            if (PERF) {
+                dv = n._dx * (f.Vx[c + sx] - f.Vx[c]) + n._dy * (f.Vy[c + sy] - f.Vy[c]);
+                f.divV[c] = dv;
+            } else {
+                dv = f.divV[c];
+            }
+            a.s[3] = dv * dv;
+        }
+        if (i >= 1 && i <= nx - 1 && j >= 1 && j <= ny - 2) {
+            const double R = res2_x<PERF>(f, n, c, sx, sy);
+            f.Rx[c] = R;
+            a.s[0] = R * R;
+        }
+        if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 1) {
+            const double R = res2_y<PERF>(f, n, c, sx, sy);
+            f.Ry[c] = R;
+            a.s[1] = R * R;
+        }
+    }
+    acc_block_store(a, partials);
+}
+
+// Finaliser: fixed-order sum of the block partials, then the norms of the check
+// (Stokes3D_ve_perf.jl:213-218): norm_R = norm(R)/(Pmax-Pmin)*lx/sqrt(length(R)).
+__global__ void k_check_finalize(const double* partials, int nblocks, double lx, double lenRx, double lenRy,
+                                 double lenRz, double lenDiv, int ndim, CheckResult* out) {
+    __shared__ double sm[256][kCheckSlots];
+    const int t = threadIdx.x;
+    double r[kCheckSlots] = {0.0, 0.0, 0.0, 0.0, DBL_MAX, -DBL_MAX, DBL_MAX, -DBL_MAX};
+    for (int b = t; b < nblocks; b += blockDim.x) {
+        const double* p = partials + (int64_t)b * kCheckSlots;
+        for (int q = 0; q < 4; ++q) r[q] += p[q];
+        r[4] = fmin(r[4], p[4]); r[5] = fmax(r[5], p[5]);
+        r[6] = fmin(r[6], p[6]); r[7] = fmax(r[7], p[7]);
+    }
+    for (int q = 0; q < kCheckSlots; ++q) sm[t][q] = r[q];
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (t < s) {
+            for (int q = 0; q < 4; ++q) sm[t][q] += sm[t + s][q];
+            sm[t][4] = fmin(sm[t][4], sm[t + s][4]); sm[t][5] = fmax(sm[t][5], sm[t + s][5]);
+            sm[t][6] = fmin(sm[t][6], sm[t + s][6]); sm[t][7] = fmax(sm[t][7], sm[t + s][7]);
+        }
+        __syncthreads();
+    }
+    if (t == 0) {
+        const double dP = sm[0][7] - sm[0][6], dV = sm[0][5] - sm[0][4];
+        CheckResult c;
+        c.nRx = sqrt(sm[0][0]) / dP * lx / sqrt(lenRx);
+        c.nRy = sqrt(sm[0][1]) / dP * lx / sqrt(lenRy);
+        c.nRz = (ndim == 3) ? sqrt(sm[0][2]) / dP * lx / sqrt(lenRz) : 0.0;
+        c.ndiv = sqrt(sm[0][3]) / dV * lx / sqrt(lenDiv);
+        c.vmin = sm[0][4]; c.vmax = sm[0][5]; c.pmin = sm[0][6]; c.pmax = sm[0][7];
+        const bool bad = isnan(c.nRx) || isnan(c.nRy) || isnan(c.nRz) || isnan(c.ndiv);
+        c.err = bad ? NAN : fmax(fmax(c.nRx, c.nRy), fmax(c.nRz, c.ndiv));
+        c.flag_nan = bad ? 1.0 : 0.0;
+        *out = c;
+    }
+}
+
+// ------------------------------------------------------------------ set-up kernels
+
+// Initial conditions (Stokes3D_ve_perf.jl:164-172; Stokes3D_ve_multixpu.jl:174-178 builds
+// the staggered coordinates through ImplicitGlobalGrid's x_g, which for one rank is
+// (ix-1)*dx - 0.5*dx; Stokes2D.jl:106-114 for 2D). One thread per unified point.
+template <bool D3, bool IGG>
+__global__ void k_init_inclusion(Geom g, Fields64 f, Num n, double mus0, double musi, double radius2, double ebg) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    if (i > nx || j > ny) return;
+    const int64_t c = gidx(g, i, j, k);
+    const double X = ((double)i * n.dx + 0.5 * n.dx) - 0.5 * n.lx;
+    const double Y = ((double)j * n.dy + 0.5 * n.dy) - 0.5 * n.ly;
+    if (i < nx && j < ny && k < (D3 ? nz : 1)) {
+        double rad2 = X * X + Y * Y;
+        if (D3) {
+            const double Z = ((double)k * n.dz + 0.5 * n.dz) - 0.5 * n.lz;
+            rad2 = rad2 + Z * Z;
+        }
+        f.Mus[c] = (rad2 < radius2) ? musi : mus0;
+    }
+    const double xv = IGG ? ((((double)i * n.dx + (-0.5 * n.dx)) + 0.5 * n.dx) - 0.5 * n.lx)
+                          : ((double)i * n.dx - 0.5 * n.lx);
+    if (j < ny && k < (D3 ? nz : 1)) f.Vx[c] = (-ebg) * xv;
+    if (D3) {
+        const double zv = IGG ? ((((double)k * n.dz + (-0.5 * n.dz)) + 0.5 * n.dz) - 0.5 * n.lz)
+                              : ((double)k * n.dz - 0.5 * n.lz);
+        if (i < nx && j < ny) f.Vz[c] = ebg * zv;
+    } else {
+        if (i < nx) f.Vy[c] = ebg * ((double)j * n.dy - 0.5 * n.ly);
+    }
+}
+
+// smooth! (Stokes3D_ve_perf.jl:24-27; 2D Stokes2D.jl:17-20) on the interior cells.
+template <bool D3>
+__global__ void k_smooth(Geom g, double* __restrict__ dst, const double* __restrict__ A, double coef) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (i < 1 || j < 1 || i > g.nx - 2 || j > g.ny - 2) return;
+    if (D3 && (k < 1 || k > g.nz - 2)) return;
+    const int64_t c = gidx(g, i, j, k);
+    const int64_t sy = g.px, sz = g.pxy;
+    const double a = A[c];
+    const double d2x = (A[c + 1] - a) - (a - A[c - 1]);
+    const double d2y = (A[c + sy] - a) - (a - A[c - sy]);
+    double s = d2x + d2y;
+    if (D3) s = s + ((A[c + sz] - a) - (a - A[c - sz]));
+    dst[c] = a + coef * s;
+}
+
+// compute_maxloc! + bc_x!/bc_y!/bc_z! on Musτ (Stokes3D_ve_perf.jl:29-32,178-182): the
+// boundary copies leave each boundary cell equal to the local max at its clamped index.
+template <bool D3>
+__global__ void k_maxloc(Geom g, double* __restrict__ must, const double* __restrict__ A) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (i >= g.nx || j >= g.ny) return;
+    const int ci = min(max(i, 1), g.nx - 2), cj = min(max(j, 1), g.ny - 2);
+    const int ck = D3 ? min(max(k, 1), g.nz - 2) : 0;
+    const int64_t c = gidx(g, ci, cj, ck);
+    const int64_t sy = g.px, sz = g.pxy;
+    double m = fmax(fmax(fmax(fmax(A[c - 1], A[c + 1]), A[c]), A[c - sy]), A[c + sy]);
+    if (D3) m = fmax(fmax(m, A[c - sz]), A[c + sz]);
+    must[gidx(g, i, j, k)] = m;
+}
+
+// compute_iter_params! (Stokes3D_ve_perf.jl:34-39; viscous Stokes2D.jl:27-31).
+template <bool EL>
+__global__ void k_iter_params(Geom g, Fields64 f, Num n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (i >= g.nx || j >= g.ny) return;
+    const int64_t c = gidx(g, i, j, k);
+    const double mu_eff = EL ? 1.0 / (1.0 / f.Must[c] + 1.0 / n.gdt) : f.Must[c];
+    const double dtr = n.Vpdt * n.max_l / n.Re / mu_eff;
+    f.dtRho[c] = dtr;
+    f.Gdt[c] = (n.Vpdt * n.Vpdt) / dtr / (n.r + 2.0);
+}
+
+inline dim3 blk() { return dim3(32, 8, 1); }
+inline dim3 grid_cells(const Geom& g) { return dim3((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz); }
+inline dim3 grid_faces(const Geom& g, bool d3) {
+    return dim3((g.nx + 1 + 31) / 32, (g.ny + 1 + 7) / 8, d3 ? g.nz + 1 : 1);
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ launchers
+
+cudaError_t launch_Pt_tau(int v, const Geom& g, const Fields64& f, const Num& n, int roles, bool store_divV,
+                          cudaStream_t s) {
+    const int sd = store_divV ? 1 : 0;
+    switch (v) {
+        case VE3D: k3_Pt_tau<true, false><<<grid_cells(g), blk(), 0, s>>>(g, f, n, roles, sd); break;
+        case VE3D_PERF: k3_Pt_tau<true, true><<<grid_cells(g), blk(), 0, s>>>(g, f, n, roles, sd); break;
+        case V3D: k3_Pt_tau<false, true><<<grid_cells(g), blk(), 0, s>>>(g, f, n, roles, sd); break;
+        case V2D: k2_Pt_tau<V2D><<<grid_cells(g), blk(), 0, s>>>(g, f, n, roles, sd); break;
+        case VE2D: k2_Pt_tau<VE2D><<<grid_cells(g), blk(), 0, s>>>(g, f, n, roles, sd); break;
+        case VE2D_PERF: k2_Pt_tau<VE2D_PERF><<<grid_cells(g), blk(), 0, s>>>(g, f, n, roles, sd); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_V_bc(int v, const Geom& g, const Fields64& f, const Num& n, bool update, cudaStream_t s) {
+    const int u = update ? 1 : 0;
+    switch (v) {
+        case VE3D: k3_V_bc<false><<<grid_faces(g, true), blk(), 0, s>>>(g, f, n, u); break;
+        case VE3D_PERF:
+        case V3D: k3_V_bc<true><<<grid_faces(g, true), blk(), 0, s>>>(g, f, n, u); break;
+        case V2D: k2_V_bc<V2D><<<grid_faces(g, false), blk(), 0, s>>>(g, f, n, u); break;
+        case VE2D: k2_V_bc<VE2D><<<grid_faces(g, false), blk(), 0, s>>>(g, f, n, u); break;
+        case VE2D_PERF: k2_V_bc<VE2D_PERF><<<grid_faces(g, false), blk(), 0, s>>>(g, f, n, u); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_dV(int v, const Geom& g, const Fields64& f, const Num& n, cudaStream_t s) {
+    switch (v) {
+        case VE3D: k3_dV<false><<<grid_faces(g, true), blk(), 0, s>>>(g, f, n); break;
+        case VE3D_PERF:
+        case V3D: k3_dV<true><<<grid_faces(g, true), blk(), 0, s>>>(g, f, n); break;
+        case V2D: k2_dV<V2D><<<grid_faces(g, false), blk(), 0, s>>>(g, f, n); break;
+        case VE2D: k2_dV<VE2D><<<grid_faces(g, false), blk(), 0, s>>>(g, f, n); break;
+        case VE2D_PERF: k2_dV<VE2D_PERF><<<grid_faces(g, false), blk(), 0, s>>>(g, f, n); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_add_dV(int v, const Geom& g, const Fields64& f, cudaStream_t s) {
+    if (variant_is3d(v)) k3_add_dV<<<grid_faces(g, true), blk(), 0, s>>>(g, f);
+    else k2_add_dV<<<grid_faces(g, false), blk(), 0, s>>>(g, f);
+    return cudaGetLastError();
+}
+
+static dim3 check_grid(int v, const Geom& g) {
+    if (variant_is3d(v)) return dim3((g.nx + 1 + 31) / 32, (g.ny + 7) / 8, g.nz < 32 ? g.nz : 32);
+    return dim3((g.nx + 1 + 31) / 32, (g.ny + 7) / 8, 1);
+}
+
+int check_num_blocks(int v, const Geom& g) {
+    const dim3 gr = check_grid(v, g);
+    return (int)(gr.x * gr.y * gr.z);
+}
+
+cudaError_t launch_check(int v, const Geom& g, const Fields64& f, const Num& n, double* partials, int nblocks_cap,
+                         CheckResult* result, cudaStream_t s) {
+    const dim3 gr = check_grid(v, g);
+    const int nb = (int)(gr.x * gr.y * gr.z);
+    if (nb > nblocks_cap) return cudaErrorInvalidValue;
+    switch (v) {
+        case VE3D: k3_check<false><<<gr, blk(), 0, s>>>(g, f, n, partials); break;
+        case VE3D_PERF:
+        case V3D: k3_check<true><<<gr, blk(), 0, s>>>(g, f, n, partials); break;
+        case V2D: k2_check<V2D><<<gr, blk(), 0, s>>>(g, f, n, partials); break;
+        case VE2D: k2_check<VE2D><<<gr, blk(), 0, s>>>(g, f, n, partials); break;
+        case VE2D_PERF: k2_check<VE2D_PERF><<<gr, blk(), 0, s>>>(g, f, n, partials); break;
+        default: return cudaErrorInvalidValue;
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const bool d3 = variant_is3d(v);
+    const double nx = g.nx, ny = g.ny, nz = d3 ? g.nz : 1;
+    const double lenRx = d3 ? (nx - 1) * (ny - 2) * (nz - 2) : (nx - 1) * (ny - 2);
+    const double lenRy = d3 ? (nx - 2) * (ny - 1) * (nz - 2) : (nx - 2) * (ny - 1);
+    const double lenRz = d3 ? (nx - 2) * (ny - 2) * (nz - 1) : 1.0;
+    const double lenDiv = nx * ny * nz;
+    k_check_finalize<<<1, 256, 0, s>>>(partials, nb, n.lx, lenRx, lenRy, lenRz, lenDiv, d3 ? 3 : 2, result);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_init_inclusion(int v, const Geom& g, const Fields64& f, const Num& n, double mus0, double musi,
+                                  double radius2, double ebg, cudaStream_t s) {
+    const bool d3 = variant_is3d(v);
+    const dim3 gr = grid_faces(g, d3);
+    if (v == VE3D) k_init_inclusion<true, true><<<gr, blk(), 0, s>>>(g, f, n, mus0, musi, radius2, ebg);
+    else if (d3) k_init_inclusion<true, false><<<gr, blk(), 0, s>>>(g, f, n, mus0, musi, radius2, ebg);
+    else k_init_inclusion<false, false><<<gr, blk(), 0, s>>>(g, f, n, mus0, musi, radius2, ebg);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_smooth(int v, const Geom& g, double* dst, const double* src, double fact, cudaStream_t s) {
+    if (variant_is3d(v)) k_smooth<true><<<grid_cells(g), blk(), 0, s>>>(g, dst, src, 1.0 / 6.1 / fact);
+    else k_smooth<false><<<grid_cells(g), blk(), 0, s>>>(g, dst, src, 1.0 / 4.1 / fact);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_maxloc(int v, const Geom& g, double* must, const double* mus, cudaStream_t s) {
+    if (variant_is3d(v)) k_maxloc<true><<<grid_cells(g), blk(), 0, s>>>(g, must, mus);
+    else k_maxloc<false><<<grid_cells(g), blk(), 0, s>>>(g, must, mus);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_iter_params(int v, const Geom& g, const Fields64& f, const Num& n, cudaStream_t s) {
+    if (variant_elastic(v)) k_iter_params<true><<<grid_cells(g), blk(), 0, s>>>(g, f, n);
+    else k_iter_params<false><<<grid_cells(g), blk(), 0, s>>>(g, f, n);
+    return cudaGetLastError();
+}
+
+}  // namespace pts

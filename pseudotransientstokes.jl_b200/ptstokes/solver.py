@@ -1,0 +1,205 @@
+"""Solver: one PT Stokes problem on the GPU, driven through the C ABI.
+
+The methods carry the reference's kernel-role names (compute_P!, compute_τ!,
+compute_dV!, compute_V!, compute_Pt_τ!, compute_Res!, assign_τ!, bc_*!) and act on the
+fields the context owns on the device. Fields cross to and from the host as Float64
+column-major numpy arrays with the reference's own extents.
+"""
+import ctypes
+import math
+
+import numpy as np
+
+from . import _abi
+from ._abi import FIELD_ID, PtsCheck, PtsDesc, PtsSolveInfo, check
+
+PI = math.pi
+
+# Physics and numerics of each script (the constants at the top of Stokes2D_()/Stokes3D_()).
+VARIANT_DEFAULTS = {
+    # scripts/Stokes2D.jl:74-84
+    "2d_v": dict(nt=1, iter_max=1e5, nout=500, eps=1e-8, CFL=0.9 / math.sqrt(2), Re=5 * PI, r=1.0),
+    # scripts/Stokes2D_ve.jl:89-103
+    "2d_ve": dict(nt=5, iter_max=2e5, nout=200, eps=1e-8, CFL=0.8 / math.sqrt(2), Re=5 * PI, r=1.0),
+    # scripts/Stokes2D_ve_perf.jl:82-97
+    "2d_ve_perf": dict(nt=1, iter_max=100, nout=2000, eps=1e-8, CFL=0.8 / math.sqrt(2), Re=5 * PI, r=1.0),
+    # scripts/stokes_3D/Stokes3D_ve_multixpu.jl:120-134
+    "3d_ve": dict(nt=5, iter_max=2e5, nout=200, eps=1e-8, CFL=0.8 / math.sqrt(3), Re=6 * PI, r=1.0),
+    # scripts/stokes_3D/Stokes3D_ve_perf.jl:118-132
+    "3d_ve_perf": dict(nt=1, iter_max=200, nout=2000, eps=1e-8, CFL=0.8 / math.sqrt(3), Re=6 * PI, r=1.0),
+    # 3D viscous (no script): the 3D numerics, one "time step"
+    "3d_v": dict(nt=1, iter_max=2e5, nout=200, eps=1e-8, CFL=0.8 / math.sqrt(3), Re=6 * PI, r=1.0),
+}
+
+
+def linrange(a, b, n):
+    """Values of Julia's ``LinRange(a, b, n)``: (1-t)*a + t*b, t = (i-1)/(n-1)."""
+    d = n - 1
+    return np.array([(1 - (j / d)) * a + (j / d) * b if d > 0 else a for j in range(n)])
+
+
+class Solver:
+    """A PT Stokes context (``pts_ctx``) with its device fields.
+
+    ``variant`` is one of ``2d_v, 2d_ve, 2d_ve_perf, 3d_ve, 3d_ve_perf, 3d_v``.
+    Keyword arguments override the script defaults (``VARIANT_DEFAULTS``) and the
+    physics (``lx, ly, lz, G, xi, mus0``: ``dt = mus0/(G*xi)`` as in the scripts).
+    """
+
+    def __init__(self, variant, nx, ny, nz=None, precision="fp64", lib=None, **kw):
+        self.lib = lib or _abi.load()
+        self.variant = variant
+        self.ndim = 3 if variant.startswith("3d") else 2
+        p = dict(lx=10.0, ly=10.0, lz=10.0, xi=1.0, mus0=1.0, G=1.0, max_l=0.0, mixed_inner=0)
+        p.update(VARIANT_DEFAULTS[variant])
+        p.update(kw)
+        self.p = p
+        self.nx, self.ny, self.nz = nx, ny, (nz if self.ndim == 3 else 1)
+        self.dt = p["mus0"] / (p["G"] * p["xi"])
+        d = PtsDesc()
+        d.variant = _abi.VARIANTS[variant]
+        d.precision = _abi.PRECISIONS[precision]
+        d.nx, d.ny, d.nz = nx, ny, (nz if self.ndim == 3 else 1)
+        d.nout = int(p["nout"])
+        d.lx, d.ly, d.lz = p["lx"], p["ly"], p["lz"]
+        d.G, d.dt = p["G"], self.dt
+        d.r, d.Re, d.CFL = p["r"], p["Re"], p["CFL"]
+        d.max_l, d.eps, d.iter_max = p["max_l"], p["eps"], float(p["iter_max"])
+        d.mixed_inner = int(p["mixed_inner"])
+        self.desc = d
+        ctx = ctypes.c_void_p()
+        check(self.lib, None, self.lib.pts_create(ctypes.byref(d), ctypes.byref(ctx)))
+        self.ctx = ctx
+        self.dx = p["lx"] / nx
+        self.dy = p["ly"] / ny
+        self.dz = p["lz"] / nz if self.ndim == 3 else 1.0
+
+    # ---------------------------------------------------------------- lifetime
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.lib.pts_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _ck(self, rc):
+        return check(self.lib, self.ctx, rc)
+
+    # ---------------------------------------------------------------- fields
+    def shape(self, name):
+        s = (ctypes.c_int64 * 3)()
+        self._ck(self.lib.pts_field_shape(self.ctx, FIELD_ID[name], s))
+        return tuple(s[: self.ndim])
+
+    def get(self, name):
+        shp = self.shape(name)
+        out = np.empty(shp, dtype=np.float64, order="F")
+        self._ck(self.lib.pts_get_field(self.ctx, FIELD_ID[name], out.ctypes.data, out.size))
+        return out
+
+    def set(self, name, a):
+        a = np.asfortranarray(a, dtype=np.float64)
+        if a.shape != self.shape(name):
+            raise ValueError(f"{name}: expected shape {self.shape(name)}, got {a.shape}")
+        self._ck(self.lib.pts_set_field(self.ctx, FIELD_ID[name], a.ctypes.data, a.size))
+
+    def set_device(self, name, ptr, n):
+        self._ck(self.lib.pts_set_field_device(self.ctx, FIELD_ID[name], ptr, n))
+
+    def get_device(self, name, ptr, n):
+        self._ck(self.lib.pts_get_field_device(self.ctx, FIELD_ID[name], ptr, n))
+
+    # ---------------------------------------------------------------- set-up
+    def init_inclusion(self, mus0=1.0, musi=1e-3, radius2=1.0, ebg=1.0):
+        self._ck(self.lib.pts_init_inclusion(self.ctx, mus0, musi, radius2, ebg))
+
+    def smooth(self, nsweeps=10, fact=1.0):
+        self._ck(self.lib.pts_smooth(self.ctx, nsweeps, fact))
+
+    def compute_maxloc(self):
+        self._ck(self.lib.pts_compute_maxloc(self.ctx))
+
+    def compute_iter_params(self):
+        self._ck(self.lib.pts_compute_iter_params(self.ctx))
+
+    def setup_inclusion(self, musi=1e-3, radius2=1.0, ebg=1.0, nsmooth=10):
+        """The scripts' set-up: ICs, 10x smooth!, maxloc + bc, iteration parameters."""
+        self.init_inclusion(self.p["mus0"], musi, radius2, ebg)
+        self.smooth(nsmooth, 1.0)
+        self.compute_maxloc()
+        self.compute_iter_params()
+        return self
+
+    # ---------------------------------------------------------------- roles
+    def assign_tau(self):
+        self._ck(self.lib.pts_assign_tau(self.ctx))
+
+    def compute_P(self):
+        self._ck(self.lib.pts_compute_P(self.ctx))
+
+    def compute_tau(self):
+        self._ck(self.lib.pts_compute_tau(self.ctx))
+
+    def compute_dV(self):
+        self._ck(self.lib.pts_compute_dV(self.ctx))
+
+    def compute_V(self):
+        self._ck(self.lib.pts_compute_V(self.ctx))
+
+    def apply_bc(self):
+        self._ck(self.lib.pts_apply_bc(self.ctx))
+
+    def compute_Pt_tau(self):
+        self._ck(self.lib.pts_compute_Pt_tau(self.ctx))
+
+    def compute_V_bc(self):
+        self._ck(self.lib.pts_compute_V_bc(self.ctx))
+
+    def compute_res(self):
+        c = PtsCheck()
+        self._ck(self.lib.pts_compute_res(self.ctx, ctypes.byref(c)))
+        return c.as_dict()
+
+    # ---------------------------------------------------------------- drivers
+    def iterate(self, n):
+        self._ck(self.lib.pts_iterate(self.ctx, int(n)))
+
+    def stream_handle(self):
+        """The context's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""
+        h = ctypes.c_void_p()
+        self._ck(self.lib.pts_stream(self.ctx, ctypes.byref(h)))
+        return h.value or 0
+
+    def sync(self):
+        self._ck(self.lib.pts_sync(self.ctx))
+
+    def solve(self):
+        info = PtsSolveInfo()
+        self._ck(self.lib.pts_solve(self.ctx, ctypes.byref(info)))
+        return dict(iters=info.iters, converged=bool(info.converged), nchecks=info.nchecks, last=info.last.as_dict())
+
+    def run(self, nt=None):
+        nt = self.p["nt"] if nt is None else nt
+        per = (ctypes.c_int64 * max(nt, 1))()
+        info = PtsSolveInfo()
+        self._ck(self.lib.pts_run(self.ctx, nt, per, ctypes.byref(info)))
+        return dict(ittot=info.iters, iters=list(per[:nt]), converged=bool(info.converged), last=info.last.as_dict())
+
+    # ---------------------------------------------------------------- grid
+    def centres(self):
+        """xc, yc[, zc] = LinRange(dx/2, lx-dx/2, nx), ... (Stokes3D_ve_perf.jl:139)."""
+        p = self.p
+        out = [linrange(self.dx / 2, p["lx"] - self.dx / 2, self.nx), linrange(self.dy / 2, p["ly"] - self.dy / 2, self.ny)]
+        if self.ndim == 3:
+            out.append(linrange(self.dz / 2, p["lz"] - self.dz / 2, self.nz))
+        return out

@@ -1,0 +1,203 @@
+"""GPU (libptstokes.so, through the C ABI) against the CPU oracle, variant by variant.
+
+The FP64 kernels are built without FMA contraction and evaluate every expression in
+the reference's order, so the bar here is bit-for-bit equality of every field
+(a stricter form of the <=1e-12 relative-per-field requirement). Norms of the
+convergence check are reductions in a different summation order; they must agree to
+1e-12 relative.
+"""
+import numpy as np
+import pytest
+
+from conftest import julia_isapprox, load_golden
+
+pytestmark = pytest.mark.gpu
+
+F2 = ["Pt", "Vx", "Vy", "txx", "tyy", "txy", "Mus", "Must", "Gdt", "dtRho"]
+F3 = F2 + ["Vz", "tzz", "txz", "tyz"]
+CASES = [
+    ("2d_v", (47, 39)),
+    ("2d_ve", (47, 39)),
+    ("2d_ve_perf", (47, 39)),
+    ("3d_ve", (23, 19, 17)),
+    ("3d_ve_perf", (23, 19, 17)),
+    ("3d_v", (23, 19, 17)),
+]
+
+
+def make_pair(gpu_lib, variant, dims, **kw):
+    import ptstokes
+    from oracle import scripts as S
+    okw = dict(kw)
+    if "iter_max" in okw:
+        okw["iterMax"] = okw.pop("iter_max")
+    o = S.make(variant, *dims, **okw)
+    g = ptstokes.Solver(variant, *dims, lib=gpu_lib, **kw)
+    g.setup_inclusion()
+    return o, g
+
+
+def fields(variant):
+    return F3 if variant.startswith("3d") else F2
+
+
+def assert_fields_equal(o, g, names):
+    bad = []
+    for n in names:
+        a, b = g.get(n), o.f[n]
+        assert a.shape == b.shape, (n, a.shape, b.shape)
+        if not np.array_equal(a, b):
+            rel = np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+            bad.append((n, float(np.abs(a - b).max()), float(rel)))
+    assert not bad, bad
+
+
+@pytest.mark.parametrize("variant,dims", CASES)
+def test_setup_bit_exact(gpu_lib, variant, dims):
+    """ICs, 10x smooth!, maxloc + bc and iteration parameters built on the device."""
+    o, g = make_pair(gpu_lib, variant, dims)
+    names = ["Vx", "Vy", "Mus", "Must", "Gdt", "dtRho"] + (["Vz"] if variant.startswith("3d") else [])
+    assert_fields_equal(o, g, names)
+    g.close()
+
+
+@pytest.mark.parametrize("variant,dims", CASES)
+def test_iterations_bit_exact(gpu_lib, variant, dims):
+    """Two 'physical steps' of PT iterations on the fast path (assign_τ! between them)."""
+    o, g = make_pair(gpu_lib, variant, dims)
+    for nit in (37, 23):
+        if o.elastic:
+            o.assign_tau()
+            g.assign_tau()
+        for _ in range(nit):
+            o.iteration()
+        g.iterate(nit)
+        g.sync()
+        assert_fields_equal(o, g, fields(variant))
+    g.close()
+
+
+@pytest.mark.parametrize("variant,dims", CASES)
+def test_check_matches_oracle(gpu_lib, variant, dims):
+    """compute_Res! arrays bit-exact, norms and extrema of the check to 1e-12."""
+    o, g = make_pair(gpu_lib, variant, dims)
+    if o.elastic:
+        o.assign_tau()
+        g.assign_tau()
+    for _ in range(41):
+        o.iteration()
+    g.iterate(41)
+    err_o, norms_o = o.check()
+    chk = g.compute_res()
+    names = ["Rx", "Ry", "divV"] + (["Rz"] if variant.startswith("3d") else [])
+    assert_fields_equal(o, g, names)
+    got = [chk["norm_Rx"], chk["norm_Ry"]] + ([chk["norm_Rz"]] if variant.startswith("3d") else []) + [chk["norm_divV"]]
+    np.testing.assert_allclose(got, norms_o, rtol=1e-12)
+    assert abs(chk["err"] - err_o) <= 1e-12 * err_o
+    assert chk["Vmin"] == o.f["Vx"].min() and chk["Vmax"] == o.f["Vx"].max()
+    assert chk["Pmin"] == o.f["Pt"].min() and chk["Pmax"] == o.f["Pt"].max()
+    g.close()
+
+
+@pytest.mark.parametrize("variant,dims", CASES)
+def test_role_kernels_bit_exact(gpu_lib, variant, dims):
+    """The four roles called one by one (compute_P!, compute_τ!, compute_dV!, compute_V!)
+    plus the bc calls equal the reference iteration."""
+    o, g = make_pair(gpu_lib, variant, dims)
+    if o.elastic:
+        o.assign_tau()
+        g.assign_tau()
+    for _ in range(13):
+        o.iteration()
+        g.compute_P()
+        g.compute_tau()
+        g.compute_dV()
+        g.compute_V()
+        g.apply_bc()
+    g.sync()
+    assert_fields_equal(o, g, fields(variant))
+    if variant in ("2d_v", "2d_ve", "3d_ve"):
+        assert_fields_equal(o, g, ["dVx", "dVy"] + (["dVz"] if variant == "3d_ve" else []))
+    g.close()
+
+
+@pytest.mark.parametrize("variant,dims", [("2d_ve_perf", (31, 27)), ("3d_ve_perf", (15, 13, 11))])
+def test_fused_role_pair_bit_exact(gpu_lib, variant, dims):
+    """compute_Pt_τ! + compute_V! (+bc) called as roles."""
+    o, g = make_pair(gpu_lib, variant, dims)
+    o.assign_tau()
+    g.assign_tau()
+    for _ in range(17):
+        o.iteration()
+        g.compute_Pt_tau()
+        g.compute_V_bc()
+    g.sync()
+    assert_fields_equal(o, g, fields(variant))
+    g.close()
+
+
+@pytest.mark.parametrize("variant,dims,kw", [
+    ("2d_v", (31, 31), dict(nout=100)),
+    ("2d_ve", (31, 27), dict(nout=100, nt=2)),
+    ("3d_ve", (15, 15, 13), dict(nout=100, nt=2)),
+    ("3d_v", (15, 13, 15), dict(nout=100, nt=1)),
+])
+def test_converged_solve_matches_oracle(gpu_lib, variant, dims, kw):
+    """The whole time loop to tolerance 1e-8: same iteration count per step, same fields."""
+    o, g = make_pair(gpu_lib, variant, dims, **kw)
+    o.run()
+    res = g.run()
+    assert res["iters"] == o.iters
+    assert_fields_equal(o, g, fields(variant))
+    g.close()
+
+
+FIXTURE_SCRIPTS = [
+    ("test_Stokes_2D_v", "Stokes2D"),
+    ("test_Stokes_2D_ve", "Stokes2D_ve"),
+    ("test_Stokes_2D_ve_perf", "Stokes2D_ve_perf"),
+    ("test_Stokes3D_ve_multixpu", "Stokes3D_ve"),
+    ("test_Stokes3D_ve_perf", "Stokes3D_ve_perf"),
+]
+
+
+@pytest.mark.parametrize("name,fn", FIXTURE_SCRIPTS)
+def test_reference_fixtures_on_gpu(gpu_lib, name, fn):
+    """The reference's own regression fixtures, reproduced by the GPU script mirrors."""
+    from ptstokes import scripts
+    from oracle.scripts import linrange
+    meta, P, X = load_golden(name)
+    out = getattr(scripts, fn)(*meta["grid"])
+    Pt = out[-1]
+    idx = [np.ceil(linrange(1.0, float(n), 12)).astype(np.int64) - 1 for n in meta["grid"]]
+    p = Pt[np.ix_(*idx)]
+    x = out[0][idx[0]]
+    assert julia_isapprox(p, P) and julia_isapprox(x, X)
+    assert np.array_equal(p, P)
+
+
+def test_nan_is_reported(gpu_lib):
+    import ptstokes
+    from ptstokes import _abi
+    g = ptstokes.Solver("2d_ve", 31, 31, lib=gpu_lib, nout=10)
+    g.setup_inclusion()
+    P = g.get("Pt")
+    P[5, 5] = np.nan
+    g.set("Pt", P)
+    with pytest.raises(ptstokes.PtsError) as e:
+        g.run(nt=1)
+    assert e.value.code == _abi.PTS_E_NAN
+    g.close()
+
+
+def test_field_roundtrip_and_shape_errors(gpu_lib):
+    import ptstokes
+    g = ptstokes.Solver("3d_ve_perf", 11, 9, 7, lib=gpu_lib)
+    rng = np.random.default_rng(1)
+    for n in ("Pt", "Vx", "Vy", "Vz", "txx", "tyy", "tzz", "txy", "txz", "tyz", "txx_o", "Mus"):
+        a = rng.standard_normal(g.shape(n))
+        g.set(n, a)
+        assert np.array_equal(g.get(n), a)
+    with pytest.raises(ValueError):
+        g.set("Pt", np.zeros((3, 3, 3)))
+    g.close()

@@ -1,0 +1,49 @@
+"""The CPU oracle against the reference's own regression fixtures (test/reftest-files).
+
+Each fixture pins the pressure Pt (sampled 12 points per dimension) and the cell
+centres xc of one reference script run on the CPU Threads backend. The oracle must
+reproduce them within Julia's `isapprox` (the reference's own comparison,
+test/test_2D.jl:14); it in fact reproduces them bit for bit, which is asserted too.
+"""
+import numpy as np
+import pytest
+
+from conftest import julia_isapprox, load_golden
+
+FIXTURES = [
+    "test_Stokes_2D_v",
+    "test_Stokes_2D_ve",
+    "test_Stokes_2D_ve_perf",
+    "test_Stokes3D_ve_multixpu",
+    "test_Stokes3D_ve_multixpu_perf",
+    "test_Stokes3D_ve_perf",
+]
+
+
+@pytest.mark.parametrize("name", FIXTURES)
+def test_oracle_reproduces_reference_fixture(name):
+    from oracle import scripts as S
+    meta, P, X = load_golden(name)
+    case = S.make(meta["variant"], *meta["grid"]).run()
+    x, p = S.fixture_sample(case)
+    assert p.shape == P.shape
+    assert julia_isapprox(p, P) and julia_isapprox(x, X)
+    # bit-exact: same kernels, same operation order, no FMA contraction
+    assert np.array_equal(p, P)
+    assert np.array_equal(x, X)
+
+
+def test_oracle_iteration_counts_fixed():
+    """The perf scripts run `iterMax+1` iterations (loop `iter <= iterMax`, nout > iterMax)."""
+    from oracle import scripts as S
+    assert S.make("2d_ve_perf", 15, 15).run().iters == [101]
+    assert S.make("3d_ve_perf", 9, 9, 9).run().iters == [201]
+
+
+def test_oracle_nan_raises():
+    """A poisoned field makes the check's err NaN, which the scripts turn into error("NaN")."""
+    from oracle import scripts as S
+    c = S.make("2d_ve", 15, 15, nout=10)
+    c.f["Pt"][3, 3] = np.nan
+    with pytest.raises(FloatingPointError):
+        c.run(nt=1)
