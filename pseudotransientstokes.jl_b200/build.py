@@ -44,9 +44,17 @@ def _stale(target, deps):
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(force=False, ptxas_verbose=False, quiet=False):
+def build(force=False, ptxas_verbose=False, quiet=False, defines=(), out=None):
+    """Compile and link libptstokes.so. `defines` (NAME=VALUE) and `out` build a variant
+    library elsewhere (for A/B timing of compile-time tunables); the default is in-tree."""
+    global BUILD, LIB
+    if out:
+        BUILD = os.path.join(os.path.dirname(os.path.abspath(out)), "_build_variant")
+        LIB = os.path.abspath(out)
+        force = True
     os.makedirs(BUILD, exist_ok=True)
-    os.makedirs(LIBDIR, exist_ok=True)
+    os.makedirs(os.path.dirname(LIB), exist_ok=True)
+    dflags = [f"-D{d}" for d in defines]
     headers = [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith((".h", ".cuh"))]
     headers.append(os.path.join(INCLUDE, "ptstokes.h"))
     objs = []
@@ -55,7 +63,7 @@ def build(force=False, ptxas_verbose=False, quiet=False):
         obj = os.path.join(BUILD, unit.replace(".cu", ".o"))
         objs.append(obj)
         if force or _stale(obj, [src, *headers, __file__]):
-            cmd = [nvcc(), *ARCH, *COMMON, *extra, "-c", src, "-o", obj]
+            cmd = [nvcc(), *ARCH, *COMMON, *dflags, *extra, "-c", src, "-o", obj]
             if ptxas_verbose:
                 cmd.insert(1, "-Xptxas=-v")
             if not quiet:
@@ -73,6 +81,8 @@ if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--force", action="store_true")
     ap.add_argument("--verbose-ptxas", action="store_true")
+    ap.add_argument("--define", action="append", default=[], help="NAME=VALUE passed as -D to nvcc")
+    ap.add_argument("--out", default=None, help="write the library here instead of in-tree")
     a = ap.parse_args()
-    print(build(force=a.force, ptxas_verbose=a.verbose_ptxas))
+    print(build(force=a.force, ptxas_verbose=a.verbose_ptxas, defines=a.define, out=a.out))
     sys.exit(0)

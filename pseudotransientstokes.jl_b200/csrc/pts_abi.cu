@@ -28,13 +28,17 @@ struct pts_ctx {
     Num n{};
     int device = 0;
     cudaStream_t stream = nullptr;
-    Fields64 f{};
+    Fields64 f{};    // current fields
+    Fields64 alt{};  // second buffers of the ten iterated fields (single-pass 3D path)
+    bool fused = false;
+    int parity = 0;  // number of buffer swaps mod 2
     std::vector<double*> owned;  // every device allocation
     double* partials = nullptr;
     int partials_cap = 0;
     CheckResult* d_result = nullptr;
     CheckResult* h_result = nullptr;  // pinned
-    cudaGraphExec_t chunk = nullptr;  // nout iterations + check
+    cudaGraphExec_t chunk[2] = {nullptr, nullptr};  // nout iterations + check, per starting parity
+    int* d_kerr = nullptr;  // set by a kernel whose bounded wait timed out
     std::string err;
 };
 
@@ -136,15 +140,41 @@ int alloc_field(pts_ctx* c, double** p) {
 }
 
 void drop_graph(pts_ctx* c) {
-    if (c->chunk) {
-        cudaGraphExecDestroy(c->chunk);
-        c->chunk = nullptr;
-    }
+    for (auto& g : c->chunk)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+}
+
+// The ten fields one PT iteration rewrites (Pt, τ, V): the single-pass kernel reads them
+// from one buffer and writes the next iterate into the other.
+double** iterated(Fields64& f, int q) {
+    double** p[] = {&f.Pt, &f.Vx, &f.Vy, &f.Vz, &f.txx, &f.tyy, &f.tzz, &f.txy, &f.txz, &f.tyz};
+    return p[q];
+}
+
+void swap_buffers(pts_ctx* c) {
+    for (int q = 0; q < 10; ++q) std::swap(*iterated(c->f, q), *iterated(c->alt, q));
+    c->parity ^= 1;
 }
 
 int enter(pts_ctx* c) {
     if (!c) return PTS_E_INVAL;
     CK(cudaSetDevice(c->device));
+    return PTS_OK;
+}
+
+// Wait for the stream, then report a kernel whose bounded wait gave up (its results are
+// not to be trusted; the flag is cleared so the context stays usable).
+int synced(pts_ctx* c) {
+    CK(cudaStreamSynchronize(c->stream));
+    int flag = 0;
+    CK(cudaMemcpy(&flag, c->d_kerr, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) {
+        CK(cudaMemset(c->d_kerr, 0, sizeof(int)));
+        return fail(c, PTS_E_CUDA, "a shared-memory staging wait in the single-pass kernel timed out");
+    }
     return PTS_OK;
 }
 
@@ -179,9 +209,31 @@ int copy3d(pts_ctx* c, int id, const double* src_dense, double* dst_dense, int64
     return PTS_OK;
 }
 
-// One PT iteration on the fast path: compute_Pt_τ! then compute_V! + bc.
+// One PT iteration with the two-kernel path: compute_Pt_τ! then compute_V! + bc.
 int iteration(pts_ctx* c, bool store_divV) {
     CK(launch_Pt_tau(c->v, c->g, c->f, c->n, ROLE_P | ROLE_TAU, store_divV && !c->perf, c->stream));
+    CK(launch_V_bc(c->v, c->g, c->f, c->n, true, c->stream));
+    return PTS_OK;
+}
+
+// m PT iterations. Single-pass 3D path: compute_Pt_τ! of iteration 1, then m-1 launches
+// of the fused kernel (V of iteration q, then Pt/τ of q+1, into the other buffers), then
+// compute_V! + bc of iteration m. ∇V of the last iteration is kept for the check of the
+// role variants.
+int enqueue_block(pts_ctx* c, int64_t m, bool store_last) {
+    if (m <= 0) return PTS_OK;
+    if (!c->fused) {
+        for (int64_t q = 0; q < m; ++q) {
+            int rc = iteration(c, store_last && q == m - 1);
+            if (rc) return rc;
+        }
+        return PTS_OK;
+    }
+    CK(launch_Pt_tau(c->v, c->g, c->f, c->n, ROLE_P | ROLE_TAU, store_last && m == 1 && !c->perf, c->stream));
+    for (int64_t q = 1; q < m; ++q) {
+        CK(launch_fused3(c->v, c->g, c->f, c->alt, c->n, store_last && q == m - 1 && !c->perf, c->d_kerr, c->stream));
+        swap_buffers(c);
+    }
     CK(launch_V_bc(c->v, c->g, c->f, c->n, true, c->stream));
     return PTS_OK;
 }
@@ -192,25 +244,39 @@ int enqueue_check(pts_ctx* c) {
     return PTS_OK;
 }
 
+// Swaps one block of m iterations performs on the host-side buffer pointers.
+bool block_swaps_odd(const pts_ctx* c, int64_t m) { return c->fused && m > 1 && ((m - 1) & 1); }
+
+// Capture `nout` iterations + the check as a graph for the current buffer parity. The
+// capture itself runs nothing, so the pointer swaps it made are undone afterwards.
 int build_chunk(pts_ctx* c) {
-    if (c->chunk) return PTS_OK;
+    const int p = c->parity;
+    if (c->chunk[p]) return PTS_OK;
     cudaGraph_t graph = nullptr;
     CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    int rc = PTS_OK;
-    for (int q = 0; q < c->d.nout && rc == PTS_OK; ++q) rc = iteration(c, q == c->d.nout - 1);
+    int rc = enqueue_block(c, c->d.nout, true);
     if (rc == PTS_OK) rc = enqueue_check(c);
     cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+    if (c->parity != p) swap_buffers(c);
     if (rc != PTS_OK) {
         if (graph) cudaGraphDestroy(graph);
         return rc;
     }
     if (e != cudaSuccess) return fail(c, PTS_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
-    e = cudaGraphInstantiate(&c->chunk, graph, 0);
+    e = cudaGraphInstantiate(&c->chunk[p], graph, 0);
     cudaGraphDestroy(graph);
     if (e != cudaSuccess) {
-        c->chunk = nullptr;
+        c->chunk[p] = nullptr;
         return fail(c, PTS_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
     }
+    return PTS_OK;
+}
+
+int launch_chunk(pts_ctx* c) {
+    int rc = build_chunk(c);
+    if (rc) return rc;
+    CK(cudaGraphLaunch(c->chunk[c->parity], c->stream));
+    if (block_swaps_odd(c, c->d.nout)) swap_buffers(c);
     return PTS_OK;
 }
 
@@ -313,9 +379,16 @@ int pts_create(const pts_desc* d, pts_ctx** out) {
                 if ((rc = alloc_field(c, p)) != PTS_OK) return bail(rc);
         }
     }
+    c->fused = variant_fused(c->v);
+    if (c->fused) {
+        for (int q = 0; q < 10; ++q)
+            if ((rc = alloc_field(c, iterated(c->alt, q))) != PTS_OK) return bail(rc);
+    }
     c->partials_cap = check_num_blocks(c->v, g);
     if (cudaMalloc((void**)&c->partials, (size_t)c->partials_cap * kCheckSlots * sizeof(double)) != cudaSuccess ||
         cudaMalloc((void**)&c->d_result, sizeof(CheckResult)) != cudaSuccess ||
+        cudaMalloc((void**)&c->d_kerr, sizeof(int)) != cudaSuccess ||
+        cudaMemsetAsync(c->d_kerr, 0, sizeof(int), c->stream) != cudaSuccess ||
         cudaMallocHost((void**)&c->h_result, sizeof(CheckResult)) != cudaSuccess) {
         cudaGetLastError();
         c->err = "allocation of the check buffers failed";
@@ -337,6 +410,7 @@ int pts_destroy(pts_ctx* c) {
     for (double* p : c->owned) cudaFree(p);
     if (c->partials) cudaFree(c->partials);
     if (c->d_result) cudaFree(c->d_result);
+    if (c->d_kerr) cudaFree(c->d_kerr);
     if (c->h_result) cudaFreeHost(c->h_result);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -346,8 +420,7 @@ int pts_destroy(pts_ctx* c) {
 int pts_sync(pts_ctx* c) {
     int rc = enter(c);
     if (rc) return rc;
-    CK(cudaStreamSynchronize(c->stream));
-    return PTS_OK;
+    return synced(c);
 }
 
 int pts_stream(pts_ctx* c, void** stream) {
@@ -504,7 +577,7 @@ int pts_compute_res(pts_ctx* c, pts_check* out) {
     int rc = enter(c);
     if (rc) return rc;
     if ((rc = enqueue_check(c)) != PTS_OK) return rc;
-    CK(cudaStreamSynchronize(c->stream));
+    if ((rc = synced(c)) != PTS_OK) return rc;
     if (out) to_check(*c->h_result, out);
     return c->h_result->flag_nan != 0.0 ? fail(c, PTS_E_NAN, "NaN in the residual check") : PTS_OK;
 }
@@ -513,9 +586,7 @@ int pts_iterate(pts_ctx* c, int64_t niter) {
     int rc = enter(c);
     if (rc) return rc;
     if (niter < 0) return fail(c, PTS_E_INVAL, "niter < 0");
-    for (int64_t q = 0; q < niter; ++q)
-        if ((rc = iteration(c, q == niter - 1)) != PTS_OK) return rc;
-    return PTS_OK;
+    return enqueue_block(c, niter, true);
 }
 
 int pts_solve(pts_ctx* c, pts_solve_info* info) {
@@ -535,13 +606,12 @@ int pts_solve(pts_ctx* c, pts_solve_info* info) {
         const int64_t remaining = last_iter - iter + 1;
         if (remaining >= till_check) {
             if (till_check == nout) {
-                if ((rc = build_chunk(c)) != PTS_OK) return rc;
-                CK(cudaGraphLaunch(c->chunk, c->stream));
+                if ((rc = launch_chunk(c)) != PTS_OK) return rc;
             } else {
                 if ((rc = pts_iterate(c, till_check)) != PTS_OK) return rc;
                 if ((rc = enqueue_check(c)) != PTS_OK) return rc;
             }
-            CK(cudaStreamSynchronize(c->stream));
+            if ((rc = synced(c)) != PTS_OK) return rc;
             iter += till_check;
             to_check(*c->h_result, &res.last);
             res.nchecks++;
@@ -555,7 +625,7 @@ int pts_solve(pts_ctx* c, pts_solve_info* info) {
         } else {
             if ((rc = pts_iterate(c, remaining)) != PTS_OK) return rc;
             iter += remaining;
-            CK(cudaStreamSynchronize(c->stream));
+            if ((rc = synced(c)) != PTS_OK) return rc;
         }
     }
     res.iters = iter;

@@ -90,5 +90,10 @@ cudaError_t launch_init_inclusion(int variant, const Geom& g, const Fields64& f,
 cudaError_t launch_smooth(int variant, const Geom& g, double* dst, const double* src, double fact, cudaStream_t s);
 cudaError_t launch_maxloc(int variant, const Geom& g, double* must, const double* mus, cudaStream_t s);
 cudaError_t launch_iter_params(int variant, const Geom& g, const Fields64& f, const Num& n, cudaStream_t s);
+// single-pass 3D kernel: V update of iteration n from `cur`, then Pt/τ of n+1, into `nxt`
+// `err` is a device flag the kernel sets if one of its bounded staging waits timed out.
+cudaError_t launch_fused3(int variant, const Geom& g, const Fields64& cur, const Fields64& nxt, const Num& n,
+                          bool store_divV, int* err, cudaStream_t s);
+inline bool variant_fused(int v) { return variant_is3d(v); }
 
 }  // namespace pts

@@ -10,6 +10,7 @@
 // the single-pass z-streaming kernel in pts_fused3d.cu.
 #include <cfloat>
 #include <cmath>
+#include <cstdlib>
 
 #include "pts_internal.h"
 
@@ -730,6 +731,69 @@ cudaError_t launch_iter_params(int v, const Geom& g, const Fields64& f, const Nu
     if (variant_elastic(v)) k_iter_params<true><<<grid_cells(g), blk(), 0, s>>>(g, f, n);
     else k_iter_params<false><<<grid_cells(g), blk(), 0, s>>>(g, f, n);
     return cudaGetLastError();
+}
+
+}  // namespace pts
+
+// ------------------------------------------------------------------ single-pass 3D (FP64)
+#include "pts_fused3d.cuh"
+
+namespace pts {
+
+static Fused3Args<double> fused_args(const Fields64& cur, const Fields64& nxt, int* err) {
+    Fused3Args<double> a{};
+    const double* g1[] = {cur.txx, cur.tyy, cur.tzz, cur.txy, cur.txz, cur.tyz, cur.Pt, cur.dtRho};
+    for (int q = 0; q < 8; ++q) a.g1[q] = g1[q];
+    a.g2[0] = cur.Vx; a.g2[1] = cur.Vy; a.g2[2] = cur.Vz;
+    a.g3[0] = cur.Gdt; a.g3[1] = cur.Mus;
+    const double* g4[] = {cur.txx_o, cur.tyy_o, cur.tzz_o, cur.txy_o, cur.txz_o, cur.tyz_o};
+    for (int q = 0; q < 6; ++q) a.g4[q] = g4[q];
+    a.Vx2 = nxt.Vx; a.Vy2 = nxt.Vy; a.Vz2 = nxt.Vz;
+    a.txx2 = nxt.txx; a.tyy2 = nxt.tyy; a.tzz2 = nxt.tzz; a.txy2 = nxt.txy; a.txz2 = nxt.txz; a.tyz2 = nxt.tyz;
+    a.Pt2 = nxt.Pt;
+    a.divV = cur.divV;
+    a.err = err;
+    return a;
+}
+
+// z-planes per CTA: enough CTAs for ~8 waves at one resident CTA per SM, long z runs to
+// amortise the two recomputed boundary planes of each chunk.
+int fused3_zchunk(const Geom& g) {
+    const int tiles = ((g.nx + 1 + fused3::TX - 1) / fused3::TX) * ((g.ny + 1 + fused3::TY - 1) / fused3::TY);
+    int zch = g.nz + 1;
+    while (zch > 16 && (int64_t)tiles * ((g.nz + 1 + zch - 1) / zch) < 148 * 8) zch = (zch + 1) / 2;
+    return zch;
+}
+
+template <typename T, bool EL, bool PERF, bool CORR>
+cudaError_t launch_fused3_t(const Geom& g, const Fused3Args<T>& a, const NumT<T>& n, bool store_divV, cudaStream_t s) {
+    using C = fused3::Cfg<T, EL, CORR>;
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(k3_fused_BA<T, EL, PERF, CORR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)C::smem_bytes);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    const int zch = fused3_zchunk(g);
+    const dim3 grid((g.nx + 1 + fused3::TX - 1) / fused3::TX, (g.ny + 1 + fused3::TY - 1) / fused3::TY,
+                    (g.nz + 1 + zch - 1) / zch);
+    k3_fused_BA<T, EL, PERF, CORR><<<grid, dim3(fused3::TX, fused3::TY, 1), C::smem_bytes, s>>>(g, a, n, zch,
+                                                                                              store_divV ? 1 : 0);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fused3(int v, const Geom& g, const Fields64& cur, const Fields64& nxt, const Num& nm,
+                          bool store_divV, int* err, cudaStream_t s) {
+    const Fused3Args<double> a = fused_args(cur, nxt, err);
+    NumT<double> n{nm.dx, nm.dy, nm.dz, nm._dx, nm._dy, nm._dz, nm.r, nm.gdt, 2.0, 0.5, 1.0, 0.25,
+                   nm.gdt == 1.0 ? 1 : 0};
+    switch (v) {
+        case VE3D_PERF: return launch_fused3_t<double, true, true, false>(g, a, n, store_divV, s);
+        case V3D: return launch_fused3_t<double, false, true, false>(g, a, n, store_divV, s);
+        case VE3D: return launch_fused3_t<double, true, false, false>(g, a, n, store_divV, s);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 }  // namespace pts

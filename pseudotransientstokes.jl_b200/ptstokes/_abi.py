@@ -112,7 +112,7 @@ def load(path=None):
     global _lib
     if _lib is not None and path is None:
         return _lib
-    p = path or LIB_PATH
+    p = path or os.environ.get("PTSTOKES_LIB") or LIB_PATH
     if not os.path.exists(p):
         raise OSError(f"libptstokes.so not found at {p}; build it with "
                       f"`python pseudotransientstokes.jl_b200/build.py`")

@@ -201,3 +201,34 @@ def test_field_roundtrip_and_shape_errors(gpu_lib):
     with pytest.raises(ValueError):
         g.set("Pt", np.zeros((3, 3, 3)))
     g.close()
+
+
+@pytest.mark.parametrize("variant", ["3d_ve_perf", "3d_v", "3d_ve"])
+def test_single_pass_blocks_of_every_length(gpu_lib, variant):
+    """The single-pass 3D path runs a block of m iterations as A [BA]^(m-1) B with
+    ping-pong buffers; blocks of odd and even length must leave the same fields."""
+    o, g = make_pair(gpu_lib, variant, (21, 18, 16))
+    if o.elastic:
+        o.assign_tau()
+        g.assign_tau()
+    for m in (1, 2, 3, 6, 1, 5):
+        for _ in range(m):
+            o.iteration()
+        g.iterate(m)
+        g.sync()
+        assert_fields_equal(o, g, fields(variant))
+    g.close()
+
+
+@pytest.mark.parametrize("nout", [50, 51])
+def test_graph_blocks_with_buffer_swaps(gpu_lib, nout):
+    """Graph-captured check blocks whose swap count is odd (nout=50) or even (nout=51)."""
+    o, g = make_pair(gpu_lib, "3d_ve_perf", (15, 14, 13), nout=nout, iter_max=10 * nout + 7, eps=1e-300)
+    o.assign_tau()
+    g.assign_tau()
+    info = g.solve()
+    for _ in range(info["iters"]):
+        o.iteration()
+    assert info["iters"] == 10 * nout + 8 and not info["converged"]
+    assert_fields_equal(o, g, fields("3d_ve_perf"))
+    g.close()
