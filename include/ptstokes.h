@@ -74,7 +74,8 @@ typedef struct pts_desc {
     double eps;         /* tolerance ε on err (Stokes3D_ve_perf.jl:132) */
     double iter_max;    /* `while err > ε && iter <= iterMax` */
     int32_t mixed_inner;    /* MIXED: FP32 sweeps between FP64 corrections; 0 => nout */
-    int32_t reserved[7];
+    int32_t single_pass;    /* 3D: 1 = one-launch-per-iteration staged kernel, 0 = two launches */
+    int32_t reserved[6];
 } pts_desc;
 
 /* Fields, by the reference's names. Extents are the reference's (pts_field_shape). */

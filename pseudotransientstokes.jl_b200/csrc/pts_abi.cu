@@ -379,7 +379,7 @@ int pts_create(const pts_desc* d, pts_ctx** out) {
                 if ((rc = alloc_field(c, p)) != PTS_OK) return bail(rc);
         }
     }
-    c->fused = variant_fused(c->v);
+    c->fused = variant_fused(c->v) && d->single_pass != 0;
     if (c->fused) {
         for (int q = 0; q < 10; ++q)
             if ((rc = alloc_field(c, iterated(c->alt, q))) != PTS_OK) return bail(rc);

@@ -21,6 +21,13 @@ constexpr unsigned kFull = 0xffffffffu;
 
 // ------------------------------------------------------------------ expression helpers
 
+// Gr = Gdτ/(G*dt). When G*dt is exactly 1.0 the quotient is Gdτ itself (IEEE division by
+// one is exact), so the division is skipped; the result is the same bits either way.
+__device__ __forceinline__ double gr_of(double g, double gdt) {
+    if (gdt == 1.0) return g;
+    return g / gdt;
+}
+
 // Normal stress update. Perf form (Stokes3D_ve_perf.jl:71-73):
 //   (τ + τ_o*Gr + 2.0*Gdτ*(_dx*d)) / (1.0 + Gdτ/Mus + Gr),  Gr = Gdτ/(G*dt)
 // Role form (Stokes3D_ve_multixpu.jl:70-72): the same with (d/dx).
@@ -30,7 +37,7 @@ __device__ __forceinline__ double tau_n(double t, double to, double g, double m,
                                         double d) {
     const double e = PERF ? (ih * d) : (d / h);
     if (EL) {
-        const double Gr = g / gdt;
+        const double Gr = gr_of(g, gdt);
         return ((t + to * Gr) + (2.0 * g) * e) / ((1.0 + g / m) + Gr);
     }
     return (t + (2.0 * g) * e) / (1.0 + g / m);
@@ -43,7 +50,7 @@ __device__ __forceinline__ double tau_s(double t, double to, double ag, double a
                                         double d1, double h2, double ih2, double d2) {
     const double s = PERF ? (ih1 * d1 + ih2 * d2) : (d1 / h1 + d2 / h2);
     if (EL) {
-        const double Gr = ag / gdt;
+        const double Gr = gr_of(ag, gdt);
         return ((t + to * Gr) + (2.0 * ag) * (0.5 * s)) / ((1.0 + ag / am) + Gr);
     }
     return (t + (2.0 * ag) * (0.5 * s)) / (1.0 + ag / am);
@@ -256,7 +263,7 @@ __global__ void __launch_bounds__(256) k2_Pt_tau(Geom g, Fields64 f, Num n, int 
         f.txx[c] = (f.txx[c] + ((2.0 * Gc) * dvx) / n.dx) / (Gc / Mc + 1.0);
         f.tyy[c] = (f.tyy[c] + ((2.0 * Gc) * dvy) / n.dy) / (Gc / Mc + 1.0);
     } else {
-        const double Gr = Gc / n.gdt;
+        const double Gr = gr_of(Gc, n.gdt);
         const double ex = (VAR == VE2D_PERF) ? n._dx * dvx : dvx / n.dx;
         const double ey = (VAR == VE2D_PERF) ? n._dy * dvy : dvy / n.dy;
         f.txx[c] = ((f.txx[c] + f.txx_o[c] * Gr) + (2.0 * Gc) * ex) / ((1.0 + Gc / Mc) + Gr);
@@ -271,11 +278,11 @@ __global__ void __launch_bounds__(256) k2_Pt_tau(Geom g, Fields64 f, Num n, int 
         if (VAR == V2D) {
             f.txy[c] = (f.txy[c] + (2.0 * ag) * (0.5 * (d1 / n.dy + d2 / n.dx))) / (ag / am + 1.0);
         } else if (VAR == VE2D) {
-            const double Gr = ag / n.gdt;
+            const double Gr = gr_of(ag, n.gdt);
             f.txy[c] = ((f.txy[c] + f.txy_o[c] * Gr) + (2.0 * ag) * (0.5 * (d1 / n.dy + d2 / n.dx))) /
                        ((1.0 + ag / am) + Gr);
         } else {
-            const double Gr = ag / n.gdt;
+            const double Gr = gr_of(ag, n.gdt);
             f.txy[c] = ((f.txy[c] + f.txy_o[c] * Gr) + ((2.0 * ag) * 0.5) * (n._dy * d1 + n._dx * d2)) /
                        ((1.0 + ag / am) + Gr);
         }

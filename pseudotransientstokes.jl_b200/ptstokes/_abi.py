@@ -45,7 +45,7 @@ class PtsDesc(ctypes.Structure):
         ("G", ctypes.c_double), ("dt", ctypes.c_double),
         ("r", ctypes.c_double), ("Re", ctypes.c_double), ("CFL", ctypes.c_double),
         ("max_l", ctypes.c_double), ("eps", ctypes.c_double), ("iter_max", ctypes.c_double),
-        ("mixed_inner", ctypes.c_int32), ("reserved", ctypes.c_int32 * 7),
+        ("mixed_inner", ctypes.c_int32), ("single_pass", ctypes.c_int32), ("reserved", ctypes.c_int32 * 6),
     ]
 
 

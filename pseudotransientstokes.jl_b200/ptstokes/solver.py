@@ -50,7 +50,7 @@ class Solver:
         self.lib = lib or _abi.load()
         self.variant = variant
         self.ndim = 3 if variant.startswith("3d") else 2
-        p = dict(lx=10.0, ly=10.0, lz=10.0, xi=1.0, mus0=1.0, G=1.0, max_l=0.0, mixed_inner=0)
+        p = dict(lx=10.0, ly=10.0, lz=10.0, xi=1.0, mus0=1.0, G=1.0, max_l=0.0, mixed_inner=0, single_pass=0)
         p.update(VARIANT_DEFAULTS[variant])
         p.update(kw)
         self.p = p
@@ -66,6 +66,7 @@ class Solver:
         d.r, d.Re, d.CFL = p["r"], p["Re"], p["CFL"]
         d.max_l, d.eps, d.iter_max = p["max_l"], p["eps"], float(p["iter_max"])
         d.mixed_inner = int(p["mixed_inner"])
+        d.single_pass = int(p["single_pass"])
         self.desc = d
         ctx = ctypes.c_void_p()
         check(self.lib, None, self.lib.pts_create(ctypes.byref(d), ctypes.byref(ctx)))
