@@ -181,7 +181,8 @@ def run_ours(args, ws, rank, local, pg):
     n = args.n
     nout = args.iters_per_step
     variant = args.variant
-    s = ptstokes.Solver(variant, n, n, n, nout=nout, eps=1e-300, iter_max=nout - 1)
+    s = ptstokes.Solver(variant, n, n, n, nout=nout, eps=1e-300, iter_max=nout - 1,
+                        single_pass=1 if args.single_pass else 0)
     s.setup_inclusion()
     s.assign_tau()
     stream = torch.cuda.ExternalStream(s.stream_handle())
@@ -324,6 +325,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=511)
     ap.add_argument("--variant", default="3d_ve_perf", choices=["3d_ve_perf", "3d_ve", "3d_v"])
+    ap.add_argument("--single-pass", action="store_true", help="use the staged one-launch-per-iteration kernel")
     ap.add_argument("--iters-per-step", type=int, default=200)
     ap.add_argument("--cpu-n", type=int, default=255)
     ap.add_argument("--cpu-iters", type=int, default=8)

@@ -1,0 +1,128 @@
+# PTStokesB200.jl -- Julia `ccall` binding of libptstokes.so (the B200 PT Stokes solver).
+#
+# Keeps the kernel-role names of the reference scripts (compute_P!, compute_τ!,
+# compute_dV!, compute_V!, compute_Pt_τ!, compute_Res!, assign_τ!, bc!) so a script can
+# replace its `@parallel` calls with these. Fields live on the device inside the context;
+# `set_field!`/`get_field` move Julia Arrays (Float64, the reference's extents), and
+# `set_field_device!` takes a CuArray's pointer.
+#
+# This file is written against include/ptstokes.h; no Julia runtime was available where
+# it was written, so it has not been executed.
+module PTStokesB200
+
+const libpts = get(ENV, "PTSTOKES_LIB", joinpath(@__DIR__, "..", "lib", "libptstokes.so"))
+
+const PTS_OK = Cint(0)
+@enum Variant::Int32 V2D = 0 VE2D = 1 VE2D_PERF = 2 VE3D = 3 VE3D_PERF = 4 V3D = 5
+const FIELDS = (:Pt, :Vx, :Vy, :Vz, :τxx, :τyy, :τzz, :τxy, :τxz, :τyz,
+                :τxx_o, :τyy_o, :τzz_o, :τxy_o, :τxz_o, :τyz_o,
+                :Mus, :Musτ, :Gdτ, :dτ_Rho, :∇V, :Rx, :Ry, :Rz, :dVx, :dVy, :dVz)
+field_id(s::Symbol) = Int32(findfirst(==(s), FIELDS) - 1)
+
+# pts_desc (include/ptstokes.h)
+struct Desc
+    variant::Int32; precision::Int32
+    nx::Int32; ny::Int32; nz::Int32; nout::Int32
+    lx::Float64; ly::Float64; lz::Float64
+    G::Float64; dt::Float64
+    r::Float64; Re::Float64; CFL::Float64
+    max_l::Float64; eps::Float64; iter_max::Float64
+    mixed_inner::Int32; single_pass::Int32
+    reserved::NTuple{6,Int32}
+end
+
+struct Check
+    err::Float64; norm_Rx::Float64; norm_Ry::Float64; norm_Rz::Float64; norm_∇V::Float64
+    Vmin::Float64; Vmax::Float64; Pmin::Float64; Pmax::Float64
+end
+
+struct SolveInfo
+    iters::Int64; converged::Int32; nchecks::Int32; last::Check
+end
+
+mutable struct Ctx
+    ptr::Ptr{Cvoid}
+end
+
+function check(ctx, rc)
+    if rc != PTS_OK
+        msg = unsafe_string(ccall((:pts_last_error, libpts), Cstring, (Ptr{Cvoid},), ctx === nothing ? C_NULL : ctx.ptr))
+        error("ptstokes error $rc: $msg")
+    end
+    return nothing
+end
+
+"""
+    Ctx(variant, nx, ny, nz; lx=10, ly=10, lz=10, G=1, dt=1, r=1, Re, CFL, nout, ε=1e-8, iterMax)
+
+A device context for one problem (the scripts' `Stokes2D_()`/`Stokes3D_()` state).
+"""
+function Ctx(variant::Variant, nx, ny, nz=1; lx=10.0, ly=10.0, lz=10.0, G=1.0, dt=1.0, r=1.0, Re, CFL,
+             nout=200, ε=1e-8, iterMax=2e5, max_l=0.0, precision=0, single_pass=0)
+    d = Desc(Int32(variant), Int32(precision), nx, ny, nz, nout, lx, ly, lz, G, dt, r, Re, CFL, max_l, ε, iterMax,
+             0, single_pass, ntuple(_ -> Int32(0), 6))
+    out = Ref{Ptr{Cvoid}}(C_NULL)
+    check(nothing, ccall((:pts_create, libpts), Cint, (Ref{Desc}, Ref{Ptr{Cvoid}}), d, out))
+    ctx = Ctx(out[])
+    finalizer(c -> ccall((:pts_destroy, libpts), Cint, (Ptr{Cvoid},), c.ptr), ctx)
+    return ctx
+end
+
+function field_shape(ctx::Ctx, f::Symbol)
+    s = zeros(Int64, 3)
+    check(ctx, ccall((:pts_field_shape, libpts), Cint, (Ptr{Cvoid}, Int32, Ptr{Int64}), ctx.ptr, field_id(f), s))
+    return Tuple(s)
+end
+
+set_field!(ctx::Ctx, f::Symbol, A::Array{Float64}) =
+    check(ctx, ccall((:pts_set_field, libpts), Cint, (Ptr{Cvoid}, Int32, Ptr{Float64}, Int64), ctx.ptr, field_id(f), A, length(A)))
+
+function get_field(ctx::Ctx, f::Symbol)
+    s = field_shape(ctx, f)
+    A = zeros(Float64, s...)
+    check(ctx, ccall((:pts_get_field, libpts), Cint, (Ptr{Cvoid}, Int32, Ptr{Float64}, Int64), ctx.ptr, field_id(f), A, length(A)))
+    return A
+end
+
+# A CuArray's device pointer (e.g. `pointer(A)` converted with `UInt(pointer(A))`).
+set_field_device!(ctx::Ctx, f::Symbol, devptr::UInt, n::Integer) =
+    check(ctx, ccall((:pts_set_field_device, libpts), Cint, (Ptr{Cvoid}, Int32, UInt, Int64), ctx.ptr, field_id(f), devptr, n))
+
+for (jl, c) in ((:init_inclusion!, :pts_init_inclusion),)
+    @eval $jl(ctx::Ctx; μs0=1.0, μsi=1e-3, radius2=1.0, εbg=1.0) =
+        check(ctx, ccall(($(QuoteNode(c)), libpts), Cint, (Ptr{Cvoid}, Float64, Float64, Float64, Float64), ctx.ptr, μs0, μsi, radius2, εbg))
+end
+smooth!(ctx::Ctx, nsweeps=10, fact=1.0) = check(ctx, ccall((:pts_smooth, libpts), Cint, (Ptr{Cvoid}, Int32, Float64), ctx.ptr, nsweeps, fact))
+
+# Roles (each replaces the `@parallel` call of the same name in the scripts)
+for (jl, c) in ((:compute_maxloc!, :pts_compute_maxloc), (:compute_iter_params!, :pts_compute_iter_params),
+                (:assign_τ!, :pts_assign_tau), (:compute_P!, :pts_compute_P), (:compute_τ!, :pts_compute_tau),
+                (:compute_dV!, :pts_compute_dV), (:compute_V!, :pts_compute_V), (:bc!, :pts_apply_bc),
+                (:compute_Pt_τ!, :pts_compute_Pt_tau), (:compute_V_bc!, :pts_compute_V_bc))
+    @eval $jl(ctx::Ctx) = check(ctx, ccall(($(QuoteNode(c)), libpts), Cint, (Ptr{Cvoid},), ctx.ptr))
+end
+
+function compute_Res!(ctx::Ctx)
+    r = Ref{Check}()
+    check(ctx, ccall((:pts_compute_res, libpts), Cint, (Ptr{Cvoid}, Ref{Check}), ctx.ptr, r))
+    return r[]
+end
+
+iterate!(ctx::Ctx, n) = check(ctx, ccall((:pts_iterate, libpts), Cint, (Ptr{Cvoid}, Int64), ctx.ptr, n))
+
+"The PT loop of one physical step (`while err > ε && iter <= iterMax`)."
+function solve!(ctx::Ctx)
+    r = Ref{SolveInfo}()
+    check(ctx, ccall((:pts_solve, libpts), Cint, (Ptr{Cvoid}, Ref{SolveInfo}), ctx.ptr, r))
+    return r[]
+end
+
+"The time loop `for it = 1:nt` (assign_τ! + PT loop per step); returns per-step iterations."
+function run!(ctx::Ctx, nt)
+    per = zeros(Int64, nt)
+    r = Ref{SolveInfo}()
+    check(ctx, ccall((:pts_run, libpts), Cint, (Ptr{Cvoid}, Int32, Ptr{Int64}, Ref{SolveInfo}), ctx.ptr, nt, per, r))
+    return per, r[]
+end
+
+end # module
