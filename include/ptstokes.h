@@ -165,6 +165,27 @@ PTS_API int pts_solve(pts_ctx* ctx, pts_solve_info* info);
  * info (may be NULL) receives the last step's outcome with iters = ittot. */
 PTS_API int pts_run(pts_ctx* ctx, int32_t nt, int64_t* iters_per_step, pts_solve_info* info);
 
+/* ---- convergence check without any allocation ----
+ * This entry point has no counterpart in the reference. It is for callers that cannot
+ * allocate device memory: programs whose device memory all belongs to another allocator
+ * (CUDA.jl's pool for Julia CuArrays, PyTorch's caching allocator) or that partition the
+ * GPU up front and forbid later cudaMalloc calls. It computes the same check as
+ * pts_compute_res -- compute_Res! and the norms of Stokes3D_ve_perf.jl:90-96,210-218 --
+ * directly on the caller's arrays, and calls no cudaMalloc, cudaFree or allocating library.
+ *   desc     sizes, extents and variant; only PTS_2D_VE_PERF, PTS_3D_VE_PERF, PTS_3D_V
+ *   fields   device pointers indexed by pts_field (PTS_F_PT .. PTS_F_TYZ): dense column-major
+ *            Float64 arrays with the reference's extents; in 2D Vz, τzz, τxz, τyz are unused
+ *   out      device pointer to a pts_check the result is written to (err is NaN on NaN)
+ *   stream   cudaStream_t to run on (NULL: the default stream); the call is asynchronous
+ * Limit: the block partials of the reduction live in a fixed 256 KB array inside the
+ * library (held by every GPU that loads it, until exit), which bounds the grid:
+ * ceil((nx+1)/32) * ceil(ny/8) <= 4096; larger sizes return PTS_E_INVAL with a message in
+ * pts_last_error(NULL). The first call on a device looks up that array's device address
+ * (once per device, with the device current); make that first call before any stream
+ * capture. All calls share the array and overwrite what they read, so calls whose kernels
+ * overlap on the GPU race and must be ordered by the caller. */
+PTS_API int pts_check_noalloc(const pts_desc* desc, const double* const fields[10], pts_check* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -26,6 +26,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hi
 # translation unit -> extra flags
 UNITS = {
     "pts_kernels64.cu": ["--fmad=false"],
+    "pts_noalloc.cu": ["--fmad=false"],
     "pts_abi.cu": [],
 }
 

@@ -20,6 +20,10 @@ namespace {
 std::string g_create_err;
 }
 
+namespace pts {
+void set_global_error(const char* msg) { g_create_err = msg; }
+}  // namespace pts
+
 struct pts_ctx {
     pts_desc d{};
     int v = 0;

@@ -96,4 +96,7 @@ cudaError_t launch_fused3(int variant, const Geom& g, const Fields64& cur, const
                           bool store_divV, int* err, cudaStream_t s);
 inline bool variant_fused(int v) { return variant_is3d(v); }
 
+// Message returned by pts_last_error(NULL) (for entry points without a context).
+void set_global_error(const char* msg);
+
 }  // namespace pts

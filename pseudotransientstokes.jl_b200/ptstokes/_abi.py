@@ -102,6 +102,8 @@ SIGNATURES = {
     "pts_iterate": ([_P, _I64], ctypes.c_int),
     "pts_solve": ([_P, ctypes.POINTER(PtsSolveInfo)], ctypes.c_int),
     "pts_run": ([_P, _I32, ctypes.POINTER(_I64), ctypes.POINTER(PtsSolveInfo)], ctypes.c_int),
+    # residual check on caller-owned device arrays; allocates nothing
+    "pts_check_noalloc": ([ctypes.POINTER(PtsDesc), ctypes.POINTER(_P), _P, _P], ctypes.c_int),
 }
 
 _lib = None
