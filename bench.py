@@ -182,7 +182,7 @@ def run_ours(args, ws, rank, local, pg):
     nout = args.iters_per_step
     variant = args.variant
     s = ptstokes.Solver(variant, n, n, n, nout=nout, eps=1e-300, iter_max=nout - 1,
-                        single_pass=1 if args.single_pass else 0)
+                        single_pass=1 if args.single_pass else 0, precision=args.precision)
     s.setup_inclusion()
     s.assign_tau()
     stream = torch.cuda.ExternalStream(s.stream_handle())
@@ -326,6 +326,7 @@ def main():
     ap.add_argument("--n", type=int, default=511)
     ap.add_argument("--variant", default="3d_ve_perf", choices=["3d_ve_perf", "3d_ve", "3d_v"])
     ap.add_argument("--single-pass", action="store_true", help="use the staged one-launch-per-iteration kernel")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--iters-per-step", type=int, default=200)
     ap.add_argument("--cpu-n", type=int, default=255)
     ap.add_argument("--cpu-iters", type=int, default=8)

@@ -35,6 +35,9 @@ struct pts_ctx {
     Fields64 f{};    // current fields
     Fields64 alt{};  // second buffers of the ten iterated fields (single-pass 3D path)
     bool fused = false;
+    bool mixed = false;      // FP32 inner sweeps + FP64 defect correction
+    Mixed32 m{};
+    std::vector<float*> owned32;
     int parity = 0;  // number of buffer swaps mod 2
     std::vector<double*> owned;  // every device allocation
     double* partials = nullptr;
@@ -226,6 +229,16 @@ int iteration(pts_ctx* c, bool store_divV) {
 // role variants.
 int enqueue_block(pts_ctx* c, int64_t m, bool store_last) {
     if (m <= 0) return PTS_OK;
+    if (c->mixed) {
+        // m FP32 sweeps on the correction, then the FP64 fold X += δ (δ = 0 again). The
+        // sources must already describe the current X (mixed_prepare or a previous check).
+        for (int64_t q = 0; q < m; ++q) {
+            CK(launch_corr_A32(c->v, c->g, c->m, c->n, c->stream));
+            CK(launch_corr_B32(c->v, c->g, c->m, c->n, c->stream));
+        }
+        CK(launch_fold(c->g, c->f, c->m, c->stream));
+        return PTS_OK;
+    }
     if (!c->fused) {
         for (int64_t q = 0; q < m; ++q) {
             int rc = iteration(c, store_last && q == m - 1);
@@ -242,9 +255,23 @@ int enqueue_block(pts_ctx* c, int64_t m, bool store_last) {
     return PTS_OK;
 }
 
+// The convergence check of the current FP64 iterate. In mixed precision the same pass
+// also writes the FP32 residual sources for the next sweeps (the check's R and ∇V are
+// two of them).
 int enqueue_check(pts_ctx* c) {
-    CK(launch_check(c->v, c->g, c->f, c->n, c->partials, c->partials_cap, c->d_result, c->stream));
+    if (c->mixed)
+        CK(launch_sources(c->v, c->g, c->f, c->m, c->n, c->partials, c->partials_cap, c->d_result, c->stream));
+    else
+        CK(launch_check(c->v, c->g, c->f, c->n, c->partials, c->partials_cap, c->d_result, c->stream));
     CK(cudaMemcpyAsync(c->h_result, c->d_result, sizeof(CheckResult), cudaMemcpyDeviceToHost, c->stream));
+    return PTS_OK;
+}
+
+// Mixed precision: FP32 copies of the coefficients and the sources of the current iterate
+// (called when the FP64 state may have changed outside the sweeps).
+int mixed_prepare(pts_ctx* c) {
+    CK(launch_coef32(c->g, c->f, c->m, c->stream));
+    CK(launch_sources(c->v, c->g, c->f, c->m, c->n, c->partials, c->partials_cap, c->d_result, c->stream));
     return PTS_OK;
 }
 
@@ -310,7 +337,8 @@ int pts_create(const pts_desc* d, pts_ctx** out) {
     *out = nullptr;
     if (d->variant < PTS_2D_V || d->variant > PTS_3D_V) return fail(nullptr, PTS_E_INVAL, "unknown variant");
     if (d->precision != PTS_FP64 && d->precision != PTS_MIXED) return fail(nullptr, PTS_E_INVAL, "unknown precision");
-    if (d->precision == PTS_MIXED) return fail(nullptr, PTS_E_INVAL, "mixed precision is not available in this build");
+    if (d->precision == PTS_MIXED && d->variant != PTS_3D_VE_PERF && d->variant != PTS_3D_V)
+        return fail(nullptr, PTS_E_INVAL, "mixed precision is implemented for PTS_3D_VE_PERF and PTS_3D_V");
     const bool d3 = variant_is3d(d->variant);
     if (d->nx < 3 || d->ny < 3 || (d3 && d->nz < 3)) return fail(nullptr, PTS_E_INVAL, "each of nx, ny(, nz) must be >= 3");
     if ((int64_t)d->nx + 1 > (1 << 20) || (int64_t)d->ny + 1 > (1 << 20) || (d3 && (int64_t)d->nz + 1 > (1 << 20)))
@@ -383,7 +411,24 @@ int pts_create(const pts_desc* d, pts_ctx** out) {
                 if ((rc = alloc_field(c, p)) != PTS_OK) return bail(rc);
         }
     }
-    c->fused = variant_fused(c->v) && d->single_pass != 0;
+    c->mixed = d->precision == PTS_MIXED;
+    c->fused = variant_fused(c->v) && d->single_pass != 0 && !c->mixed;
+    if (c->mixed) {
+        float** p32[] = {&c->m.dPt, &c->m.dVx, &c->m.dVy, &c->m.dVz, &c->m.dtxx, &c->m.dtyy, &c->m.dtzz, &c->m.dtxy,
+                         &c->m.dtxz, &c->m.dtyz, &c->m.aP, &c->m.atxx, &c->m.atyy, &c->m.atzz, &c->m.atxy,
+                         &c->m.atxz, &c->m.atyz, &c->m.aVx, &c->m.aVy, &c->m.aVz, &c->m.Gdt, &c->m.Mus, &c->m.dtRho};
+        for (float** p : p32) {
+            void* q = nullptr;
+            if (cudaMalloc(&q, (size_t)g.n * sizeof(float)) != cudaSuccess ||
+                cudaMemsetAsync(q, 0, (size_t)g.n * sizeof(float), c->stream) != cudaSuccess) {
+                cudaGetLastError();
+                c->err = "allocation of the FP32 fields failed";
+                return bail(PTS_E_NOMEM);
+            }
+            *p = (float*)q;
+            c->owned32.push_back(*p);
+        }
+    }
     if (c->fused) {
         for (int q = 0; q < 10; ++q)
             if ((rc = alloc_field(c, iterated(c->alt, q))) != PTS_OK) return bail(rc);
@@ -412,6 +457,7 @@ int pts_destroy(pts_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     drop_graph(c);
     for (double* p : c->owned) cudaFree(p);
+    for (float* p : c->owned32) cudaFree(p);
     if (c->partials) cudaFree(c->partials);
     if (c->d_result) cudaFree(c->d_result);
     if (c->d_kerr) cudaFree(c->d_kerr);
@@ -590,12 +636,14 @@ int pts_iterate(pts_ctx* c, int64_t niter) {
     int rc = enter(c);
     if (rc) return rc;
     if (niter < 0) return fail(c, PTS_E_INVAL, "niter < 0");
+    if (c->mixed && niter > 0 && (rc = mixed_prepare(c)) != PTS_OK) return rc;
     return enqueue_block(c, niter, true);
 }
 
 int pts_solve(pts_ctx* c, pts_solve_info* info) {
     int rc = enter(c);
     if (rc) return rc;
+    if (c->mixed && (rc = mixed_prepare(c)) != PTS_OK) return rc;
     const int64_t nout = c->d.nout;
     const double eps = c->d.eps;
     const int64_t last_iter = (int64_t)std::floor(c->d.iter_max);  // loop runs while iter <= iter_max
@@ -612,7 +660,7 @@ int pts_solve(pts_ctx* c, pts_solve_info* info) {
             if (till_check == nout) {
                 if ((rc = launch_chunk(c)) != PTS_OK) return rc;
             } else {
-                if ((rc = pts_iterate(c, till_check)) != PTS_OK) return rc;
+                if ((rc = enqueue_block(c, till_check, true)) != PTS_OK) return rc;
                 if ((rc = enqueue_check(c)) != PTS_OK) return rc;
             }
             if ((rc = synced(c)) != PTS_OK) return rc;
@@ -627,7 +675,7 @@ int pts_solve(pts_ctx* c, pts_solve_info* info) {
             }
             if (!(err > eps)) converged = true;
         } else {
-            if ((rc = pts_iterate(c, remaining)) != PTS_OK) return rc;
+            if ((rc = enqueue_block(c, remaining, true)) != PTS_OK) return rc;
             iter += remaining;
             if ((rc = synced(c)) != PTS_OK) return rc;
         }

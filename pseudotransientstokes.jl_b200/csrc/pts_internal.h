@@ -99,4 +99,24 @@ inline bool variant_fused(int v) { return variant_is3d(v); }
 // Message returned by pts_last_error(NULL) (for entry points without a context).
 void set_global_error(const char* msg);
 
+// ---- mixed precision (3D explicit-index variants) ----
+// FP32 fields of the inner sweeps: the correction δ of the ten iterated fields, the FP64
+// residual sources of the current iterate (rounded once), and FP32 copies of the
+// coefficients. Same unified layout and extents as the FP64 fields.
+struct Mixed32 {
+    float *dPt, *dVx, *dVy, *dVz, *dtxx, *dtyy, *dtzz, *dtxy, *dtxz, *dtyz;
+    float *aP, *atxx, *atyy, *atzz, *atxy, *atxz, *atyz, *aVx, *aVy, *aVz;
+    float *Gdt, *Mus, *dtRho;
+};
+// FP32 inner sweep (pts_kernels32.cu): δ-form compute_Pt_τ! and compute_V! + bc.
+cudaError_t launch_corr_A32(int variant, const Geom& g, const Mixed32& m, const Num& n, cudaStream_t s);
+cudaError_t launch_corr_B32(int variant, const Geom& g, const Mixed32& m, const Num& n, cudaStream_t s);
+// FP64 outer step (pts_kernels64.cu): fold X += δ and clear δ; residual sources of X
+// (aP = ∇·V, aτ = constitutive residual, aV = momentum residual R) with the check
+// partials and its finaliser; FP32 copies of the coefficients.
+cudaError_t launch_fold(const Geom& g, const Fields64& f, const Mixed32& m, cudaStream_t s);
+cudaError_t launch_sources(int variant, const Geom& g, const Fields64& f, const Mixed32& m, const Num& n,
+                           double* partials, int nblocks_cap, CheckResult* result, cudaStream_t s);
+cudaError_t launch_coef32(const Geom& g, const Fields64& f, const Mixed32& m, cudaStream_t s);
+
 }  // namespace pts

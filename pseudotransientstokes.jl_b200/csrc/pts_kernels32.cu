@@ -1,0 +1,154 @@
+// pts_kernels32.cu -- FP32 inner sweeps of the mixed-precision PT solve (3D, _dx form).
+//
+// The state of the sweeps is a correction δ to the FP64 iterate X (Pt, τ, V). The FP64
+// residuals of X enter as sources, computed once per outer step (pts_kernels64.cu):
+//   aP = ∇·V_X,  aτ = τ_o*Gr + 2Gdτ*ε̇(V_X) - τ_X*(Gdτ/Mus + Gr),  aV = R(τ_X, Pt_X)
+// and the sweep is the reference's PT iteration (compute_Pt_τ!, compute_V! + bc,
+// Stokes3D_ve_perf.jl:69-88,202-207) written for X + δ with X held fixed:
+//   δPt' = δPt - r*Gdτ*(aP + ∇·δV)
+//   δτ'  = (δτ + aτ + 2Gdτ*ε̇(δV)) / (1 + Gdτ/Mus + Gr)
+//   δV'  = δV + (R(δτ', δPt') + aV) * av(dτ_Rho)
+// In exact arithmetic X + δ follows the FP64 iteration step for step; in FP32 the
+// rounding is relative to the size of δ, which the outer step folds into X (in FP64)
+// and resets every nout sweeps. The stress and velocity fields move half the bytes of
+// the FP64 kernels. Compiled with FMA contraction (no bit-exact target here).
+#include <cuda_runtime.h>
+
+#include "pts_internal.h"
+
+namespace pts {
+namespace {
+
+struct Num32 {
+    float _dx, _dy, _dz, r, gdt;
+    int gdt_one;
+};
+
+__device__ __forceinline__ float gr32(float g, const Num32& n) { return n.gdt_one ? g : g / n.gdt; }
+
+// δ-form compute_Pt_τ!, one thread per cell.
+template <bool EL>
+__global__ void __launch_bounds__(256) k3_corrA(Geom g, Mixed32 m, Num32 n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    if (i >= nx || j >= ny) return;
+    const int64_t c = gidx(g, i, j, k);
+    const int64_t sx = 1, sy = g.px, sz = g.pxy;
+    const float dvx = m.dVx[c + sx] - m.dVx[c];
+    const float dvy = m.dVy[c + sy] - m.dVy[c];
+    const float dvz = m.dVz[c + sz] - m.dVz[c];
+    const float Gc = m.Gdt[c], Mc = m.Mus[c];
+    m.dPt[c] = m.dPt[c] - n.r * Gc * (m.aP[c] + ((n._dx * dvx + n._dy * dvy) + n._dz * dvz));
+    const float Dn = (1.0f + Gc / Mc) + (EL ? gr32(Gc, n) : 0.0f);
+    const float G2 = 2.0f * Gc;
+    if (j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2)
+        m.dtxx[c] = ((m.dtxx[c] + m.atxx[c]) + G2 * (n._dx * dvx)) / Dn;
+    if (i >= 1 && i <= nx - 2 && k >= 1 && k <= nz - 2)
+        m.dtyy[c] = ((m.dtyy[c] + m.atyy[c]) + G2 * (n._dy * dvy)) / Dn;
+    if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2)
+        m.dtzz[c] = ((m.dtzz[c] + m.atzz[c]) + G2 * (n._dz * dvz)) / Dn;
+    if (i >= 1 && j >= 1 && k >= 1 && k <= nz - 2) {
+        const float ag = (((m.Gdt[c - sx - sy] + m.Gdt[c - sy]) + m.Gdt[c - sx]) + Gc) * 0.25f;
+        const float am = (((m.Mus[c - sx - sy] + m.Mus[c - sy]) + m.Mus[c - sx]) + Mc) * 0.25f;
+        const float s = 0.5f * (n._dy * (m.dVx[c] - m.dVx[c - sy]) + n._dx * (m.dVy[c] - m.dVy[c - sx]));
+        m.dtxy[c] = ((m.dtxy[c] + m.atxy[c]) + (2.0f * ag) * s) / ((1.0f + ag / am) + (EL ? gr32(ag, n) : 0.0f));
+    }
+    if (i >= 1 && j >= 1 && j <= ny - 2 && k >= 1) {
+        const float ag = (((m.Gdt[c - sx - sz] + m.Gdt[c - sz]) + m.Gdt[c - sx]) + Gc) * 0.25f;
+        const float am = (((m.Mus[c - sx - sz] + m.Mus[c - sz]) + m.Mus[c - sx]) + Mc) * 0.25f;
+        const float s = 0.5f * (n._dz * (m.dVx[c] - m.dVx[c - sz]) + n._dx * (m.dVz[c] - m.dVz[c - sx]));
+        m.dtxz[c] = ((m.dtxz[c] + m.atxz[c]) + (2.0f * ag) * s) / ((1.0f + ag / am) + (EL ? gr32(ag, n) : 0.0f));
+    }
+    if (i >= 1 && i <= nx - 2 && j >= 1 && k >= 1) {
+        const float ag = (((m.Gdt[c - sy - sz] + m.Gdt[c - sz]) + m.Gdt[c - sy]) + Gc) * 0.25f;
+        const float am = (((m.Mus[c - sy - sz] + m.Mus[c - sz]) + m.Mus[c - sy]) + Mc) * 0.25f;
+        const float s = 0.5f * (n._dz * (m.dVy[c] - m.dVy[c - sz]) + n._dy * (m.dVz[c] - m.dVz[c - sy]));
+        m.dtyz[c] = ((m.dtyz[c] + m.atyz[c]) + (2.0f * ag) * s) / ((1.0f + ag / am) + (EL ? gr32(ag, n) : 0.0f));
+    }
+}
+
+__device__ __forceinline__ void bc_copies32(float* A, int64_t c, float v, int a, int alo, int ahi, int64_t sa, int b,
+                                            int blo, int bhi, int64_t sb) {
+    const int da = (a == alo) ? -1 : 0, ua = (a == ahi) ? 1 : 0;
+    const int db = (b == blo) ? -1 : 0, ub = (b == bhi) ? 1 : 0;
+    if (da) A[c - sa] = v;
+    if (ua) A[c + sa] = v;
+    if (db) A[c - sb] = v;
+    if (ub) A[c + sb] = v;
+    if (da && db) A[c - sa - sb] = v;
+    if (da && ub) A[c - sa + sb] = v;
+    if (ua && db) A[c + sa - sb] = v;
+    if (ua && ub) A[c + sa + sb] = v;
+}
+
+// δ-form compute_V! with the free-slip copies, one thread per face point.
+__global__ void __launch_bounds__(256) k3_corrB(Geom g, Mixed32 m, Num32 n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    if (i > nx || j > ny) return;
+    const int64_t c = gidx(g, i, j, k);
+    const int64_t sx = 1, sy = g.px, sz = g.pxy;
+    if (j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2) {
+        float v = m.dVx[c];
+        if (i >= 1 && i <= nx - 1) {
+            const float R = (((n._dx * (m.dtxx[c] - m.dtxx[c - sx]) + n._dy * (m.dtxy[c + sy] - m.dtxy[c])) +
+                              n._dz * (m.dtxz[c + sz] - m.dtxz[c])) -
+                             n._dx * (m.dPt[c] - m.dPt[c - sx])) +
+                            m.aVx[c];
+            v = v + R * ((m.dtRho[c - sx] + m.dtRho[c]) * 0.5f);
+            m.dVx[c] = v;
+        }
+        bc_copies32(m.dVx, c, v, j, 1, ny - 2, sy, k, 1, nz - 2, sz);
+    }
+    if (i >= 1 && i <= nx - 2 && k >= 1 && k <= nz - 2) {
+        float v = m.dVy[c];
+        if (j >= 1 && j <= ny - 1) {
+            const float R = (((n._dy * (m.dtyy[c] - m.dtyy[c - sy]) + n._dx * (m.dtxy[c + sx] - m.dtxy[c])) +
+                              n._dz * (m.dtyz[c + sz] - m.dtyz[c])) -
+                             n._dy * (m.dPt[c] - m.dPt[c - sy])) +
+                            m.aVy[c];
+            v = v + R * ((m.dtRho[c - sy] + m.dtRho[c]) * 0.5f);
+            m.dVy[c] = v;
+        }
+        bc_copies32(m.dVy, c, v, i, 1, nx - 2, sx, k, 1, nz - 2, sz);
+    }
+    if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2) {
+        float v = m.dVz[c];
+        if (k >= 1 && k <= nz - 1) {
+            const float R = (((n._dz * (m.dtzz[c] - m.dtzz[c - sz]) + n._dx * (m.dtxz[c + sx] - m.dtxz[c])) +
+                              n._dy * (m.dtyz[c + sy] - m.dtyz[c])) -
+                             n._dz * (m.dPt[c] - m.dPt[c - sz])) +
+                            m.aVz[c];
+            v = v + R * ((m.dtRho[c - sz] + m.dtRho[c]) * 0.5f);
+            m.dVz[c] = v;
+        }
+        bc_copies32(m.dVz, c, v, i, 1, nx - 2, sx, j, 1, ny - 2, sy);
+    }
+}
+
+Num32 num32(const Num& n) {
+    return Num32{(float)n._dx, (float)n._dy, (float)n._dz, (float)n.r, (float)n.gdt, n.gdt == 1.0 ? 1 : 0};
+}
+
+}  // namespace
+
+cudaError_t launch_corr_A32(int v, const Geom& g, const Mixed32& m, const Num& n, cudaStream_t s) {
+    const dim3 grid((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz), blk(32, 8, 1);
+    if (v == VE3D_PERF) k3_corrA<true><<<grid, blk, 0, s>>>(g, m, num32(n));
+    else if (v == V3D) k3_corrA<false><<<grid, blk, 0, s>>>(g, m, num32(n));
+    else return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_corr_B32(int v, const Geom& g, const Mixed32& m, const Num& n, cudaStream_t s) {
+    if (v != VE3D_PERF && v != V3D) return cudaErrorInvalidValue;
+    const dim3 grid((g.nx + 1 + 31) / 32, (g.ny + 1 + 7) / 8, g.nz + 1), blk(32, 8, 1);
+    k3_corrB<<<grid, blk, 0, s>>>(g, m, num32(n));
+    return cudaGetLastError();
+}
+
+}  // namespace pts

@@ -534,6 +534,107 @@ __global__ void k_check_finalize(const double* partials, int nblocks, double lx,
     }
 }
 
+// ------------------------------------------------------------------ mixed precision: FP64 outer step
+
+// X += δ for the ten iterated fields, then δ = 0 (elementwise over the padded arrays).
+__global__ void k_fold(int64_t n, Fields64 f, Mixed32 m) {
+    double* X[10] = {f.Pt, f.Vx, f.Vy, f.Vz, f.txx, f.tyy, f.tzz, f.txy, f.txz, f.tyz};
+    float* D[10] = {m.dPt, m.dVx, m.dVy, m.dVz, m.dtxx, m.dtyy, m.dtzz, m.dtxy, m.dtxz, m.dtyz};
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int q = 0; q < 10; ++q) {
+            X[q][e] = X[q][e] + (double)D[q][e];
+            D[q][e] = 0.0f;
+        }
+    }
+}
+
+// Residual sources of the FP64 iterate for the FP32 sweeps, and the convergence check of
+// that iterate (compute_Res! + norms, Stokes3D_ve_perf.jl:90-96,210-218) in one pass:
+//   aP = ∇·V (the check's ∇V), aV = R (the check's Rx, Ry, Rz),
+//   aτ = τ_o*Gr + 2Gdτ*ε̇(V) - τ*(Gdτ/Mus + Gr)   (zero when τ satisfies its PT update)
+template <bool EL>
+__global__ void __launch_bounds__(256) k3_sources(Geom g, Fields64 f, Mixed32 m, Num n, double* partials) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const int64_t sx = 1, sy = g.px, sz = g.pxy;
+    Acc a;
+    acc_init(a);
+    if (i <= nx && j < ny) {
+        for (int k = blockIdx.z; k < nz; k += gridDim.z) {
+            const int64_t c = gidx(g, i, j, k);
+            const double vx = f.Vx[c];
+            a.vmin = fmin(a.vmin, vx);
+            a.vmax = fmax(a.vmax, vx);
+            if (i < nx) {
+                const double p = f.Pt[c];
+                a.pmin = fmin(a.pmin, p);
+                a.pmax = fmax(a.pmax, p);
+                const double dvx = f.Vx[c + sx] - vx, dvy = f.Vy[c + sy] - f.Vy[c], dvz = f.Vz[c + sz] - f.Vz[c];
+                const double dv = (n._dx * dvx + n._dy * dvy) + n._dz * dvz;
+                f.divV[c] = dv;
+                m.aP[c] = (float)dv;
+                a.s[3] += dv * dv;
+                const double Gc = f.Gdt[c], Mc = f.Mus[c];
+                const double Gr = EL ? gr_of(Gc, n.gdt) : 0.0;
+                const double Dm = Gc / Mc + Gr;  // D - 1
+                auto a_n = [&](const double* t, const double* to, double e) {
+                    return ((EL ? to[c] * Gr : 0.0) + (2.0 * Gc) * e) - t[c] * Dm;
+                };
+                if (j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2) m.atxx[c] = (float)a_n(f.txx, f.txx_o, n._dx * dvx);
+                if (i >= 1 && i <= nx - 2 && k >= 1 && k <= nz - 2) m.atyy[c] = (float)a_n(f.tyy, f.tyy_o, n._dy * dvy);
+                if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2) m.atzz[c] = (float)a_n(f.tzz, f.tzz_o, n._dz * dvz);
+            }
+            if (i < nx) {
+                auto a_s = [&](const double* t, const double* to, int64_t o1, int64_t o2, double s) {
+                    const double ag = (((f.Gdt[c - o1 - o2] + f.Gdt[c - o2]) + f.Gdt[c - o1]) + f.Gdt[c]) * 0.25;
+                    const double am = (((f.Mus[c - o1 - o2] + f.Mus[c - o2]) + f.Mus[c - o1]) + f.Mus[c]) * 0.25;
+                    const double Gr = EL ? gr_of(ag, n.gdt) : 0.0;
+                    return ((EL ? to[c] * Gr : 0.0) + (2.0 * ag) * (0.5 * s)) - t[c] * (ag / am + Gr);
+                };
+                if (i >= 1 && j >= 1 && k >= 1 && k <= nz - 2)
+                    m.atxy[c] = (float)a_s(f.txy, f.txy_o, sx, sy,
+                                           n._dy * (f.Vx[c] - f.Vx[c - sy]) + n._dx * (f.Vy[c] - f.Vy[c - sx]));
+                if (i >= 1 && j >= 1 && j <= ny - 2 && k >= 1)
+                    m.atxz[c] = (float)a_s(f.txz, f.txz_o, sx, sz,
+                                           n._dz * (f.Vx[c] - f.Vx[c - sz]) + n._dx * (f.Vz[c] - f.Vz[c - sx]));
+                if (i >= 1 && i <= nx - 2 && j >= 1 && k >= 1)
+                    m.atyz[c] = (float)a_s(f.tyz, f.tyz_o, sy, sz,
+                                           n._dz * (f.Vy[c] - f.Vy[c - sz]) + n._dy * (f.Vz[c] - f.Vz[c - sy]));
+            }
+            if (i >= 1 && i <= nx - 1 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2) {
+                const double R = res3_x<true>(f, n, c, sx, sy, sz);
+                f.Rx[c] = R;
+                m.aVx[c] = (float)R;
+                a.s[0] += R * R;
+            }
+            if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 1 && k >= 1 && k <= nz - 2) {
+                const double R = res3_y<true>(f, n, c, sx, sy, sz);
+                f.Ry[c] = R;
+                m.aVy[c] = (float)R;
+                a.s[1] += R * R;
+            }
+            if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 1) {
+                const double R = res3_z<true>(f, n, c, sx, sy, sz);
+                f.Rz[c] = R;
+                m.aVz[c] = (float)R;
+                a.s[2] += R * R;
+            }
+        }
+    }
+    acc_block_store(a, partials);
+}
+
+__global__ void k_coef32(int64_t n, const double* Gdt, const double* Mus, const double* dtRho, float* G32, float* M32,
+                         float* R32) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        G32[e] = (float)Gdt[e];
+        M32[e] = (float)Mus[e];
+        R32[e] = (float)dtRho[e];
+    }
+}
+
 // ------------------------------------------------------------------ set-up kernels
 
 // Initial conditions (Stokes3D_ve_perf.jl:164-172; Stokes3D_ve_multixpu.jl:174-178 builds
@@ -709,6 +810,32 @@ cudaError_t launch_check(int v, const Geom& g, const Fields64& f, const Num& n, 
     const double lenRz = d3 ? (nx - 2) * (ny - 2) * (nz - 1) : 1.0;
     const double lenDiv = nx * ny * nz;
     k_check_finalize<<<1, 256, 0, s>>>(partials, nb, n.lx, lenRx, lenRy, lenRz, lenDiv, d3 ? 3 : 2, result);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fold(const Geom& g, const Fields64& f, const Mixed32& m, cudaStream_t s) {
+    k_fold<<<148 * 8, 256, 0, s>>>(g.n, f, m);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sources(int v, const Geom& g, const Fields64& f, const Mixed32& m, const Num& n, double* partials,
+                           int nblocks_cap, CheckResult* result, cudaStream_t s) {
+    const dim3 gr = check_grid(v, g);
+    const int nb = (int)(gr.x * gr.y * gr.z);
+    if (nb > nblocks_cap) return cudaErrorInvalidValue;
+    if (v == VE3D_PERF) k3_sources<true><<<gr, blk(), 0, s>>>(g, f, m, n, partials);
+    else if (v == V3D) k3_sources<false><<<gr, blk(), 0, s>>>(g, f, m, n, partials);
+    else return cudaErrorInvalidValue;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const double nx = g.nx, ny = g.ny, nz = g.nz;
+    k_check_finalize<<<1, 256, 0, s>>>(partials, nb, n.lx, (nx - 1) * (ny - 2) * (nz - 2), (nx - 2) * (ny - 1) * (nz - 2),
+                                       (nx - 2) * (ny - 2) * (nz - 1), nx * ny * nz, 3, result);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_coef32(const Geom& g, const Fields64& f, const Mixed32& m, cudaStream_t s) {
+    k_coef32<<<148 * 8, 256, 0, s>>>(g.n, f.Gdt, f.Mus, f.dtRho, m.Gdt, m.Mus, m.dtRho);
     return cudaGetLastError();
 }
 
