@@ -231,7 +231,7 @@ def run_ours(args, ws, rank, local, pg):
     bytes_A = 25 * n ** 3 * 8
     achieved = bytes_A / (ms_A / 1e3) / 1e9
     traffic = None
-    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    tp = os.path.join(ROOT, "profiles", "dram_traffic_per_cell.txt")  # from the committed ncu capture
     if os.path.exists(tp):
         try:
             tj = json.load(open(tp)).get("k3_Pt_tau")
@@ -295,7 +295,11 @@ def run_ours(args, ws, rank, local, pg):
                "sample": f"oracle (C++/OpenMP FP64 restatement of Stokes3D_ve_perf.jl) at {args.cpu_n}^3, "
                          f"{args.cpu_iters} PT iterations, {dt:.1f} s"}
 
-    launches = args.steps * (2 * nout + 2)
+    launches = args.steps * (2 * nout + 2) if args.precision == "fp64" else args.steps * (2 * nout + 3)
+    s.close()
+    ttt = None
+    if args.ttt_n > 0:
+        ttt = time_to_tol(args, stream_cls=torch.cuda.ExternalStream)
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": ws, "steps": args.steps,
@@ -312,9 +316,46 @@ def run_ours(args, ws, rank, local, pg):
                          "other_kernel": {"name": "k3_V_bc", "ms": round(ms_B, 4),
                                           "achieved": round(14 * n ** 3 * 8 / (ms_B / 1e3) / 1e9, 1)}},
             "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clocks,
+            "time_to_tol": ttt,
         }
         print(json.dumps(line), flush=True)
-    s.close()
+
+
+def time_to_tol(args, stream_cls):
+    """Time to tolerance of the converged problem of the metric: `nt` physical steps of
+    3D VE, each PT loop run to err <= 1e-8 with a check every 200 iterations
+    (Stokes3D_ve_multixpu.jl:128-134 numerics on the Stokes3D_ve_perf.jl kernels), plain
+    FP64 vs FP32 sweeps + FP64 defect correction, same problem, same check."""
+    import numpy as np
+    import torch
+
+    import ptstokes
+
+    n = args.ttt_n
+    out = {"grid": n, "nt": args.ttt_nt, "eps": 1e-8, "nout": 200}
+    fields = {}
+    for prec in ("fp64", "mixed"):
+        s = ptstokes.Solver("3d_ve_perf", n, n, n, precision=prec, nt=args.ttt_nt, nout=200, iter_max=2e5, eps=1e-8)
+        s.setup_inclusion()
+        s.sync()
+        st = stream_cls(s.stream_handle())
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        res = s.run()
+        b.record(st)
+        b.synchronize()
+        sec = a.elapsed_time(b) / 1e3
+        out[prec] = {"seconds": round(sec, 3), "iters": res["iters"], "ittot": res["ittot"],
+                     "converged": res["converged"], "err": res["last"]["err"],
+                     "T_eff_GBs": round(a_eff(n) * res["ittot"] / sec / 1e9, 1)}
+        fields[prec] = {k: s.get(k) for k in ("Pt", "Vx", "Vy", "Vz", "txx", "tyy", "tzz", "txy", "txz", "tyz")}
+        s.close()
+    out["speedup_mixed_vs_fp64"] = round(out["fp64"]["seconds"] / out["mixed"]["seconds"], 3)
+    out["mixed_rel_err_vs_fp64"] = {
+        k: float(np.linalg.norm(fields["mixed"][k] - fields["fp64"][k]) / max(np.linalg.norm(fields["fp64"][k]), 1e-300))
+        for k in fields["fp64"]}
+    return out
 
 
 def main():
@@ -327,9 +368,11 @@ def main():
     ap.add_argument("--variant", default="3d_ve_perf", choices=["3d_ve_perf", "3d_ve", "3d_v"])
     ap.add_argument("--single-pass", action="store_true", help="use the staged one-launch-per-iteration kernel")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--ttt-n", type=int, default=255, help="grid of the time-to-tolerance comparison (0: skip)")
+    ap.add_argument("--ttt-nt", type=int, default=5, help="physical steps of the time-to-tolerance comparison")
     ap.add_argument("--iters-per-step", type=int, default=200)
-    ap.add_argument("--cpu-n", type=int, default=255)
-    ap.add_argument("--cpu-iters", type=int, default=8)
+    ap.add_argument("--cpu-n", type=int, default=511)
+    ap.add_argument("--cpu-iters", type=int, default=25)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

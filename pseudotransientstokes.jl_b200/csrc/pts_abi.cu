@@ -360,6 +360,10 @@ int pts_create(const pts_desc* d, pts_ctx** out) {
     g.pz = d3 ? d->nz + 1 : 1;
     g.pxy = (int64_t)g.px * g.py;
     g.n = g.pxy * g.pz;
+    if (g.n >= ((int64_t)1 << 31)) {
+        delete c;
+        return fail(nullptr, PTS_E_INVAL, "grid too large: more than 2^31 elements per field");
+    }
     Num& n = c->n;
     n.lx = d->lx; n.ly = d->ly; n.lz = d3 ? d->lz : 1.0;
     n.dx = d->lx / d->nx;

@@ -46,6 +46,12 @@ __host__ __device__ inline int64_t gidx(const Geom& g, int i, int j, int k) {
     return (int64_t)i + (int64_t)g.px * ((int64_t)j + (int64_t)g.py * (int64_t)k);
 }
 
+// Element index inside one field in 32 bits: every problem that fits on one device has
+// fewer than 2^31 elements per field (pts_create rejects larger ones), and 32-bit offsets
+// save the 64-bit multiply-adds on each of a stencil's ~30 loads.
+typedef int idx_t;
+__host__ __device__ inline idx_t gidx32(const Geom& g, int i, int j, int k) { return i + g.px * (j + g.py * k); }
+
 // Scalars of the scripts' "Derived numerics" (Stokes3D_ve_perf.jl:135-138).
 struct Num {
     double dx, dy, dz, _dx, _dy, _dz;

@@ -24,7 +24,7 @@ struct Num32 {
     int gdt_one;
 };
 
-__device__ __forceinline__ float gr32(float g, const Num32& n) { return n.gdt_one ? g : g / n.gdt; }
+__device__ __forceinline__ float gr32(float g, const Num32& n) { return n.gdt_one ? g : __fdividef(g, n.gdt); }
 
 // δ-form compute_Pt_τ!, one thread per cell.
 template <bool EL>
@@ -34,43 +34,44 @@ __global__ void __launch_bounds__(256) k3_corrA(Geom g, Mixed32 m, Num32 n) {
     const int k = blockIdx.z;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     if (i >= nx || j >= ny) return;
-    const int64_t c = gidx(g, i, j, k);
-    const int64_t sx = 1, sy = g.px, sz = g.pxy;
+    const idx_t c = gidx32(g, i, j, k);
+    const idx_t sx = 1, sy = g.px, sz = (idx_t)g.pxy;
     const float dvx = m.dVx[c + sx] - m.dVx[c];
     const float dvy = m.dVy[c + sy] - m.dVy[c];
     const float dvz = m.dVz[c + sz] - m.dVz[c];
     const float Gc = m.Gdt[c], Mc = m.Mus[c];
     m.dPt[c] = m.dPt[c] - n.r * Gc * (m.aP[c] + ((n._dx * dvx + n._dy * dvy) + n._dz * dvz));
-    const float Dn = (1.0f + Gc / Mc) + (EL ? gr32(Gc, n) : 0.0f);
+    const float Dn = (1.0f + __fdividef(Gc, Mc)) + (EL ? gr32(Gc, n) : 0.0f);
     const float G2 = 2.0f * Gc;
+    const float rDn = __fdividef(1.0f, Dn);
     if (j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2)
-        m.dtxx[c] = ((m.dtxx[c] + m.atxx[c]) + G2 * (n._dx * dvx)) / Dn;
+        m.dtxx[c] = ((m.dtxx[c] + m.atxx[c]) + G2 * (n._dx * dvx)) * rDn;
     if (i >= 1 && i <= nx - 2 && k >= 1 && k <= nz - 2)
-        m.dtyy[c] = ((m.dtyy[c] + m.atyy[c]) + G2 * (n._dy * dvy)) / Dn;
+        m.dtyy[c] = ((m.dtyy[c] + m.atyy[c]) + G2 * (n._dy * dvy)) * rDn;
     if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2)
-        m.dtzz[c] = ((m.dtzz[c] + m.atzz[c]) + G2 * (n._dz * dvz)) / Dn;
+        m.dtzz[c] = ((m.dtzz[c] + m.atzz[c]) + G2 * (n._dz * dvz)) * rDn;
     if (i >= 1 && j >= 1 && k >= 1 && k <= nz - 2) {
         const float ag = (((m.Gdt[c - sx - sy] + m.Gdt[c - sy]) + m.Gdt[c - sx]) + Gc) * 0.25f;
         const float am = (((m.Mus[c - sx - sy] + m.Mus[c - sy]) + m.Mus[c - sx]) + Mc) * 0.25f;
         const float s = 0.5f * (n._dy * (m.dVx[c] - m.dVx[c - sy]) + n._dx * (m.dVy[c] - m.dVy[c - sx]));
-        m.dtxy[c] = ((m.dtxy[c] + m.atxy[c]) + (2.0f * ag) * s) / ((1.0f + ag / am) + (EL ? gr32(ag, n) : 0.0f));
+        m.dtxy[c] = __fdividef((m.dtxy[c] + m.atxy[c]) + (2.0f * ag) * s, (1.0f + __fdividef(ag, am)) + (EL ? gr32(ag, n) : 0.0f));
     }
     if (i >= 1 && j >= 1 && j <= ny - 2 && k >= 1) {
         const float ag = (((m.Gdt[c - sx - sz] + m.Gdt[c - sz]) + m.Gdt[c - sx]) + Gc) * 0.25f;
         const float am = (((m.Mus[c - sx - sz] + m.Mus[c - sz]) + m.Mus[c - sx]) + Mc) * 0.25f;
         const float s = 0.5f * (n._dz * (m.dVx[c] - m.dVx[c - sz]) + n._dx * (m.dVz[c] - m.dVz[c - sx]));
-        m.dtxz[c] = ((m.dtxz[c] + m.atxz[c]) + (2.0f * ag) * s) / ((1.0f + ag / am) + (EL ? gr32(ag, n) : 0.0f));
+        m.dtxz[c] = __fdividef((m.dtxz[c] + m.atxz[c]) + (2.0f * ag) * s, (1.0f + __fdividef(ag, am)) + (EL ? gr32(ag, n) : 0.0f));
     }
     if (i >= 1 && i <= nx - 2 && j >= 1 && k >= 1) {
         const float ag = (((m.Gdt[c - sy - sz] + m.Gdt[c - sz]) + m.Gdt[c - sy]) + Gc) * 0.25f;
         const float am = (((m.Mus[c - sy - sz] + m.Mus[c - sz]) + m.Mus[c - sy]) + Mc) * 0.25f;
         const float s = 0.5f * (n._dz * (m.dVy[c] - m.dVy[c - sz]) + n._dy * (m.dVz[c] - m.dVz[c - sy]));
-        m.dtyz[c] = ((m.dtyz[c] + m.atyz[c]) + (2.0f * ag) * s) / ((1.0f + ag / am) + (EL ? gr32(ag, n) : 0.0f));
+        m.dtyz[c] = __fdividef((m.dtyz[c] + m.atyz[c]) + (2.0f * ag) * s, (1.0f + __fdividef(ag, am)) + (EL ? gr32(ag, n) : 0.0f));
     }
 }
 
-__device__ __forceinline__ void bc_copies32(float* A, int64_t c, float v, int a, int alo, int ahi, int64_t sa, int b,
-                                            int blo, int bhi, int64_t sb) {
+__device__ __forceinline__ void bc_copies32(float* A, idx_t c, float v, int a, int alo, int ahi, idx_t sa, int b,
+                                            int blo, int bhi, idx_t sb) {
     const int da = (a == alo) ? -1 : 0, ua = (a == ahi) ? 1 : 0;
     const int db = (b == blo) ? -1 : 0, ub = (b == bhi) ? 1 : 0;
     if (da) A[c - sa] = v;
@@ -90,8 +91,8 @@ __global__ void __launch_bounds__(256) k3_corrB(Geom g, Mixed32 m, Num32 n) {
     const int k = blockIdx.z;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     if (i > nx || j > ny) return;
-    const int64_t c = gidx(g, i, j, k);
-    const int64_t sx = 1, sy = g.px, sz = g.pxy;
+    const idx_t c = gidx32(g, i, j, k);
+    const idx_t sx = 1, sy = g.px, sz = (idx_t)g.pxy;
     if (j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2) {
         float v = m.dVx[c];
         if (i >= 1 && i <= nx - 1) {

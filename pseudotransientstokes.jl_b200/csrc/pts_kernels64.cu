@@ -71,8 +71,8 @@ __global__ void __launch_bounds__(256) k3_Pt_tau(Geom g, Fields64 f, Num n, int 
     const int k = blockIdx.z;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     if (i >= nx || j >= ny) return;
-    const int64_t c = gidx(g, i, j, k);
-    const int64_t sx = 1, sy = g.px, sz = g.pxy;
+    const idx_t c = gidx32(g, i, j, k);
+    const idx_t sx = 1, sy = g.px, sz = (idx_t)g.pxy;
     const double dvx = f.Vx[c + sx] - f.Vx[c];
     const double dvy = f.Vy[c + sy] - f.Vy[c];
     const double dvz = f.Vz[c + sz] - f.Vz[c];
@@ -121,22 +121,22 @@ __global__ void __launch_bounds__(256) k3_Pt_tau(Geom g, Fields64 f, Num n, int 
 // Momentum residuals at interior faces (compute_Res!, Stokes3D_ve_perf.jl:92-94;
 // compute_dV!/compute_Res!, Stokes3D_ve_multixpu.jl:80-82,94-96).
 template <bool PERF>
-__device__ __forceinline__ double res3_x(const Fields64& f, const Num& n, int64_t c, int64_t sx, int64_t sy,
-                                         int64_t sz) {
+__device__ __forceinline__ double res3_x(const Fields64& f, const Num& n, idx_t c, idx_t sx, idx_t sy,
+                                         idx_t sz) {
     return ((dsc<PERF>(f.txx[c] - f.txx[c - sx], n.dx, n._dx) + dsc<PERF>(f.txy[c + sy] - f.txy[c], n.dy, n._dy)) +
             dsc<PERF>(f.txz[c + sz] - f.txz[c], n.dz, n._dz)) -
            dsc<PERF>(f.Pt[c] - f.Pt[c - sx], n.dx, n._dx);
 }
 template <bool PERF>
-__device__ __forceinline__ double res3_y(const Fields64& f, const Num& n, int64_t c, int64_t sx, int64_t sy,
-                                         int64_t sz) {
+__device__ __forceinline__ double res3_y(const Fields64& f, const Num& n, idx_t c, idx_t sx, idx_t sy,
+                                         idx_t sz) {
     return ((dsc<PERF>(f.tyy[c] - f.tyy[c - sy], n.dy, n._dy) + dsc<PERF>(f.txy[c + sx] - f.txy[c], n.dx, n._dx)) +
             dsc<PERF>(f.tyz[c + sz] - f.tyz[c], n.dz, n._dz)) -
            dsc<PERF>(f.Pt[c] - f.Pt[c - sy], n.dy, n._dy);
 }
 template <bool PERF>
-__device__ __forceinline__ double res3_z(const Fields64& f, const Num& n, int64_t c, int64_t sx, int64_t sy,
-                                         int64_t sz) {
+__device__ __forceinline__ double res3_z(const Fields64& f, const Num& n, idx_t c, idx_t sx, idx_t sy,
+                                         idx_t sz) {
     return ((dsc<PERF>(f.tzz[c] - f.tzz[c - sz], n.dz, n._dz) + dsc<PERF>(f.txz[c + sx] - f.txz[c], n.dx, n._dx)) +
             dsc<PERF>(f.tyz[c + sy] - f.tyz[c], n.dy, n._dy)) -
            dsc<PERF>(f.Pt[c] - f.Pt[c - sz], n.dz, n._dz);
@@ -148,8 +148,8 @@ __device__ __forceinline__ double res3_z(const Fields64& f, const Num& n, int64_
 // (Stokes3D_ve_perf.jl:202-207), which leaves every boundary face equal to the face at
 // its tangential indices clamped into the interior; writing from the source face gives
 // exactly that, with no face read after another thread wrote it.
-__device__ __forceinline__ void bc_copies(double* A, int64_t c, double v, int a, int alo, int ahi, int64_t sa, int b,
-                                          int blo, int bhi, int64_t sb) {
+__device__ __forceinline__ void bc_copies(double* A, idx_t c, double v, int a, int alo, int ahi, idx_t sa, int b,
+                                          int blo, int bhi, idx_t sb) {
     const int da = (a == alo) ? -1 : 0, ua = (a == ahi) ? 1 : 0;
     const int db = (b == blo) ? -1 : 0, ub = (b == bhi) ? 1 : 0;
     if (da) A[c - sa] = v;
@@ -171,8 +171,8 @@ __global__ void __launch_bounds__(256) k3_V_bc(Geom g, Fields64 f, Num n, int up
     const int k = blockIdx.z;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     if (i > nx || j > ny) return;
-    const int64_t c = gidx(g, i, j, k);
-    const int64_t sx = 1, sy = g.px, sz = g.pxy;
+    const idx_t c = gidx32(g, i, j, k);
+    const idx_t sx = 1, sy = g.px, sz = (idx_t)g.pxy;
     // Vx: source faces j in [1,ny-2], k in [1,nz-2]; updated for i in [1,nx-1]
     if (j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2) {
         double v = f.Vx[c];
@@ -210,8 +210,8 @@ __global__ void k3_dV(Geom g, Fields64 f, Num n) {
     const int k = blockIdx.z;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     if (i > nx || j > ny) return;
-    const int64_t c = gidx(g, i, j, k);
-    const int64_t sx = 1, sy = g.px, sz = g.pxy;
+    const idx_t c = gidx32(g, i, j, k);
+    const idx_t sx = 1, sy = g.px, sz = (idx_t)g.pxy;
     if (i >= 1 && i <= nx - 1 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2)
         f.dVx[c] = res3_x<PERF>(f, n, c, sx, sy, sz) * ((f.dtRho[c - sx] + f.dtRho[c]) * 0.5);
     if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 1 && k >= 1 && k <= nz - 2)
@@ -227,7 +227,7 @@ __global__ void k3_add_dV(Geom g, Fields64 f) {
     const int k = blockIdx.z;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     if (i > nx || j > ny) return;
-    const int64_t c = gidx(g, i, j, k);
+    const idx_t c = gidx32(g, i, j, k);
     if (i >= 1 && i <= nx - 1 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2) f.Vx[c] = f.Vx[c] + f.dVx[c];
     if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 1 && k >= 1 && k <= nz - 2) f.Vy[c] = f.Vy[c] + f.dVy[c];
     if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 1) f.Vz[c] = f.Vz[c] + f.dVz[c];
@@ -243,8 +243,8 @@ __global__ void __launch_bounds__(256) k2_Pt_tau(Geom g, Fields64 f, Num n, int 
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int nx = g.nx, ny = g.ny;
     if (i >= nx || j >= ny) return;
-    const int64_t c = gidx(g, i, j, 0);
-    const int64_t sx = 1, sy = g.px;
+    const idx_t c = gidx32(g, i, j, 0);
+    const idx_t sx = 1, sy = g.px;
     const double dvx = f.Vx[c + sx] - f.Vx[c];
     const double dvy = f.Vy[c + sy] - f.Vy[c];
     const double Gc = f.Gdt[c];
@@ -290,12 +290,12 @@ __global__ void __launch_bounds__(256) k2_Pt_tau(Geom g, Fields64 f, Num n, int 
 }
 
 template <bool PERF>
-__device__ __forceinline__ double res2_x(const Fields64& f, const Num& n, int64_t c, int64_t sx, int64_t sy) {
+__device__ __forceinline__ double res2_x(const Fields64& f, const Num& n, idx_t c, idx_t sx, idx_t sy) {
     return (dsc<PERF>(f.txx[c] - f.txx[c - sx], n.dx, n._dx) + dsc<PERF>(f.txy[c + sy] - f.txy[c], n.dy, n._dy)) -
            dsc<PERF>(f.Pt[c] - f.Pt[c - sx], n.dx, n._dx);
 }
 template <bool PERF>
-__device__ __forceinline__ double res2_y(const Fields64& f, const Num& n, int64_t c, int64_t sx, int64_t sy) {
+__device__ __forceinline__ double res2_y(const Fields64& f, const Num& n, idx_t c, idx_t sx, idx_t sy) {
     return (dsc<PERF>(f.tyy[c] - f.tyy[c - sy], n.dy, n._dy) + dsc<PERF>(f.txy[c + sx] - f.txy[c], n.dx, n._dx)) -
            dsc<PERF>(f.Pt[c] - f.Pt[c - sy], n.dy, n._dy);
 }
@@ -309,8 +309,8 @@ __global__ void __launch_bounds__(256) k2_V_bc(Geom g, Fields64 f, Num n, int up
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int nx = g.nx, ny = g.ny;
     if (i > nx || j > ny) return;
-    const int64_t c = gidx(g, i, j, 0);
-    const int64_t sx = 1, sy = g.px;
+    const idx_t c = gidx32(g, i, j, 0);
+    const idx_t sx = 1, sy = g.px;
     if (j >= 1 && j <= ny - 2) {  // Vx source faces (bc_y!)
         double v = f.Vx[c];
         if (update && i >= 1 && i <= nx - 1) {
@@ -339,8 +339,8 @@ __global__ void k2_dV(Geom g, Fields64 f, Num n) {
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int nx = g.nx, ny = g.ny;
     if (i > nx || j > ny) return;
-    const int64_t c = gidx(g, i, j, 0);
-    const int64_t sx = 1, sy = g.px;
+    const idx_t c = gidx32(g, i, j, 0);
+    const idx_t sx = 1, sy = g.px;
     if (i >= 1 && i <= nx - 1 && j >= 1 && j <= ny - 2) {
         const double R = res2_x<PERF>(f, n, c, sx, sy);
         if (VAR == V2D) f.Rx[c] = R;
@@ -358,7 +358,7 @@ __global__ void k2_add_dV(Geom g, Fields64 f) {
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int nx = g.nx, ny = g.ny;
     if (i > nx || j > ny) return;
-    const int64_t c = gidx(g, i, j, 0);
+    const idx_t c = gidx32(g, i, j, 0);
     if (i >= 1 && i <= nx - 1 && j >= 1 && j <= ny - 2) f.Vx[c] = f.Vx[c] + f.dVx[c];
     if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 1) f.Vy[c] = f.Vy[c] + f.dVy[c];
 }
@@ -414,12 +414,12 @@ __global__ void __launch_bounds__(256) k3_check(Geom g, Fields64 f, Num n, doubl
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
-    const int64_t sx = 1, sy = g.px, sz = g.pxy;
+    const idx_t sx = 1, sy = g.px, sz = (idx_t)g.pxy;
     Acc a;
     acc_init(a);
     if (i <= nx && j < ny) {
         for (int k = blockIdx.z; k < nz; k += gridDim.z) {
-            const int64_t c = gidx(g, i, j, k);
+            const idx_t c = gidx32(g, i, j, k);
             const double vx = f.Vx[c];
             a.vmin = fmin(a.vmin, vx);
             a.vmax = fmax(a.vmax, vx);
@@ -463,11 +463,11 @@ __global__ void __launch_bounds__(256) k2_check(Geom g, Fields64 f, Num n, doubl
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int nx = g.nx, ny = g.ny;
-    const int64_t sx = 1, sy = g.px;
+    const idx_t sx = 1, sy = g.px;
     Acc a;
     acc_init(a);
     if (i <= nx && j < ny) {
-        const int64_t c = gidx(g, i, j, 0);
+        const idx_t c = gidx32(g, i, j, 0);
         const double vx = f.Vx[c];
         a.vmin = vx;
         a.vmax = vx;
@@ -558,12 +558,12 @@ __global__ void __launch_bounds__(256) k3_sources(Geom g, Fields64 f, Mixed32 m,
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
-    const int64_t sx = 1, sy = g.px, sz = g.pxy;
+    const idx_t sx = 1, sy = g.px, sz = (idx_t)g.pxy;
     Acc a;
     acc_init(a);
     if (i <= nx && j < ny) {
         for (int k = blockIdx.z; k < nz; k += gridDim.z) {
-            const int64_t c = gidx(g, i, j, k);
+            const idx_t c = gidx32(g, i, j, k);
             const double vx = f.Vx[c];
             a.vmin = fmin(a.vmin, vx);
             a.vmax = fmax(a.vmax, vx);
@@ -587,7 +587,7 @@ __global__ void __launch_bounds__(256) k3_sources(Geom g, Fields64 f, Mixed32 m,
                 if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2) m.atzz[c] = (float)a_n(f.tzz, f.tzz_o, n._dz * dvz);
             }
             if (i < nx) {
-                auto a_s = [&](const double* t, const double* to, int64_t o1, int64_t o2, double s) {
+                auto a_s = [&](const double* t, const double* to, idx_t o1, idx_t o2, double s) {
                     const double ag = (((f.Gdt[c - o1 - o2] + f.Gdt[c - o2]) + f.Gdt[c - o1]) + f.Gdt[c]) * 0.25;
                     const double am = (((f.Mus[c - o1 - o2] + f.Mus[c - o2]) + f.Mus[c - o1]) + f.Mus[c]) * 0.25;
                     const double Gr = EL ? gr_of(ag, n.gdt) : 0.0;
@@ -647,7 +647,7 @@ __global__ void k_init_inclusion(Geom g, Fields64 f, Num n, double mus0, double 
     const int k = blockIdx.z;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     if (i > nx || j > ny) return;
-    const int64_t c = gidx(g, i, j, k);
+    const idx_t c = gidx32(g, i, j, k);
     const double X = ((double)i * n.dx + 0.5 * n.dx) - 0.5 * n.lx;
     const double Y = ((double)j * n.dy + 0.5 * n.dy) - 0.5 * n.ly;
     if (i < nx && j < ny && k < (D3 ? nz : 1)) {
@@ -678,8 +678,8 @@ __global__ void k_smooth(Geom g, double* __restrict__ dst, const double* __restr
     const int k = blockIdx.z;
     if (i < 1 || j < 1 || i > g.nx - 2 || j > g.ny - 2) return;
     if (D3 && (k < 1 || k > g.nz - 2)) return;
-    const int64_t c = gidx(g, i, j, k);
-    const int64_t sy = g.px, sz = g.pxy;
+    const idx_t c = gidx32(g, i, j, k);
+    const idx_t sy = g.px, sz = (idx_t)g.pxy;
     const double a = A[c];
     const double d2x = (A[c + 1] - a) - (a - A[c - 1]);
     const double d2y = (A[c + sy] - a) - (a - A[c - sy]);
@@ -698,11 +698,11 @@ __global__ void k_maxloc(Geom g, double* __restrict__ must, const double* __rest
     if (i >= g.nx || j >= g.ny) return;
     const int ci = min(max(i, 1), g.nx - 2), cj = min(max(j, 1), g.ny - 2);
     const int ck = D3 ? min(max(k, 1), g.nz - 2) : 0;
-    const int64_t c = gidx(g, ci, cj, ck);
-    const int64_t sy = g.px, sz = g.pxy;
+    const idx_t c = gidx32(g, ci, cj, ck);
+    const idx_t sy = g.px, sz = (idx_t)g.pxy;
     double m = fmax(fmax(fmax(fmax(A[c - 1], A[c + 1]), A[c]), A[c - sy]), A[c + sy]);
     if (D3) m = fmax(fmax(m, A[c - sz]), A[c + sz]);
-    must[gidx(g, i, j, k)] = m;
+    must[gidx32(g, i, j, k)] = m;
 }
 
 // compute_iter_params! (Stokes3D_ve_perf.jl:34-39; viscous Stokes2D.jl:27-31).
@@ -712,7 +712,7 @@ __global__ void k_iter_params(Geom g, Fields64 f, Num n) {
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int k = blockIdx.z;
     if (i >= g.nx || j >= g.ny) return;
-    const int64_t c = gidx(g, i, j, k);
+    const idx_t c = gidx32(g, i, j, k);
     const double mu_eff = EL ? 1.0 / (1.0 / f.Must[c] + 1.0 / n.gdt) : f.Must[c];
     const double dtr = n.Vpdt * n.max_l / n.Re / mu_eff;
     f.dtRho[c] = dtr;
