@@ -91,6 +91,7 @@ enum pts_field {
     PTS_F_DIVV,     /* ∇V                                  */
     PTS_F_RX, PTS_F_RY, PTS_F_RZ,
     PTS_F_DVX, PTS_F_DVY, PTS_F_DVZ,
+    PTS_F_RHOG,     /* ρg (batched sweep only)            */
     PTS_F_COUNT
 };
 
@@ -164,6 +165,49 @@ PTS_API int pts_solve(pts_ctx* ctx, pts_solve_info* info);
  * `for it = 1:nt` (Stokes3D_ve_perf.jl:194-226). iters_per_step (length nt) may be NULL;
  * info (may be NULL) receives the last step's outcome with iters = ittot. */
 PTS_API int pts_run(pts_ctx* ctx, int32_t nt, int64_t* iters_per_step, pts_solve_info* info);
+
+/* ---- batched 2D viscous sweep: many uneven grids, one persistent launch ----
+ * Replaces the reference's parameter sweeps, which run one Julia process per instance
+ * (scripts/runme_Stokes2D_{shear,gravity}_weak.jl:23-25 launching Stokes2D_param.jl). Each
+ * instance is the scripts/Stokes2D.jl problem (kernels, local iteration parameters from
+ * the smoothed local-max viscosity) with the buoyancy term of Stokes2D_param.jl:59, a box
+ * lx x ly (Stokes2D_ve_param.jl:99-102), one centred inclusion (viscosity musi,
+ * density contrast rhogi) and pure shear ebg. All instances iterate in one cooperative
+ * launch; an instance stops when its check (every nout iterations; Stokes2D_param.jl:203-210
+ * with one tolerance, norms scaled by ly) reaches eps. */
+typedef struct pts_batch_instance {
+    int32_t nx, ny;   /* cells, each >= 3 */
+    double lx, ly;    /* box */
+    double musi;      /* inclusion viscosity (matrix 1) */
+    double radius2;   /* squared inclusion radius (centred) */
+    double rhogi;     /* inclusion ρg (matrix 0) */
+    double ebg;       /* background pure-shear strain rate */
+} pts_batch_instance;
+
+typedef struct pts_batch_desc {
+    int32_t nout;      /* check cadence */
+    int32_t tile;      /* tile shape 0..3 = 32x4, 32x8, 64x4, 32x16 (pts_batch_set_tile) */
+    double eps;        /* tolerance */
+    double iter_max;   /* `iter <= iterMax` */
+    double r, Re, CFL; /* iteration parameters (Stokes2D.jl:82-84) */
+    int32_t reserved[4];
+} pts_batch_desc;
+
+typedef struct pts_batch pts_batch;
+PTS_API int pts_batch_create(const pts_batch_desc* desc, const pts_batch_instance* inst, int32_t n, pts_batch** out);
+PTS_API int pts_batch_destroy(pts_batch* b);
+PTS_API const char* pts_batch_last_error(const pts_batch* b);
+/* ICs, smooth! x10 of Mus and ρg, compute_maxloc! + bc, compute_iter_params! for every instance */
+PTS_API int pts_batch_setup(pts_batch* b);
+PTS_API int pts_batch_set_tile(pts_batch* b, int32_t tile);
+/* The persistent launch (captured in a CUDA graph when the driver allows it): runs until
+ * every instance has converged or iter_limit (< 0: desc.iter_max) is passed. Synchronous.
+ * iters/err/converged (length n, may be NULL) receive each instance's outcome. */
+PTS_API int pts_batch_solve(pts_batch* b, int64_t iter_limit, int64_t* iters, double* err, int32_t* converged,
+                            int32_t* used_graph);
+/* A field of one instance (fields Pt Vx Vy τxx τyy τxy Mus Musτ Gdτ dτ_Rho ∇V Rx Ry ρg) */
+PTS_API int pts_batch_get_field(pts_batch* b, int32_t instance, int32_t field, double* host, int64_t n);
+PTS_API int pts_batch_stream(pts_batch* b, void** stream);
 
 /* ---- convergence check without any allocation ----
  * This entry point has no counterpart in the reference. It is for callers that cannot

@@ -184,6 +184,80 @@ class V2D(_Case2D):
         return self.norm_err(("Rx", "Ry"), "divV")
 
 
+class V2DSweep(V2D):
+    """One instance of the batched 2D viscous sweep: scripts/Stokes2D.jl's kernels with
+    the buoyancy term of scripts/Stokes2D_param.jl:59 (Ry -= @av_yi(ρg)), a box
+    lx = aspect*ly (scripts/Stokes2D_ve_param.jl:99-102), one centred circular inclusion of
+    radius 1 with viscosity musi and density contrast rhogi, pure shear ebg; Mus and ρg
+    are smoothed alike (Stokes2D_param.jl:184-189). The check is Stokes2D_param.jl's
+    (Vmin/Vmax over Vy, :204-208) with the norms scaled by ly (Stokes2D_ve_param.jl:175-176)
+    and a single tolerance on max(norm_Rx, norm_Ry, norm_∇V)."""
+
+    defaults = dict(nt=1, iterMax=2e5, nout=200, eps=1e-8, CFL=0.9 / math.sqrt(2), Re=5 * PI, r=1.0, rhogi=0.0)
+
+    def setup(self):
+        nx, ny = self.nx, self.ny
+        self.ly = 10.0 if "ly" not in self.p else self.p["ly"]
+        self.dx, self.dy = self.lx / nx, self.ly / ny
+        self._dx, self._dy = 1.0 / self.dx, 1.0 / self.dy
+        self.max_lxy = max(self.lx, self.ly)
+        self.Vpdt = min(self.dx, self.dy) * self.CFL
+        self.xc = linrange(self.dx / 2, self.lx - self.dx / 2, nx)
+        self.yc = linrange(self.dy / 2, self.ly - self.dy / 2, ny)
+        self.alloc(Pt=(nx, ny), divV=(nx, ny), txx=(nx, ny), tyy=(nx, ny), txy=(nx - 1, ny - 1),
+                   Rx=(nx - 1, ny - 2), Ry=(nx - 2, ny - 1), dVx=(nx - 1, ny - 2), dVy=(nx - 2, ny - 1),
+                   Mus2=(nx, ny), Must=(nx, ny), Gdt=(nx, ny), dtRho=(nx, ny), rhog2=(nx, ny))
+        dx, dy, lx, ly = self.dx, self.dy, self.lx, self.ly
+        ix = np.arange(1, nx + 2, dtype=np.float64)
+        iy = np.arange(1, ny + 2, dtype=np.float64)
+        X = (ix[:nx] - 1) * dx + 0.5 * dx - 0.5 * lx
+        Y = (iy[:ny] - 1) * dy + 0.5 * dy - 0.5 * ly
+        Rad2 = np.asfortranarray(X[:, None] ** 2 + Y[None, :] ** 2)
+        self.f["Vx"] = np.asfortranarray(np.repeat((-self.ebg * ((ix - 1) * dx - 0.5 * lx))[:, None], ny, axis=1))
+        self.f["Vy"] = np.asfortranarray(np.repeat((self.ebg * ((iy - 1) * dy - 0.5 * ly))[None, :], nx, axis=0))
+        Mus = self.mus0 * np.ones((nx, ny), order="F")
+        Mus[Rad2 < 1.0] = self.musi
+        rhog = np.zeros((nx, ny), order="F")
+        rhog[Rad2 < 1.0] = self.rhogi
+        L = self.L
+        Mus2, rhog2 = self.f["Mus2"], self.f["rhog2"]
+        Mus2[...] = Mus
+        rhog2[...] = rhog
+        for _ in range(10):
+            L.ora2_smooth(arr(Mus2), arr(Mus), 1.0)
+            Mus, Mus2 = Mus2, Mus
+            L.ora2_smooth(arr(rhog2), arr(rhog), 1.0)
+            rhog, rhog2 = rhog2, rhog
+        self.f["Mus"], self.f["Mus2"], self.f["rhog"], self.f["rhog2"] = Mus, Mus2, rhog, rhog2
+        Must = self.f["Must"]
+        Must[...] = Mus
+        L.ora2_maxloc(arr(Must), arr(Mus))
+        L.ora2_bc_x(arr(Must))
+        L.ora2_bc_y(arr(Must))
+        self.iter_params()
+        return self
+
+    def iteration(self):
+        L, A = self.L, self.A
+        L.ora2_compute_P(A("divV"), A("Pt"), A("Vx"), A("Vy"), A("Gdt"), self.r, self.dx, self.dy)
+        L.ora2v_compute_tau(A("txx"), A("tyy"), A("txy"), A("Vx"), A("Vy"), A("Mus"), A("Gdt"), self.dx, self.dy)
+        L.ora2s_compute_dV(A("Rx"), A("Ry"), A("dVx"), A("dVy"), A("Pt"), A("txx"), A("tyy"), A("txy"),
+                           A("dtRho"), A("rhog"), self.dx, self.dy)
+        L.ora2_compute_V(A("Vx"), A("Vy"), A("dVx"), A("dVy"))
+        self.bc()
+
+    def check(self):
+        _, vmin, vmax = stats(self.f["Vy"])
+        _, pmin, pmax = stats(self.f["Pt"])
+        norms = []
+        for n in ("Rx", "Ry"):
+            s, _, _ = stats(self.f[n])
+            norms.append(math.sqrt(s) / (pmax - pmin) * self.ly / math.sqrt(self.f[n].size))
+        s, _, _ = stats(self.f["divV"])
+        norms.append(math.sqrt(s) / (vmax - vmin) * self.ly / math.sqrt(self.f["divV"].size))
+        return max(norms), norms
+
+
 class VE2D(_Case2D):
     """scripts/Stokes2D_ve.jl (2D Maxwell visco-elastic, role kernels)."""
 

@@ -29,6 +29,7 @@ UNITS = {
     "pts_noalloc.cu": ["--fmad=false"],
     "pts_kernels32.cu": [],
     "pts_abi.cu": [],
+    "pts_batch.cu": [],
 }
 
 

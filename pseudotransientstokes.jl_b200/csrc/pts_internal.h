@@ -68,6 +68,7 @@ struct FieldsT {
     T *Mus, *Must, *Gdt, *dtRho, *divV;
     T *Rx, *Ry, *Rz, *dVx, *dVy, *dVz;
     T *Mus2;
+    T *rhog, *rhog2;  // buoyancy ρg of the batched sweep (Stokes2D_param.jl), else null
 };
 using Fields64 = FieldsT<double>;
 
@@ -124,5 +125,35 @@ cudaError_t launch_fold(const Geom& g, const Fields64& f, const Mixed32& m, cuda
 cudaError_t launch_sources(int variant, const Geom& g, const Fields64& f, const Mixed32& m, const Num& n,
                            double* partials, int nblocks_cap, CheckResult* result, cudaStream_t s);
 cudaError_t launch_coef32(const Geom& g, const Fields64& f, const Mixed32& m, cudaStream_t s);
+
+// ---- batched 2D sweep (pts_batch.cu host side, kernels in pts_kernels64.cu) ----
+// One instance: its geometry and numerics, where its fields start in every arena, and
+// the first of its TX x TY tiles in the flattened tile list.
+struct BInst {
+    Geom g;
+    Num n;
+    int64_t off;
+    int tile0, ntx, nty;
+    double lenRx, lenRy, lenDiv, ly;
+};
+struct BState {
+    int* converged;   // per instance: its PT loop has ended on the tolerance (or NaN)
+    int64_t* iters;   // per instance: PT iterations done
+    double* err;      // per instance: err of the last check
+    double* partials; // per tile: 8 partial sums/extrema of the check
+    int* nactive;     // instances still iterating
+    int* nan_flag;
+};
+constexpr int kBatchTileShapes = 4;
+inline void batch_tile_dims(int tile, int* tx, int* ty) {
+    static const int d[kBatchTileShapes][2] = {{32, 4}, {32, 8}, {64, 4}, {32, 16}};
+    *tx = d[tile][0];
+    *ty = d[tile][1];
+}
+cudaError_t launch_batch(int tile, const BInst* d_inst, const int* d_tile_inst, int ntiles, int ninst,
+                         const Fields64& F, const BState& st, int nout, int64_t iter_last, double eps, cudaStream_t s);
+// ICs of one sweep instance: Mus/ρg = inclusion (radius2) ? (musi, rhogi) : (1, 0), pure shear ebg
+cudaError_t launch_init_sweep(const Geom& g, const Fields64& f, const Num& n, double musi, double radius2,
+                              double rhogi, double ebg, cudaStream_t s);
 
 }  // namespace pts

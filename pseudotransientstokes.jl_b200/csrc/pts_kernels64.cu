@@ -8,6 +8,8 @@
 // Kernels here are the straightforward one-thread-per-point forms (two launches per PT
 // iteration: compute_Pt_τ! and compute_V! + bc); the 3D visco-elastic hot path also has
 // the single-pass z-streaming kernel in pts_fused3d.cu.
+#include <cooperative_groups.h>
+
 #include <cfloat>
 #include <cmath>
 #include <cstdlib>
@@ -237,10 +239,10 @@ __global__ void k3_add_dV(Geom g, Fields64 f) {
 
 // compute_P! + compute_τ! for the three 2D scripts:
 //   V2D        Stokes2D.jl:33-44      VE2D  Stokes2D_ve.jl:42-55     VE2D_PERF  Stokes2D_ve_perf.jl:47-53
+// (the body is a device function so the batched sweep kernel runs the same code per point)
 template <int VAR>
-__global__ void __launch_bounds__(256) k2_Pt_tau(Geom g, Fields64 f, Num n, int roles, int store_divV) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void pt_tau_2d(const Geom& g, const Fields64& f, const Num& n, int i, int j, int roles,
+                                          int store_divV) {
     const int nx = g.nx, ny = g.ny;
     if (i >= nx || j >= ny) return;
     const idx_t c = gidx32(g, i, j, 0);
@@ -289,24 +291,31 @@ __global__ void __launch_bounds__(256) k2_Pt_tau(Geom g, Fields64 f, Num n, int 
     }
 }
 
+template <int VAR>
+__global__ void __launch_bounds__(256) k2_Pt_tau(Geom g, Fields64 f, Num n, int roles, int store_divV) {
+    pt_tau_2d<VAR>(g, f, n, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y * blockDim.y + threadIdx.y, roles,
+                   store_divV);
+}
+
 template <bool PERF>
 __device__ __forceinline__ double res2_x(const Fields64& f, const Num& n, idx_t c, idx_t sx, idx_t sy) {
     return (dsc<PERF>(f.txx[c] - f.txx[c - sx], n.dx, n._dx) + dsc<PERF>(f.txy[c + sy] - f.txy[c], n.dy, n._dy)) -
            dsc<PERF>(f.Pt[c] - f.Pt[c - sx], n.dx, n._dx);
 }
-template <bool PERF>
+// With RHOG the buoyancy term of Stokes2D_param.jl:59: Ry -= @av_yi(ρg).
+template <bool PERF, bool RHOG = false>
 __device__ __forceinline__ double res2_y(const Fields64& f, const Num& n, idx_t c, idx_t sx, idx_t sy) {
-    return (dsc<PERF>(f.tyy[c] - f.tyy[c - sy], n.dy, n._dy) + dsc<PERF>(f.txy[c + sx] - f.txy[c], n.dx, n._dx)) -
-           dsc<PERF>(f.Pt[c] - f.Pt[c - sy], n.dy, n._dy);
+    const double R = (dsc<PERF>(f.tyy[c] - f.tyy[c - sy], n.dy, n._dy) + dsc<PERF>(f.txy[c + sx] - f.txy[c], n.dx, n._dx)) -
+                     dsc<PERF>(f.Pt[c] - f.Pt[c - sy], n.dy, n._dy);
+    if (RHOG) return R - (f.rhog[c - sy] + f.rhog[c]) * 0.5;
+    return R;
 }
 
 // compute_V! (+ compute_dV!) with bc_y!(Vx), bc_x!(Vy) (Stokes2D.jl:46-58,133-134;
 // Stokes2D_ve_perf.jl:55-59,151-152).
-template <int VAR>
-__global__ void __launch_bounds__(256) k2_V_bc(Geom g, Fields64 f, Num n, int update) {
+template <int VAR, bool RHOG = false>
+__device__ __forceinline__ void v_bc_2d(const Geom& g, const Fields64& f, const Num& n, int i, int j, int update) {
     constexpr bool PERF = (VAR == VE2D_PERF);
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int nx = g.nx, ny = g.ny;
     if (i > nx || j > ny) return;
     const idx_t c = gidx32(g, i, j, 0);
@@ -323,12 +332,17 @@ __global__ void __launch_bounds__(256) k2_V_bc(Geom g, Fields64 f, Num n, int up
     if (i >= 1 && i <= nx - 2) {  // Vy source faces (bc_x!)
         double v = f.Vy[c];
         if (update && j >= 1 && j <= ny - 1) {
-            v = v + res2_y<PERF>(f, n, c, sx, sy) * ((f.dtRho[c - sy] + f.dtRho[c]) * 0.5);
+            v = v + res2_y<PERF, RHOG>(f, n, c, sx, sy) * ((f.dtRho[c - sy] + f.dtRho[c]) * 0.5);
             f.Vy[c] = v;
         }
         if (i == 1) f.Vy[c - sx] = v;
         if (i == nx - 2) f.Vy[c + sx] = v;
     }
+}
+
+template <int VAR>
+__global__ void __launch_bounds__(256) k2_V_bc(Geom g, Fields64 f, Num n, int update) {
+    v_bc_2d<VAR>(g, f, n, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y * blockDim.y + threadIdx.y, update);
 }
 
 // compute_dV! alone; Stokes2D.jl:46-52 also stores Rx, Ry.
@@ -534,6 +548,168 @@ __global__ void k_check_finalize(const double* partials, int nblocks, double lx,
     }
 }
 
+// ------------------------------------------------------------------ batched 2D sweep (persistent)
+
+__device__ __forceinline__ Fields64 shift_fields(const Fields64& F, int64_t off) {
+    Fields64 f = F;
+    double** p[] = {&f.Pt, &f.Vx, &f.Vy, &f.txx, &f.tyy, &f.txy, &f.Mus, &f.Must, &f.Gdt, &f.dtRho, &f.divV,
+                    &f.Rx, &f.Ry, &f.rhog};
+    for (double** q : p) *q = *q + off;
+    return f;
+}
+
+// Block reduction of one Acc into out[0..7] (fixed order, as acc_block_store).
+__device__ void acc_block_store_to(Acc& a, double* out) {
+    for (int o = 16; o > 0; o >>= 1) {
+        for (int q = 0; q < 4; ++q) a.s[q] += __shfl_down_sync(kFull, a.s[q], o);
+        a.vmin = fmin(a.vmin, __shfl_down_sync(kFull, a.vmin, o));
+        a.vmax = fmax(a.vmax, __shfl_down_sync(kFull, a.vmax, o));
+        a.pmin = fmin(a.pmin, __shfl_down_sync(kFull, a.pmin, o));
+        a.pmax = fmax(a.pmax, __shfl_down_sync(kFull, a.pmax, o));
+    }
+    __shared__ double sm[32][kCheckSlots];
+    const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+    const int nw = (blockDim.x * blockDim.y + 31) >> 5;
+    if ((tid & 31) == 0) {
+        const int w = tid >> 5;
+        sm[w][0] = a.s[0]; sm[w][1] = a.s[1]; sm[w][2] = a.s[2]; sm[w][3] = a.s[3];
+        sm[w][4] = a.vmin; sm[w][5] = a.vmax; sm[w][6] = a.pmin; sm[w][7] = a.pmax;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double r[kCheckSlots];
+        for (int q = 0; q < kCheckSlots; ++q) r[q] = sm[0][q];
+        for (int w = 1; w < nw; ++w) {
+            for (int q = 0; q < 4; ++q) r[q] += sm[w][q];
+            r[4] = fmin(r[4], sm[w][4]); r[5] = fmax(r[5], sm[w][5]);
+            r[6] = fmin(r[6], sm[w][6]); r[7] = fmax(r[7], sm[w][7]);
+        }
+        for (int q = 0; q < kCheckSlots; ++q) out[q] = r[q];
+    }
+    __syncthreads();
+}
+
+// All instances of a sweep iterate in lockstep inside one cooperative launch; a block walks
+// the flattened list of TX x TY tiles (instance by instance) and skips converged
+// instances. Per PT iteration: compute_P! + compute_τ! (Stokes2D.jl:33-44), grid barrier,
+// compute_dV! with the buoyancy term (Stokes2D_param.jl:57-63) + compute_V! + bc_y!/bc_x!
+// (Stokes2D.jl:54-58,133-134), grid barrier. Every nout iterations each instance's check
+// (Stokes2D_param.jl:203-210 with a single tolerance, norms scaled by ly) is reduced in a
+// fixed order from per-tile partials, and an instance whose err <= eps (or NaN) is frozen
+// -- its `while err > ε` loop ended. The launch ends when no instance is active or after
+// iteration iter_last, like `iter <= iterMax`.
+template <int TX, int TY>
+__global__ void __launch_bounds__(TX* TY) k2_batch(const BInst* __restrict__ inst, const int* __restrict__ tile_inst,
+                                                   int ntiles, int ninst, Fields64 F, BState st, int nout,
+                                                   int64_t iter_last, double eps) {
+    cooperative_groups::grid_group grid = cooperative_groups::this_grid();
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + TX * ty;
+    int64_t iter = 0;
+    for (;;) {
+        if (*(volatile int*)st.nactive == 0 || iter > iter_last) break;
+        const bool chk = ((iter + 1) % nout == 0);
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+            const int b = tile_inst[t];
+            if (st.converged[b]) continue;
+            const BInst& I = inst[b];
+            const int q = t - I.tile0;
+            pt_tau_2d<V2D>(I.g, shift_fields(F, I.off), I.n, (q % I.ntx) * TX + tx, (q / I.ntx) * TY + ty,
+                           ROLE_P | ROLE_TAU, chk ? 1 : 0);
+        }
+        grid.sync();
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+            const int b = tile_inst[t];
+            if (st.converged[b]) continue;
+            const BInst& I = inst[b];
+            const int q = t - I.tile0;
+            v_bc_2d<V2D, true>(I.g, shift_fields(F, I.off), I.n, (q % I.ntx) * TX + tx, (q / I.ntx) * TY + ty, 1);
+        }
+        grid.sync();
+        ++iter;
+        if (!chk) continue;
+        // per-tile partials of the check
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+            const int b = tile_inst[t];
+            if (st.converged[b]) continue;
+            const BInst& I = inst[b];
+            const int q = t - I.tile0;
+            const int i = (q % I.ntx) * TX + tx, j = (q / I.ntx) * TY + ty;
+            const int nx = I.g.nx, ny = I.g.ny;
+            const Fields64 f = shift_fields(F, I.off);
+            Acc a;
+            acc_init(a);
+            const idx_t c = gidx32(I.g, i, j, 0);
+            const idx_t sx = 1, sy = I.g.px;
+            if (i < nx && j <= ny) {
+                const double vy = f.Vy[c];
+                a.vmin = vy;
+                a.vmax = vy;
+            }
+            if (i < nx && j < ny) {
+                a.pmin = a.pmax = f.Pt[c];
+                const double dv = f.divV[c];
+                a.s[3] = dv * dv;
+            }
+            if (i >= 1 && i <= nx - 1 && j >= 1 && j <= ny - 2) {
+                const double R = res2_x<false>(f, I.n, c, sx, sy);
+                f.Rx[c] = R;
+                a.s[0] = R * R;
+            }
+            if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 1) {
+                const double R = res2_y<false, true>(f, I.n, c, sx, sy);
+                f.Ry[c] = R;
+                a.s[1] = R * R;
+            }
+            acc_block_store_to(a, st.partials + (int64_t)t * kCheckSlots);
+        }
+        grid.sync();
+        // per-instance finalisation: one block per instance, fixed-order reduction
+        __shared__ double red[TX * TY][kCheckSlots];
+        for (int b = blockIdx.x; b < ninst; b += gridDim.x) {
+            if (st.converged[b]) continue;
+            const BInst& I = inst[b];
+            const int nt = I.ntx * I.nty;
+            double r[kCheckSlots] = {0.0, 0.0, 0.0, 0.0, DBL_MAX, -DBL_MAX, DBL_MAX, -DBL_MAX};
+            for (int u = tid; u < nt; u += TX * TY) {
+                const double* p = st.partials + (int64_t)(I.tile0 + u) * kCheckSlots;
+                for (int w = 0; w < 4; ++w) r[w] += p[w];
+                r[4] = fmin(r[4], p[4]); r[5] = fmax(r[5], p[5]);
+                r[6] = fmin(r[6], p[6]); r[7] = fmax(r[7], p[7]);
+            }
+            for (int w = 0; w < kCheckSlots; ++w) red[tid][w] = r[w];
+            __syncthreads();
+            for (int s = (TX * TY) / 2; s > 0; s >>= 1) {
+                if (tid < s) {
+                    for (int w = 0; w < 4; ++w) red[tid][w] += red[tid + s][w];
+                    red[tid][4] = fmin(red[tid][4], red[tid + s][4]); red[tid][5] = fmax(red[tid][5], red[tid + s][5]);
+                    red[tid][6] = fmin(red[tid][6], red[tid + s][6]); red[tid][7] = fmax(red[tid][7], red[tid + s][7]);
+                }
+                __syncthreads();
+            }
+            if (tid == 0) {
+                const double dP = red[0][7] - red[0][6], dV = red[0][5] - red[0][4];
+                const double nRx = sqrt(red[0][0]) / dP * I.ly / sqrt(I.lenRx);
+                const double nRy = sqrt(red[0][1]) / dP * I.ly / sqrt(I.lenRy);
+                const double nDv = sqrt(red[0][3]) / dV * I.ly / sqrt(I.lenDiv);
+                const bool bad = isnan(nRx) || isnan(nRy) || isnan(nDv);
+                const double err = bad ? NAN : fmax(fmax(nRx, nRy), nDv);
+                st.err[b] = err;
+                st.iters[b] = iter;
+                if (bad) atomicExch(st.nan_flag, 1);
+                if (!(err > eps)) {
+                    st.converged[b] = 1;
+                    atomicSub(st.nactive, 1);
+                }
+            }
+            __syncthreads();
+        }
+        grid.sync();
+    }
+    // instances whose loop ended on iter_max: iterations done = iter
+    for (int b = blockIdx.x * TX * TY + tid; b < ninst; b += gridDim.x * TX * TY)
+        if (!st.converged[b]) st.iters[b] = iter;
+}
+
 // ------------------------------------------------------------------ mixed precision: FP64 outer step
 
 // X += δ for the ten iterated fields, then δ = 0 (elementwise over the padded arrays).
@@ -668,6 +844,24 @@ __global__ void k_init_inclusion(Geom g, Fields64 f, Num n, double mus0, double 
     } else {
         if (i < nx) f.Vy[c] = ebg * ((double)j * n.dy - 0.5 * n.ly);
     }
+}
+
+// ICs of one batched-sweep instance (Stokes2D_param.jl:176-181 with one centred inclusion;
+// the box lx x ly of Stokes2D_ve_param.jl:99-102): the same operations as the oracle.
+__global__ void k2_init_sweep(Geom g, Fields64 f, Num n, double musi, double radius2, double rhogi, double ebg) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i > g.nx || j > g.ny) return;
+    const idx_t c = gidx32(g, i, j, 0);
+    if (i < g.nx && j < g.ny) {
+        const double X = ((double)i * n.dx + 0.5 * n.dx) - 0.5 * n.lx;
+        const double Y = ((double)j * n.dy + 0.5 * n.dy) - 0.5 * n.ly;
+        const bool in = (X * X + Y * Y) < radius2;
+        f.Mus[c] = in ? musi : 1.0;
+        f.rhog[c] = in ? rhogi : 0.0;
+    }
+    if (j < g.ny) f.Vx[c] = (-ebg) * ((double)i * n.dx - 0.5 * n.lx);
+    if (i < g.nx) f.Vy[c] = ebg * ((double)j * n.dy - 0.5 * n.ly);
 }
 
 // smooth! (Stokes3D_ve_perf.jl:24-27; 2D Stokes2D.jl:17-20) on the interior cells.
@@ -811,6 +1005,40 @@ cudaError_t launch_check(int v, const Geom& g, const Fields64& f, const Num& n, 
     const double lenDiv = nx * ny * nz;
     k_check_finalize<<<1, 256, 0, s>>>(partials, nb, n.lx, lenRx, lenRy, lenRz, lenDiv, d3 ? 3 : 2, result);
     return cudaGetLastError();
+}
+
+cudaError_t launch_init_sweep(const Geom& g, const Fields64& f, const Num& n, double musi, double radius2,
+                              double rhogi, double ebg, cudaStream_t s) {
+    k2_init_sweep<<<grid_faces(g, false), blk(), 0, s>>>(g, f, n, musi, radius2, rhogi, ebg);
+    return cudaGetLastError();
+}
+
+template <int TX, int TY>
+static cudaError_t launch_batch_t(const BInst* d_inst, const int* d_tile_inst, int ntiles, int ninst, Fields64 F,
+                                  BState st, int nout, int64_t iter_last, double eps, cudaStream_t s) {
+    int per_sm = 0, dev = 0, nsm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k2_batch<TX, TY>, TX * TY, 0);
+    if (e != cudaSuccess) return e;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    int grid = per_sm * nsm;  // every block co-resident, as grid.sync() requires
+    const int want = ntiles > ninst ? ntiles : ninst;
+    if (grid > want) grid = want;
+    if (grid < 1) return cudaErrorInvalidConfiguration;
+    void* args[] = {(void*)&d_inst, (void*)&d_tile_inst, (void*)&ntiles, (void*)&ninst, (void*)&F,
+                    (void*)&st,     (void*)&nout,        (void*)&iter_last, (void*)&eps};
+    return cudaLaunchCooperativeKernel((const void*)k2_batch<TX, TY>, dim3(grid), dim3(TX, TY), args, 0, s);
+}
+
+cudaError_t launch_batch(int tile, const BInst* d_inst, const int* d_tile_inst, int ntiles, int ninst,
+                         const Fields64& F, const BState& st, int nout, int64_t iter_last, double eps, cudaStream_t s) {
+    switch (tile) {
+        case 0: return launch_batch_t<32, 4>(d_inst, d_tile_inst, ntiles, ninst, F, st, nout, iter_last, eps, s);
+        case 1: return launch_batch_t<32, 8>(d_inst, d_tile_inst, ntiles, ninst, F, st, nout, iter_last, eps, s);
+        case 2: return launch_batch_t<64, 4>(d_inst, d_tile_inst, ntiles, ninst, F, st, nout, iter_last, eps, s);
+        case 3: return launch_batch_t<32, 16>(d_inst, d_tile_inst, ntiles, ninst, F, st, nout, iter_last, eps, s);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 cudaError_t launch_fold(const Geom& g, const Fields64& f, const Mixed32& m, cudaStream_t s) {

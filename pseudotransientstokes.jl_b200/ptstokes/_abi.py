@@ -32,6 +32,7 @@ FIELDS = [
     "txx_o", "tyy_o", "tzz_o", "txy_o", "txz_o", "tyz_o",
     "Mus", "Must", "Gdt", "dtRho", "divV",
     "Rx", "Ry", "Rz", "dVx", "dVy", "dVz",
+    "rhog",
 ]
 FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
 
@@ -60,6 +61,18 @@ class PtsCheck(ctypes.Structure):
 class PtsSolveInfo(ctypes.Structure):
     _fields_ = [("iters", ctypes.c_int64), ("converged", ctypes.c_int32), ("nchecks", ctypes.c_int32),
                 ("last", PtsCheck)]
+
+
+class PtsBatchInstance(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("lx", ctypes.c_double), ("ly", ctypes.c_double),
+                ("musi", ctypes.c_double), ("radius2", ctypes.c_double), ("rhogi", ctypes.c_double),
+                ("ebg", ctypes.c_double)]
+
+
+class PtsBatchDesc(ctypes.Structure):
+    _fields_ = [("nout", ctypes.c_int32), ("tile", ctypes.c_int32), ("eps", ctypes.c_double),
+                ("iter_max", ctypes.c_double), ("r", ctypes.c_double), ("Re", ctypes.c_double),
+                ("CFL", ctypes.c_double), ("reserved", ctypes.c_int32 * 4)]
 
 
 class PtsError(RuntimeError):
@@ -104,6 +117,17 @@ SIGNATURES = {
     "pts_run": ([_P, _I32, ctypes.POINTER(_I64), ctypes.POINTER(PtsSolveInfo)], ctypes.c_int),
     # residual check on caller-owned device arrays; allocates nothing
     "pts_check_noalloc": ([ctypes.POINTER(PtsDesc), ctypes.POINTER(_P), _P, _P], ctypes.c_int),
+    # batched 2D sweep
+    "pts_batch_create": ([ctypes.POINTER(PtsBatchDesc), ctypes.POINTER(PtsBatchInstance), _I32, ctypes.POINTER(_P)],
+                         ctypes.c_int),
+    "pts_batch_destroy": ([_P], ctypes.c_int),
+    "pts_batch_last_error": ([_P], ctypes.c_char_p),
+    "pts_batch_setup": ([_P], ctypes.c_int),
+    "pts_batch_set_tile": ([_P, _I32], ctypes.c_int),
+    "pts_batch_solve": ([_P, _I64, ctypes.POINTER(_I64), ctypes.POINTER(_D), ctypes.POINTER(_I32),
+                         ctypes.POINTER(_I32)], ctypes.c_int),
+    "pts_batch_get_field": ([_P, _I32, _I32, _DP, _I64], ctypes.c_int),
+    "pts_batch_stream": ([_P, ctypes.POINTER(_P)], ctypes.c_int),
 }
 
 _lib = None

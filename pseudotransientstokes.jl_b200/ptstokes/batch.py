@@ -1,0 +1,163 @@
+"""Batched 2D viscous sweeps: many uneven instances in one persistent GPU launch.
+
+The reference runs its parameter sweeps as one Julia process per instance
+(scripts/runme_Stokes2D_shear_weak.jl:1-26, runme_Stokes2D_gravity_weak.jl:1-26,
+runme_Stokes2D_aspect_ratio.jl:1-24). ``Batch`` runs a whole sweep in one cooperative
+launch with per-instance convergence (``pts_batch_*`` in include/ptstokes.h);
+``sweep_instances`` draws the seeded sweep of 256 instances; ``autotune`` picks the tile
+shape by timing the candidates on the batch itself and caches the choice.
+"""
+import ctypes
+import json
+import math
+import os
+import time
+
+import numpy as np
+
+from . import _abi
+from ._abi import FIELD_ID, PtsBatchDesc, PtsBatchInstance
+
+TILE_SHAPES = [(32, 4), (32, 8), (64, 4), (32, 16)]
+
+
+def sweep_instances(n=256, seed=1855, sizes=(63, 127, 255, 511), ly=10.0):
+    """The seeded sweep: nx in `sizes`, lx/ly ~ U[1,4] (ly = 10, ny so that dy ~ dx), one
+    centred inclusion of radius 1 with log10 viscosity contrast ~ U[-6,-1], and either
+    buoyancy-driven (inclusion Δρg = 1, no background flow) or pure shear (εbg = 1), 50/50."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        nx = int(rng.choice(sizes))
+        aspect = float(rng.uniform(1.0, 4.0))
+        lx = aspect * ly
+        ny = max(15, int(round((nx + 1) / aspect)) - 1)
+        musi = float(10.0 ** rng.uniform(-6.0, -1.0))
+        gravity = bool(rng.random() < 0.5)
+        out.append(dict(nx=nx, ny=ny, lx=lx, ly=ly, musi=musi, radius2=1.0,
+                        rhogi=1.0 if gravity else 0.0, ebg=0.0 if gravity else 1.0))
+    return out
+
+
+class Batch:
+    def __init__(self, instances, nout=200, eps=1e-8, iter_max=2e5, tile=1, r=1.0, Re=5 * math.pi,
+                 CFL=0.9 / math.sqrt(2), lib=None):
+        self.lib = lib or _abi.load()
+        self.instances = [dict(d) for d in instances]
+        n = len(self.instances)
+        arr = (PtsBatchInstance * n)()
+        for q, d in enumerate(self.instances):
+            arr[q] = PtsBatchInstance(d["nx"], d["ny"], d["lx"], d["ly"], d["musi"], d.get("radius2", 1.0),
+                                      d.get("rhogi", 0.0), d.get("ebg", 1.0))
+        desc = PtsBatchDesc()
+        desc.nout, desc.tile, desc.eps, desc.iter_max = nout, tile, eps, float(iter_max)
+        desc.r, desc.Re, desc.CFL = r, Re, CFL
+        self.desc = desc
+        h = ctypes.c_void_p()
+        rc = self.lib.pts_batch_create(ctypes.byref(desc), arr, n, ctypes.byref(h))
+        if rc != 0:
+            raise _abi.PtsError(rc, (self.lib.pts_last_error(None) or b"").decode())
+        self.h = h
+        self.n = n
+        self.tile = tile
+
+    def _ck(self, rc):
+        if rc != 0:
+            raise _abi.PtsError(rc, (self.lib.pts_batch_last_error(self.h) or b"").decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.pts_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def setup(self):
+        self._ck(self.lib.pts_batch_setup(self.h))
+        return self
+
+    def set_tile(self, tile):
+        self._ck(self.lib.pts_batch_set_tile(self.h, int(tile)))
+        self.tile = int(tile)
+
+    def stream_handle(self):
+        s = ctypes.c_void_p()
+        self._ck(self.lib.pts_batch_stream(self.h, ctypes.byref(s)))
+        return s.value or 0
+
+    def solve(self, iter_limit=-1):
+        n = self.n
+        iters = (ctypes.c_int64 * n)()
+        err = (ctypes.c_double * n)()
+        conv = (ctypes.c_int32 * n)()
+        graph = ctypes.c_int32()
+        self._ck(self.lib.pts_batch_solve(self.h, int(iter_limit), iters, err, conv, ctypes.byref(graph)))
+        return dict(iters=list(iters), err=list(err), converged=[bool(c) for c in conv], used_graph=bool(graph.value))
+
+    def shape(self, q, name):
+        nx, ny = self.instances[q]["nx"], self.instances[q]["ny"]
+        return {"Vx": (nx + 1, ny), "Vy": (nx, ny + 1), "txy": (nx - 1, ny - 1), "Rx": (nx - 1, ny - 2),
+                "Ry": (nx - 2, ny - 1)}.get(name, (nx, ny))
+
+    def get(self, q, name):
+        out = np.empty(self.shape(q, name), dtype=np.float64, order="F")
+        self._ck(self.lib.pts_batch_get_field(self.h, q, FIELD_ID[name], out.ctypes.data, out.size))
+        return out
+
+
+def _cache_path():
+    base = os.environ.get("XDG_CACHE_HOME") or os.path.join(os.path.expanduser("~"), ".cache")
+    return os.path.join(base, "ptstokes", "autotune.json")
+
+
+def _batch_key(batch):
+    cells = sum(d["nx"] * d["ny"] for d in batch.instances)
+    classes = sorted({d["nx"] for d in batch.instances})
+    return f"2d|fp64|n={batch.n}|cells~{2 ** int(math.log2(max(cells, 1)))}|nx={','.join(map(str, classes))}"
+
+
+def autotune(batch, iters=None, use_cache=True):
+    """Time each tile shape on `batch` for a short run (from its set-up state) and keep the
+    fastest; the choice is cached per (dimension, precision, batch size class)."""
+    import torch
+
+    key = _batch_key(batch)
+    path = _cache_path()
+    cache = {}
+    if use_cache and os.path.exists(path):
+        try:
+            cache = json.load(open(path))
+        except Exception:
+            cache = {}
+    if use_cache and key in cache:
+        batch.set_tile(cache[key]["tile"])
+        return cache[key]
+    iters = iters or 2 * batch.desc.nout - 1
+    stream = torch.cuda.ExternalStream(batch.stream_handle())
+    timings = {}
+    for t in range(len(TILE_SHAPES)):
+        batch.set_tile(t)
+        batch.setup()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        batch.solve(iter_limit=iters)
+        b.record(stream)
+        b.synchronize()
+        timings[t] = a.elapsed_time(b)
+    best = min(timings, key=timings.get)
+    batch.set_tile(best)
+    batch.setup()
+    entry = {"tile": best, "shape": TILE_SHAPES[best], "ms": timings, "iters": iters, "when": time.time()}
+    if use_cache:
+        try:
+            os.makedirs(os.path.dirname(path), exist_ok=True)
+            cache[key] = entry
+            json.dump(cache, open(path, "w"), indent=1)
+        except OSError:
+            pass
+    return entry
