@@ -169,12 +169,12 @@ PTS_API int pts_run(pts_ctx* ctx, int32_t nt, int64_t* iters_per_step, pts_solve
 /* ---- batched 2D viscous sweep: many uneven grids, one persistent launch ----
  * Replaces the reference's parameter sweeps, which run one Julia process per instance
  * (scripts/runme_Stokes2D_{shear,gravity}_weak.jl:23-25 launching Stokes2D_param.jl). Each
- * instance is the scripts/Stokes2D.jl problem (kernels, local iteration parameters from
- * the smoothed local-max viscosity) with the buoyancy term of Stokes2D_param.jl:59, a box
- * lx x ly (Stokes2D_ve_param.jl:99-102), one centred inclusion (viscosity musi,
- * density contrast rhogi) and pure shear ebg. All instances iterate in one cooperative
- * launch; an instance stops when its check (every nout iterations; Stokes2D_param.jl:203-210
- * with one tolerance, norms scaled by ly) reaches eps. */
+ * instance has that script's numerics -- its compute_τ! form (:48-55), buoyancy term (:59)
+ * and uniform iteration parameters from Musτ .= μs0 (:190-192) -- on a box lx x ly
+ * (Stokes2D_ve_param.jl:99-102) with one centred inclusion (viscosity musi, density
+ * contrast rhogi) and pure shear ebg. All instances iterate in one cooperative launch; an
+ * instance stops when its check (every nout iterations; Stokes2D_param.jl:203-210 with one
+ * tolerance, norms scaled by ly) reaches eps, or after its iterMax. */
 typedef struct pts_batch_instance {
     int32_t nx, ny;   /* cells, each >= 3 */
     double lx, ly;    /* box */
@@ -188,8 +188,8 @@ typedef struct pts_batch_desc {
     int32_t nout;      /* check cadence */
     int32_t tile;      /* tile shape 0..3 = 32x4, 32x8, 64x4, 32x16 (pts_batch_set_tile) */
     double eps;        /* tolerance */
-    double iter_max;   /* `iter <= iterMax` */
-    double r, Re, CFL; /* iteration parameters (Stokes2D.jl:82-84) */
+    double iter_max;   /* `iter <= iterMax`; <= 0: 100*max(nx,ny) per instance (Stokes2D_param.jl:146) */
+    double r, Re, CFL; /* iteration parameters (Stokes2D_param.jl:150-152) */
     int32_t reserved[4];
 } pts_batch_desc;
 
@@ -197,15 +197,18 @@ typedef struct pts_batch pts_batch;
 PTS_API int pts_batch_create(const pts_batch_desc* desc, const pts_batch_instance* inst, int32_t n, pts_batch** out);
 PTS_API int pts_batch_destroy(pts_batch* b);
 PTS_API const char* pts_batch_last_error(const pts_batch* b);
-/* ICs, smooth! x10 of Mus and ρg, compute_maxloc! + bc, compute_iter_params! for every instance */
+/* ICs and smooth! x10 of Mus and ρg for every instance (Stokes2D_param.jl:179-189) */
 PTS_API int pts_batch_setup(pts_batch* b);
 PTS_API int pts_batch_set_tile(pts_batch* b, int32_t tile);
 /* The persistent launch (captured in a CUDA graph when the driver allows it): runs until
- * every instance has converged or iter_limit (< 0: desc.iter_max) is passed. Synchronous.
- * iters/err/converged (length n, may be NULL) receive each instance's outcome. */
+ * every instance has converged or passed its iterMax; iter_limit >= 0 is a further ceiling
+ * common to all. Synchronous. iters/err/converged (length n, may be NULL) receive each
+ * instance's outcome; converged is 0 for an instance stopped by iterMax or by NaN (the call
+ * then returns PTS_E_NAN). */
 PTS_API int pts_batch_solve(pts_batch* b, int64_t iter_limit, int64_t* iters, double* err, int32_t* converged,
                             int32_t* used_graph);
-/* A field of one instance (fields Pt Vx Vy τxx τyy τxy Mus Musτ Gdτ dτ_Rho ∇V Rx Ry ρg) */
+/* A field of one instance (fields Pt Vx Vy τxx τyy τxy Mus Musτ Gdτ dτ_Rho ∇V Rx Ry ρg;
+ * Musτ, Gdτ and dτ_Rho are uniform per instance and are returned as that value filled) */
 PTS_API int pts_batch_get_field(pts_batch* b, int32_t instance, int32_t field, double* host, int64_t n);
 PTS_API int pts_batch_stream(pts_batch* b, void** stream);
 

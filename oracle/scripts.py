@@ -185,18 +185,27 @@ class V2D(_Case2D):
 
 
 class V2DSweep(V2D):
-    """One instance of the batched 2D viscous sweep: scripts/Stokes2D.jl's kernels with
-    the buoyancy term of scripts/Stokes2D_param.jl:59 (Ry -= @av_yi(ρg)), a box
-    lx = aspect*ly (scripts/Stokes2D_ve_param.jl:99-102), one centred circular inclusion of
-    radius 1 with viscosity musi and density contrast rhogi, pure shear ebg; Mus and ρg
-    are smoothed alike (Stokes2D_param.jl:184-189). The check is Stokes2D_param.jl's
-    (Vmin/Vmax over Vy, :204-208) with the norms scaled by ly (Stokes2D_ve_param.jl:175-176)
-    and a single tolerance on max(norm_Rx, norm_Ry, norm_∇V)."""
+    """One instance of the batched 2D viscous sweep, with the numerics of the reference's
+    sweep script scripts/Stokes2D_param.jl: its compute_τ! form
+    τ = 2μ_veτ(ε̇ + τ/Gdτ/2), μ_veτ = 1/(1/Gdτ + 1/Mus) (:48-55), its buoyancy term
+    Ry -= @av_yi(ρg) (:59), and uniform iteration parameters from Musτ .= μs0 (:190-192), so
+    Gdτ and dτ_Rho hold one value per instance; a box lx = aspect*ly
+    (scripts/Stokes2D_ve_param.jl:99-102); one centred circular inclusion of radius 1 with
+    viscosity musi and density contrast rhogi; pure shear ebg; Mus and ρg smoothed alike
+    (Stokes2D_param.jl:184-189); iterMax = 100max(nx,ny) unless given (:146). The check is
+    Stokes2D_param.jl's (Vmin/Vmax over Vy, :204-208) with the norms scaled by ly
+    (Stokes2D_ve_param.jl:175-176) and a single tolerance on max(norm_Rx, norm_Ry, norm_∇V).
 
-    defaults = dict(nt=1, iterMax=2e5, nout=200, eps=1e-8, CFL=0.9 / math.sqrt(2), Re=5 * PI, r=1.0, rhogi=0.0)
+    Stokes2D.jl's own form (iteration parameters from the local maxloc of Mus) diverges at
+    the sweep's strongest contrasts (musi ~ 1e-5..1e-6 on 255 and 511 cells); the param
+    script's uniform parameters do not."""
+
+    defaults = dict(nt=1, iterMax=None, nout=200, eps=1e-8, CFL=0.9 / math.sqrt(2), Re=5 * PI, r=1.0, rhogi=0.0)
 
     def setup(self):
         nx, ny = self.nx, self.ny
+        if self.iterMax is None:
+            self.iterMax = 100 * max(nx, ny)
         self.ly = 10.0 if "ly" not in self.p else self.p["ly"]
         self.dx, self.dy = self.lx / nx, self.ly / ny
         self._dx, self._dy = 1.0 / self.dx, 1.0 / self.dy
@@ -229,18 +238,14 @@ class V2DSweep(V2D):
             L.ora2_smooth(arr(rhog2), arr(rhog), 1.0)
             rhog, rhog2 = rhog2, rhog
         self.f["Mus"], self.f["Mus2"], self.f["rhog"], self.f["rhog2"] = Mus, Mus2, rhog, rhog2
-        Must = self.f["Must"]
-        Must[...] = Mus
-        L.ora2_maxloc(arr(Must), arr(Mus))
-        L.ora2_bc_x(arr(Must))
-        L.ora2_bc_y(arr(Must))
+        self.f["Must"][...] = self.mus0  # Musτ .= μs0
         self.iter_params()
         return self
 
     def iteration(self):
         L, A = self.L, self.A
         L.ora2_compute_P(A("divV"), A("Pt"), A("Vx"), A("Vy"), A("Gdt"), self.r, self.dx, self.dy)
-        L.ora2v_compute_tau(A("txx"), A("tyy"), A("txy"), A("Vx"), A("Vy"), A("Mus"), A("Gdt"), self.dx, self.dy)
+        L.ora2s_compute_tau(A("txx"), A("tyy"), A("txy"), A("Vx"), A("Vy"), A("Mus"), A("Gdt"), self.dx, self.dy)
         L.ora2s_compute_dV(A("Rx"), A("Ry"), A("dVx"), A("dVy"), A("Pt"), A("txx"), A("tyy"), A("txy"),
                            A("dtRho"), A("rhog"), self.dx, self.dy)
         L.ora2_compute_V(A("Vx"), A("Vy"), A("dVx"), A("dVy"))

@@ -5,6 +5,11 @@
 // unified layout (px = round_up(nx+1, 16), py = ny+1) and starting on a 256-byte boundary;
 // BInst carries each instance's geometry, numerics, offset and tile range. The tile list
 // depends on the tile shape, which the autotuner picks (pts_batch_set_tile).
+//
+// Numerics are those of the reference's sweep script (scripts/Stokes2D_param.jl): the
+// iteration parameters come from Musτ .= μs0 (:190-192), so Gdτ and dτ_Rho are one number
+// per instance, computed here in compute_iter_params!'s order and held in BInst; no array
+// of Musτ, Gdτ or dτ_Rho is stored or read.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -27,7 +32,6 @@ struct pts_batch {
     Fields64 F{};
     BState st{};
     BInst* d_inst = nullptr;
-    int* d_tile_inst = nullptr;
     std::vector<void*> owned;
     int* h_nactive = nullptr;  // pinned: n, copied to the device at each solve
     cudaGraphExec_t graph = nullptr;
@@ -53,7 +57,7 @@ int bfail(pts_batch* b, int code, const std::string& m) {
 
 Fields64 shifted(const Fields64& F, int64_t off) {
     Fields64 f = F;
-    double** p[] = {&f.Pt, &f.Vx, &f.Vy, &f.txx, &f.tyy, &f.txy, &f.Mus, &f.Must, &f.Gdt, &f.dtRho, &f.divV,
+    double** p[] = {&f.Pt, &f.Vx, &f.Vy, &f.txx, &f.tyy, &f.txy, &f.Mus, &f.divV,
                     &f.Rx, &f.Ry, &f.Mus2, &f.rhog, &f.rhog2};
     for (double** q : p)
         if (*q) *q = *q + off;
@@ -70,22 +74,19 @@ void drop_graph(pts_batch* b) {
 int build_tiles(pts_batch* b) {
     int tx, ty;
     batch_tile_dims(b->tile, &tx, &ty);
-    std::vector<int> tile_inst;
+    int64_t ntiles = 0;
     for (int q = 0; q < b->n; ++q) {
         BInst& I = b->hi[q];
         I.ntx = (I.g.nx + 1 + tx - 1) / tx;
         I.nty = (I.g.ny + 1 + ty - 1) / ty;
-        I.tile0 = (int)tile_inst.size();
-        for (int t = 0; t < I.ntx * I.nty; ++t) tile_inst.push_back(q);
+        I.tile0 = (int)ntiles;
+        ntiles += (int64_t)I.ntx * I.nty;
     }
-    b->ntiles = (int)tile_inst.size();
-    if (b->d_tile_inst) cudaFree(b->d_tile_inst);
+    if (ntiles >= (int64_t)1 << 31) return bfail(b, PTS_E_INVAL, "too many tiles in the sweep");
+    b->ntiles = (int)ntiles;
     if (b->st.partials) cudaFree(b->st.partials);
-    b->d_tile_inst = nullptr;
     b->st.partials = nullptr;
-    BCK(cudaMalloc((void**)&b->d_tile_inst, sizeof(int) * tile_inst.size()));
-    BCK(cudaMalloc((void**)&b->st.partials, sizeof(double) * kCheckSlots * tile_inst.size()));
-    BCK(cudaMemcpy(b->d_tile_inst, tile_inst.data(), sizeof(int) * tile_inst.size(), cudaMemcpyHostToDevice));
+    BCK(cudaMalloc((void**)&b->st.partials, sizeof(double) * kCheckSlots * ntiles));
     BCK(cudaMemcpy(b->d_inst, b->hi.data(), sizeof(BInst) * b->n, cudaMemcpyHostToDevice));
     drop_graph(b);
     return PTS_OK;
@@ -151,6 +152,12 @@ int pts_batch_create(const pts_batch_desc* d, const pts_batch_instance* inst, in
         I.lenRx = (double)(s.nx - 1) * (s.ny - 2);
         I.lenRy = (double)(s.nx - 2) * (s.ny - 1);
         I.lenDiv = (double)s.nx * s.ny;
+        // compute_iter_params! with Musτ = μs0 = 1 (Stokes2D_param.jl:36-40,190-192)
+        const double mus0 = 1.0;
+        I.dR = m.Vpdt * m.max_l / m.Re / mus0;
+        I.Gd = (m.Vpdt * m.Vpdt) / I.dR / (m.r + 2.0);
+        // iterMax = 100max(nx,ny) (Stokes2D_param.jl:146) unless the descriptor sets one
+        I.iter_last = d->iter_max > 0 ? (int64_t)std::floor(d->iter_max) : 100 * (int64_t)std::max(s.nx, s.ny);
         off += (I.g.pxy + 31) / 32 * 32;
     }
     b->total = total;
@@ -165,7 +172,7 @@ int pts_batch_create(const pts_batch_desc* d, const pts_batch_instance* inst, in
         return bail(PTS_E_CUDA);
     }
     Fields64& F = b->F;
-    double** arenas[] = {&F.Pt, &F.Vx, &F.Vy, &F.txx, &F.tyy, &F.txy, &F.Mus, &F.Must, &F.Gdt, &F.dtRho, &F.divV,
+    double** arenas[] = {&F.Pt, &F.Vx, &F.Vy, &F.txx, &F.tyy, &F.txy, &F.Mus, &F.divV,
                          &F.Rx, &F.Ry, &F.Mus2, &F.rhog, &F.rhog2};
     for (double** p : arenas) {
         void* q = nullptr;
@@ -178,22 +185,24 @@ int pts_batch_create(const pts_batch_desc* d, const pts_batch_instance* inst, in
         *p = (double*)q;
         b->owned.push_back(q);
     }
-    void *c1 = nullptr, *c2 = nullptr, *c3 = nullptr, *c4 = nullptr, *c5 = nullptr, *c6 = nullptr;
+    void *c1 = nullptr, *c2 = nullptr, *c3 = nullptr, *c4 = nullptr, *c5 = nullptr, *c6 = nullptr, *c7 = nullptr;
     if (cudaMalloc(&c1, sizeof(int) * n) != cudaSuccess || cudaMalloc(&c2, sizeof(int64_t) * n) != cudaSuccess ||
         cudaMalloc(&c3, sizeof(double) * n) != cudaSuccess || cudaMalloc(&c4, sizeof(int)) != cudaSuccess ||
         cudaMalloc(&c5, sizeof(int)) != cudaSuccess || cudaMalloc(&c6, sizeof(BInst) * n) != cudaSuccess ||
+        cudaMalloc(&c7, sizeof(int) * (2 * (size_t)n + 3)) != cudaSuccess ||
         cudaMallocHost((void**)&b->h_nactive, sizeof(int)) != cudaSuccess) {
         cudaGetLastError();
         b->err = "allocation of the sweep state failed";
         return bail(PTS_E_NOMEM);
     }
-    for (void* p : {c1, c2, c3, c4, c5, c6}) b->owned.push_back(p);
+    for (void* p : {c1, c2, c3, c4, c5, c6, c7}) b->owned.push_back(p);
     b->st.converged = (int*)c1;
     b->st.iters = (int64_t*)c2;
     b->st.err = (double*)c3;
     b->st.nactive = (int*)c4;
     b->st.nan_flag = (int*)c5;
     b->d_inst = (BInst*)c6;
+    b->st.act = (int*)c7;
     *b->h_nactive = n;
     int rc = build_tiles(b);
     if (rc != PTS_OK) return bail(rc);
@@ -211,7 +220,6 @@ int pts_batch_destroy(pts_batch* b) {
     if (b->stream) cudaStreamSynchronize(b->stream);
     drop_graph(b);
     for (void* p : b->owned) cudaFree(p);
-    if (b->d_tile_inst) cudaFree(b->d_tile_inst);
     if (b->st.partials) cudaFree(b->st.partials);
     if (b->h_nactive) cudaFreeHost(b->h_nactive);
     if (b->stream) cudaStreamDestroy(b->stream);
@@ -256,11 +264,6 @@ int pts_batch_setup(pts_batch* b) {
             BCK(launch_smooth(V2D, b->hi[q].g, F.rhog2 + b->hi[q].off, F.rhog + b->hi[q].off, 1.0, b->stream));
         std::swap(F.rhog, F.rhog2);
     }
-    for (int q = 0; q < b->n; ++q) {
-        const BInst& I = b->hi[q];
-        BCK(launch_maxloc(V2D, I.g, F.Must + I.off, F.Mus + I.off, b->stream));
-        BCK(launch_iter_params(V2D, I.g, shifted(F, I.off), I.n, b->stream));
-    }
     drop_graph(b);  // the arenas of Mus and ρg may have swapped
     BCK(cudaStreamSynchronize(b->stream));
     return PTS_OK;
@@ -270,7 +273,9 @@ int pts_batch_solve(pts_batch* b, int64_t iter_limit, int64_t* iters, double* er
                     int32_t* used_graph) {
     if (!b) return PTS_E_INVAL;
     BCK(cudaSetDevice(b->device));
-    const int64_t iter_last = iter_limit >= 0 ? iter_limit : (int64_t)std::floor(b->d.iter_max);
+    int64_t iter_last = iter_limit;  // launch-wide ceiling; each instance also stops at its own
+    if (iter_last < 0)
+        for (const BInst& I : b->hi) iter_last = std::max(iter_last, I.iter_last);
     const int n = b->n;
     auto enqueue = [&]() -> cudaError_t {
         cudaError_t e;
@@ -281,8 +286,8 @@ int pts_batch_solve(pts_batch* b, int64_t iter_limit, int64_t* iters, double* er
         if ((e = cudaMemcpyAsync(b->st.nactive, b->h_nactive, sizeof(int), cudaMemcpyHostToDevice, b->stream)) !=
             cudaSuccess)
             return e;
-        return launch_batch(b->tile, b->d_inst, b->d_tile_inst, b->ntiles, n, b->F, b->st, b->d.nout, iter_last,
-                            b->d.eps, b->stream);
+        return launch_batch(b->tile, b->d_inst, b->ntiles, n, b->F, b->st, b->d.nout, iter_last, b->d.eps,
+                            b->stream);
     };
     int graph_ok = 0;
     if (!b->graph || b->graph_iter_last != iter_last || b->graph_tile != b->tile) {
@@ -315,7 +320,7 @@ int pts_batch_solve(pts_batch* b, int64_t iter_limit, int64_t* iters, double* er
     if (iters) BCK(cudaMemcpy(iters, b->st.iters, sizeof(int64_t) * n, cudaMemcpyDeviceToHost));
     if (err) BCK(cudaMemcpy(err, b->st.err, sizeof(double) * n, cudaMemcpyDeviceToHost));
     if (converged)
-        for (int q = 0; q < n; ++q) converged[q] = conv[q];
+        for (int q = 0; q < n; ++q) converged[q] = conv[q] == 1;
     if (used_graph) *used_graph = graph_ok;
     if (nan_flag) return bfail(b, PTS_E_NAN, "NaN in the check of at least one instance");
     return PTS_OK;
@@ -339,9 +344,14 @@ int pts_batch_get_field(pts_batch* b, int32_t q, int32_t id, double* host, int64
         case PTS_F_TYY: base = F.tyy; e0 = nx; e1 = ny; break;
         case PTS_F_TXY: base = F.txy; e0 = nx - 1; e1 = ny - 1; s0 = s1 = 1; break;
         case PTS_F_MUS: base = F.Mus; e0 = nx; e1 = ny; break;
-        case PTS_F_MUS_TAU: base = F.Must; e0 = nx; e1 = ny; break;
-        case PTS_F_GDTAU: base = F.Gdt; e0 = nx; e1 = ny; break;
-        case PTS_F_DTAU_RHO: base = F.dtRho; e0 = nx; e1 = ny; break;
+        case PTS_F_MUS_TAU:
+        case PTS_F_GDTAU:
+        case PTS_F_DTAU_RHO: {  // uniform per instance: the reference's arrays hold one value
+            if (nel != (int64_t)nx * ny) return bfail(b, PTS_E_INVAL, "wrong element count for this field");
+            const double v = id == PTS_F_MUS_TAU ? 1.0 : id == PTS_F_GDTAU ? I.Gd : I.dR;
+            for (int64_t e = 0; e < nel; ++e) host[e] = v;
+            return PTS_OK;
+        }
         case PTS_F_DIVV: base = F.divV; e0 = nx; e1 = ny; break;
         case PTS_F_RX: base = F.Rx; e0 = nx - 1; e1 = ny - 2; s0 = s1 = 1; break;
         case PTS_F_RY: base = F.Ry; e0 = nx - 2; e1 = ny - 1; s0 = s1 = 1; break;

@@ -135,13 +135,16 @@ struct BInst {
     int64_t off;
     int tile0, ntx, nty;
     double lenRx, lenRy, lenDiv, ly;
+    double Gd, dR;     // the instance's uniform Gdτ and dτ_Rho (Musτ .= μs0)
+    int64_t iter_last; // its PT loop runs while iter <= iter_last (iterMax)
 };
 struct BState {
-    int* converged;   // per instance: its PT loop has ended on the tolerance (or NaN)
+    int* converged;   // per instance: 1 its PT loop has ended on the tolerance, 2 frozen on NaN
     int64_t* iters;   // per instance: PT iterations done
     double* err;      // per instance: err of the last check
     double* partials; // per tile: 8 partial sums/extrema of the check
     int* nactive;     // instances still iterating
+    int* act;         // active list rebuilt at each check: K, T, first tile[K+1], instance[K] (2n+3 ints)
     int* nan_flag;
 };
 constexpr int kBatchTileShapes = 4;
@@ -150,7 +153,7 @@ inline void batch_tile_dims(int tile, int* tx, int* ty) {
     *tx = d[tile][0];
     *ty = d[tile][1];
 }
-cudaError_t launch_batch(int tile, const BInst* d_inst, const int* d_tile_inst, int ntiles, int ninst,
+cudaError_t launch_batch(int tile, const BInst* d_inst, int ntiles, int ninst,
                          const Fields64& F, const BState& st, int nout, int64_t iter_last, double eps, cudaStream_t s);
 // ICs of one sweep instance: Mus/ρg = inclusion (radius2) ? (musi, rhogi) : (1, 0), pure shear ebg
 cudaError_t launch_init_sweep(const Geom& g, const Fields64& f, const Num& n, double musi, double radius2,

@@ -550,14 +550,6 @@ __global__ void k_check_finalize(const double* partials, int nblocks, double lx,
 
 // ------------------------------------------------------------------ batched 2D sweep (persistent)
 
-__device__ __forceinline__ Fields64 shift_fields(const Fields64& F, int64_t off) {
-    Fields64 f = F;
-    double** p[] = {&f.Pt, &f.Vx, &f.Vy, &f.txx, &f.tyy, &f.txy, &f.Mus, &f.Must, &f.Gdt, &f.dtRho, &f.divV,
-                    &f.Rx, &f.Ry, &f.rhog};
-    for (double** q : p) *q = *q + off;
-    return f;
-}
-
 // Block reduction of one Acc into out[0..7] (fixed order, as acc_block_store).
 __device__ void acc_block_store_to(Acc& a, double* out) {
     for (int o = 16; o > 0; o >>= 1) {
@@ -589,57 +581,259 @@ __device__ void acc_block_store_to(Acc& a, double* out) {
     __syncthreads();
 }
 
-// All instances of a sweep iterate in lockstep inside one cooperative launch; a block walks
-// the flattened list of TX x TY tiles (instance by instance) and skips converged
-// instances. Per PT iteration: compute_P! + compute_τ! (Stokes2D.jl:33-44), grid barrier,
-// compute_dV! with the buoyancy term (Stokes2D_param.jl:57-63) + compute_V! + bc_y!/bc_x!
-// (Stokes2D.jl:54-58,133-134), grid barrier. Every nout iterations each instance's check
+// The arrays of the sweep (one arena per field, instances back to back).
+struct SweepF {
+    double *Pt, *Vx, *Vy, *txx, *tyy, *txy, *Mus, *divV, *Rx, *Ry, *rhog;
+};
+__device__ __forceinline__ SweepF sweep_at(const SweepF& F, int64_t off) {
+    return {F.Pt + off,  F.Vx + off,   F.Vy + off, F.txx + off, F.tyy + off, F.txy + off,
+            F.Mus + off, F.divV + off, F.Rx + off, F.Ry + off,  F.rhog + off};
+}
+
+// What a tile of the sweep needs of its instance, loaded into registers when a block's walk
+// enters the instance.
+struct SweepP {
+    int nx, ny, px, ntx, tile0;
+    int64_t off, cap;
+    double dx, dy, r, G, R;  // G = Gdτ, R = dτ_Rho (uniform per instance)
+};
+
+__device__ __forceinline__ SweepP sweep_params(const BInst& I, int64_t iter_last) {
+    SweepP P;
+    P.nx = I.g.nx; P.ny = I.g.ny; P.px = I.g.px; P.ntx = I.ntx; P.tile0 = I.tile0;
+    P.off = I.off;
+    P.cap = I.iter_last < iter_last ? I.iter_last : iter_last;
+    P.dx = I.n.dx; P.dy = I.n.dy; P.r = I.n.r; P.G = I.Gd; P.R = I.dR;
+    return P;
+}
+
+// compute_P! + compute_τ! of the sweep script (Stokes2D_param.jl:42-55) with its uniform
+// iteration parameters (Musτ .= μs0, :190-192): Gdτ is one number G per instance, so
+// @av(Gdτ) is formed from it in the reference's order and no Gdτ array is read. Every load
+// is issued before the first store (the fields are distinct arrays), so a point costs one
+// round trip to memory rather than one per store.
+__device__ __forceinline__ void pt_tau_sweep(const SweepF& f, const SweepP& P, int i, int j, bool store_divV) {
+    if (i >= P.nx || j >= P.ny) return;
+    const idx_t sx = 1, sy = P.px;
+    const idx_t c = i + sy * j;
+    const bool edge = (i >= 1 && j >= 1);
+    const double vx0 = f.Vx[c], vx1 = f.Vx[c + sx], vy0 = f.Vy[c], vy1 = f.Vy[c + sy];
+    const double pt = f.Pt[c], Mc = f.Mus[c], sxx = f.txx[c], syy = f.tyy[c];
+    double m11 = 0.0, m01 = 0.0, m10 = 0.0, vxs = 0.0, vys = 0.0, sxy = 0.0;
+    if (edge) {
+        m11 = f.Mus[c - sx - sy];
+        m01 = f.Mus[c - sy];
+        m10 = f.Mus[c - sx];
+        vxs = f.Vx[c - sy];
+        vys = f.Vy[c - sx];
+        sxy = f.txy[c];
+    }
+    const double G = P.G;
+    const double dvx = vx1 - vx0, dvy = vy1 - vy0;
+    const double dv = dvx / P.dx + dvy / P.dy;
+    const double mu = 1.0 / (1.0 / G + 1.0 / Mc);  // @μ_veτ
+    if (store_divV) f.divV[c] = dv;
+    f.Pt[c] = pt - P.r * G * dv;
+    f.txx[c] = 2.0 * mu * (dvx / P.dx + sxx / G / 2.0);
+    f.tyy[c] = 2.0 * mu * (dvy / P.dy + syy / G / 2.0);
+    if (edge) {
+        const double ag = (((G + G) + G) + G) * 0.25;
+        const double am = (((m11 + m01) + m10) + Mc) * 0.25;
+        const double mua = 1.0 / (1.0 / ag + 1.0 / am);  // @μ_veτ_av
+        const double d1 = vx0 - vxs;                       // @d_yi(Vx)
+        const double d2 = vy0 - vys;                       // @d_xi(Vy)
+        f.txy[c] = 2.0 * mua * (0.5 * (d1 / P.dy + d2 / P.dx) + sxy / ag / 2.0);
+    }
+}
+
+// Rx, Ry of compute_dV! (Stokes2D_param.jl:58-59), Ry with the buoyancy term -@av_yi(ρg)
+__device__ __forceinline__ double res_sweep_x(const SweepF& f, const SweepP& P, idx_t c, idx_t sy) {
+    return ((f.txx[c] - f.txx[c - 1]) / P.dx + (f.txy[c + sy] - f.txy[c]) / P.dy) - (f.Pt[c] - f.Pt[c - 1]) / P.dx;
+}
+__device__ __forceinline__ double res_sweep_y(const SweepF& f, const SweepP& P, idx_t c, idx_t sy) {
+    const double R = ((f.tyy[c] - f.tyy[c - sy]) / P.dy + (f.txy[c + 1] - f.txy[c]) / P.dx) - (f.Pt[c] - f.Pt[c - sy]) / P.dy;
+    return R - (f.rhog[c - sy] + f.rhog[c]) * 0.5;
+}
+
+// compute_dV! + compute_V! + bc_y!(Vx), bc_x!(Vy) of the sweep script (Stokes2D_param.jl:57-81,
+// 198-200) with the uniform dτ_Rho R: @av_xi(dτ_Rho) = (R + R)*0.5. Loads first, as above.
+__device__ __forceinline__ void v_bc_sweep(const SweepF& f, const SweepP& P, int i, int j) {
+    const int nx = P.nx, ny = P.ny;
+    if (i > nx || j > ny) return;
+    const idx_t sx = 1, sy = P.px;
+    const idx_t c = i + sy * j;
+    const bool fx = (j >= 1 && j <= ny - 2), ux = fx && (i >= 1 && i <= nx - 1);
+    const bool fy = (i >= 1 && i <= nx - 2), uy = fy && (j >= 1 && j <= ny - 1);
+    double vx = 0.0, vy = 0.0, Rx = 0.0, Ry = 0.0;
+    if (fx) vx = f.Vx[c];
+    if (fy) vy = f.Vy[c];
+    if (ux) Rx = res_sweep_x(f, P, c, sy);
+    if (uy) Ry = res_sweep_y(f, P, c, sy);
+    const double aR = (P.R + P.R) * 0.5;
+    if (fx) {
+        if (ux) {
+            vx = vx + Rx * aR;
+            f.Vx[c] = vx;
+        }
+        if (j == 1) f.Vx[c - sy] = vx;
+        if (j == ny - 2) f.Vx[c + sy] = vx;
+    }
+    if (fy) {
+        if (uy) {
+            vy = vy + Ry * aR;
+            f.Vy[c] = vy;
+        }
+        if (i == 1) f.Vy[c - sx] = vy;
+        if (i == nx - 2) f.Vy[c + sx] = vy;
+    }
+}
+
+// Active list of the sweep (built by block 0): act[0] = K instances still iterating,
+// act[1] = T their tiles, act[2 .. 2+K] = first virtual tile of each (act[2+K] = T),
+// act[3+n .. 3+n+K) = their instance ids, in instance order.
+__device__ void build_active_list(const BInst* __restrict__ inst, int ninst, const BState& st, int64_t iter,
+                                  int64_t iter_last, int* s_cnt) {
+    const int nt = blockDim.x * blockDim.y, tid = threadIdx.x + blockDim.x * threadIdx.y;
+    const int per = (ninst + nt - 1) / nt, b0 = tid * per, b1 = min(ninst, b0 + per);
+    int k = 0, t = 0;
+    auto active = [&](int b) {
+        const int64_t cap = inst[b].iter_last < iter_last ? inst[b].iter_last : iter_last;
+        return *(volatile const int*)&st.converged[b] == 0 && iter <= cap;
+    };
+    for (int b = b0; b < b1; ++b)
+        if (active(b)) { ++k; t += inst[b].ntx * inst[b].nty; }
+    s_cnt[2 * tid] = k;
+    s_cnt[2 * tid + 1] = t;
+    __syncthreads();
+    if (tid == 0) {  // exclusive scan over the threads' chunks (instance order)
+        int K = 0, T = 0;
+        for (int u = 0; u < nt; ++u) {
+            const int dk = s_cnt[2 * u], dt = s_cnt[2 * u + 1];
+            s_cnt[2 * u] = K;
+            s_cnt[2 * u + 1] = T;
+            K += dk;
+            T += dt;
+        }
+        st.act[0] = K;
+        st.act[1] = T;
+        st.act[2 + K] = T;
+    }
+    __syncthreads();
+    k = s_cnt[2 * tid];
+    t = s_cnt[2 * tid + 1];
+    for (int b = b0; b < b1; ++b)
+        if (active(b)) {
+            st.act[2 + k] = t;
+            st.act[3 + ninst + k] = b;
+            ++k;
+            t += inst[b].ntx * inst[b].nty;
+        }
+    __syncthreads();
+}
+
+// All instances of a sweep iterate in lockstep inside one cooperative launch. Each block
+// walks a contiguous chunk of the active instances' TX x TY tiles (the active list is
+// rebuilt after every check, when instances converge). Per PT iteration: compute_P! +
+// compute_τ!, grid barrier, compute_dV! + compute_V! + bc_y!/bc_x!, grid barrier
+// (Stokes2D_param.jl:195-200). Every nout iterations each instance's check
 // (Stokes2D_param.jl:203-210 with a single tolerance, norms scaled by ly) is reduced in a
 // fixed order from per-tile partials, and an instance whose err <= eps (or NaN) is frozen
-// -- its `while err > ε` loop ended. The launch ends when no instance is active or after
-// iteration iter_last, like `iter <= iterMax`.
+// -- its `while err > ε` loop ended. An instance also ends after its iteration iter_last
+// (`iter <= iterMax`, with the launch-wide iter_last as a ceiling); until the next rebuild
+// its tiles are skipped. nactive counts the instances still iterating; it changes only
+// before a grid barrier, so every block reads the same value at the top of the loop and
+// they all leave together.
+constexpr int kListSmem = 1024;  // active lists up to this many instances are walked from shared memory
+// Resident threads per SM the sweep kernel is compiled for (bounds its registers per thread).
+#ifndef PTS_SWEEP_THREADS_PER_SM
+#define PTS_SWEEP_THREADS_PER_SM 1024
+#endif
 template <int TX, int TY>
-__global__ void __launch_bounds__(TX* TY) k2_batch(const BInst* __restrict__ inst, const int* __restrict__ tile_inst,
-                                                   int ntiles, int ninst, Fields64 F, BState st, int nout,
-                                                   int64_t iter_last, double eps) {
+__global__ void __launch_bounds__(TX* TY, PTS_SWEEP_THREADS_PER_SM / (TX * TY)) k2_batch(const BInst* __restrict__ inst, int ntiles, int ninst, SweepF F,
+                                                   BState st, int nout, int64_t iter_last, double eps) {
+    (void)ntiles;
     cooperative_groups::grid_group grid = cooperative_groups::this_grid();
     const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + TX * ty;
+    __shared__ int s_first[kListSmem + 1];
+    __shared__ int s_id[kListSmem];
+    __shared__ int s_cnt[2 * TX * TY];
+    __shared__ int s_KT[2];
+    const int* g_first = st.act + 2;
+    const int* g_id = st.act + 3 + ninst;
+    int K = 0, T = 0;
+    bool in_smem = false;
+    // the active list of this epoch into shared memory (when it fits)
+    auto load_list = [&]() {
+        if (tid == 0) {
+            s_KT[0] = *(volatile int*)&st.act[0];
+            s_KT[1] = *(volatile int*)&st.act[1];
+        }
+        __syncthreads();
+        K = s_KT[0];
+        T = s_KT[1];
+        in_smem = K <= kListSmem;
+        if (in_smem) {
+            for (int u = tid; u <= K; u += TX * TY) s_first[u] = ((volatile const int*)g_first)[u];
+            for (int u = tid; u < K; u += TX * TY) s_id[u] = ((volatile const int*)g_id)[u];
+        }
+        __syncthreads();
+    };
+    auto first_at = [&](int k) { return in_smem ? s_first[k] : ((volatile const int*)g_first)[k]; };
+    auto id_at = [&](int k) { return in_smem ? s_id[k] : ((volatile const int*)g_id)[k]; };
+    // body(P, b, t, i, j) for every point of this block's chunk of the active tiles
+    auto walk = [&](auto&& body) {
+        const int chunk = (T + (int)gridDim.x - 1) / (int)gridDim.x;
+        const int v0 = (int)blockIdx.x * chunk, v1 = min(T, v0 + chunk);
+        if (v0 >= v1) return;
+        int lo = 0, hi = K - 1;  // last k with first_at(k) <= v0
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (first_at(mid) <= v0) lo = mid;
+            else hi = mid - 1;
+        }
+        int k = lo, b = id_at(k), f0 = first_at(k), f1 = first_at(k + 1);
+        SweepP P = sweep_params(inst[b], iter_last);
+        for (int v = v0; v < v1; ++v) {
+            if (v >= f1) {
+                do { ++k; f0 = f1; f1 = first_at(k + 1); } while (v >= f1);
+                b = id_at(k);
+                P = sweep_params(inst[b], iter_last);
+            }
+            const int q = v - f0;
+            body(P, b, P.tile0 + q, (q % P.ntx) * TX + tx, (q / P.ntx) * TY + ty);
+        }
+    };
+    if (blockIdx.x == 0) build_active_list(inst, ninst, st, 0, iter_last, s_cnt);
+    grid.sync();
+    load_list();
     int64_t iter = 0;
     for (;;) {
         if (*(volatile int*)st.nactive == 0 || iter > iter_last) break;
         const bool chk = ((iter + 1) % nout == 0);
-        for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-            const int b = tile_inst[t];
-            if (st.converged[b]) continue;
-            const BInst& I = inst[b];
-            const int q = t - I.tile0;
-            pt_tau_2d<V2D>(I.g, shift_fields(F, I.off), I.n, (q % I.ntx) * TX + tx, (q / I.ntx) * TY + ty,
-                           ROLE_P | ROLE_TAU, chk ? 1 : 0);
-        }
+        walk([&](const SweepP& P, int, int, int i, int j) {
+            if (iter <= P.cap) pt_tau_sweep(sweep_at(F, P.off), P, i, j, chk);
+        });
         grid.sync();
-        for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-            const int b = tile_inst[t];
-            if (st.converged[b]) continue;
-            const BInst& I = inst[b];
-            const int q = t - I.tile0;
-            v_bc_2d<V2D, true>(I.g, shift_fields(F, I.off), I.n, (q % I.ntx) * TX + tx, (q / I.ntx) * TY + ty, 1);
+        walk([&](const SweepP& P, int, int, int i, int j) {
+            if (iter <= P.cap) v_bc_sweep(sweep_at(F, P.off), P, i, j);
+        });
+        // an instance doing its last allowed iteration leaves the active count here
+        for (int b = blockIdx.x * TX * TY + tid; b < ninst; b += gridDim.x * TX * TY) {
+            const int64_t cap = inst[b].iter_last < iter_last ? inst[b].iter_last : iter_last;
+            if (!st.converged[b] && iter == cap) atomicSub(st.nactive, 1);
         }
         grid.sync();
         ++iter;
         if (!chk) continue;
-        // per-tile partials of the check
-        for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-            const int b = tile_inst[t];
-            if (st.converged[b]) continue;
-            const BInst& I = inst[b];
-            const int q = t - I.tile0;
-            const int i = (q % I.ntx) * TX + tx, j = (q / I.ntx) * TY + ty;
-            const int nx = I.g.nx, ny = I.g.ny;
-            const Fields64 f = shift_fields(F, I.off);
+        // per-tile partials of the check (instances that did this iteration)
+        walk([&](const SweepP& P, int, int t, int i, int j) {
+            if (iter > P.cap + 1) return;
+            const int nx = P.nx, ny = P.ny;
+            const SweepF f = sweep_at(F, P.off);
             Acc a;
             acc_init(a);
-            const idx_t c = gidx32(I.g, i, j, 0);
-            const idx_t sx = 1, sy = I.g.px;
+            const idx_t sy = P.px;
+            const idx_t c = i + sy * j;
             if (i < nx && j <= ny) {
                 const double vy = f.Vy[c];
                 a.vmin = vy;
@@ -651,23 +845,24 @@ __global__ void __launch_bounds__(TX* TY) k2_batch(const BInst* __restrict__ ins
                 a.s[3] = dv * dv;
             }
             if (i >= 1 && i <= nx - 1 && j >= 1 && j <= ny - 2) {
-                const double R = res2_x<false>(f, I.n, c, sx, sy);
+                const double R = res_sweep_x(f, P, c, sy);
                 f.Rx[c] = R;
                 a.s[0] = R * R;
             }
             if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 1) {
-                const double R = res2_y<false, true>(f, I.n, c, sx, sy);
+                const double R = res_sweep_y(f, P, c, sy);
                 f.Ry[c] = R;
                 a.s[1] = R * R;
             }
             acc_block_store_to(a, st.partials + (int64_t)t * kCheckSlots);
-        }
+        });
         grid.sync();
         // per-instance finalisation: one block per instance, fixed-order reduction
         __shared__ double red[TX * TY][kCheckSlots];
         for (int b = blockIdx.x; b < ninst; b += gridDim.x) {
-            if (st.converged[b]) continue;
             const BInst& I = inst[b];
+            const int64_t cap = I.iter_last < iter_last ? I.iter_last : iter_last;
+            if (st.converged[b] || iter > cap + 1) continue;
             const int nt = I.ntx * I.nty;
             double r[kCheckSlots] = {0.0, 0.0, 0.0, 0.0, DBL_MAX, -DBL_MAX, DBL_MAX, -DBL_MAX};
             for (int u = tid; u < nt; u += TX * TY) {
@@ -697,17 +892,22 @@ __global__ void __launch_bounds__(TX* TY) k2_batch(const BInst* __restrict__ ins
                 st.iters[b] = iter;
                 if (bad) atomicExch(st.nan_flag, 1);
                 if (!(err > eps)) {
-                    st.converged[b] = 1;
-                    atomicSub(st.nactive, 1);
+                    st.converged[b] = bad ? 2 : 1;                 // 2: frozen on NaN
+                    if (iter <= cap) atomicSub(st.nactive, 1);  // else already left at its cap
                 }
             }
             __syncthreads();
         }
         grid.sync();
+        if (blockIdx.x == 0) build_active_list(inst, ninst, st, iter, iter_last, s_cnt);
+        grid.sync();
+        load_list();
     }
-    // instances whose loop ended on iter_max: iterations done = iter
-    for (int b = blockIdx.x * TX * TY + tid; b < ninst; b += gridDim.x * TX * TY)
-        if (!st.converged[b]) st.iters[b] = iter;
+    // instances whose loop ended on iterMax: iterations done = iter_last + 1
+    for (int b = blockIdx.x * TX * TY + tid; b < ninst; b += gridDim.x * TX * TY) {
+        const int64_t cap = inst[b].iter_last < iter_last ? inst[b].iter_last : iter_last;
+        if (!st.converged[b]) st.iters[b] = iter < cap + 1 ? iter : cap + 1;
+    }
 }
 
 // ------------------------------------------------------------------ mixed precision: FP64 outer step
@@ -1014,8 +1214,9 @@ cudaError_t launch_init_sweep(const Geom& g, const Fields64& f, const Num& n, do
 }
 
 template <int TX, int TY>
-static cudaError_t launch_batch_t(const BInst* d_inst, const int* d_tile_inst, int ntiles, int ninst, Fields64 F,
-                                  BState st, int nout, int64_t iter_last, double eps, cudaStream_t s) {
+static cudaError_t launch_batch_t(const BInst* d_inst, int ntiles, int ninst, const Fields64& F64, BState st,
+                                  int nout, int64_t iter_last, double eps, cudaStream_t s) {
+    SweepF F{F64.Pt, F64.Vx, F64.Vy, F64.txx, F64.tyy, F64.txy, F64.Mus, F64.divV, F64.Rx, F64.Ry, F64.rhog};
     int per_sm = 0, dev = 0, nsm = 0;
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k2_batch<TX, TY>, TX * TY, 0);
     if (e != cudaSuccess) return e;
@@ -1025,18 +1226,18 @@ static cudaError_t launch_batch_t(const BInst* d_inst, const int* d_tile_inst, i
     const int want = ntiles > ninst ? ntiles : ninst;
     if (grid > want) grid = want;
     if (grid < 1) return cudaErrorInvalidConfiguration;
-    void* args[] = {(void*)&d_inst, (void*)&d_tile_inst, (void*)&ntiles, (void*)&ninst, (void*)&F,
-                    (void*)&st,     (void*)&nout,        (void*)&iter_last, (void*)&eps};
+    void* args[] = {(void*)&d_inst, (void*)&ntiles,    (void*)&ninst, (void*)&F,
+                    (void*)&st,     (void*)&nout,      (void*)&iter_last, (void*)&eps};
     return cudaLaunchCooperativeKernel((const void*)k2_batch<TX, TY>, dim3(grid), dim3(TX, TY), args, 0, s);
 }
 
-cudaError_t launch_batch(int tile, const BInst* d_inst, const int* d_tile_inst, int ntiles, int ninst,
+cudaError_t launch_batch(int tile, const BInst* d_inst, int ntiles, int ninst,
                          const Fields64& F, const BState& st, int nout, int64_t iter_last, double eps, cudaStream_t s) {
     switch (tile) {
-        case 0: return launch_batch_t<32, 4>(d_inst, d_tile_inst, ntiles, ninst, F, st, nout, iter_last, eps, s);
-        case 1: return launch_batch_t<32, 8>(d_inst, d_tile_inst, ntiles, ninst, F, st, nout, iter_last, eps, s);
-        case 2: return launch_batch_t<64, 4>(d_inst, d_tile_inst, ntiles, ninst, F, st, nout, iter_last, eps, s);
-        case 3: return launch_batch_t<32, 16>(d_inst, d_tile_inst, ntiles, ninst, F, st, nout, iter_last, eps, s);
+        case 0: return launch_batch_t<32, 4>(d_inst, ntiles, ninst, F, st, nout, iter_last, eps, s);
+        case 1: return launch_batch_t<32, 8>(d_inst, ntiles, ninst, F, st, nout, iter_last, eps, s);
+        case 2: return launch_batch_t<64, 4>(d_inst, ntiles, ninst, F, st, nout, iter_last, eps, s);
+        case 3: return launch_batch_t<32, 16>(d_inst, ntiles, ninst, F, st, nout, iter_last, eps, s);
         default: return cudaErrorInvalidValue;
     }
 }

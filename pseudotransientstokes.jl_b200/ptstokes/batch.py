@@ -40,8 +40,10 @@ def sweep_instances(n=256, seed=1855, sizes=(63, 127, 255, 511), ly=10.0):
 
 
 class Batch:
-    def __init__(self, instances, nout=200, eps=1e-8, iter_max=2e5, tile=1, r=1.0, Re=5 * math.pi,
+    def __init__(self, instances, nout=200, eps=1e-8, iter_max=0, tile=1, r=1.0, Re=5 * math.pi,
                  CFL=0.9 / math.sqrt(2), lib=None):
+        """`iter_max` <= 0 gives each instance the sweep script's iterMax = 100max(nx,ny)
+        (scripts/Stokes2D_param.jl:146); a positive value is a common iterMax."""
         self.lib = lib or _abi.load()
         self.instances = [dict(d) for d in instances]
         n = len(self.instances)
@@ -89,14 +91,20 @@ class Batch:
         self._ck(self.lib.pts_batch_stream(self.h, ctypes.byref(s)))
         return s.value or 0
 
-    def solve(self, iter_limit=-1):
+    def solve(self, iter_limit=-1, raise_on_nan=True):
+        """Run the sweep. An instance whose check gives NaN is frozen there (converged False);
+        with raise_on_nan the call then raises PtsError(PTS_E_NAN), else the result has
+        nan=True and the other instances' outcomes stand."""
         n = self.n
         iters = (ctypes.c_int64 * n)()
         err = (ctypes.c_double * n)()
         conv = (ctypes.c_int32 * n)()
         graph = ctypes.c_int32()
-        self._ck(self.lib.pts_batch_solve(self.h, int(iter_limit), iters, err, conv, ctypes.byref(graph)))
-        return dict(iters=list(iters), err=list(err), converged=[bool(c) for c in conv], used_graph=bool(graph.value))
+        rc = self.lib.pts_batch_solve(self.h, int(iter_limit), iters, err, conv, ctypes.byref(graph))
+        if rc != 0 and (raise_on_nan or rc != _abi.PTS_E_NAN):
+            self._ck(rc)
+        return dict(iters=list(iters), err=list(err), converged=[bool(c) for c in conv], used_graph=bool(graph.value),
+                    nan=rc == _abi.PTS_E_NAN)
 
     def shape(self, q, name):
         nx, ny = self.instances[q]["nx"], self.instances[q]["ny"]

@@ -3,6 +3,8 @@
 Each instance of the batch must equal, bit for bit, the oracle's single-instance run of
 the same problem (oracle.scripts.V2DSweep): the same iteration count to tolerance and
 the same fields. The tile shape chosen by the autotuner must not change any result.
+Instances that do not converge stop at their own iterMax inside the shared launch, and a
+NaN in one instance freezes that instance only.
 """
 import numpy as np
 import pytest
@@ -66,4 +68,44 @@ def test_batch_autotune_and_iter_limit(gpu_lib, tmp_path, monkeypatch):
     o = oracle_case(CASES[2], nout=100, iterMax=150).run()
     assert res["iters"][2] == o.iters[0] == 151
     assert np.array_equal(b.get(2, "Pt"), o.f["Pt"])
+    b.close()
+
+
+@pytest.mark.gpu
+def test_batch_each_instance_stops_at_its_own_iter_max(gpu_lib):
+    """eps = 1e-300 is never reached: every instance runs to iterMax = 100max(nx,ny)
+    (Stokes2D_param.jl:146), i.e. 100max(nx,ny) + 1 iterations, all in one launch."""
+    from ptstokes.batch import Batch
+    cases = [dict(nx=15, ny=11, lx=13.6, ly=10.0, musi=1e-3, radius2=1.0, rhogi=0.0, ebg=1.0),
+             dict(nx=23, ny=17, lx=13.5, ly=10.0, musi=1e-5, radius2=1.0, rhogi=1.0, ebg=0.0),
+             dict(nx=31, ny=9, lx=34.0, ly=10.0, musi=1e-2, radius2=1.0, rhogi=1.0, ebg=0.0)]
+    b = Batch(cases, nout=100, eps=1e-300, iter_max=0, lib=gpu_lib).setup()
+    res = b.solve()
+    assert res["iters"] == [1501, 2301, 3101] and not any(res["converged"])
+    for q, d in enumerate(cases):
+        o = oracle_case(d, nout=100, eps=1e-300).run()
+        assert o.iters[0] == res["iters"][q]
+        for name in ("Pt", "Vx", "Vy", "txy"):
+            assert np.array_equal(b.get(q, name), o.f[name]), (q, name)
+    b.close()
+
+
+@pytest.mark.gpu
+def test_batch_nan_freezes_only_its_instance(gpu_lib):
+    """A NaN density in one instance makes its check NaN: that instance is frozen and
+    reported as not converged, the call reports PTS_E_NAN, the other instance converges
+    exactly as it does alone."""
+    from ptstokes import PtsError
+    from ptstokes.batch import Batch
+    good = CASES[1]
+    bad = dict(good, rhogi=float("nan"))
+    b = Batch([good, bad], nout=100, eps=1e-8, iter_max=2e5, lib=gpu_lib).setup()
+    res = b.solve(raise_on_nan=False)
+    assert res["nan"] and res["converged"] == [True, False] and res["iters"][1] == 100
+    o = oracle_case(good, nout=100, iterMax=2e5).run()
+    assert res["iters"][0] == o.iters[0]
+    assert np.array_equal(b.get(0, "Vy"), o.f["Vy"])
+    b.setup()
+    with pytest.raises(PtsError):
+        b.solve()
     b.close()
