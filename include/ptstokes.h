@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define PTS_ABI_VERSION 1
+#define PTS_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define PTS_API __attribute__((visibility("default")))
@@ -75,7 +75,8 @@ typedef struct pts_desc {
     double iter_max;    /* `while err > ε && iter <= iterMax` */
     int32_t mixed_inner;    /* MIXED: FP32 sweeps between FP64 corrections; 0 => nout */
     int32_t single_pass;    /* 3D: 1 = one-launch-per-iteration staged kernel, 0 = two launches */
-    int32_t reserved[6];
+    int32_t adjoint;        /* PTS_3D_V: 1 = solve the transposed (adjoint) system, see below */
+    int32_t reserved[5];
 } pts_desc;
 
 /* Fields, by the reference's names. Extents are the reference's (pts_field_shape). */
@@ -92,6 +93,10 @@ enum pts_field {
     PTS_F_RX, PTS_F_RY, PTS_F_RZ,
     PTS_F_DVX, PTS_F_DVY, PTS_F_DVZ,
     PTS_F_RHOG,     /* ρg (batched sweep only)            */
+    /* Momentum sources on the interior faces (extents of Rx, Ry, Rz), added to the residual:
+     * R = ∇·τ − ∇P + F. Absent (zero) until first set; 3D_V and 3D_VE_PERF, FP64 two-kernel path. */
+    PTS_F_FX, PTS_F_FY, PTS_F_FZ,
+    PTS_F_GRAD,     /* ∂J/∂log μ per cell (nx, ny, nz), written by pts_gradient_logmu */
     PTS_F_COUNT
 };
 
@@ -165,6 +170,28 @@ PTS_API int pts_solve(pts_ctx* ctx, pts_solve_info* info);
  * `for it = 1:nt` (Stokes3D_ve_perf.jl:194-226). iters_per_step (length nt) may be NULL;
  * info (may be NULL) receives the last step's outcome with iters = ittot. */
 PTS_API int pts_run(pts_ctx* ctx, int32_t nt, int64_t* iters_per_step, pts_solve_info* info);
+
+/* ---- adjoint of the 3D viscous solve (PTS_3D_V, FP64) ----
+ * No counterpart in the reference. The converged PTS_3D_V iterate solves A(μ)[V;P] = b with
+ * A = [[K, -G], [div∘B, 0]]: B extends the interior velocities to the free-slip ghosts by
+ * copying, the walls' normal velocities are data, K = D·2μ·S·B (S the strain rates, D the
+ * stress divergence on the interior faces). The copies make K unsymmetric, so the adjoint
+ * of a misfit J(V) solves the transposed system: a PTS_3D_V context created with
+ * desc.adjoint = 1 and the same Mus, zero fields and the momentum source F = ∂J/∂V
+ * (PTS_F_FX/FY/FZ), solved with pts_solve. In that mode the ghosts stay zero (no copies)
+ * and the residual of every ghost face -- the same stencil, reading zeros where no stress
+ * point exists -- is added to the residual of the interior face it copies (the transpose of
+ * the copy). Then, with λ the adjoint velocity,
+ *   ∂J/∂log μ_c = -μ_c [2 Σ_n ε̇_n(V) ε̇_n(λ) + Σ_{edges e around c} ε̇_s(V) ε̇_s(λ)]
+ * (normal rates on the cells compute_τ! updates, shear rates on the interior edges, each
+ * edge averaging 4 cells), with log μ the viscosity the solver uses (after any smoothing). */
+/* τ = 2·Mus·ε̇(V) (the fixed point of compute_τ!), then the check: Rx, Ry, Rz = ∇·τ − ∇P + F
+ * (folded onto the interior faces in adjoint mode) and ∇V of the current fields -- one
+ * application of A or its transpose, for symmetry tests. Synchronous. */
+PTS_API int pts_apply_operator(pts_ctx* ctx, pts_check* out);
+/* ∂J/∂log μ into fwd's PTS_F_GRAD from fwd's V (the forward solution) and adj's V (the adjoint
+ * solution of an adjoint-mode context); same grid, both PTS_3D_V FP64. Synchronous. */
+PTS_API int pts_gradient_logmu(pts_ctx* fwd, pts_ctx* adj);
 
 /* ---- batched 2D viscous sweep: many uneven grids, one persistent launch ----
  * Replaces the reference's parameter sweeps, which run one Julia process per instance

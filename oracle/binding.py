@@ -73,6 +73,11 @@ _SIGS = {
     "ora3_compute_V": [Arr] * 6,
     "ora3p_compute_Pt_tau": [Arr] * 18 + [_D] * 6 + [_I],
     "ora3p_compute_V": [Arr] * 11 + [_D] * 3,
+    "ora3p_compute_V_src": [Arr] * 14 + [_D] * 3,
+    "ora3v_tau_exact": [Arr] * 10 + [_D] * 3,
+    "ora3v_grad_logmu": [Arr] * 8 + [_D] * 3,
+    "ora3v_res_adj": [Arr] * 10 + [_D] * 3,
+    "ora3v_update_V": [Arr] * 10,
     "ora3p_compute_Res": [Arr] * 14 + [_D] * 3,
     "ora_stats": [Arr, ctypes.POINTER(_D), ctypes.POINTER(_D), ctypes.POINTER(_D)],
     "ora_num_threads": [],

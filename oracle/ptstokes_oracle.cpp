@@ -704,6 +704,214 @@ void ora3p_compute_V(oarr Vx_, oarr Vy_, oarr Vz_, oarr Pt_, oarr txx_, oarr tyy
             }
 }
 
+// compute_V! with momentum sources (adjoint solves; no reference counterpart): as
+// ora3p_compute_V with V += (R + F)*@av(dτ_Rho), F on the interior faces (extents of Rx, Ry, Rz).
+void ora3p_compute_V_src(oarr Vx_, oarr Vy_, oarr Vz_, oarr Pt_, oarr txx_, oarr tyy_, oarr tzz_, oarr txy_,
+                         oarr txz_, oarr tyz_, oarr dtRho_, oarr Fx_, oarr Fy_, oarr Fz_, double _dx, double _dy,
+                         double _dz) {
+    F3 Vx(Vx_), Vy(Vy_), Vz(Vz_), Pt(Pt_), txx(txx_), tyy(tyy_), tzz(tzz_), txy(txy_), txz(txz_), tyz(tyz_), d(dtRho_),
+        Fx(Fx_), Fy(Fy_), Fz(Fz_);
+    const int64_t nx = Pt.n1, ny = Pt.n2, nz = Pt.n3;
+    const int64_t nx_1 = nx - 1, nx_2 = nx - 2, ny_1 = ny - 1, ny_2 = ny - 2, nz_1 = nz - 1, nz_2 = nz - 2;
+#pragma omp parallel for schedule(static)
+    for (int64_t iz = 1; iz <= nz_1; ++iz)
+        for (int64_t iy = 1; iy <= ny_1; ++iy)
+            for (int64_t ix = 1; ix <= nx_1; ++ix) {
+                if (ix <= nx_1 && iy <= ny_2 && iz <= nz_2) {
+                    const double R = _dx * (txx(ix + 1, iy, iz) - txx(ix, iy, iz)) + _dy * (txy(ix, iy + 1, iz) - txy(ix, iy, iz)) +
+                                     _dz * (txz(ix, iy, iz + 1) - txz(ix, iy, iz)) - _dx * (Pt(ix + 1, iy + 1, iz + 1) - Pt(ix, iy + 1, iz + 1));
+                    Vx(ix + 1, iy + 1, iz + 1) = Vx(ix + 1, iy + 1, iz + 1) +
+                                                 (R + Fx(ix, iy, iz)) * ((d(ix, iy + 1, iz + 1) + d(ix + 1, iy + 1, iz + 1)) * 0.5);
+                }
+                if (ix <= nx_2 && iy <= ny_1 && iz <= nz_2) {
+                    const double R = _dy * (tyy(ix, iy + 1, iz) - tyy(ix, iy, iz)) + _dx * (txy(ix + 1, iy, iz) - txy(ix, iy, iz)) +
+                                     _dz * (tyz(ix, iy, iz + 1) - tyz(ix, iy, iz)) - _dy * (Pt(ix + 1, iy + 1, iz + 1) - Pt(ix + 1, iy, iz + 1));
+                    Vy(ix + 1, iy + 1, iz + 1) = Vy(ix + 1, iy + 1, iz + 1) +
+                                                 (R + Fy(ix, iy, iz)) * ((d(ix + 1, iy, iz + 1) + d(ix + 1, iy + 1, iz + 1)) * 0.5);
+                }
+                if (ix <= nx_2 && iy <= ny_2 && iz <= nz_1) {
+                    const double R = _dz * (tzz(ix, iy, iz + 1) - tzz(ix, iy, iz)) + _dx * (txz(ix + 1, iy, iz) - txz(ix, iy, iz)) +
+                                     _dy * (tyz(ix, iy + 1, iz) - tyz(ix, iy, iz)) - _dz * (Pt(ix + 1, iy + 1, iz + 1) - Pt(ix + 1, iy + 1, iz));
+                    Vz(ix + 1, iy + 1, iz + 1) = Vz(ix + 1, iy + 1, iz + 1) +
+                                                 (R + Fz(ix, iy, iz)) * ((d(ix + 1, iy + 1, iz) + d(ix + 1, iy + 1, iz + 1)) * 0.5);
+                }
+            }
+}
+
+// τ = 2·Mus·ε̇(V), the fixed point of the viscous compute_Pt_τ! update (explicit-index _dx form;
+// shear rates 0.5*(_dy*∂Vx + _dx*∂Vy) with the 4-cell average of Mus as in :57-62).
+void ora3v_tau_exact(oarr txx_, oarr tyy_, oarr tzz_, oarr txy_, oarr txz_, oarr tyz_, oarr Vx_, oarr Vy_, oarr Vz_,
+                     oarr Mus_, double _dx, double _dy, double _dz) {
+    F3 txx(txx_), tyy(tyy_), tzz(tzz_), txy(txy_), txz(txz_), tyz(tyz_), Vx(Vx_), Vy(Vy_), Vz(Vz_), M(Mus_);
+#pragma omp parallel for schedule(static)
+    for (int64_t iz = 1; iz <= M.n3; ++iz)
+        for (int64_t iy = 1; iy <= M.n2; ++iy)
+            for (int64_t ix = 1; ix <= M.n1; ++ix) {
+                if (ix <= txx.n1 && iy <= txx.n2 && iz <= txx.n3)
+                    txx(ix, iy, iz) = 2.0 * M(ix, iy + 1, iz + 1) * (_dx * (Vx(ix + 1, iy + 1, iz + 1) - Vx(ix, iy + 1, iz + 1)));
+                if (ix <= tyy.n1 && iy <= tyy.n2 && iz <= tyy.n3)
+                    tyy(ix, iy, iz) = 2.0 * M(ix + 1, iy, iz + 1) * (_dy * (Vy(ix + 1, iy + 1, iz + 1) - Vy(ix + 1, iy, iz + 1)));
+                if (ix <= tzz.n1 && iy <= tzz.n2 && iz <= tzz.n3)
+                    tzz(ix, iy, iz) = 2.0 * M(ix + 1, iy + 1, iz) * (_dz * (Vz(ix + 1, iy + 1, iz + 1) - Vz(ix + 1, iy + 1, iz)));
+                if (ix <= txy.n1 && iy <= txy.n2 && iz <= txy.n3) {
+                    const double am = (M(ix, iy, iz + 1) + M(ix + 1, iy, iz + 1) + M(ix, iy + 1, iz + 1) + M(ix + 1, iy + 1, iz + 1)) * 0.25;
+                    txy(ix, iy, iz) = 2.0 * am * (0.5 * (_dy * (Vx(ix + 1, iy + 1, iz + 1) - Vx(ix + 1, iy, iz + 1)) +
+                                                         _dx * (Vy(ix + 1, iy + 1, iz + 1) - Vy(ix, iy + 1, iz + 1))));
+                }
+                if (ix <= txz.n1 && iy <= txz.n2 && iz <= txz.n3) {
+                    const double am = (M(ix, iy + 1, iz) + M(ix + 1, iy + 1, iz) + M(ix, iy + 1, iz + 1) + M(ix + 1, iy + 1, iz + 1)) * 0.25;
+                    txz(ix, iy, iz) = 2.0 * am * (0.5 * (_dz * (Vx(ix + 1, iy + 1, iz + 1) - Vx(ix + 1, iy + 1, iz)) +
+                                                         _dx * (Vz(ix + 1, iy + 1, iz + 1) - Vz(ix, iy + 1, iz + 1))));
+                }
+                if (ix <= tyz.n1 && iy <= tyz.n2 && iz <= tyz.n3) {
+                    const double am = (M(ix + 1, iy, iz) + M(ix + 1, iy + 1, iz) + M(ix + 1, iy, iz + 1) + M(ix + 1, iy + 1, iz + 1)) * 0.25;
+                    tyz(ix, iy, iz) = 2.0 * am * (0.5 * (_dz * (Vy(ix + 1, iy + 1, iz + 1) - Vy(ix + 1, iy + 1, iz)) +
+                                                         _dy * (Vz(ix + 1, iy + 1, iz + 1) - Vz(ix + 1, iy, iz + 1))));
+                }
+            }
+}
+
+// Residual of the transposed (adjoint) system at the interior faces of a 3D_V problem (no
+// reference counterpart). With B the free-slip extension (ghost faces copy their clamped
+// interior face), the adjoint of the momentum rows sums, at each interior face, its own
+// residual and those of the ghost faces copying it; a ghost's residual is the interior
+// stencil with zero wherever it reaches a stress point that does not exist. Order: own,
+// ghosts below/above along the first tangential axis, along the second, then corners.
+// Written with 0-based unified coordinates: a field's element (a,b,c) sits at reference
+// index (a-s0+1, b-s1+1, c-s2+1) for the field's start (s0,s1,s2) (zero outside its extents).
+void ora3v_res_adj(oarr Rx_, oarr Ry_, oarr Rz_, oarr Pt_, oarr txx_, oarr tyy_, oarr tzz_, oarr txy_, oarr txz_,
+                   oarr tyz_, double _dx, double _dy, double _dz) {
+    F3 Rx(Rx_), Ry(Ry_), Rz(Rz_), P(Pt_), txx(txx_), tyy(tyy_), tzz(tzz_), txy(txy_), txz(txz_), tyz(tyz_);
+    const int64_t nx = P.n1, ny = P.n2, nz = P.n3;
+    auto T = [](const F3& A, int s0, int s1, int s2, int64_t a, int64_t b, int64_t c) -> double {
+        const int64_t u = a - s0 + 1, v = b - s1 + 1, w = c - s2 + 1;
+        if (u < 1 || u > A.n1 || v < 1 || v > A.n2 || w < 1 || w > A.n3) return 0.0;
+        return A(u, v, w);
+    };
+    auto rx = [&](int64_t i, int64_t j, int64_t k) {
+        return ((_dx * (T(txx, 0, 1, 1, i, j, k) - T(txx, 0, 1, 1, i - 1, j, k)) +
+                 _dy * (T(txy, 1, 1, 1, i, j + 1, k) - T(txy, 1, 1, 1, i, j, k))) +
+                _dz * (T(txz, 1, 1, 1, i, j, k + 1) - T(txz, 1, 1, 1, i, j, k))) -
+               _dx * (T(P, 0, 0, 0, i, j, k) - T(P, 0, 0, 0, i - 1, j, k));
+    };
+    auto ry = [&](int64_t i, int64_t j, int64_t k) {
+        return ((_dy * (T(tyy, 1, 0, 1, i, j, k) - T(tyy, 1, 0, 1, i, j - 1, k)) +
+                 _dx * (T(txy, 1, 1, 1, i + 1, j, k) - T(txy, 1, 1, 1, i, j, k))) +
+                _dz * (T(tyz, 1, 1, 1, i, j, k + 1) - T(tyz, 1, 1, 1, i, j, k))) -
+               _dy * (T(P, 0, 0, 0, i, j, k) - T(P, 0, 0, 0, i, j - 1, k));
+    };
+    auto rz = [&](int64_t i, int64_t j, int64_t k) {
+        return ((_dz * (T(tzz, 1, 1, 0, i, j, k) - T(tzz, 1, 1, 0, i, j, k - 1)) +
+                 _dx * (T(txz, 1, 1, 1, i + 1, j, k) - T(txz, 1, 1, 1, i, j, k))) +
+                _dy * (T(tyz, 1, 1, 1, i, j + 1, k) - T(tyz, 1, 1, 1, i, j, k))) -
+               _dz * (T(P, 0, 0, 0, i, j, k) - T(P, 0, 0, 0, i, j, k - 1));
+    };
+    // fold over (a, b): the two tangential coordinates with interior range [1, ahi] x [1, bhi]
+    auto fold = [](auto&& at, int64_t a, int64_t b, int64_t ahi, int64_t bhi) {
+        const int64_t ga0 = (a == 1) ? 0 : -1, ga1 = (a == ahi) ? ahi + 1 : -1;
+        const int64_t gb0 = (b == 1) ? 0 : -1, gb1 = (b == bhi) ? bhi + 1 : -1;
+        double R = at(a, b);
+        if (ga0 >= 0) R = R + at(ga0, b);
+        if (ga1 >= 0) R = R + at(ga1, b);
+        if (gb0 >= 0) R = R + at(a, gb0);
+        if (gb1 >= 0) R = R + at(a, gb1);
+        if (ga0 >= 0 && gb0 >= 0) R = R + at(ga0, gb0);
+        if (ga0 >= 0 && gb1 >= 0) R = R + at(ga0, gb1);
+        if (ga1 >= 0 && gb0 >= 0) R = R + at(ga1, gb0);
+        if (ga1 >= 0 && gb1 >= 0) R = R + at(ga1, gb1);
+        return R;
+    };
+#pragma omp parallel for schedule(static)
+    for (int64_t k = 1; k <= nz - 1; ++k)
+        for (int64_t j = 1; j <= ny - 1; ++j)
+            for (int64_t i = 1; i <= nx - 1; ++i) {
+                if (j <= ny - 2 && k <= nz - 2)
+                    Rx(i, j, k) = fold([&](int64_t a, int64_t b) { return rx(i, a, b); }, j, k, ny - 2, nz - 2);
+                if (i <= nx - 2 && k <= nz - 2)
+                    Ry(i, j, k) = fold([&](int64_t a, int64_t b) { return ry(a, j, b); }, i, k, nx - 2, nz - 2);
+                if (i <= nx - 2 && j <= ny - 2)
+                    Rz(i, j, k) = fold([&](int64_t a, int64_t b) { return rz(a, b, k); }, i, j, nx - 2, ny - 2);
+            }
+}
+
+// V += (R + F)*@av(dτ_Rho) on the interior faces from given residuals (the adjoint-mode V
+// update; no free-slip copies). R and F have the extents of Rx, Ry, Rz.
+void ora3v_update_V(oarr Vx_, oarr Vy_, oarr Vz_, oarr Rx_, oarr Ry_, oarr Rz_, oarr Fx_, oarr Fy_, oarr Fz_,
+                    oarr dtRho_) {
+    F3 Vx(Vx_), Vy(Vy_), Vz(Vz_), Rx(Rx_), Ry(Ry_), Rz(Rz_), Fx(Fx_), Fy(Fy_), Fz(Fz_), d(dtRho_);
+    const int64_t nx = d.n1, ny = d.n2, nz = d.n3;
+#pragma omp parallel for schedule(static)
+    for (int64_t iz = 1; iz <= nz - 1; ++iz)
+        for (int64_t iy = 1; iy <= ny - 1; ++iy)
+            for (int64_t ix = 1; ix <= nx - 1; ++ix) {
+                if (iy <= ny - 2 && iz <= nz - 2)
+                    Vx(ix + 1, iy + 1, iz + 1) = Vx(ix + 1, iy + 1, iz + 1) +
+                                                 (Rx(ix, iy, iz) + Fx(ix, iy, iz)) * ((d(ix, iy + 1, iz + 1) + d(ix + 1, iy + 1, iz + 1)) * 0.5);
+                if (ix <= nx - 2 && iz <= nz - 2)
+                    Vy(ix + 1, iy + 1, iz + 1) = Vy(ix + 1, iy + 1, iz + 1) +
+                                                 (Ry(ix, iy, iz) + Fy(ix, iy, iz)) * ((d(ix + 1, iy, iz + 1) + d(ix + 1, iy + 1, iz + 1)) * 0.5);
+                if (ix <= nx - 2 && iy <= ny - 2)
+                    Vz(ix + 1, iy + 1, iz + 1) = Vz(ix + 1, iy + 1, iz + 1) +
+                                                 (Rz(ix, iy, iz) + Fz(ix, iy, iz)) * ((d(ix + 1, iy + 1, iz) + d(ix + 1, iy + 1, iz + 1)) * 0.5);
+            }
+}
+
+// ∂J/∂log μ per cell for the 3D viscous operator (no reference counterpart), from the forward
+// velocity V and the adjoint velocity L (the transposed system's solution, zero ghosts):
+//   g_c = -Mus_c (2 Σ_n ε̇_n(V) ε̇_n(L) + Σ_{edges around c} ε̇_s(V) ε̇_s(L)),
+// normal rates on the cells where compute_τ! updates them, shear rates on the interior edges
+// (each averaging 4 cells). Written with 0-based cell coordinates (i,j,k); a face or edge
+// takes the coordinates of the cell above it.
+void ora3v_grad_logmu(oarr grad_, oarr Vx_, oarr Vy_, oarr Vz_, oarr Lx_, oarr Ly_, oarr Lz_, oarr Mus_, double _dx,
+                      double _dy, double _dz) {
+    F3 G(grad_), Vx(Vx_), Vy(Vy_), Vz(Vz_), Lx(Lx_), Ly(Ly_), Lz(Lz_), M(Mus_);
+    const int64_t nx = M.n1, ny = M.n2, nz = M.n3;
+    auto at = [](const F3& A, int64_t i, int64_t j, int64_t k) { return A(i + 1, j + 1, k + 1); };
+    auto rxy = [&](const F3& X, const F3& Y, int64_t i, int64_t j, int64_t k) {
+        return 0.5 * (_dy * (at(X, i, j, k) - at(X, i, j - 1, k)) + _dx * (at(Y, i, j, k) - at(Y, i - 1, j, k)));
+    };
+    auto rxz = [&](const F3& X, const F3& Z, int64_t i, int64_t j, int64_t k) {
+        return 0.5 * (_dz * (at(X, i, j, k) - at(X, i, j, k - 1)) + _dx * (at(Z, i, j, k) - at(Z, i - 1, j, k)));
+    };
+    auto ryz = [&](const F3& Y, const F3& Z, int64_t i, int64_t j, int64_t k) {
+        return 0.5 * (_dz * (at(Y, i, j, k) - at(Y, i, j, k - 1)) + _dy * (at(Z, i, j, k) - at(Z, i, j - 1, k)));
+    };
+#pragma omp parallel for schedule(static)
+    for (int64_t k = 0; k < nz; ++k)
+        for (int64_t j = 0; j < ny; ++j)
+            for (int64_t i = 0; i < nx; ++i) {
+                double nrm = 0.0, shr = 0.0;
+                if (j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2)
+                    nrm = nrm + (_dx * (at(Vx, i + 1, j, k) - at(Vx, i, j, k))) * (_dx * (at(Lx, i + 1, j, k) - at(Lx, i, j, k)));
+                if (i >= 1 && i <= nx - 2 && k >= 1 && k <= nz - 2)
+                    nrm = nrm + (_dy * (at(Vy, i, j + 1, k) - at(Vy, i, j, k))) * (_dy * (at(Ly, i, j + 1, k) - at(Ly, i, j, k)));
+                if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2)
+                    nrm = nrm + (_dz * (at(Vz, i, j, k + 1) - at(Vz, i, j, k))) * (_dz * (at(Lz, i, j, k + 1) - at(Lz, i, j, k)));
+                if (k >= 1 && k <= nz - 2)
+                    for (int dj = 0; dj < 2; ++dj)
+                        for (int di = 0; di < 2; ++di) {
+                            const int64_t ie = i + di, je = j + dj;
+                            if (ie < 1 || ie > nx - 1 || je < 1 || je > ny - 1) continue;
+                            shr = shr + rxy(Vx, Vy, ie, je, k) * rxy(Lx, Ly, ie, je, k);
+                        }
+                if (j >= 1 && j <= ny - 2)
+                    for (int dk = 0; dk < 2; ++dk)
+                        for (int di = 0; di < 2; ++di) {
+                            const int64_t ie = i + di, ke = k + dk;
+                            if (ie < 1 || ie > nx - 1 || ke < 1 || ke > nz - 1) continue;
+                            shr = shr + rxz(Vx, Vz, ie, j, ke) * rxz(Lx, Lz, ie, j, ke);
+                        }
+                if (i >= 1 && i <= nx - 2)
+                    for (int dk = 0; dk < 2; ++dk)
+                        for (int dj = 0; dj < 2; ++dj) {
+                            const int64_t je = j + dj, ke = k + dk;
+                            if (je < 1 || je > ny - 1 || ke < 1 || ke > nz - 1) continue;
+                            shr = shr + ryz(Vy, Vz, i, je, ke) * ryz(Ly, Lz, i, je, ke);
+                        }
+                G(i + 1, j + 1, k + 1) = -(at(M, i, j, k) * (2.0 * nrm + shr));
+            }
+}
+
 // compute_Res! (Stokes3D_ve_perf.jl:90-96): ∇V from the current V plus Rx, Ry, Rz.
 void ora3p_compute_Res(oarr divV_, oarr Rx_, oarr Ry_, oarr Rz_, oarr Vx_, oarr Vy_, oarr Vz_, oarr Pt_, oarr txx_,
                        oarr tyy_, oarr tzz_, oarr txy_, oarr txz_, oarr tyz_, double _dx, double _dy, double _dz) {

@@ -453,10 +453,68 @@ class VE3DPerf(_Case3D):
 
 
 class V3D(VE3DPerf):
-    """3D viscous Stokes: the fused 3D kernels without elastic terms (no reference script)."""
+    """3D viscous Stokes: the fused 3D kernels without elastic terms (no reference script).
+
+    Adjoint support (no reference counterpart): momentum sources F added to the residual
+    (set_sources), one application of the operator -- τ = 2με̇(V), then R = ∇·τ − ∇P + F and
+    ∇V (apply_operator) -- and ∂J/∂log μ from this case's V and an adjoint case's V
+    (grad_logmu). With adjoint=True the case iterates the transposed system: the free-slip
+    ghosts stay zero and each ghost face's residual is added to the interior face it copies
+    (ora3v_res_adj)."""
 
     elastic = False
-    defaults = dict(nt=1, iterMax=2e5, nout=200, eps=1e-8, CFL=0.8 / math.sqrt(3), Re=6 * PI, r=1.0)
+    defaults = dict(nt=1, iterMax=2e5, nout=200, eps=1e-8, CFL=0.8 / math.sqrt(3), Re=6 * PI, r=1.0,
+                    adjoint=False)
+
+    def clear_state(self):
+        """Zero V, Pt and τ (walls and ghosts included): the adjoint's initial state."""
+        for n in ("Pt", "Vx", "Vy", "Vz", "txx", "tyy", "tzz", "txy", "txz", "tyz"):
+            self.f[n][...] = 0.0
+
+    def set_sources(self, Fx, Fy, Fz):
+        for name, a in (("Fx", Fx), ("Fy", Fy), ("Fz", Fz)):
+            assert a.shape == self.f["R" + name[1]].shape
+            self.f[name] = np.asfortranarray(a, dtype=np.float64)
+
+    def iteration(self):
+        L, A = self.L, self.A
+        if not self.adjoint and "Fx" not in self.f:
+            return super().iteration()
+        L.ora3p_compute_Pt_tau(A("Pt"), *self._tau(), *self._tau_o(), A("Vx"), A("Vy"), A("Vz"), A("Mus"), A("Gdt"),
+                               self.r, self.G, self.dt, self._dx, self._dy, self._dz, 0)
+        if self.adjoint:
+            if "Fx" not in self.f:
+                self.set_sources(*(np.zeros_like(self.f["R" + c]) for c in "xyz"))
+            L.ora3v_res_adj(A("Rx"), A("Ry"), A("Rz"), A("Pt"), *self._tau(), self._dx, self._dy, self._dz)
+            L.ora3v_update_V(A("Vx"), A("Vy"), A("Vz"), A("Rx"), A("Ry"), A("Rz"), A("Fx"), A("Fy"), A("Fz"),
+                             A("dtRho"))
+            return
+        L.ora3p_compute_V_src(A("Vx"), A("Vy"), A("Vz"), A("Pt"), *self._tau(), A("dtRho"), A("Fx"), A("Fy"),
+                              A("Fz"), self._dx, self._dy, self._dz)
+        self.bc()
+
+    def check(self):
+        A = self.A
+        self.L.ora3p_compute_Res(A("divV"), A("Rx"), A("Ry"), A("Rz"), A("Vx"), A("Vy"), A("Vz"), A("Pt"),
+                                 *self._tau(), self._dx, self._dy, self._dz)
+        if self.adjoint:
+            self.L.ora3v_res_adj(A("Rx"), A("Ry"), A("Rz"), A("Pt"), *self._tau(), self._dx, self._dy, self._dz)
+        if "Fx" in self.f:
+            for c in "xyz":
+                self.f["R" + c][...] = self.f["R" + c] + self.f["F" + c]
+        return self.norm_err(("Rx", "Ry", "Rz"), "divV")
+
+    def apply_operator(self):
+        A = self.A
+        self.L.ora3v_tau_exact(*self._tau(), A("Vx"), A("Vy"), A("Vz"), A("Mus"), self._dx, self._dy, self._dz)
+        return self.check()
+
+    def grad_logmu(self, adj):
+        g = zeros(self.nx, self.ny, self.nz)
+        A, B = self.A, adj.A
+        self.L.ora3v_grad_logmu(arr(g), A("Vx"), A("Vy"), A("Vz"), B("Vx"), B("Vy"), B("Vz"), A("Mus"), self._dx,
+                                self._dy, self._dz)
+        return g
 
 
 VARIANTS = {

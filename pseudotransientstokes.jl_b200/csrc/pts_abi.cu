@@ -69,6 +69,11 @@ struct FInfo {
     int s[3];      // unified start of the reference's element [1,1,1]
 };
 
+// Momentum sources exist for the 3D explicit-index variants on the FP64 two-kernel path.
+bool has_sources(const pts_ctx* c) {
+    return (c->v == PTS_3D_V || c->v == PTS_3D_VE_PERF) && !c->mixed && !c->fused;
+}
+
 // Field table: reference extents (Stokes3D_ve_perf.jl:141-162, Stokes2D_ve_perf.jl:105-118)
 // and where each field's first element sits in the unified staggered layout.
 bool field_info(pts_ctx* c, int id, FInfo* o) {
@@ -127,6 +132,10 @@ bool field_info(pts_ctx* c, int id, FInfo* o) {
             if (!d3) return false;
             set(id == PTS_F_RZ ? &f.Rz : &f.dVz, nx - 2, ny - 2, nz - 1, 1, 1, 1);
             break;
+        case PTS_F_FX: if (!has_sources(c)) return false; set(&f.Fx, nx - 1, ny - 2, nz - 2, 1, 1, 1); break;
+        case PTS_F_FY: if (!has_sources(c)) return false; set(&f.Fy, nx - 2, ny - 1, nz - 2, 1, 1, 1); break;
+        case PTS_F_FZ: if (!has_sources(c)) return false; set(&f.Fz, nx - 2, ny - 2, nz - 1, 1, 1, 1); break;
+        case PTS_F_GRAD: if (c->v != PTS_3D_V) return false; set(&f.grad, nx, ny, nz, 0, 0, 0); break;
         default: return false;
     }
     return true;
@@ -152,6 +161,20 @@ void drop_graph(pts_ctx* c) {
             cudaGraphExecDestroy(g);
             g = nullptr;
         }
+}
+
+// The first source set allocates all three (zero) and switches the V update and the check
+// to their source-adding forms (the captured graphs are dropped).
+int ensure_sources(pts_ctx* c, int id) {
+    if (id != PTS_F_FX && id != PTS_F_FY && id != PTS_F_FZ) return PTS_OK;
+    if (!has_sources(c)) return fail(c, PTS_E_INVAL, "momentum sources need 3D_V or 3D_VE_PERF on the FP64 two-kernel path");
+    if (c->f.Fx) return PTS_OK;
+    int rc;
+    if ((rc = alloc_field(c, &c->f.Fx)) != PTS_OK || (rc = alloc_field(c, &c->f.Fy)) != PTS_OK ||
+        (rc = alloc_field(c, &c->f.Fz)) != PTS_OK)
+        return rc;
+    drop_graph(c);
+    return PTS_OK;
 }
 
 // The ten fields one PT iteration rewrites (Pt, τ, V): the single-pass kernel reads them
@@ -345,6 +368,8 @@ int pts_create(const pts_desc* d, pts_ctx** out) {
         return fail(nullptr, PTS_E_INVAL, "grid extent too large");
     if (d->nout < 1) return fail(nullptr, PTS_E_INVAL, "nout must be >= 1");
     if (!(d->lx > 0) || !(d->ly > 0) || (d3 && !(d->lz > 0))) return fail(nullptr, PTS_E_INVAL, "domain extents must be > 0");
+    if (d->adjoint && (d->variant != PTS_3D_V || d->precision != PTS_FP64 || d->single_pass))
+        return fail(nullptr, PTS_E_INVAL, "adjoint mode is implemented for PTS_3D_V in FP64 on the two-kernel path");
     c = new pts_ctx();
     c->d = *d;
     c->v = d->variant;
@@ -379,6 +404,7 @@ int pts_create(const pts_desc* d, pts_ctx** out) {
     n.Re = d->Re;
     n.Vpdt = (d3 ? std::min(std::min(n.dx, n.dy), n.dz) : std::min(n.dx, n.dy)) * d->CFL;
     n.max_l = d->max_l > 0 ? d->max_l : (d3 ? std::max(std::max(d->lx, d->ly), d->lz) : std::max(d->lx, d->ly));
+    n.adjoint = d->adjoint ? 1 : 0;
     int rc = PTS_OK;
     auto bail = [&](int code) {
         g_create_err = c->err;
@@ -502,6 +528,7 @@ int pts_set_field(pts_ctx* c, int32_t id, const double* host, int64_t n) {
     if ((id == PTS_F_DVX || id == PTS_F_DVY || id == PTS_F_DVZ) && field_info(c, id, &fi) &&
         (rc = alloc_field(c, fi.ptr)) != PTS_OK)
         return rc;
+    if ((rc = ensure_sources(c, id)) != PTS_OK) return rc;
     return copy3d(c, id, host, nullptr, n, cudaMemcpyHostToDevice);
 }
 
@@ -516,6 +543,7 @@ int pts_set_field_device(pts_ctx* c, int32_t id, const double* dev, int64_t n) {
     int rc = enter(c);
     if (rc) return rc;
     if (!dev) return fail(c, PTS_E_INVAL, "null device pointer");
+    if ((rc = ensure_sources(c, id)) != PTS_OK) return rc;
     return copy3d(c, id, dev, nullptr, n, cudaMemcpyDeviceToDevice);
 }
 
@@ -591,6 +619,7 @@ int pts_compute_tau(pts_ctx* c) {
 int pts_compute_dV(pts_ctx* c) {
     int rc = enter(c);
     if (rc) return rc;
+    if (c->n.adjoint) return fail(c, PTS_E_INVAL, "adjoint mode iterates with pts_compute_V_bc / pts_iterate / pts_solve");
     double** dv[] = {&c->f.dVx, &c->f.dVy, &c->f.dVz};
     for (int q = 0; q < (c->d3 ? 3 : 2); ++q)
         if ((rc = alloc_field(c, dv[q])) != PTS_OK) return rc;
@@ -601,6 +630,7 @@ int pts_compute_dV(pts_ctx* c) {
 int pts_compute_V(pts_ctx* c) {
     int rc = enter(c);
     if (rc) return rc;
+    if (c->n.adjoint) return fail(c, PTS_E_INVAL, "adjoint mode iterates with pts_compute_V_bc / pts_iterate / pts_solve");
     if (!c->f.dVx) return fail(c, PTS_E_STATE, "compute_V needs dV: call pts_compute_dV first");
     CK(launch_add_dV(c->v, c->g, c->f, c->stream));
     return PTS_OK;
@@ -609,6 +639,7 @@ int pts_compute_V(pts_ctx* c) {
 int pts_apply_bc(pts_ctx* c) {
     int rc = enter(c);
     if (rc) return rc;
+    if (c->n.adjoint) return fail(c, PTS_E_INVAL, "adjoint mode keeps the ghosts at zero: no free-slip copies");
     CK(launch_V_bc(c->v, c->g, c->f, c->n, false, c->stream));
     return PTS_OK;
 }
@@ -634,6 +665,35 @@ int pts_compute_res(pts_ctx* c, pts_check* out) {
     if ((rc = synced(c)) != PTS_OK) return rc;
     if (out) to_check(*c->h_result, out);
     return c->h_result->flag_nan != 0.0 ? fail(c, PTS_E_NAN, "NaN in the residual check") : PTS_OK;
+}
+
+int pts_apply_operator(pts_ctx* c, pts_check* out) {
+    int rc = enter(c);
+    if (rc) return rc;
+    if (c->v != PTS_3D_V || c->mixed) return fail(c, PTS_E_INVAL, "pts_apply_operator needs 3D_V in FP64");
+    CK(launch_tau_exact(c->g, c->f, c->n, c->stream));
+    if ((rc = enqueue_check(c)) != PTS_OK) return rc;
+    if ((rc = synced(c)) != PTS_OK) return rc;
+    if (out) to_check(*c->h_result, out);
+    return PTS_OK;
+}
+
+int pts_gradient_logmu(pts_ctx* fwd, pts_ctx* adj) {
+    pts_ctx* c = fwd;
+    int rc = enter(c);
+    if (rc) return rc;
+    if (!adj) return fail(c, PTS_E_INVAL, "null adjoint context");
+    if (c->v != PTS_3D_V || adj->v != PTS_3D_V || c->mixed || adj->mixed)
+        return fail(c, PTS_E_INVAL, "pts_gradient_logmu needs two 3D_V contexts in FP64");
+    if (c->n.adjoint || !adj->n.adjoint)
+        return fail(c, PTS_E_INVAL, "pts_gradient_logmu takes a forward context and an adjoint-mode context");
+    if (adj->g.nx != c->g.nx || adj->g.ny != c->g.ny || adj->g.nz != c->g.nz || adj->n.dx != c->n.dx ||
+        adj->n.dy != c->n.dy || adj->n.dz != c->n.dz || adj->device != c->device)
+        return fail(c, PTS_E_INVAL, "forward and adjoint contexts differ in grid, spacing or device");
+    if ((rc = alloc_field(c, &c->f.grad)) != PTS_OK) return rc;
+    CK(cudaStreamSynchronize(adj->stream));
+    CK(launch_grad_logmu(c->g, c->f, adj->f, c->n, c->stream));
+    return synced(c);
 }
 
 int pts_iterate(pts_ctx* c, int64_t niter) {

@@ -58,6 +58,7 @@ struct Num {
     double r, G, dt, gdt;  // gdt = G*dt
     double Vpdt, max_l, Re;
     double lx, ly, lz;
+    int adjoint;  // 3D_V: iterate the transposed (adjoint) system, ghosts folded (pts_abi.cu)
 };
 
 template <typename T>
@@ -69,6 +70,8 @@ struct FieldsT {
     T *Rx, *Ry, *Rz, *dVx, *dVy, *dVz;
     T *Mus2;
     T *rhog, *rhog2;  // buoyancy ρg of the batched sweep (Stokes2D_param.jl), else null
+    T *Fx, *Fy, *Fz;  // momentum sources on interior faces (adjoint solves), else null
+    T *grad;          // ∂J/∂log μ per cell, else null
 };
 using Fields64 = FieldsT<double>;
 
@@ -97,6 +100,11 @@ cudaError_t launch_init_inclusion(int variant, const Geom& g, const Fields64& f,
 cudaError_t launch_smooth(int variant, const Geom& g, double* dst, const double* src, double fact, cudaStream_t s);
 cudaError_t launch_maxloc(int variant, const Geom& g, double* must, const double* mus, cudaStream_t s);
 cudaError_t launch_iter_params(int variant, const Geom& g, const Fields64& f, const Num& n, cudaStream_t s);
+// ---- adjoint of the 3D viscous solve (3D_V) ----
+// τ = 2·Mus·ε̇(V), the converged value of compute_τ! (the exact viscous operator's stresses)
+cudaError_t launch_tau_exact(const Geom& g, const Fields64& f, const Num& n, cudaStream_t s);
+// ∂J/∂log μ into fwd.grad, from the forward solution (fwd) and the adjoint solution (adj)
+cudaError_t launch_grad_logmu(const Geom& g, const Fields64& fwd, const Fields64& adj, const Num& n, cudaStream_t s);
 // single-pass 3D kernel: V update of iteration n from `cur`, then Pt/τ of n+1, into `nxt`
 // `err` is a device flag the kernel sets if one of its bounded staging waits timed out.
 cudaError_t launch_fused3(int variant, const Geom& g, const Fields64& cur, const Fields64& nxt, const Num& n,

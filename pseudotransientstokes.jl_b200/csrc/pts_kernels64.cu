@@ -144,6 +144,43 @@ __device__ __forceinline__ double res3_z(const Fields64& f, const Num& n, idx_t 
            dsc<PERF>(f.Pt[c] - f.Pt[c - sz], n.dz, n._dz);
 }
 
+// Residual of the transposed system at an interior face (adjoint mode of 3D_V): the face's
+// own residual plus those of the free-slip ghost faces that copy it -- the transpose of the
+// copy. A ghost's stencil is the interior one; where it reaches a stress point that does
+// not exist the array holds zero (compute_τ! never writes outside its ranges). Summed in a
+// fixed order: own, ghosts below/above along the first tangential axis, along the second,
+// then the corner ghosts. AX = 0, 1, 2 for Vx (tangential y, z), Vy (x, z), Vz (x, y).
+template <int AX>
+__device__ __forceinline__ double res3_fold(const Geom& g, const Fields64& f, const Num& n, int i, int j, int k) {
+    const idx_t sx = 1, sy = g.px, sz = (idx_t)g.pxy;
+    auto R_at = [&](int ii, int jj, int kk) -> double {
+        const idx_t cc = gidx32(g, ii, jj, kk);
+        if (AX == 0) return res3_x<true>(f, n, cc, sx, sy, sz);
+        if (AX == 1) return res3_y<true>(f, n, cc, sx, sy, sz);
+        return res3_z<true>(f, n, cc, sx, sy, sz);
+    };
+    // tangential coordinates (a, b) and their interior bounds [1, ahi], [1, bhi]
+    const int a = (AX == 0) ? j : i, b = (AX == 2) ? j : k;
+    const int ahi = (AX == 0) ? g.ny - 2 : g.nx - 2, bhi = (AX == 2) ? g.ny - 2 : g.nz - 2;
+    auto at = [&](int aa, int bb) -> double {
+        if (AX == 0) return R_at(i, aa, bb);
+        if (AX == 1) return R_at(aa, j, bb);
+        return R_at(aa, bb, k);
+    };
+    const int ga0 = (a == 1) ? 0 : -1, ga1 = (a == ahi) ? ahi + 1 : -1;
+    const int gb0 = (b == 1) ? 0 : -1, gb1 = (b == bhi) ? bhi + 1 : -1;
+    double R = at(a, b);
+    if (ga0 >= 0) R = R + at(ga0, b);
+    if (ga1 >= 0) R = R + at(ga1, b);
+    if (gb0 >= 0) R = R + at(a, gb0);
+    if (gb1 >= 0) R = R + at(a, gb1);
+    if (ga0 >= 0 && gb0 >= 0) R = R + at(ga0, gb0);
+    if (ga0 >= 0 && gb1 >= 0) R = R + at(ga0, gb1);
+    if (ga1 >= 0 && gb0 >= 0) R = R + at(ga1, gb0);
+    if (ga1 >= 0 && gb1 >= 0) R = R + at(ga1, gb1);
+    return R;
+}
+
 // Free-slip copies folded into the update: a face whose tangential indices are the first
 // or last interior ones also writes its value onto the adjacent boundary faces. The
 // reference's bc_x!/bc_y!/bc_z! calls copy whole planes in sequence
@@ -165,8 +202,11 @@ __device__ __forceinline__ void bc_copies(double* A, idx_t c, double v, int a, i
 }
 
 // compute_V! (perf: Stokes3D_ve_perf.jl:83-88; roles: compute_dV! + compute_V!,
-// Stokes3D_ve_multixpu.jl:79-91) with the six bc copies, one thread per face point.
-template <bool PERF>
+// Stokes3D_ve_multixpu.jl:79-91) with the six bc copies, one thread per face point. With
+// SRC the momentum sources F join the residual: V += (R + F)*@av(dτ_Rho). With ADJ
+// (adjoint mode, explicit-index form only) the residual is the folded one and the ghosts
+// are not written (they stay zero).
+template <bool PERF, bool SRC = false, bool ADJ = false>
 __global__ void __launch_bounds__(256) k3_V_bc(Geom g, Fields64 f, Num n, int update) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -179,33 +219,40 @@ __global__ void __launch_bounds__(256) k3_V_bc(Geom g, Fields64 f, Num n, int up
     if (j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2) {
         double v = f.Vx[c];
         if (update && i >= 1 && i <= nx - 1) {
-            v = v + res3_x<PERF>(f, n, c, sx, sy, sz) * ((f.dtRho[c - sx] + f.dtRho[c]) * 0.5);
+            const double R0 = ADJ ? res3_fold<0>(g, f, n, i, j, k) : res3_x<PERF>(f, n, c, sx, sy, sz);
+            const double R = SRC ? R0 + f.Fx[c] : R0;
+            v = v + R * ((f.dtRho[c - sx] + f.dtRho[c]) * 0.5);
             f.Vx[c] = v;
         }
-        bc_copies(f.Vx, c, v, j, 1, ny - 2, sy, k, 1, nz - 2, sz);
+        if (!ADJ) bc_copies(f.Vx, c, v, j, 1, ny - 2, sy, k, 1, nz - 2, sz);
     }
     // Vy: source faces i in [1,nx-2], k in [1,nz-2]; updated for j in [1,ny-1]
     if (i >= 1 && i <= nx - 2 && k >= 1 && k <= nz - 2) {
         double v = f.Vy[c];
         if (update && j >= 1 && j <= ny - 1) {
-            v = v + res3_y<PERF>(f, n, c, sx, sy, sz) * ((f.dtRho[c - sy] + f.dtRho[c]) * 0.5);
+            const double R0 = ADJ ? res3_fold<1>(g, f, n, i, j, k) : res3_y<PERF>(f, n, c, sx, sy, sz);
+            const double R = SRC ? R0 + f.Fy[c] : R0;
+            v = v + R * ((f.dtRho[c - sy] + f.dtRho[c]) * 0.5);
             f.Vy[c] = v;
         }
-        bc_copies(f.Vy, c, v, i, 1, nx - 2, sx, k, 1, nz - 2, sz);
+        if (!ADJ) bc_copies(f.Vy, c, v, i, 1, nx - 2, sx, k, 1, nz - 2, sz);
     }
     // Vz: source faces i in [1,nx-2], j in [1,ny-2]; updated for k in [1,nz-1]
     if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2) {
         double v = f.Vz[c];
         if (update && k >= 1 && k <= nz - 1) {
-            v = v + res3_z<PERF>(f, n, c, sx, sy, sz) * ((f.dtRho[c - sz] + f.dtRho[c]) * 0.5);
+            const double R0 = ADJ ? res3_fold<2>(g, f, n, i, j, k) : res3_z<PERF>(f, n, c, sx, sy, sz);
+            const double R = SRC ? R0 + f.Fz[c] : R0;
+            v = v + R * ((f.dtRho[c - sz] + f.dtRho[c]) * 0.5);
             f.Vz[c] = v;
         }
-        bc_copies(f.Vz, c, v, i, 1, nx - 2, sx, j, 1, ny - 2, sy);
+        if (!ADJ) bc_copies(f.Vz, c, v, i, 1, nx - 2, sx, j, 1, ny - 2, sy);
     }
 }
 
-// compute_dV! alone (Stokes3D_ve_multixpu.jl:79-84): dV = R*@av_xi(dτ_Rho) at interior faces.
-template <bool PERF>
+// compute_dV! alone (Stokes3D_ve_multixpu.jl:79-84): dV = R*@av_xi(dτ_Rho) at interior faces
+// (R + F with SRC).
+template <bool PERF, bool SRC = false>
 __global__ void k3_dV(Geom g, Fields64 f, Num n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -215,11 +262,14 @@ __global__ void k3_dV(Geom g, Fields64 f, Num n) {
     const idx_t c = gidx32(g, i, j, k);
     const idx_t sx = 1, sy = g.px, sz = (idx_t)g.pxy;
     if (i >= 1 && i <= nx - 1 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2)
-        f.dVx[c] = res3_x<PERF>(f, n, c, sx, sy, sz) * ((f.dtRho[c - sx] + f.dtRho[c]) * 0.5);
+        f.dVx[c] = (SRC ? res3_x<PERF>(f, n, c, sx, sy, sz) + f.Fx[c] : res3_x<PERF>(f, n, c, sx, sy, sz)) *
+                   ((f.dtRho[c - sx] + f.dtRho[c]) * 0.5);
     if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 1 && k >= 1 && k <= nz - 2)
-        f.dVy[c] = res3_y<PERF>(f, n, c, sx, sy, sz) * ((f.dtRho[c - sy] + f.dtRho[c]) * 0.5);
+        f.dVy[c] = (SRC ? res3_y<PERF>(f, n, c, sx, sy, sz) + f.Fy[c] : res3_y<PERF>(f, n, c, sx, sy, sz)) *
+                   ((f.dtRho[c - sy] + f.dtRho[c]) * 0.5);
     if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 1)
-        f.dVz[c] = res3_z<PERF>(f, n, c, sx, sy, sz) * ((f.dtRho[c - sz] + f.dtRho[c]) * 0.5);
+        f.dVz[c] = (SRC ? res3_z<PERF>(f, n, c, sx, sy, sz) + f.Fz[c] : res3_z<PERF>(f, n, c, sx, sy, sz)) *
+                   ((f.dtRho[c - sz] + f.dtRho[c]) * 0.5);
 }
 
 // compute_V! alone (Stokes3D_ve_multixpu.jl:86-91): @inn(V) = @inn(V) + @all(dV).
@@ -422,8 +472,9 @@ __device__ void acc_block_store(Acc& a, double* out) {
 }
 
 // 3D check: compute_Res! (perf: ∇V from the current V) / stored ∇V (roles), the residual
-// arrays and the per-block partial norms and extrema. Blocks stride over z.
-template <bool PERF>
+// arrays (R + F with SRC, folded with ADJ) and the per-block partial norms and extrema.
+// Blocks stride over z.
+template <bool PERF, bool SRC = false, bool ADJ = false>
 __global__ void __launch_bounds__(256) k3_check(Geom g, Fields64 f, Num n, double* partials) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -452,17 +503,20 @@ __global__ void __launch_bounds__(256) k3_check(Geom g, Fields64 f, Num n, doubl
                 a.s[3] += dv * dv;
             }
             if (i >= 1 && i <= nx - 1 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2) {
-                const double R = res3_x<PERF>(f, n, c, sx, sy, sz);
+                const double R0 = ADJ ? res3_fold<0>(g, f, n, i, j, k) : res3_x<PERF>(f, n, c, sx, sy, sz);
+                const double R = SRC ? R0 + f.Fx[c] : R0;
                 f.Rx[c] = R;
                 a.s[0] += R * R;
             }
             if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 1 && k >= 1 && k <= nz - 2) {
-                const double R = res3_y<PERF>(f, n, c, sx, sy, sz);
+                const double R0 = ADJ ? res3_fold<1>(g, f, n, i, j, k) : res3_y<PERF>(f, n, c, sx, sy, sz);
+                const double R = SRC ? R0 + f.Fy[c] : R0;
                 f.Ry[c] = R;
                 a.s[1] += R * R;
             }
             if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 1) {
-                const double R = res3_z<PERF>(f, n, c, sx, sy, sz);
+                const double R0 = ADJ ? res3_fold<2>(g, f, n, i, j, k) : res3_z<PERF>(f, n, c, sx, sy, sz);
+                const double R = SRC ? R0 + f.Fz[c] : R0;
                 f.Rz[c] = R;
                 a.s[2] += R * R;
             }
@@ -546,6 +600,101 @@ __global__ void k_check_finalize(const double* partials, int nblocks, double lx,
         c.flag_nan = bad ? 1.0 : 0.0;
         *out = c;
     }
+}
+
+// ------------------------------------------------------------------ adjoint of the 3D viscous solve
+//
+// The forward 3D_V iterate converges to R = D·τ(B V) − ∇P = 0, ∇·(B V) = 0 with τ = 2μ ε̇,
+// B the free-slip extension (ghosts copy their interior faces). For a misfit J(V), with λ the
+// solution of the transposed system (adjoint mode: ghosts zero, ghost residuals folded onto
+// the faces they copy),
+//   ∂J/∂μ_c = −[2 Σ_n ε̇_n(V) ε̇_n(λ) + Σ_{edges e around c} ε̇_s(V) ε̇_s(λ)]
+// (normal rates where compute_τ! updates them, shear rates on the interior edges, each edge
+// averaging 4 cells): λᵀ ∂R/∂μ_c, as τ is linear in μ and W = diag(1 normal, 2 shear).
+
+// Shear strain rates in the explicit-index (·_dx) form of the 3D_V kernels.
+__device__ __forceinline__ double rate_xy(const Fields64& f, const Num& n, idx_t e, idx_t sx, idx_t sy) {
+    return 0.5 * (n._dy * (f.Vx[e] - f.Vx[e - sy]) + n._dx * (f.Vy[e] - f.Vy[e - sx]));
+}
+__device__ __forceinline__ double rate_xz(const Fields64& f, const Num& n, idx_t e, idx_t sx, idx_t sz) {
+    return 0.5 * (n._dz * (f.Vx[e] - f.Vx[e - sz]) + n._dx * (f.Vz[e] - f.Vz[e - sx]));
+}
+__device__ __forceinline__ double rate_yz(const Fields64& f, const Num& n, idx_t e, idx_t sy, idx_t sz) {
+    return 0.5 * (n._dz * (f.Vy[e] - f.Vy[e - sz]) + n._dy * (f.Vz[e] - f.Vz[e - sy]));
+}
+
+// τ = 2·Mus·ε̇(V) on the points compute_τ! updates (the fixed point of the viscous update).
+__global__ void __launch_bounds__(256) k3_tau_exact(Geom g, Fields64 f, Num n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    if (i >= nx || j >= ny) return;
+    const idx_t c = gidx32(g, i, j, k);
+    const idx_t sx = 1, sy = g.px, sz = (idx_t)g.pxy;
+    const double Mc = f.Mus[c];
+    if (j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2) f.txx[c] = 2.0 * Mc * (n._dx * (f.Vx[c + sx] - f.Vx[c]));
+    if (i >= 1 && i <= nx - 2 && k >= 1 && k <= nz - 2) f.tyy[c] = 2.0 * Mc * (n._dy * (f.Vy[c + sy] - f.Vy[c]));
+    if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2) f.tzz[c] = 2.0 * Mc * (n._dz * (f.Vz[c + sz] - f.Vz[c]));
+    if (i >= 1 && j >= 1 && k >= 1 && k <= nz - 2) {
+        const double am = (((f.Mus[c - sx - sy] + f.Mus[c - sy]) + f.Mus[c - sx]) + Mc) * 0.25;
+        f.txy[c] = 2.0 * am * rate_xy(f, n, c, sx, sy);
+    }
+    if (i >= 1 && j >= 1 && j <= ny - 2 && k >= 1) {
+        const double am = (((f.Mus[c - sx - sz] + f.Mus[c - sz]) + f.Mus[c - sx]) + Mc) * 0.25;
+        f.txz[c] = 2.0 * am * rate_xz(f, n, c, sx, sz);
+    }
+    if (i >= 1 && i <= nx - 2 && j >= 1 && k >= 1) {
+        const double am = (((f.Mus[c - sy - sz] + f.Mus[c - sz]) + f.Mus[c - sy]) + Mc) * 0.25;
+        f.tyz[c] = 2.0 * am * rate_yz(f, n, c, sy, sz);
+    }
+}
+
+// ∂J/∂log μ_c = μ_c ∂J/∂μ_c at every cell, from the forward fields f and the adjoint fields a
+// (same geometry), written to f.grad. The edge sums run in a fixed order.
+__global__ void __launch_bounds__(256) k3_grad_logmu(Geom g, Fields64 f, Fields64 a, Num n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    if (i >= nx || j >= ny) return;
+    const idx_t c = gidx32(g, i, j, k);
+    const idx_t sx = 1, sy = g.px, sz = (idx_t)g.pxy;
+    double nrm = 0.0, shr = 0.0;
+    if (j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2)
+        nrm = nrm + (n._dx * (f.Vx[c + sx] - f.Vx[c])) * (n._dx * (a.Vx[c + sx] - a.Vx[c]));
+    if (i >= 1 && i <= nx - 2 && k >= 1 && k <= nz - 2)
+        nrm = nrm + (n._dy * (f.Vy[c + sy] - f.Vy[c])) * (n._dy * (a.Vy[c + sy] - a.Vy[c]));
+    if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2)
+        nrm = nrm + (n._dz * (f.Vz[c + sz] - f.Vz[c])) * (n._dz * (a.Vz[c + sz] - a.Vz[c]));
+    // xy edges (x-face i', y-face j', cell k): i' in {i, i+1} ∩ [1,nx-1], j' in {j, j+1} ∩ [1,ny-1]
+    if (k >= 1 && k <= nz - 2)
+        for (int dj = 0; dj < 2; ++dj)
+            for (int di = 0; di < 2; ++di) {
+                const int ie = i + di, je = j + dj;
+                if (ie < 1 || ie > nx - 1 || je < 1 || je > ny - 1) continue;
+                const idx_t e = c + di * sx + dj * sy;
+                shr = shr + rate_xy(f, n, e, sx, sy) * rate_xy(a, n, e, sx, sy);
+            }
+    // xz edges (x-face i', cell j, z-face k')
+    if (j >= 1 && j <= ny - 2)
+        for (int dk = 0; dk < 2; ++dk)
+            for (int di = 0; di < 2; ++di) {
+                const int ie = i + di, ke = k + dk;
+                if (ie < 1 || ie > nx - 1 || ke < 1 || ke > nz - 1) continue;
+                const idx_t e = c + di * sx + dk * sz;
+                shr = shr + rate_xz(f, n, e, sx, sz) * rate_xz(a, n, e, sx, sz);
+            }
+    // yz edges (cell i, y-face j', z-face k')
+    if (i >= 1 && i <= nx - 2)
+        for (int dk = 0; dk < 2; ++dk)
+            for (int dj = 0; dj < 2; ++dj) {
+                const int je = j + dj, ke = k + dk;
+                if (je < 1 || je > ny - 1 || ke < 1 || ke > nz - 1) continue;
+                const idx_t e = c + dj * sy + dk * sz;
+                shr = shr + rate_yz(f, n, e, sy, sz) * rate_yz(a, n, e, sy, sz);
+            }
+    f.grad[c] = -(f.Mus[c] * (2.0 * nrm + shr));
 }
 
 // ------------------------------------------------------------------ batched 2D sweep (persistent)
@@ -1143,7 +1292,16 @@ cudaError_t launch_V_bc(int v, const Geom& g, const Fields64& f, const Num& n, b
     switch (v) {
         case VE3D: k3_V_bc<false><<<grid_faces(g, true), blk(), 0, s>>>(g, f, n, u); break;
         case VE3D_PERF:
-        case V3D: k3_V_bc<true><<<grid_faces(g, true), blk(), 0, s>>>(g, f, n, u); break;
+        case V3D:
+            if (n.adjoint) {
+                if (f.Fx) k3_V_bc<true, true, true><<<grid_faces(g, true), blk(), 0, s>>>(g, f, n, u);
+                else k3_V_bc<true, false, true><<<grid_faces(g, true), blk(), 0, s>>>(g, f, n, u);
+            } else if (f.Fx) {
+                k3_V_bc<true, true><<<grid_faces(g, true), blk(), 0, s>>>(g, f, n, u);
+            } else {
+                k3_V_bc<true><<<grid_faces(g, true), blk(), 0, s>>>(g, f, n, u);
+            }
+            break;
         case V2D: k2_V_bc<V2D><<<grid_faces(g, false), blk(), 0, s>>>(g, f, n, u); break;
         case VE2D: k2_V_bc<VE2D><<<grid_faces(g, false), blk(), 0, s>>>(g, f, n, u); break;
         case VE2D_PERF: k2_V_bc<VE2D_PERF><<<grid_faces(g, false), blk(), 0, s>>>(g, f, n, u); break;
@@ -1156,7 +1314,10 @@ cudaError_t launch_dV(int v, const Geom& g, const Fields64& f, const Num& n, cud
     switch (v) {
         case VE3D: k3_dV<false><<<grid_faces(g, true), blk(), 0, s>>>(g, f, n); break;
         case VE3D_PERF:
-        case V3D: k3_dV<true><<<grid_faces(g, true), blk(), 0, s>>>(g, f, n); break;
+        case V3D:
+            if (f.Fx) k3_dV<true, true><<<grid_faces(g, true), blk(), 0, s>>>(g, f, n);
+            else k3_dV<true><<<grid_faces(g, true), blk(), 0, s>>>(g, f, n);
+            break;
         case V2D: k2_dV<V2D><<<grid_faces(g, false), blk(), 0, s>>>(g, f, n); break;
         case VE2D: k2_dV<VE2D><<<grid_faces(g, false), blk(), 0, s>>>(g, f, n); break;
         case VE2D_PERF: k2_dV<VE2D_PERF><<<grid_faces(g, false), blk(), 0, s>>>(g, f, n); break;
@@ -1189,7 +1350,16 @@ cudaError_t launch_check(int v, const Geom& g, const Fields64& f, const Num& n, 
     switch (v) {
         case VE3D: k3_check<false><<<gr, blk(), 0, s>>>(g, f, n, partials); break;
         case VE3D_PERF:
-        case V3D: k3_check<true><<<gr, blk(), 0, s>>>(g, f, n, partials); break;
+        case V3D:
+            if (n.adjoint) {
+                if (f.Fx) k3_check<true, true, true><<<gr, blk(), 0, s>>>(g, f, n, partials);
+                else k3_check<true, false, true><<<gr, blk(), 0, s>>>(g, f, n, partials);
+            } else if (f.Fx) {
+                k3_check<true, true><<<gr, blk(), 0, s>>>(g, f, n, partials);
+            } else {
+                k3_check<true><<<gr, blk(), 0, s>>>(g, f, n, partials);
+            }
+            break;
         case V2D: k2_check<V2D><<<gr, blk(), 0, s>>>(g, f, n, partials); break;
         case VE2D: k2_check<VE2D><<<gr, blk(), 0, s>>>(g, f, n, partials); break;
         case VE2D_PERF: k2_check<VE2D_PERF><<<gr, blk(), 0, s>>>(g, f, n, partials); break;
@@ -1293,6 +1463,17 @@ cudaError_t launch_maxloc(int v, const Geom& g, double* must, const double* mus,
 cudaError_t launch_iter_params(int v, const Geom& g, const Fields64& f, const Num& n, cudaStream_t s) {
     if (variant_elastic(v)) k_iter_params<true><<<grid_cells(g), blk(), 0, s>>>(g, f, n);
     else k_iter_params<false><<<grid_cells(g), blk(), 0, s>>>(g, f, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tau_exact(const Geom& g, const Fields64& f, const Num& n, cudaStream_t s) {
+    k3_tau_exact<<<grid_cells(g), blk(), 0, s>>>(g, f, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_grad_logmu(const Geom& g, const Fields64& fwd, const Fields64& adj, const Num& n, cudaStream_t s) {
+    if (!fwd.grad) return cudaErrorInvalidValue;
+    k3_grad_logmu<<<grid_cells(g), blk(), 0, s>>>(g, fwd, adj, n);
     return cudaGetLastError();
 }
 

@@ -16,7 +16,8 @@ const PTS_OK = Cint(0)
 @enum Variant::Int32 V2D = 0 VE2D = 1 VE2D_PERF = 2 VE3D = 3 VE3D_PERF = 4 V3D = 5
 const FIELDS = (:Pt, :Vx, :Vy, :Vz, :τxx, :τyy, :τzz, :τxy, :τxz, :τyz,
                 :τxx_o, :τyy_o, :τzz_o, :τxy_o, :τxz_o, :τyz_o,
-                :Mus, :Musτ, :Gdτ, :dτ_Rho, :∇V, :Rx, :Ry, :Rz, :dVx, :dVy, :dVz)
+                :Mus, :Musτ, :Gdτ, :dτ_Rho, :∇V, :Rx, :Ry, :Rz, :dVx, :dVy, :dVz,
+                :ρg, :Fx, :Fy, :Fz, :grad)
 field_id(s::Symbol) = Int32(findfirst(==(s), FIELDS) - 1)
 
 # pts_desc (include/ptstokes.h)
@@ -27,8 +28,8 @@ struct Desc
     G::Float64; dt::Float64
     r::Float64; Re::Float64; CFL::Float64
     max_l::Float64; eps::Float64; iter_max::Float64
-    mixed_inner::Int32; single_pass::Int32
-    reserved::NTuple{6,Int32}
+    mixed_inner::Int32; single_pass::Int32; adjoint::Int32
+    reserved::NTuple{5,Int32}
 end
 
 struct Check
@@ -58,9 +59,9 @@ end
 A device context for one problem (the scripts' `Stokes2D_()`/`Stokes3D_()` state).
 """
 function Ctx(variant::Variant, nx, ny, nz=1; lx=10.0, ly=10.0, lz=10.0, G=1.0, dt=1.0, r=1.0, Re, CFL,
-             nout=200, ε=1e-8, iterMax=2e5, max_l=0.0, precision=0, single_pass=0)
+             nout=200, ε=1e-8, iterMax=2e5, max_l=0.0, precision=0, single_pass=0, adjoint=0)
     d = Desc(Int32(variant), Int32(precision), nx, ny, nz, nout, lx, ly, lz, G, dt, r, Re, CFL, max_l, ε, iterMax,
-             0, single_pass, ntuple(_ -> Int32(0), 6))
+             0, single_pass, adjoint, ntuple(_ -> Int32(0), 5))
     out = Ref{Ptr{Cvoid}}(C_NULL)
     check(nothing, ccall((:pts_create, libpts), Cint, (Ref{Desc}, Ref{Ptr{Cvoid}}), d, out))
     ctx = Ctx(out[])

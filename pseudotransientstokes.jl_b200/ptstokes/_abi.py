@@ -33,6 +33,8 @@ FIELDS = [
     "Mus", "Must", "Gdt", "dtRho", "divV",
     "Rx", "Ry", "Rz", "dVx", "dVy", "dVz",
     "rhog",
+    "Fx", "Fy", "Fz",
+    "grad",
 ]
 FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
 
@@ -46,7 +48,8 @@ class PtsDesc(ctypes.Structure):
         ("G", ctypes.c_double), ("dt", ctypes.c_double),
         ("r", ctypes.c_double), ("Re", ctypes.c_double), ("CFL", ctypes.c_double),
         ("max_l", ctypes.c_double), ("eps", ctypes.c_double), ("iter_max", ctypes.c_double),
-        ("mixed_inner", ctypes.c_int32), ("single_pass", ctypes.c_int32), ("reserved", ctypes.c_int32 * 6),
+        ("mixed_inner", ctypes.c_int32), ("single_pass", ctypes.c_int32), ("adjoint", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 5),
     ]
 
 
@@ -115,6 +118,9 @@ SIGNATURES = {
     "pts_iterate": ([_P, _I64], ctypes.c_int),
     "pts_solve": ([_P, ctypes.POINTER(PtsSolveInfo)], ctypes.c_int),
     "pts_run": ([_P, _I32, ctypes.POINTER(_I64), ctypes.POINTER(PtsSolveInfo)], ctypes.c_int),
+    # adjoint of the 3D viscous solve
+    "pts_apply_operator": ([_P, ctypes.POINTER(PtsCheck)], ctypes.c_int),
+    "pts_gradient_logmu": ([_P, _P], ctypes.c_int),
     # residual check on caller-owned device arrays; allocates nothing
     "pts_check_noalloc": ([ctypes.POINTER(PtsDesc), ctypes.POINTER(_P), _P, _P], ctypes.c_int),
     # batched 2D sweep

@@ -31,7 +31,7 @@ def test_library_exports_every_declared_symbol():
     lib = ptstokes.load()
     missing = [n for n in declared_symbols() if not hasattr(lib, n)]
     assert not missing, missing
-    assert lib.pts_abi_version() == 1
+    assert lib.pts_abi_version() == 2
 
 
 def test_python_binding_covers_the_header():
