@@ -1,0 +1,156 @@
+"""Adjoint gradients of the 3D viscous PT solve: ∂J/∂log μ through the C ABI.
+
+The reference has no adjoint. The forward problem is the 3D_V solve (the 3D kernels of
+scripts/stokes_3D/Stokes3D_ve_perf.jl without elastic terms) with pure-shear walls; the
+objective is a misfit of the vertical velocity on the top interior face plane,
+J = ½‖Vz(top) − Vobs‖². ``ViscousAdjoint`` runs the forward solve, the transposed
+(adjoint) solve with the source ∂J/∂Vz on that plane, and the pointwise gradient kernel,
+all on the device (``pts_gradient_logmu`` in include/ptstokes.h). ``TopVz`` wraps the
+same steps as a ``torch.autograd.Function`` of log μ (the viscosity the solver uses, after
+any smoothing). ``inclusion_set``, ``viscosity_field`` and ``lognormal_factor`` draw the
+seeded 20-inclusion field and its log-normal perturbation.
+"""
+import numpy as np
+
+from .solver import Solver
+
+
+def inclusion_set(count=20, seed=1855, box=(10.0, 10.0, 10.0), radius=(0.3, 0.8), log10_mu=(-4.0, 4.0)):
+    """`count` spheres: centres uniform in the box, radii uniform in `radius`, log10 of the
+    inclusion viscosity uniform in `log10_mu` (matrix viscosity 1)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        c = [float(rng.uniform(0.0, L)) for L in box]
+        out.append(dict(centre=c, radius=float(rng.uniform(*radius)), log10_mu=float(rng.uniform(*log10_mu))))
+    return out
+
+
+def viscosity_field(nx, ny, nz, inclusions, box=(10.0, 10.0, 10.0), mus0=1.0):
+    """Cell-centred viscosity (nx, ny, nz), column-major: mus0, and 10**log10_mu inside each
+    sphere (cell centre strictly inside; a later sphere overwrites an earlier one)."""
+    lx, ly, lz = box
+    dx, dy, dz = lx / nx, ly / ny, lz / nz
+    mus = np.full((nx, ny, nz), mus0, dtype=np.float64, order="F")
+    for inc in inclusions:
+        (cx, cy, cz), r = inc["centre"], inc["radius"]
+        lo = [max(0, int(np.floor((c - r) / h)) - 1) for c, h in ((cx, dx), (cy, dy), (cz, dz))]
+        hi = [min(n, int(np.ceil((c + r) / h)) + 1) for c, h, n in ((cx, dx, nx), (cy, dy, ny), (cz, dz, nz))]
+        x = (np.arange(lo[0], hi[0]) + 0.5) * dx - cx
+        y = (np.arange(lo[1], hi[1]) + 0.5) * dy - cy
+        z = (np.arange(lo[2], hi[2]) + 0.5) * dz - cz
+        inside = (x[:, None, None] ** 2 + y[None, :, None] ** 2 + z[None, None, :] ** 2) < r * r
+        sub = mus[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]]
+        sub[inside] = 10.0 ** inc["log10_mu"]
+    return mus
+
+
+def lognormal_factor(shape, sigma=0.5, corr=8.0, seed=7):
+    """10**(sigma·ξ): ξ is white noise smoothed by a periodic Gaussian of standard deviation
+    `corr` cells and rescaled to unit standard deviation."""
+    from scipy.ndimage import gaussian_filter
+
+    rng = np.random.default_rng(seed)
+    xi = gaussian_filter(rng.standard_normal(shape), corr, mode="wrap")
+    xi = xi / xi.std()
+    return np.asfortranarray(10.0 ** (sigma * xi))
+
+
+def top_plane(vz):
+    """Vz on the top interior face plane: the (nx-2, ny-2) interior faces of z-face nz-1."""
+    nx, ny, nz1 = vz.shape
+    return vz[1:nx - 1, 1:ny - 1, nz1 - 2]
+
+
+class ViscousAdjoint:
+    """Forward solve, adjoint solve and ∂J/∂log μ for J = ½‖Vz(top) − Vobs‖² (or any J whose
+    derivative lives on the top Vz plane), on two 3d_v contexts of the same grid."""
+
+    def __init__(self, nx, ny, nz, ebg=1.0, lib=None, **kw):
+        self.nx, self.ny, self.nz, self.ebg = nx, ny, nz, ebg
+        self.fwd = Solver("3d_v", nx, ny, nz, lib=lib, **kw)
+        self.adj = Solver("3d_v", nx, ny, nz, lib=lib, adjoint=1, **kw)
+        self.mus = None
+
+    def close(self):
+        self.fwd.close()
+        self.adj.close()
+
+    def set_viscosity(self, mus, nsmooth=10):
+        """Mus = mus smoothed nsmooth times on the device (smooth!, as the scripts do). The
+        gradient is with respect to the log of the smoothed field (``self.mus``)."""
+        f = self.fwd
+        f.init_inclusion(1.0, 1.0, 0.0, self.ebg)
+        f.set("Mus", mus)
+        if nsmooth:
+            f.smooth(nsmooth, 1.0)
+        self.mus = f.get("Mus")
+        return self
+
+    def forward(self):
+        """The forward PT solve from the pure-shear initial state (walls and ICs, Mus, the
+        local-max viscosity and the iteration parameters); returns its outcome (pts_solve)."""
+        f = self.fwd
+        f.init_inclusion(1.0, 1.0, 0.0, self.ebg)
+        f.set("Mus", self.mus)
+        f.compute_maxloc()
+        f.compute_iter_params()
+        return f.solve()
+
+    def top_vz(self):
+        return top_plane(self.fwd.get("Vz")).copy(order="F")
+
+    def adjoint(self, dJ_dtop):
+        """The transposed solve with the momentum source dJ/dVz on the top interior plane."""
+        a = self.adj
+        a.init_inclusion(1.0, 1.0, 0.0, 0.0)  # every field zero; walls and ghosts zero
+        a.set("Mus", self.mus)
+        a.compute_maxloc()
+        a.compute_iter_params()
+        Fz = np.zeros(a.shape("Fz"), order="F")
+        Fz[:, :, -1] = dJ_dtop
+        a.set("Fz", Fz)
+        return a.solve()
+
+    def gradient(self):
+        """∂J/∂log μ per cell (nx, ny, nz) from the last forward and adjoint solves."""
+        self.fwd.gradient_logmu(self.adj)
+        return self.fwd.get("grad")
+
+    def misfit_gradient(self, vobs):
+        """J and ∂J/∂log μ for J = ½‖Vz(top) − Vobs‖² at the current viscosity."""
+        fo = self.forward()
+        r = self.top_vz() - vobs
+        J = 0.5 * float(np.sum(r * r))
+        ao = self.adjoint(r)
+        return J, self.gradient(), fo, ao
+
+
+def _torch_function():
+    import torch
+
+    class TopVz(torch.autograd.Function):
+        """Vz on the top interior plane as a differentiable function of log μ (float64,
+        shape (nx, ny, nz), the viscosity the solver uses). Forward: one PT solve; backward:
+        the transposed solve with the incoming gradient as source, then ∂/∂log μ."""
+
+        @staticmethod
+        def forward(ctx, logmu, problem):
+            mus = torch.exp(logmu.detach()).cpu().numpy()
+            problem.set_viscosity(np.asfortranarray(mus), nsmooth=0)
+            problem.forward()
+            ctx.problem = problem
+            return torch.from_numpy(problem.top_vz()).to(logmu.device)
+
+        @staticmethod
+        def backward(ctx, g):
+            p = ctx.problem
+            p.adjoint(np.asfortranarray(g.detach().cpu().numpy()))
+            return torch.from_numpy(p.gradient()).to(g.device), None
+
+    return TopVz
+
+
+def top_vz(logmu, problem):
+    """Differentiable Vz(top) of log μ (see ``TopVz``)."""
+    return _torch_function().apply(logmu, problem)

@@ -50,7 +50,8 @@ class Solver:
         self.lib = lib or _abi.load()
         self.variant = variant
         self.ndim = 3 if variant.startswith("3d") else 2
-        p = dict(lx=10.0, ly=10.0, lz=10.0, xi=1.0, mus0=1.0, G=1.0, max_l=0.0, mixed_inner=0, single_pass=0)
+        p = dict(lx=10.0, ly=10.0, lz=10.0, xi=1.0, mus0=1.0, G=1.0, max_l=0.0, mixed_inner=0, single_pass=0,
+                 adjoint=0)
         p.update(VARIANT_DEFAULTS[variant])
         p.update(kw)
         self.p = p
@@ -67,6 +68,7 @@ class Solver:
         d.max_l, d.eps, d.iter_max = p["max_l"], p["eps"], float(p["iter_max"])
         d.mixed_inner = int(p["mixed_inner"])
         d.single_pass = int(p["single_pass"])
+        d.adjoint = int(p["adjoint"])
         self.desc = d
         ctx = ctypes.c_void_p()
         check(self.lib, None, self.lib.pts_create(ctypes.byref(d), ctypes.byref(ctx)))
@@ -170,6 +172,18 @@ class Solver:
         c = PtsCheck()
         self._ck(self.lib.pts_compute_res(self.ctx, ctypes.byref(c)))
         return c.as_dict()
+
+    # ---------------------------------------------------------------- adjoint (3d_v)
+    def apply_operator(self):
+        """τ = 2·Mus·ε̇(V), then Rx, Ry, Rz and ∇V of the current fields: one application of the
+        forward operator, or of its transpose for a context created with adjoint=1."""
+        c = PtsCheck()
+        self._ck(self.lib.pts_apply_operator(self.ctx, ctypes.byref(c)))
+        return c.as_dict()
+
+    def gradient_logmu(self, adj):
+        """∂J/∂log μ into this (forward) context's "grad" field from the adjoint context adj."""
+        self._ck(self.lib.pts_gradient_logmu(self.ctx, adj.ctx))
 
     # ---------------------------------------------------------------- drivers
     def iterate(self, n):
