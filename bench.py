@@ -364,6 +364,134 @@ def run_batch(args, ws, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_adjoint(args, ws, rank, local):
+    """Adjoint gradient of the 3D viscous solve at `--adj-n`³: viscosity = matrix 1 plus 20
+    seeded spherical inclusions (radii U[0.3,0.8], log10 μ U[-L,L], L = `--log10-range`),
+    smoothed 10x; Vobs =
+    Vz on the top interior plane from a forward solve on that field times a log-normal
+    perturbation (σ = 0.5 in log10 μ, Gaussian correlation of 8 cells); J = ½‖Vz − Vobs‖².
+    Timed: forward solve + transposed (adjoint) solve + ∂J/∂log μ, each solve to 1e-8.
+    Checked: a directional derivative of J along a smooth random direction by central
+    differences (two more forward solves)."""
+    import numpy as np
+    import torch
+
+    from ptstokes.adjoint import ViscousAdjoint, inclusion_set, lognormal_factor, viscosity_field
+
+    torch.cuda.set_device(local)
+    n = args.adj_n
+    L = args.log10_range
+    mus = viscosity_field(n, n, n, inclusion_set(seed=1855 + rank, log10_mu=(-L, L)))
+    pert = lognormal_factor((n, n, n), sigma=0.5, corr=8.0, seed=1856 + rank)
+    p = ViscousAdjoint(n, n, n, eps=1e-8, nout=200, iter_max=2e5)
+    p.set_viscosity(mus * pert)
+    obs = p.forward()
+    vobs = p.top_vz()
+    p.set_viscosity(mus)
+    st = torch.cuda.ExternalStream(p.fwd.stream_handle())
+    clk = ClockSampler(local)
+    clk.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    J, g, fo, ao = p.misfit_gradient(vobs)
+    e1.record(st)
+    e1.synchronize()
+    clocks = clk.stop()
+    sec = e0.elapsed_time(e1) / 1e3
+    # directional derivative along a smooth direction δ (unit standard deviation in log μ)
+    delta = np.log(lognormal_factor((n, n, n), sigma=1.0, corr=8.0, seed=1857 + rank)) / np.log(10.0)
+    dd_adj = float(np.sum(g * delta))
+    mus0 = p.mus.copy()
+    h = 1e-3
+    Js = []
+    for sgn in (1, -1):
+        p.mus = mus0 * np.exp(sgn * h * delta)
+        p.forward()
+        r = p.top_vz() - vobs
+        Js.append(0.5 * float(np.sum(r * r)))
+    p.mus = mus0
+    dd_fd = (Js[0] - Js[1]) / (2 * h)
+    its = fo["iters"] + ao["iters"]
+    bytes_it = 23 * n ** 3 * 8  # 3D viscous: the A_eff convention without the 6 τ_o arrays
+    line = {
+        "metric": f"adjoint gradient dJ/dlog(mu), 3D viscous {n}^3: forward + adjoint solve + gradient",
+        "value": round(sec, 3), "unit": "s", "n_gpus": ws, "higher_is_better": False, "scaling": "weak",
+        "dtype": "f64", "data": "synthetic seeded 20-inclusion field and log-normal perturbation",
+        "config": {"workload": f"3D viscous Stokes {n}^3, J = 1/2 |Vz(top) - Vobs|^2", "eps": 1e-8, "nout": 200,
+                   "inclusions": 20, "log10_mu_range": [-L, L], "perturbation": "sigma 0.5 log10, 8-cell Gaussian"},
+        "forward": {"iters": fo["iters"], "converged": fo["converged"], "err": fo["last"]["err"]},
+        "adjoint": {"iters": ao["iters"], "converged": ao["converged"], "err": ao["last"]["err"]},
+        "observation_solve_iters": obs["iters"], "J": J,
+        "T_eff_GBs": round(bytes_it * its / sec / 1e9, 1),
+        "T_eff_convention": "23 arrays x 8 B per cell and PT iteration (3D viscous)",
+        "directional_check": {"adjoint": dd_adj, "central_difference": dd_fd, "h": h,
+                              "rel_err": abs(dd_adj - dd_fd) / max(abs(dd_fd), 1e-300)},
+        "clocks": clocks,
+    }
+    p.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_inclusions(args, ws, rank, local):
+    """Mixed precision on the 20-inclusion 3D viscous problem at `--incl-n`³ (viscosity =
+    matrix 1 plus 20 seeded spheres, radii U[0.3,0.8], log10 μ U[-L,L], smoothed 10x):
+    time to err <= 1e-8 in plain FP64 and with FP32 inner sweeps + FP64 defect correction,
+    same problem and check; per-field L2 and max errors of the mixed solution against the
+    FP64 one."""
+    import numpy as np
+    import torch
+
+    import ptstokes
+    from ptstokes.adjoint import inclusion_set, viscosity_field
+
+    torch.cuda.set_device(local)
+    n, L = args.incl_n, args.log10_range
+    mus = viscosity_field(n, n, n, inclusion_set(seed=1855 + rank, log10_mu=(-L, L)))
+    out, fields = {}, {}
+    clk = ClockSampler(local)
+    clk.start()
+    for prec in ("fp64", "mixed"):
+        s = ptstokes.Solver("3d_v", n, n, n, precision=prec, eps=1e-8, nout=200, iter_max=4e5)
+        s.init_inclusion(1.0, 1.0, 0.0, 1.0)
+        s.set("Mus", mus)
+        s.smooth(10, 1.0)
+        s.compute_maxloc()
+        s.compute_iter_params()
+        s.sync()
+        st = torch.cuda.ExternalStream(s.stream_handle())
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        r = s.solve()
+        b.record(st)
+        b.synchronize()
+        sec = a.elapsed_time(b) / 1e3
+        out[prec] = {"seconds": round(sec, 3), "iters": r["iters"], "converged": r["converged"], "err": r["last"]["err"]}
+        fields[prec] = {k: s.get(k) for k in ("Pt", "Vx", "Vy", "Vz", "txx", "tyy", "tzz", "txy", "txz", "tyz")}
+        s.close()
+    clocks = clk.stop()
+    errs = {}
+    for k, ref in fields["fp64"].items():
+        d = fields["mixed"][k] - ref
+        errs[k] = {"l2_rel": float(np.linalg.norm(d) / max(np.linalg.norm(ref), 1e-300)),
+                   "max_rel": float(np.abs(d).max() / max(np.abs(ref).max(), 1e-300))}
+    line = {
+        "metric": f"time to err <= 1e-8, 3D viscous {n}^3 with 20 inclusions: FP32 inner sweeps + FP64 correction vs FP64",
+        "value": round(out["fp64"]["seconds"] / out["mixed"]["seconds"], 3), "unit": "speed-up (x)", "n_gpus": ws,
+        "higher_is_better": True, "scaling": "weak", "dtype": "f32+f64", "data": "synthetic seeded 20-inclusion field",
+        "config": {"workload": f"3D viscous Stokes {n}^3", "inclusions": 20, "log10_mu_range": [-L, L], "eps": 1e-8,
+                   "nout": 200},
+        "fp64": out["fp64"], "mixed": out["mixed"], "mixed_error_vs_fp64": errs,
+        "T_eff_GBs": {p: round(23 * n ** 3 * 8 * out[p]["iters"] / out[p]["seconds"] / 1e9, 1) for p in out},
+        "T_eff_convention": "23 arrays x 8 B per cell and PT iteration (3D viscous, FP64 bytes for both)",
+        "clocks": clocks,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def time_to_tol(args, stream_cls):
     """Time to tolerance of the converged problem of the metric: `nt` physical steps of
     3D VE, each PT loop run to err <= 1e-8 with a check every 200 iterations
@@ -415,6 +543,12 @@ def main():
     ap.add_argument("--ttt-nt", type=int, default=5, help="physical steps of the time-to-tolerance comparison")
     ap.add_argument("--batch", action="store_true", help="run the batched 2D sweep instead")
     ap.add_argument("--batch-n", type=int, default=256)
+    ap.add_argument("--adjoint", action="store_true", help="run the adjoint-gradient configuration instead")
+    ap.add_argument("--adj-n", type=int, default=255)
+    ap.add_argument("--inclusions", action="store_true", help="run the 20-inclusion mixed-precision comparison")
+    ap.add_argument("--incl-n", type=int, default=255)
+    ap.add_argument("--log10-range", type=float, default=2.0,
+                    help="inclusion log10 viscosity drawn from U[-L, L] (adjoint and inclusion modes)")
     ap.add_argument("--batch-iter-max", type=float, default=0,
                     help="common iterMax of the sweep (0: 100*max(nx,ny) per instance)")
     ap.add_argument("--iters-per-step", type=int, default=200)
@@ -430,6 +564,10 @@ def main():
             run_reference(args, ws, rank, pg)
         elif args.batch:
             run_batch(args, ws, rank, local)
+        elif args.adjoint:
+            run_adjoint(args, ws, rank, local)
+        elif args.inclusions:
+            run_inclusions(args, ws, rank, local)
         else:
             run_ours(args, ws, rank, local, pg)
     finally:
