@@ -126,4 +126,49 @@ function run!(ctx::Ctx, nt)
     return per, r[]
 end
 
+# ---- adjoint of the 3D viscous solve (pts_apply_operator, pts_gradient_logmu) ----
+
+"One application of the operator (or of its transpose on an adjoint context)."
+function apply_operator!(ctx::Ctx)
+    r = Ref{Check}()
+    check(ctx, ccall((:pts_apply_operator, libpts), Cint, (Ptr{Cvoid}, Ref{Check}), ctx.ptr, r))
+    return r[]
+end
+
+"∂J/∂log μ into the forward context's :grad field from the adjoint context's solution."
+gradient_logmu!(fwd::Ctx, adj::Ctx) =
+    check(fwd, ccall((:pts_gradient_logmu, libpts), Cint, (Ptr{Cvoid}, Ptr{Cvoid}), fwd.ptr, adj.ptr))
+
+"""
+    top_vz(logμ, fwd, adj, Vwall) -> Vz on the top interior face plane
+
+Forward solve of the 3D viscous problem for the cell viscosity exp.(logμ) (the walls and
+ICs `Vwall = (Vx, Vy, Vz)` are set first). `fwd` is a PTS_3D_V context, `adj` one created
+with `adjoint=1` on the same grid.
+"""
+function top_vz(logμ::Array{Float64,3}, fwd::Ctx, adj::Ctx, Vwall)
+    init_inclusion!(fwd; μs0=1.0, μsi=1.0, radius2=0.0, εbg=0.0)    # every field zero
+    set_field!(fwd, :Vx, Vwall[1]); set_field!(fwd, :Vy, Vwall[2]); set_field!(fwd, :Vz, Vwall[3])
+    set_field!(fwd, :Mus, exp.(logμ)); compute_maxloc!(fwd); compute_iter_params!(fwd)
+    solve!(fwd)
+    Vz = get_field(fwd, :Vz)
+    return Vz[2:end-1, 2:end-1, end-1]
+end
+
+# The ChainRulesCore rule a maintainer would add next to the shim (ChainRulesCore is not a
+# dependency of this file):
+#
+#   function ChainRulesCore.rrule(::typeof(top_vz), logμ, fwd, adj, Vwall)
+#       v = top_vz(logμ, fwd, adj, Vwall)
+#       function top_vz_pullback(v̄)
+#           init_inclusion!(adj; μs0=1.0, μsi=1.0, radius2=0.0, εbg=0.0)    # zero state
+#           set_field!(adj, :Mus, exp.(logμ)); compute_maxloc!(adj); compute_iter_params!(adj)
+#           Fz = zeros(field_shape(adj, :Fz)...); Fz[:, :, end] .= unthunk(v̄)
+#           set_field!(adj, :Fz, Fz); solve!(adj)
+#           gradient_logmu!(fwd, adj)
+#           return NoTangent(), get_field(fwd, :grad), NoTangent(), NoTangent(), NoTangent()
+#       end
+#       return v, top_vz_pullback
+#   end
+
 end # module
