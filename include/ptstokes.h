@@ -75,7 +75,7 @@ typedef struct pts_desc {
     double iter_max;    /* `while err > ε && iter <= iterMax` */
     int32_t mixed_inner;    /* MIXED: FP32 sweeps between FP64 corrections; 0 => nout */
     int32_t single_pass;    /* 3D: 1 = one-launch-per-iteration staged kernel, 0 = two launches */
-    int32_t adjoint;        /* PTS_3D_V: 1 = solve the transposed (adjoint) system, see below */
+    int32_t adjoint;        /* PTS_3D_V / PTS_3D_VE_PERF: 1 = solve the transposed (adjoint) system */
     int32_t reserved[5];
 } pts_desc;
 
@@ -171,7 +171,7 @@ PTS_API int pts_solve(pts_ctx* ctx, pts_solve_info* info);
  * info (may be NULL) receives the last step's outcome with iters = ittot. */
 PTS_API int pts_run(pts_ctx* ctx, int32_t nt, int64_t* iters_per_step, pts_solve_info* info);
 
-/* ---- adjoint of the 3D viscous solve (PTS_3D_V, FP64) ----
+/* ---- adjoint of the 3D viscous solve (PTS_3D_V, FP64; visco-elastic PTS_3D_VE_PERF below) ----
  * No counterpart in the reference. The converged PTS_3D_V iterate solves A(μ)[V;P] = b with
  * A = [[K, -G], [div∘B, 0]]: B extends the interior velocities to the free-slip ghosts by
  * copying, the walls' normal velocities are data, K = D·2μ·S·B (S the strain rates, D the
@@ -190,8 +190,19 @@ PTS_API int pts_run(pts_ctx* ctx, int32_t nt, int64_t* iters_per_step, pts_solve
  * application of A or its transpose, for symmetry tests. Synchronous. */
 PTS_API int pts_apply_operator(pts_ctx* ctx, pts_check* out);
 /* ∂J/∂log μ into fwd's PTS_F_GRAD from fwd's V (the forward solution) and adj's V (the adjoint
- * solution of an adjoint-mode context); same grid, both PTS_3D_V FP64. Synchronous. */
+ * solution of an adjoint-mode context); same grid, both PTS_3D_V FP64. Synchronous.
+ *
+ * Visco-elastic (two PTS_3D_VE_PERF contexts, no counterpart in the reference): a converged
+ * physical step has τ = η(2ε̇ + τ_o/(G dt)), η = 1/(1/μ + 1/(G dt)) (μ̄ on the shear edges).
+ * The adjoint of nt steps is the same time loop in adjoint mode run backwards: the source
+ * ∂J/∂V in the step that adjoints the last forward step, zero afterwards, and assign_τ!
+ * (τ_o ← τ) between steps exactly as forward. With τ the forward step's converged stresses
+ * (restored into fwd from a per-step checkpoint) and τa the matching adjoint step's,
+ * one step contributes
+ *   ∂J/∂log μ_c += -[Σ_n τa_n τ_n/(2μ_c) + μ_c Σ_{edges e around c} τa_e τ_e/(4 μ̄_e²)];
+ * pts_gradient_logmu writes that term, pts_gradient_logmu_add adds it. */
 PTS_API int pts_gradient_logmu(pts_ctx* fwd, pts_ctx* adj);
+PTS_API int pts_gradient_logmu_add(pts_ctx* fwd, pts_ctx* adj);
 
 /* ---- batched 2D viscous sweep: many uneven grids, one persistent launch ----
  * Replaces the reference's parameter sweeps, which run one Julia process per instance

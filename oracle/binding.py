@@ -78,6 +78,7 @@ _SIGS = {
     "ora3v_grad_logmu": [Arr] * 8 + [_D] * 3,
     "ora3v_res_adj": [Arr] * 10 + [_D] * 3,
     "ora3v_update_V": [Arr] * 10,
+    "ora3ve_grad_logmu": [Arr] * 14 + [ctypes.c_int],
     "ora3p_compute_Res": [Arr] * 14 + [_D] * 3,
     "ora_stats": [Arr, ctypes.POINTER(_D), ctypes.POINTER(_D), ctypes.POINTER(_D)],
     "ora_num_threads": [],

@@ -912,6 +912,64 @@ void ora3v_grad_logmu(oarr grad_, oarr Vx_, oarr Vy_, oarr Vz_, oarr Lx_, oarr L
             }
 }
 
+// One physical step's term of ∂J/∂log μ for the visco-elastic operator (no reference
+// counterpart), from the forward step's converged stresses T and the adjoint step's stresses A:
+//   g_c (+)= -[Σ_n A_n T_n/(2 Mus_c) + Mus_c Σ_{edges e around c} A_e T_e/(4 μ̄_e²)],
+// μ̄_e the 4-cell average of Mus on the edge. Written with 0-based unified coordinates: a
+// stress element (a,b,c) sits at reference index (a-s0+1, b-s1+1, c-s2+1) for the field's
+// start (s0,s1,s2); zero outside its extents. add != 0 accumulates into g.
+void ora3ve_grad_logmu(oarr grad_, oarr Txx_, oarr Tyy_, oarr Tzz_, oarr Txy_, oarr Txz_, oarr Tyz_, oarr Axx_,
+                       oarr Ayy_, oarr Azz_, oarr Axy_, oarr Axz_, oarr Ayz_, oarr Mus_, int add) {
+    F3 G(grad_), Txx(Txx_), Tyy(Tyy_), Tzz(Tzz_), Txy(Txy_), Txz(Txz_), Tyz(Tyz_), Axx(Axx_), Ayy(Ayy_), Azz(Azz_),
+        Axy(Axy_), Axz(Axz_), Ayz(Ayz_), M(Mus_);
+    const int64_t nx = M.n1, ny = M.n2, nz = M.n3;
+    auto T = [](const F3& A, int s0, int s1, int s2, int64_t a, int64_t b, int64_t c) -> double {
+        const int64_t u = a - s0 + 1, v = b - s1 + 1, w = c - s2 + 1;
+        if (u < 1 || u > A.n1 || v < 1 || v > A.n2 || w < 1 || w > A.n3) return 0.0;
+        return A(u, v, w);
+    };
+    auto m = [&](int64_t i, int64_t j, int64_t k) { return M(i + 1, j + 1, k + 1); };
+#pragma omp parallel for schedule(static)
+    for (int64_t k = 0; k < nz; ++k)
+        for (int64_t j = 0; j < ny; ++j)
+            for (int64_t i = 0; i < nx; ++i) {
+                const double Mc = m(i, j, k);
+                double nrm = 0.0, shr = 0.0;
+                if (j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2)
+                    nrm = nrm + T(Axx, 0, 1, 1, i, j, k) * T(Txx, 0, 1, 1, i, j, k);
+                if (i >= 1 && i <= nx - 2 && k >= 1 && k <= nz - 2)
+                    nrm = nrm + T(Ayy, 1, 0, 1, i, j, k) * T(Tyy, 1, 0, 1, i, j, k);
+                if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2)
+                    nrm = nrm + T(Azz, 1, 1, 0, i, j, k) * T(Tzz, 1, 1, 0, i, j, k);
+                if (k >= 1 && k <= nz - 2)
+                    for (int dj = 0; dj < 2; ++dj)
+                        for (int di = 0; di < 2; ++di) {
+                            const int64_t ie = i + di, je = j + dj;
+                            if (ie < 1 || ie > nx - 1 || je < 1 || je > ny - 1) continue;
+                            const double mb = (((m(ie - 1, je - 1, k) + m(ie, je - 1, k)) + m(ie - 1, je, k)) + m(ie, je, k)) * 0.25;
+                            shr = shr + T(Axy, 1, 1, 1, ie, je, k) * T(Txy, 1, 1, 1, ie, je, k) / (mb * mb);
+                        }
+                if (j >= 1 && j <= ny - 2)
+                    for (int dk = 0; dk < 2; ++dk)
+                        for (int di = 0; di < 2; ++di) {
+                            const int64_t ie = i + di, ke = k + dk;
+                            if (ie < 1 || ie > nx - 1 || ke < 1 || ke > nz - 1) continue;
+                            const double mb = (((m(ie - 1, j, ke - 1) + m(ie, j, ke - 1)) + m(ie - 1, j, ke)) + m(ie, j, ke)) * 0.25;
+                            shr = shr + T(Axz, 1, 1, 1, ie, j, ke) * T(Txz, 1, 1, 1, ie, j, ke) / (mb * mb);
+                        }
+                if (i >= 1 && i <= nx - 2)
+                    for (int dk = 0; dk < 2; ++dk)
+                        for (int dj = 0; dj < 2; ++dj) {
+                            const int64_t je = j + dj, ke = k + dk;
+                            if (je < 1 || je > ny - 1 || ke < 1 || ke > nz - 1) continue;
+                            const double mb = (((m(i, je - 1, ke - 1) + m(i, je, ke - 1)) + m(i, je - 1, ke)) + m(i, je, ke)) * 0.25;
+                            shr = shr + T(Ayz, 1, 1, 1, i, je, ke) * T(Tyz, 1, 1, 1, i, je, ke) / (mb * mb);
+                        }
+                const double t = -(nrm / (2.0 * Mc) + Mc * (shr * 0.25));
+                G(i + 1, j + 1, k + 1) = add ? G(i + 1, j + 1, k + 1) + t : t;
+            }
+}
+
 // compute_Res! (Stokes3D_ve_perf.jl:90-96): ∇V from the current V plus Rx, Ry, Rz.
 void ora3p_compute_Res(oarr divV_, oarr Rx_, oarr Ry_, oarr Rz_, oarr Vx_, oarr Vy_, oarr Vz_, oarr Pt_, oarr txx_,
                        oarr tyy_, oarr tzz_, oarr txy_, oarr txz_, oarr tyz_, double _dx, double _dy, double _dz) {

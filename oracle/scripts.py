@@ -432,38 +432,16 @@ class VE3D(_Case3D):
 
 
 class VE3DPerf(_Case3D):
-    """scripts/stokes_3D/Stokes3D_ve_perf.jl (fused explicit-index kernels, _dx form)."""
-
-    unfused = False
-    defaults = dict(nt=1, iterMax=200, nout=2000, eps=1e-8, CFL=0.8 / math.sqrt(3), Re=6 * PI, r=1.0)
-
-    def iteration(self):
-        L, A = self.L, self.A
-        L.ora3p_compute_Pt_tau(A("Pt"), *self._tau(), *self._tau_o(), A("Vx"), A("Vy"), A("Vz"), A("Mus"), A("Gdt"),
-                               self.r, self.G, self.dt, self._dx, self._dy, self._dz, int(self.elastic))
-        L.ora3p_compute_V(A("Vx"), A("Vy"), A("Vz"), A("Pt"), *self._tau(), A("dtRho"), self._dx, self._dy,
-                          self._dz)
-        self.bc()
-
-    def check(self):
-        A = self.A
-        self.L.ora3p_compute_Res(A("divV"), A("Rx"), A("Ry"), A("Rz"), A("Vx"), A("Vy"), A("Vz"), A("Pt"),
-                                 *self._tau(), self._dx, self._dy, self._dz)
-        return self.norm_err(("Rx", "Ry", "Rz"), "divV")
-
-
-class V3D(VE3DPerf):
-    """3D viscous Stokes: the fused 3D kernels without elastic terms (no reference script).
+    """scripts/stokes_3D/Stokes3D_ve_perf.jl (fused explicit-index kernels, _dx form).
 
     Adjoint support (no reference counterpart): momentum sources F added to the residual
-    (set_sources), one application of the operator -- τ = 2με̇(V), then R = ∇·τ − ∇P + F and
-    ∇V (apply_operator) -- and ∂J/∂log μ from this case's V and an adjoint case's V
-    (grad_logmu). With adjoint=True the case iterates the transposed system: the free-slip
+    (set_sources); with adjoint=True the case iterates the transposed system: the free-slip
     ghosts stay zero and each ghost face's residual is added to the interior face it copies
-    (ora3v_res_adj)."""
+    (ora3v_res_adj). grad_logmu_ve gives one visco-elastic step's ∂J/∂log μ term from this
+    (forward) case's stresses and an adjoint case's stresses."""
 
-    elastic = False
-    defaults = dict(nt=1, iterMax=2e5, nout=200, eps=1e-8, CFL=0.8 / math.sqrt(3), Re=6 * PI, r=1.0,
+    unfused = False
+    defaults = dict(nt=1, iterMax=200, nout=2000, eps=1e-8, CFL=0.8 / math.sqrt(3), Re=6 * PI, r=1.0,
                     adjoint=False)
 
     def clear_state(self):
@@ -478,10 +456,8 @@ class V3D(VE3DPerf):
 
     def iteration(self):
         L, A = self.L, self.A
-        if not self.adjoint and "Fx" not in self.f:
-            return super().iteration()
         L.ora3p_compute_Pt_tau(A("Pt"), *self._tau(), *self._tau_o(), A("Vx"), A("Vy"), A("Vz"), A("Mus"), A("Gdt"),
-                               self.r, self.G, self.dt, self._dx, self._dy, self._dz, 0)
+                               self.r, self.G, self.dt, self._dx, self._dy, self._dz, int(self.elastic))
         if self.adjoint:
             if "Fx" not in self.f:
                 self.set_sources(*(np.zeros_like(self.f["R" + c]) for c in "xyz"))
@@ -489,8 +465,12 @@ class V3D(VE3DPerf):
             L.ora3v_update_V(A("Vx"), A("Vy"), A("Vz"), A("Rx"), A("Ry"), A("Rz"), A("Fx"), A("Fy"), A("Fz"),
                              A("dtRho"))
             return
-        L.ora3p_compute_V_src(A("Vx"), A("Vy"), A("Vz"), A("Pt"), *self._tau(), A("dtRho"), A("Fx"), A("Fy"),
-                              A("Fz"), self._dx, self._dy, self._dz)
+        if "Fx" in self.f:
+            L.ora3p_compute_V_src(A("Vx"), A("Vy"), A("Vz"), A("Pt"), *self._tau(), A("dtRho"), A("Fx"), A("Fy"),
+                                  A("Fz"), self._dx, self._dy, self._dz)
+        else:
+            L.ora3p_compute_V(A("Vx"), A("Vy"), A("Vz"), A("Pt"), *self._tau(), A("dtRho"), self._dx, self._dy,
+                              self._dz)
         self.bc()
 
     def check(self):
@@ -503,6 +483,27 @@ class V3D(VE3DPerf):
             for c in "xyz":
                 self.f["R" + c][...] = self.f["R" + c] + self.f["F" + c]
         return self.norm_err(("Rx", "Ry", "Rz"), "divV")
+
+    def grad_logmu_ve(self, adj, out=None, tau=None):
+        """One visco-elastic step's ∂J/∂log μ term: written into a new array, or added to
+        `out`. `tau` (6 arrays) replaces this case's current stresses (a checkpoint)."""
+        add = out is not None
+        g = out if add else zeros(self.nx, self.ny, self.nz)
+        T = [arr(t) for t in tau] if tau is not None else self._tau()
+        self.L.ora3ve_grad_logmu(arr(g), *T, *adj._tau(), self.A("Mus"), int(add))
+        return g
+
+
+class V3D(VE3DPerf):
+    """3D viscous Stokes: the fused 3D kernels without elastic terms (no reference script).
+
+    Adjoint support as in VE3DPerf, plus one application of the operator -- τ = 2με̇(V),
+    then R = ∇·τ − ∇P + F and ∇V (apply_operator) -- and the viscous ∂J/∂log μ from this
+    case's V and an adjoint case's V (grad_logmu)."""
+
+    elastic = False
+    defaults = dict(nt=1, iterMax=2e5, nout=200, eps=1e-8, CFL=0.8 / math.sqrt(3), Re=6 * PI, r=1.0,
+                    adjoint=False)
 
     def apply_operator(self):
         A = self.A

@@ -135,7 +135,10 @@ bool field_info(pts_ctx* c, int id, FInfo* o) {
         case PTS_F_FX: if (!has_sources(c)) return false; set(&f.Fx, nx - 1, ny - 2, nz - 2, 1, 1, 1); break;
         case PTS_F_FY: if (!has_sources(c)) return false; set(&f.Fy, nx - 2, ny - 1, nz - 2, 1, 1, 1); break;
         case PTS_F_FZ: if (!has_sources(c)) return false; set(&f.Fz, nx - 2, ny - 2, nz - 1, 1, 1, 1); break;
-        case PTS_F_GRAD: if (c->v != PTS_3D_V) return false; set(&f.grad, nx, ny, nz, 0, 0, 0); break;
+        case PTS_F_GRAD:
+            if (c->v != PTS_3D_V && c->v != PTS_3D_VE_PERF) return false;
+            set(&f.grad, nx, ny, nz, 0, 0, 0);
+            break;
         default: return false;
     }
     return true;
@@ -368,8 +371,10 @@ int pts_create(const pts_desc* d, pts_ctx** out) {
         return fail(nullptr, PTS_E_INVAL, "grid extent too large");
     if (d->nout < 1) return fail(nullptr, PTS_E_INVAL, "nout must be >= 1");
     if (!(d->lx > 0) || !(d->ly > 0) || (d3 && !(d->lz > 0))) return fail(nullptr, PTS_E_INVAL, "domain extents must be > 0");
-    if (d->adjoint && (d->variant != PTS_3D_V || d->precision != PTS_FP64 || d->single_pass))
-        return fail(nullptr, PTS_E_INVAL, "adjoint mode is implemented for PTS_3D_V in FP64 on the two-kernel path");
+    if (d->adjoint && ((d->variant != PTS_3D_V && d->variant != PTS_3D_VE_PERF) || d->precision != PTS_FP64 ||
+                       d->single_pass))
+        return fail(nullptr, PTS_E_INVAL,
+                    "adjoint mode is implemented for PTS_3D_V and PTS_3D_VE_PERF in FP64 on the two-kernel path");
     c = new pts_ctx();
     c->d = *d;
     c->v = d->variant;
@@ -678,13 +683,15 @@ int pts_apply_operator(pts_ctx* c, pts_check* out) {
     return PTS_OK;
 }
 
-int pts_gradient_logmu(pts_ctx* fwd, pts_ctx* adj) {
+namespace {
+int gradient(pts_ctx* fwd, pts_ctx* adj, bool add) {
     pts_ctx* c = fwd;
     int rc = enter(c);
     if (rc) return rc;
     if (!adj) return fail(c, PTS_E_INVAL, "null adjoint context");
-    if (c->v != PTS_3D_V || adj->v != PTS_3D_V || c->mixed || adj->mixed)
-        return fail(c, PTS_E_INVAL, "pts_gradient_logmu needs two 3D_V contexts in FP64");
+    if ((c->v != PTS_3D_V && c->v != PTS_3D_VE_PERF) || adj->v != c->v || c->mixed || adj->mixed)
+        return fail(c, PTS_E_INVAL, "the gradient needs two 3D_V or two 3D_VE_PERF contexts in FP64");
+    if (add && c->v == PTS_3D_V) return fail(c, PTS_E_INVAL, "pts_gradient_logmu_add is for PTS_3D_VE_PERF");
     if (c->n.adjoint || !adj->n.adjoint)
         return fail(c, PTS_E_INVAL, "pts_gradient_logmu takes a forward context and an adjoint-mode context");
     if (adj->g.nx != c->g.nx || adj->g.ny != c->g.ny || adj->g.nz != c->g.nz || adj->n.dx != c->n.dx ||
@@ -692,9 +699,15 @@ int pts_gradient_logmu(pts_ctx* fwd, pts_ctx* adj) {
         return fail(c, PTS_E_INVAL, "forward and adjoint contexts differ in grid, spacing or device");
     if ((rc = alloc_field(c, &c->f.grad)) != PTS_OK) return rc;
     CK(cudaStreamSynchronize(adj->stream));
-    CK(launch_grad_logmu(c->g, c->f, adj->f, c->n, c->stream));
+    if (c->v == PTS_3D_V) CK(launch_grad_logmu(c->g, c->f, adj->f, c->n, c->stream));
+    else CK(launch_grad_logmu_ve(c->g, c->f, adj->f, add, c->stream));
     return synced(c);
 }
+}  // namespace
+
+int pts_gradient_logmu(pts_ctx* fwd, pts_ctx* adj) { return gradient(fwd, adj, false); }
+int pts_gradient_logmu_add(pts_ctx* fwd, pts_ctx* adj) { return gradient(fwd, adj, true); }
+
 
 int pts_iterate(pts_ctx* c, int64_t niter) {
     int rc = enter(c);

@@ -105,6 +105,9 @@ cudaError_t launch_iter_params(int variant, const Geom& g, const Fields64& f, co
 cudaError_t launch_tau_exact(const Geom& g, const Fields64& f, const Num& n, cudaStream_t s);
 // ∂J/∂log μ into fwd.grad, from the forward solution (fwd) and the adjoint solution (adj)
 cudaError_t launch_grad_logmu(const Geom& g, const Fields64& fwd, const Fields64& adj, const Num& n, cudaStream_t s);
+// one physical step's ∂J/∂log μ term of the visco-elastic operator (3D_VE_PERF) from the
+// forward and adjoint stresses, written (add = false) or added (add = true) to fwd.grad
+cudaError_t launch_grad_logmu_ve(const Geom& g, const Fields64& fwd, const Fields64& adj, bool add, cudaStream_t s);
 // single-pass 3D kernel: V update of iteration n from `cur`, then Pt/τ of n+1, into `nxt`
 // `err` is a device flag the kernel sets if one of its bounded staging waits timed out.
 cudaError_t launch_fused3(int variant, const Geom& g, const Fields64& cur, const Fields64& nxt, const Num& n,

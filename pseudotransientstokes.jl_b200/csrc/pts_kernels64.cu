@@ -697,6 +697,60 @@ __global__ void __launch_bounds__(256) k3_grad_logmu(Geom g, Fields64 f, Fields6
     f.grad[c] = -(f.Mus[c] * (2.0 * nrm + shr));
 }
 
+// One physical step's term of ∂J/∂log μ for the visco-elastic operator (3D_VE_PERF), from the
+// forward step's converged stresses τ (f) and the adjoint step's stresses τa (a). A converged
+// VE step has τ = η(2ε̇ + τ_o/(G dt)), η = 1/(1/μ + 1/(G dt)) (μ̄ on the shear edges); its
+// stress multiplier is W·τa/(2η), and the μ-derivative of the constraint gives
+//   ∂J/∂log μ_c += −[Σ_n τa_n τ_n/(2 μ_c) + μ_c Σ_{edges e around c} τa_e τ_e/(4 μ̄_e²)].
+// ADD accumulates into f.grad (the steps of a time loop), otherwise it overwrites.
+template <bool ADD>
+__global__ void __launch_bounds__(256) k3_grad_logmu_ve(Geom g, Fields64 f, Fields64 a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    if (i >= nx || j >= ny) return;
+    const idx_t c = gidx32(g, i, j, k);
+    const idx_t sx = 1, sy = g.px, sz = (idx_t)g.pxy;
+    const double Mc = f.Mus[c];
+    double nrm = 0.0, shr = 0.0;
+    if (j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2) nrm = nrm + a.txx[c] * f.txx[c];
+    if (i >= 1 && i <= nx - 2 && k >= 1 && k <= nz - 2) nrm = nrm + a.tyy[c] * f.tyy[c];
+    if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2) nrm = nrm + a.tzz[c] * f.tzz[c];
+    auto mbar = [&](idx_t e, idx_t s1, idx_t s2) {
+        return (((f.Mus[e - s1 - s2] + f.Mus[e - s2]) + f.Mus[e - s1]) + f.Mus[e]) * 0.25;
+    };
+    if (k >= 1 && k <= nz - 2)
+        for (int dj = 0; dj < 2; ++dj)
+            for (int di = 0; di < 2; ++di) {
+                const int ie = i + di, je = j + dj;
+                if (ie < 1 || ie > nx - 1 || je < 1 || je > ny - 1) continue;
+                const idx_t e = c + di * sx + dj * sy;
+                const double m = mbar(e, sx, sy);
+                shr = shr + a.txy[e] * f.txy[e] / (m * m);
+            }
+    if (j >= 1 && j <= ny - 2)
+        for (int dk = 0; dk < 2; ++dk)
+            for (int di = 0; di < 2; ++di) {
+                const int ie = i + di, ke = k + dk;
+                if (ie < 1 || ie > nx - 1 || ke < 1 || ke > nz - 1) continue;
+                const idx_t e = c + di * sx + dk * sz;
+                const double m = mbar(e, sx, sz);
+                shr = shr + a.txz[e] * f.txz[e] / (m * m);
+            }
+    if (i >= 1 && i <= nx - 2)
+        for (int dk = 0; dk < 2; ++dk)
+            for (int dj = 0; dj < 2; ++dj) {
+                const int je = j + dj, ke = k + dk;
+                if (je < 1 || je > ny - 1 || ke < 1 || ke > nz - 1) continue;
+                const idx_t e = c + dj * sy + dk * sz;
+                const double m = mbar(e, sy, sz);
+                shr = shr + a.tyz[e] * f.tyz[e] / (m * m);
+            }
+    const double t = -(nrm / (2.0 * Mc) + Mc * (shr * 0.25));
+    f.grad[c] = ADD ? f.grad[c] + t : t;
+}
+
 // ------------------------------------------------------------------ batched 2D sweep (persistent)
 
 // Block reduction of one Acc into out[0..7] (fixed order, as acc_block_store).
@@ -1474,6 +1528,13 @@ cudaError_t launch_tau_exact(const Geom& g, const Fields64& f, const Num& n, cud
 cudaError_t launch_grad_logmu(const Geom& g, const Fields64& fwd, const Fields64& adj, const Num& n, cudaStream_t s) {
     if (!fwd.grad) return cudaErrorInvalidValue;
     k3_grad_logmu<<<grid_cells(g), blk(), 0, s>>>(g, fwd, adj, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_grad_logmu_ve(const Geom& g, const Fields64& fwd, const Fields64& adj, bool add, cudaStream_t s) {
+    if (!fwd.grad) return cudaErrorInvalidValue;
+    if (add) k3_grad_logmu_ve<true><<<grid_cells(g), blk(), 0, s>>>(g, fwd, adj);
+    else k3_grad_logmu_ve<false><<<grid_cells(g), blk(), 0, s>>>(g, fwd, adj);
     return cudaGetLastError();
 }
 

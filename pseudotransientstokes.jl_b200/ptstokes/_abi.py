@@ -121,6 +121,7 @@ SIGNATURES = {
     # adjoint of the 3D viscous solve
     "pts_apply_operator": ([_P, ctypes.POINTER(PtsCheck)], ctypes.c_int),
     "pts_gradient_logmu": ([_P, _P], ctypes.c_int),
+    "pts_gradient_logmu_add": ([_P, _P], ctypes.c_int),
     # residual check on caller-owned device arrays; allocates nothing
     "pts_check_noalloc": ([ctypes.POINTER(PtsDesc), ctypes.POINTER(_P), _P, _P], ctypes.c_int),
     # batched 2D sweep

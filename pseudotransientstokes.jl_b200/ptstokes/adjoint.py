@@ -5,7 +5,8 @@ scripts/stokes_3D/Stokes3D_ve_perf.jl without elastic terms) with pure-shear wal
 objective is a misfit of the vertical velocity on the top interior face plane,
 J = ½‖Vz(top) − Vobs‖². ``ViscousAdjoint`` runs the forward solve, the transposed
 (adjoint) solve with the source ∂J/∂Vz on that plane, and the pointwise gradient kernel,
-all on the device (``pts_gradient_logmu`` in include/ptstokes.h). ``TopVz`` wraps the
+all on the device (``pts_gradient_logmu`` in include/ptstokes.h); ``ViscoElasticAdjoint``
+does the same for nt Maxwell visco-elastic steps with per-step checkpoints. ``TopVz`` wraps the
 same steps as a ``torch.autograd.Function`` of log μ (the viscosity the solver uses, after
 any smoothing). ``inclusion_set``, ``viscosity_field`` and ``lognormal_factor`` draw the
 seeded 20-inclusion field and its log-normal perturbation.
@@ -119,6 +120,82 @@ class ViscousAdjoint:
 
     def misfit_gradient(self, vobs):
         """J and ∂J/∂log μ for J = ½‖Vz(top) − Vobs‖² at the current viscosity."""
+        fo = self.forward()
+        r = self.top_vz() - vobs
+        J = 0.5 * float(np.sum(r * r))
+        ao = self.adjoint(r)
+        return J, self.gradient(), fo, ao
+
+
+class ViscoElasticAdjoint:
+    """∂J/∂log μ of J = ½‖Vz(top, last step) − Vobs‖² for nt Maxwell visco-elastic time steps
+    (the 3D_VE_PERF kernels, each step converged to eps), on two contexts of the same grid.
+
+    The forward time loop stores each step's converged stresses (a per-step checkpoint, on
+    the host). The adjoint is the same time loop on an adjoint-mode context, run backwards:
+    assign_τ! (τ_o ← τ) between steps as forward, the source ∂J/∂Vz only in the first
+    adjoint step; after adjoint step s the forward context's stresses are restored from
+    checkpoint nt-1-s and the step's gradient term is accumulated (pts_gradient_logmu_add)."""
+
+    TAU = ("txx", "tyy", "tzz", "txy", "txz", "tyz")
+
+    def __init__(self, nx, ny, nz, nt=5, ebg=1.0, lib=None, **kw):
+        kw.setdefault("nout", 200)
+        kw.setdefault("iter_max", 2e5)
+        kw.setdefault("eps", 1e-8)
+        self.nx, self.ny, self.nz, self.nt, self.ebg = nx, ny, nz, nt, ebg
+        self.fwd = Solver("3d_ve_perf", nx, ny, nz, lib=lib, **kw)
+        self.adj = Solver("3d_ve_perf", nx, ny, nz, lib=lib, adjoint=1, **kw)
+        self.mus = None
+        self.checkpoints = []
+
+    def close(self):
+        self.fwd.close()
+        self.adj.close()
+
+    set_viscosity = ViscousAdjoint.set_viscosity
+    top_vz = ViscousAdjoint.top_vz
+
+    def _prepare(self, s, ebg):
+        s.init_inclusion(1.0, 1.0, 0.0, ebg)
+        s.set("Mus", self.mus)
+        s.compute_maxloc()
+        s.compute_iter_params()
+
+    def forward(self):
+        """nt physical steps from the pure-shear initial state; returns the per-step outcomes."""
+        f = self.fwd
+        self._prepare(f, self.ebg)
+        self.checkpoints, out = [], []
+        for _ in range(self.nt):
+            f.assign_tau()
+            out.append(f.solve())
+            self.checkpoints.append([f.get(n) for n in self.TAU])
+        return out
+
+    def adjoint(self, dJ_dtop):
+        """The backward adjoint time loop with the gradient accumulated step by step."""
+        a, f = self.adj, self.fwd
+        self._prepare(a, 0.0)  # every field zero
+        Fz = np.zeros(a.shape("Fz"), order="F")
+        Fz[:, :, -1] = dJ_dtop
+        a.set("Fz", Fz)
+        out = []
+        for s in range(self.nt):
+            a.assign_tau()
+            out.append(a.solve())
+            for n, t in zip(self.TAU, self.checkpoints[self.nt - 1 - s]):
+                f.set(n, t)
+            f.gradient_logmu(a, add=s > 0)
+            if s == 0:
+                a.set("Fz", np.zeros_like(Fz))
+        return out
+
+    def gradient(self):
+        return self.fwd.get("grad")
+
+    def misfit_gradient(self, vobs):
+        """J and ∂J/∂log μ for J = ½‖Vz(top) − Vobs‖² after the last step."""
         fo = self.forward()
         r = self.top_vz() - vobs
         J = 0.5 * float(np.sum(r * r))

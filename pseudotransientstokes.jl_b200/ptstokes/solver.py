@@ -181,9 +181,11 @@ class Solver:
         self._ck(self.lib.pts_apply_operator(self.ctx, ctypes.byref(c)))
         return c.as_dict()
 
-    def gradient_logmu(self, adj):
-        """∂J/∂log μ into this (forward) context's "grad" field from the adjoint context adj."""
-        self._ck(self.lib.pts_gradient_logmu(self.ctx, adj.ctx))
+    def gradient_logmu(self, adj, add=False):
+        """∂J/∂log μ into this (forward) context's "grad" field from the adjoint context adj
+        (add=True adds one visco-elastic step's term)."""
+        fn = self.lib.pts_gradient_logmu_add if add else self.lib.pts_gradient_logmu
+        self._ck(fn(self.ctx, adj.ctx))
 
     # ---------------------------------------------------------------- drivers
     def iterate(self, n):

@@ -15,19 +15,25 @@ from oracle import scripts as S
 ITER_FIELDS = ("Pt", "Vx", "Vy", "Vz", "txx", "tyy", "tzz", "txy", "txz", "tyz")
 
 
-def oracle_case(n, adjoint=False, **kw):
-    o = S.V3D(*n, musi=1e-2, adjoint=adjoint, **kw).setup()
+ORACLE = {"3d_v": S.V3D, "3d_ve_perf": S.VE3DPerf}
+
+
+def oracle_case(n, adjoint=False, variant="3d_v", **kw):
+    o = ORACLE[variant](*n, musi=1e-2, adjoint=adjoint, **kw).setup()
     if adjoint:
         o.clear_state()
     return o
 
 
-def gpu_like(o, lib, adjoint=False):
+def gpu_like(o, lib, adjoint=False, variant="3d_v"):
     from ptstokes import Solver
-    s = Solver("3d_v", o.nx, o.ny, o.nz, lib=lib, adjoint=int(adjoint), nout=o.nout, eps=o.eps,
+    s = Solver(variant, o.nx, o.ny, o.nz, lib=lib, adjoint=int(adjoint), nout=o.nout, eps=o.eps,
                iter_max=o.iterMax)
     s.init_inclusion(1.0, 1.0, 0.0, 0.0)
-    for name in ("Mus", "Must", "Gdt", "dtRho") + ITER_FIELDS:
+    names = ("Mus", "Must", "Gdt", "dtRho") + ITER_FIELDS
+    if variant == "3d_ve_perf":
+        names += tuple(n + "_o" for n in ITER_FIELDS[4:])
+    for name in names:
         s.set(name, o.f[name])
     return s
 
@@ -37,14 +43,18 @@ def random_sources(o, rng):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("variant", ["3d_v", "3d_ve_perf"])
 @pytest.mark.parametrize("n", [(9, 8, 7), (16, 13, 11)])
 @pytest.mark.parametrize("adjoint", [False, True])
-def test_iterations_with_sources_equal_the_oracle(gpu_lib, n, adjoint):
+def test_iterations_with_sources_equal_the_oracle(gpu_lib, n, adjoint, variant):
     rng = np.random.default_rng(11)
-    o = oracle_case(n, adjoint=adjoint)
+    o = oracle_case(n, adjoint=adjoint, variant=variant)
     F = random_sources(o, rng)
     o.set_sources(*F)
-    s = gpu_like(o, gpu_lib, adjoint)
+    if variant == "3d_ve_perf":  # a pre-stress, as after assign_τ!
+        for name in ITER_FIELDS[4:]:
+            o.f[name + "_o"][...] = rng.standard_normal(o.f[name + "_o"].shape)
+    s = gpu_like(o, gpu_lib, adjoint, variant)
     for c, a in zip("xyz", F):
         s.set("F" + c, a)
     for _ in range(37):
@@ -93,6 +103,61 @@ def test_gradient_kernel_equals_the_oracle(gpu_lib):
     assert np.array_equal(fs.get("grad"), fo.grad_logmu(ao))
     fs.close()
     as_.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("add", [False, True])
+def test_visco_elastic_gradient_kernel_equals_the_oracle(gpu_lib, add):
+    rng = np.random.default_rng(13)
+    n = (13, 12, 10)
+    fo, ao = oracle_case(n, variant="3d_ve_perf"), oracle_case(n, adjoint=True, variant="3d_ve_perf")
+    for o in (fo, ao):
+        for name in ITER_FIELDS[4:]:
+            o.f[name][...] = rng.standard_normal(o.f[name].shape)
+    fs = gpu_like(fo, gpu_lib, variant="3d_ve_perf")
+    as_ = gpu_like(ao, gpu_lib, adjoint=True, variant="3d_ve_perf")
+    g0 = rng.standard_normal((13, 12, 10))
+    if add:
+        fs.gradient_logmu(as_)  # allocates "grad"
+        fs.set("grad", g0)
+    fs.gradient_logmu(as_, add=add)
+    ref = fo.grad_logmu_ve(ao, out=np.asfortranarray(g0.copy()) if add else None)
+    assert np.array_equal(fs.get("grad"), ref)
+    fs.close()
+    as_.close()
+
+
+@pytest.mark.gpu
+def test_visco_elastic_gradient_matches_central_differences(gpu_lib):
+    from ptstokes.adjoint import ViscoElasticAdjoint, inclusion_set, lognormal_factor, viscosity_field
+    n = (18, 17, 16)
+    mus = viscosity_field(*n, inclusion_set(seed=1855, log10_mu=(-2.0, 2.0)))
+    p = ViscoElasticAdjoint(*n, nt=3, lib=gpu_lib, eps=1e-12, nout=100, iter_max=1e6)
+    p.set_viscosity(mus * lognormal_factor(n, seed=1856), nsmooth=10)
+    p.forward()
+    vobs = p.top_vz()
+    p.set_viscosity(mus, nsmooth=10)
+    J0, g, fo, ao = p.misfit_gradient(vobs)
+    assert all(r["converged"] for r in fo + ao)
+    mus0 = p.mus.copy()
+    rng = np.random.default_rng(5)
+    cand = np.argwhere(np.abs(g) >= 1e-3 * np.abs(g).max())
+    cells = [tuple(c) for c in cand[rng.choice(len(cand), 12, replace=False)]]
+    h = 1e-3
+    worst = 0.0
+    for c in cells:
+        Js = []
+        for sgn in (1, -1):
+            m = mus0.copy()
+            m[c] *= math.exp(sgn * h)
+            p.mus = m
+            p.forward()
+            r = p.top_vz() - vobs
+            Js.append(0.5 * float(np.sum(r * r)))
+        fd = (Js[0] - Js[1]) / (2 * h)
+        worst = max(worst, abs(g[c] - fd) / abs(fd))
+    assert worst <= 1e-5, worst
+    p.close()
 
 
 @pytest.mark.gpu
