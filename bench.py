@@ -430,8 +430,48 @@ def run_adjoint(args, ws, rank, local):
         "clocks": clocks,
     }
     p.close()
+    if args.adj_ve_steps > 0:
+        line["visco_elastic"] = adjoint_ve(args, n, mus, pert, delta, rank)
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def adjoint_ve(args, n, mus, pert, delta, rank):
+    """The visco-elastic variant: `--adj-ve-steps` Maxwell steps (G = 1, dt = 1), each to 1e-8,
+    per-step stress checkpoints, the backward adjoint time loop; J on the last step."""
+    import numpy as np
+    import torch
+
+    from ptstokes.adjoint import ViscoElasticAdjoint
+
+    nt = args.adj_ve_steps
+    p = ViscoElasticAdjoint(n, n, n, nt=nt, eps=1e-8, nout=200, iter_max=2e5)
+    p.set_viscosity(mus * pert)
+    p.forward()
+    vobs = p.top_vz()
+    p.set_viscosity(mus)
+    st = torch.cuda.ExternalStream(p.fwd.stream_handle())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    J, g, fo, ao = p.misfit_gradient(vobs)
+    e1.record(st)
+    e1.synchronize()
+    sec = e0.elapsed_time(e1) / 1e3
+    dd_adj = float(np.sum(g * delta))
+    mus0, h, Js = p.mus.copy(), 1e-3, []
+    for sgn in (1, -1):
+        p.mus = mus0 * np.exp(sgn * h * delta)
+        p.forward()
+        r = p.top_vz() - vobs
+        Js.append(0.5 * float(np.sum(r * r)))
+    dd_fd = (Js[0] - Js[1]) / (2 * h)
+    p.close()
+    return {"steps": nt, "seconds": round(sec, 3), "forward_iters": [r["iters"] for r in fo],
+            "adjoint_iters": [r["iters"] for r in ao], "converged": all(r["converged"] for r in fo + ao),
+            "checkpoint_bytes": 6 * nt * n ** 3 * 8, "J": J,
+            "directional_check": {"adjoint": dd_adj, "central_difference": dd_fd, "h": h,
+                                  "rel_err": abs(dd_adj - dd_fd) / max(abs(dd_fd), 1e-300)}}
 
 
 def run_inclusions(args, ws, rank, local):
@@ -545,6 +585,7 @@ def main():
     ap.add_argument("--batch-n", type=int, default=256)
     ap.add_argument("--adjoint", action="store_true", help="run the adjoint-gradient configuration instead")
     ap.add_argument("--adj-n", type=int, default=255)
+    ap.add_argument("--adj-ve-steps", type=int, default=5, help="visco-elastic adjoint steps (0: skip)")
     ap.add_argument("--inclusions", action="store_true", help="run the 20-inclusion mixed-precision comparison")
     ap.add_argument("--incl-n", type=int, default=255)
     ap.add_argument("--log10-range", type=float, default=2.0,
