@@ -304,9 +304,12 @@ def run_ours(args, ws, rank, local, pg):
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(t_ms / args.steps, 3), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (the reference's own "
-            "inclusion problem: spherical inclusion r=1 mu=1e-3, pure shear, G=1, dt=1)",
-            "config": {"workload": "3D VE Stokes (Stokes3D_ve_perf.jl kernels), FP64, 511^3, box 10^3",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32 sweeps, f64 correction",
+            "data": "synthetic (the reference's own inclusion problem: spherical inclusion r=1 mu=1e-3, pure shear, "
+            "G=1, dt=1)",
+            "config": {"workload": f"3D VE Stokes (Stokes3D_ve_perf.jl kernels), {args.precision.upper()}, {n}^3, "
+                                   "box 10^3",
                        "nx": n, "ny": n, "nz": n, "iters_per_step": nout, "t_it_ms": round(t_it * 1e3, 4),
                        "path": "2 kernels per PT iteration, CUDA graph per check block",
                        "parallelism": f"replicas x{ws}", "l2": "inputs larger than L2 (1.07 GB per field)"},
@@ -520,7 +523,8 @@ def run_inclusions(args, ws, rank, local):
     line = {
         "metric": f"time to err <= 1e-8, 3D viscous {n}^3 with 20 inclusions: FP32 inner sweeps + FP64 correction vs FP64",
         "value": round(out["fp64"]["seconds"] / out["mixed"]["seconds"], 3), "unit": "speed-up (x)", "n_gpus": ws,
-        "higher_is_better": True, "scaling": "weak", "dtype": "f32+f64", "data": "synthetic seeded 20-inclusion field",
+        "higher_is_better": True, "scaling": "weak", "dtype": "f32 sweeps, f64 correction",
+        "data": "synthetic seeded 20-inclusion field",
         "config": {"workload": f"3D viscous Stokes {n}^3", "inclusions": 20, "log10_mu_range": [-L, L], "eps": 1e-8,
                    "nout": 200},
         "fp64": out["fp64"], "mixed": out["mixed"], "mixed_error_vs_fp64": errs,
