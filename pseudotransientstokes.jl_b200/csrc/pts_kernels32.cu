@@ -26,7 +26,8 @@ struct Num32 {
 
 __device__ __forceinline__ float gr32(float g, const Num32& n) { return n.gdt_one ? g : __fdividef(g, n.gdt); }
 
-// δ-form compute_Pt_τ!, one thread per cell.
+// δ-form compute_Pt_τ!, one thread per cell (arrays it only reads go through the read-only
+// data path).
 template <bool EL>
 __global__ void __launch_bounds__(256) k3_corrA(Geom g, Mixed32 m, Num32 n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -36,37 +37,37 @@ __global__ void __launch_bounds__(256) k3_corrA(Geom g, Mixed32 m, Num32 n) {
     if (i >= nx || j >= ny) return;
     const idx_t c = gidx32(g, i, j, k);
     const idx_t sx = 1, sy = g.px, sz = (idx_t)g.pxy;
-    const float dvx = m.dVx[c + sx] - m.dVx[c];
-    const float dvy = m.dVy[c + sy] - m.dVy[c];
-    const float dvz = m.dVz[c + sz] - m.dVz[c];
-    const float Gc = m.Gdt[c], Mc = m.Mus[c];
-    m.dPt[c] = m.dPt[c] - n.r * Gc * (m.aP[c] + ((n._dx * dvx + n._dy * dvy) + n._dz * dvz));
+    const float dvx = __ldg(&m.dVx[c + sx]) - __ldg(&m.dVx[c]);
+    const float dvy = __ldg(&m.dVy[c + sy]) - __ldg(&m.dVy[c]);
+    const float dvz = __ldg(&m.dVz[c + sz]) - __ldg(&m.dVz[c]);
+    const float Gc = __ldg(&m.Gdt[c]), Mc = __ldg(&m.Mus[c]);
+    m.dPt[c] = m.dPt[c] - n.r * Gc * (__ldg(&m.aP[c]) + ((n._dx * dvx + n._dy * dvy) + n._dz * dvz));
     const float Dn = (1.0f + __fdividef(Gc, Mc)) + (EL ? gr32(Gc, n) : 0.0f);
     const float G2 = 2.0f * Gc;
     const float rDn = __fdividef(1.0f, Dn);
     if (j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2)
-        m.dtxx[c] = ((m.dtxx[c] + m.atxx[c]) + G2 * (n._dx * dvx)) * rDn;
+        m.dtxx[c] = ((m.dtxx[c] + __ldg(&m.atxx[c])) + G2 * (n._dx * dvx)) * rDn;
     if (i >= 1 && i <= nx - 2 && k >= 1 && k <= nz - 2)
-        m.dtyy[c] = ((m.dtyy[c] + m.atyy[c]) + G2 * (n._dy * dvy)) * rDn;
+        m.dtyy[c] = ((m.dtyy[c] + __ldg(&m.atyy[c])) + G2 * (n._dy * dvy)) * rDn;
     if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2)
-        m.dtzz[c] = ((m.dtzz[c] + m.atzz[c]) + G2 * (n._dz * dvz)) * rDn;
+        m.dtzz[c] = ((m.dtzz[c] + __ldg(&m.atzz[c])) + G2 * (n._dz * dvz)) * rDn;
     if (i >= 1 && j >= 1 && k >= 1 && k <= nz - 2) {
-        const float ag = (((m.Gdt[c - sx - sy] + m.Gdt[c - sy]) + m.Gdt[c - sx]) + Gc) * 0.25f;
-        const float am = (((m.Mus[c - sx - sy] + m.Mus[c - sy]) + m.Mus[c - sx]) + Mc) * 0.25f;
-        const float s = 0.5f * (n._dy * (m.dVx[c] - m.dVx[c - sy]) + n._dx * (m.dVy[c] - m.dVy[c - sx]));
-        m.dtxy[c] = __fdividef((m.dtxy[c] + m.atxy[c]) + (2.0f * ag) * s, (1.0f + __fdividef(ag, am)) + (EL ? gr32(ag, n) : 0.0f));
+        const float ag = (((__ldg(&m.Gdt[c - sx - sy]) + __ldg(&m.Gdt[c - sy])) + __ldg(&m.Gdt[c - sx])) + Gc) * 0.25f;
+        const float am = (((__ldg(&m.Mus[c - sx - sy]) + __ldg(&m.Mus[c - sy])) + __ldg(&m.Mus[c - sx])) + Mc) * 0.25f;
+        const float s = 0.5f * (n._dy * (__ldg(&m.dVx[c]) - __ldg(&m.dVx[c - sy])) + n._dx * (__ldg(&m.dVy[c]) - __ldg(&m.dVy[c - sx])));
+        m.dtxy[c] = __fdividef((m.dtxy[c] + __ldg(&m.atxy[c])) + (2.0f * ag) * s, (1.0f + __fdividef(ag, am)) + (EL ? gr32(ag, n) : 0.0f));
     }
     if (i >= 1 && j >= 1 && j <= ny - 2 && k >= 1) {
-        const float ag = (((m.Gdt[c - sx - sz] + m.Gdt[c - sz]) + m.Gdt[c - sx]) + Gc) * 0.25f;
-        const float am = (((m.Mus[c - sx - sz] + m.Mus[c - sz]) + m.Mus[c - sx]) + Mc) * 0.25f;
-        const float s = 0.5f * (n._dz * (m.dVx[c] - m.dVx[c - sz]) + n._dx * (m.dVz[c] - m.dVz[c - sx]));
-        m.dtxz[c] = __fdividef((m.dtxz[c] + m.atxz[c]) + (2.0f * ag) * s, (1.0f + __fdividef(ag, am)) + (EL ? gr32(ag, n) : 0.0f));
+        const float ag = (((__ldg(&m.Gdt[c - sx - sz]) + __ldg(&m.Gdt[c - sz])) + __ldg(&m.Gdt[c - sx])) + Gc) * 0.25f;
+        const float am = (((__ldg(&m.Mus[c - sx - sz]) + __ldg(&m.Mus[c - sz])) + __ldg(&m.Mus[c - sx])) + Mc) * 0.25f;
+        const float s = 0.5f * (n._dz * (__ldg(&m.dVx[c]) - __ldg(&m.dVx[c - sz])) + n._dx * (__ldg(&m.dVz[c]) - __ldg(&m.dVz[c - sx])));
+        m.dtxz[c] = __fdividef((m.dtxz[c] + __ldg(&m.atxz[c])) + (2.0f * ag) * s, (1.0f + __fdividef(ag, am)) + (EL ? gr32(ag, n) : 0.0f));
     }
     if (i >= 1 && i <= nx - 2 && j >= 1 && k >= 1) {
-        const float ag = (((m.Gdt[c - sy - sz] + m.Gdt[c - sz]) + m.Gdt[c - sy]) + Gc) * 0.25f;
-        const float am = (((m.Mus[c - sy - sz] + m.Mus[c - sz]) + m.Mus[c - sy]) + Mc) * 0.25f;
-        const float s = 0.5f * (n._dz * (m.dVy[c] - m.dVy[c - sz]) + n._dy * (m.dVz[c] - m.dVz[c - sy]));
-        m.dtyz[c] = __fdividef((m.dtyz[c] + m.atyz[c]) + (2.0f * ag) * s, (1.0f + __fdividef(ag, am)) + (EL ? gr32(ag, n) : 0.0f));
+        const float ag = (((__ldg(&m.Gdt[c - sy - sz]) + __ldg(&m.Gdt[c - sz])) + __ldg(&m.Gdt[c - sy])) + Gc) * 0.25f;
+        const float am = (((__ldg(&m.Mus[c - sy - sz]) + __ldg(&m.Mus[c - sz])) + __ldg(&m.Mus[c - sy])) + Mc) * 0.25f;
+        const float s = 0.5f * (n._dz * (__ldg(&m.dVy[c]) - __ldg(&m.dVy[c - sz])) + n._dy * (__ldg(&m.dVz[c]) - __ldg(&m.dVz[c - sy])));
+        m.dtyz[c] = __fdividef((m.dtyz[c] + __ldg(&m.atyz[c])) + (2.0f * ag) * s, (1.0f + __fdividef(ag, am)) + (EL ? gr32(ag, n) : 0.0f));
     }
 }
 
@@ -96,11 +97,11 @@ __global__ void __launch_bounds__(256) k3_corrB(Geom g, Mixed32 m, Num32 n) {
     if (j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2) {
         float v = m.dVx[c];
         if (i >= 1 && i <= nx - 1) {
-            const float R = (((n._dx * (m.dtxx[c] - m.dtxx[c - sx]) + n._dy * (m.dtxy[c + sy] - m.dtxy[c])) +
-                              n._dz * (m.dtxz[c + sz] - m.dtxz[c])) -
-                             n._dx * (m.dPt[c] - m.dPt[c - sx])) +
-                            m.aVx[c];
-            v = v + R * ((m.dtRho[c - sx] + m.dtRho[c]) * 0.5f);
+            const float R = (((n._dx * (__ldg(&m.dtxx[c]) - __ldg(&m.dtxx[c - sx])) + n._dy * (__ldg(&m.dtxy[c + sy]) - __ldg(&m.dtxy[c]))) +
+                              n._dz * (__ldg(&m.dtxz[c + sz]) - __ldg(&m.dtxz[c]))) -
+                             n._dx * (__ldg(&m.dPt[c]) - __ldg(&m.dPt[c - sx]))) +
+                            __ldg(&m.aVx[c]);
+            v = v + R * ((__ldg(&m.dtRho[c - sx]) + __ldg(&m.dtRho[c])) * 0.5f);
             m.dVx[c] = v;
         }
         bc_copies32(m.dVx, c, v, j, 1, ny - 2, sy, k, 1, nz - 2, sz);
@@ -108,11 +109,11 @@ __global__ void __launch_bounds__(256) k3_corrB(Geom g, Mixed32 m, Num32 n) {
     if (i >= 1 && i <= nx - 2 && k >= 1 && k <= nz - 2) {
         float v = m.dVy[c];
         if (j >= 1 && j <= ny - 1) {
-            const float R = (((n._dy * (m.dtyy[c] - m.dtyy[c - sy]) + n._dx * (m.dtxy[c + sx] - m.dtxy[c])) +
-                              n._dz * (m.dtyz[c + sz] - m.dtyz[c])) -
-                             n._dy * (m.dPt[c] - m.dPt[c - sy])) +
-                            m.aVy[c];
-            v = v + R * ((m.dtRho[c - sy] + m.dtRho[c]) * 0.5f);
+            const float R = (((n._dy * (__ldg(&m.dtyy[c]) - __ldg(&m.dtyy[c - sy])) + n._dx * (__ldg(&m.dtxy[c + sx]) - __ldg(&m.dtxy[c]))) +
+                              n._dz * (__ldg(&m.dtyz[c + sz]) - __ldg(&m.dtyz[c]))) -
+                             n._dy * (__ldg(&m.dPt[c]) - __ldg(&m.dPt[c - sy]))) +
+                            __ldg(&m.aVy[c]);
+            v = v + R * ((__ldg(&m.dtRho[c - sy]) + __ldg(&m.dtRho[c])) * 0.5f);
             m.dVy[c] = v;
         }
         bc_copies32(m.dVy, c, v, i, 1, nx - 2, sx, k, 1, nz - 2, sz);
@@ -120,11 +121,11 @@ __global__ void __launch_bounds__(256) k3_corrB(Geom g, Mixed32 m, Num32 n) {
     if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2) {
         float v = m.dVz[c];
         if (k >= 1 && k <= nz - 1) {
-            const float R = (((n._dz * (m.dtzz[c] - m.dtzz[c - sz]) + n._dx * (m.dtxz[c + sx] - m.dtxz[c])) +
-                              n._dy * (m.dtyz[c + sy] - m.dtyz[c])) -
-                             n._dz * (m.dPt[c] - m.dPt[c - sz])) +
-                            m.aVz[c];
-            v = v + R * ((m.dtRho[c - sz] + m.dtRho[c]) * 0.5f);
+            const float R = (((n._dz * (__ldg(&m.dtzz[c]) - __ldg(&m.dtzz[c - sz])) + n._dx * (__ldg(&m.dtxz[c + sx]) - __ldg(&m.dtxz[c]))) +
+                              n._dy * (__ldg(&m.dtyz[c + sy]) - __ldg(&m.dtyz[c]))) -
+                             n._dz * (__ldg(&m.dPt[c]) - __ldg(&m.dPt[c - sz]))) +
+                            __ldg(&m.aVz[c]);
+            v = v + R * ((__ldg(&m.dtRho[c - sz]) + __ldg(&m.dtRho[c])) * 0.5f);
             m.dVz[c] = v;
         }
         bc_copies32(m.dVz, c, v, i, 1, nx - 2, sx, j, 1, ny - 2, sy);

@@ -66,6 +66,7 @@ __device__ __forceinline__ double dsc(double d, double h, double ih) {
 // ------------------------------------------------------------------ 3D kernels
 
 // compute_P! + compute_τ! (roles) == compute_Pt_τ! (perf), one thread per cell (i,j,k).
+// Arrays the kernel only reads (V, Gdτ, Mus, τ_o) go through the read-only data path.
 template <bool EL, bool PERF>
 __global__ void __launch_bounds__(256) k3_Pt_tau(Geom g, Fields64 f, Num n, int roles, int store_divV) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -75,10 +76,10 @@ __global__ void __launch_bounds__(256) k3_Pt_tau(Geom g, Fields64 f, Num n, int 
     if (i >= nx || j >= ny) return;
     const idx_t c = gidx32(g, i, j, k);
     const idx_t sx = 1, sy = g.px, sz = (idx_t)g.pxy;
-    const double dvx = f.Vx[c + sx] - f.Vx[c];
-    const double dvy = f.Vy[c + sy] - f.Vy[c];
-    const double dvz = f.Vz[c + sz] - f.Vz[c];
-    const double Gc = f.Gdt[c];
+    const double dvx = __ldg(&f.Vx[c + sx]) - __ldg(&f.Vx[c]);
+    const double dvy = __ldg(&f.Vy[c + sy]) - __ldg(&f.Vy[c]);
+    const double dvz = __ldg(&f.Vz[c + sz]) - __ldg(&f.Vz[c]);
+    const double Gc = __ldg(&f.Gdt[c]);
     if (roles & ROLE_P) {
         if (PERF) {
             f.Pt[c] = f.Pt[c] - n.r * Gc * ((n._dx * dvx + n._dy * dvy) + n._dz * dvz);
@@ -89,34 +90,34 @@ __global__ void __launch_bounds__(256) k3_Pt_tau(Geom g, Fields64 f, Num n, int 
         }
     }
     if (!(roles & ROLE_TAU)) return;
-    const double Mc = f.Mus[c];
+    const double Mc = __ldg(&f.Mus[c]);
     const double gdt = n.gdt;
     if (j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2)
-        f.txx[c] = tau_n<EL, PERF>(f.txx[c], EL ? f.txx_o[c] : 0.0, Gc, Mc, gdt, n.dx, n._dx, dvx);
+        f.txx[c] = tau_n<EL, PERF>(f.txx[c], EL ? __ldg(&f.txx_o[c]) : 0.0, Gc, Mc, gdt, n.dx, n._dx, dvx);
     if (i >= 1 && i <= nx - 2 && k >= 1 && k <= nz - 2)
-        f.tyy[c] = tau_n<EL, PERF>(f.tyy[c], EL ? f.tyy_o[c] : 0.0, Gc, Mc, gdt, n.dy, n._dy, dvy);
+        f.tyy[c] = tau_n<EL, PERF>(f.tyy[c], EL ? __ldg(&f.tyy_o[c]) : 0.0, Gc, Mc, gdt, n.dy, n._dy, dvy);
     if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2)
-        f.tzz[c] = tau_n<EL, PERF>(f.tzz[c], EL ? f.tzz_o[c] : 0.0, Gc, Mc, gdt, n.dz, n._dz, dvz);
+        f.tzz[c] = tau_n<EL, PERF>(f.tzz[c], EL ? __ldg(&f.tzz_o[c]) : 0.0, Gc, Mc, gdt, n.dz, n._dz, dvz);
     // τxy on edge (x-face i, y-face j, cell k): i in [1,nx-1], j in [1,ny-1], k in [1,nz-2]
     if (i >= 1 && j >= 1 && k >= 1 && k <= nz - 2) {
-        const double ag = (((f.Gdt[c - sx - sy] + f.Gdt[c - sy]) + f.Gdt[c - sx]) + Gc) * 0.25;
-        const double am = (((f.Mus[c - sx - sy] + f.Mus[c - sy]) + f.Mus[c - sx]) + Mc) * 0.25;
-        f.txy[c] = tau_s<EL, PERF>(f.txy[c], EL ? f.txy_o[c] : 0.0, ag, am, gdt, n.dy, n._dy, f.Vx[c] - f.Vx[c - sy],
-                                   n.dx, n._dx, f.Vy[c] - f.Vy[c - sx]);
+        const double ag = (((__ldg(&f.Gdt[c - sx - sy]) + __ldg(&f.Gdt[c - sy])) + __ldg(&f.Gdt[c - sx])) + Gc) * 0.25;
+        const double am = (((__ldg(&f.Mus[c - sx - sy]) + __ldg(&f.Mus[c - sy])) + __ldg(&f.Mus[c - sx])) + Mc) * 0.25;
+        f.txy[c] = tau_s<EL, PERF>(f.txy[c], EL ? __ldg(&f.txy_o[c]) : 0.0, ag, am, gdt, n.dy, n._dy, __ldg(&f.Vx[c]) - __ldg(&f.Vx[c - sy]),
+                                   n.dx, n._dx, __ldg(&f.Vy[c]) - __ldg(&f.Vy[c - sx]));
     }
     // τxz on edge (x-face i, cell j, z-face k): i in [1,nx-1], j in [1,ny-2], k in [1,nz-1]
     if (i >= 1 && j >= 1 && j <= ny - 2 && k >= 1) {
-        const double ag = (((f.Gdt[c - sx - sz] + f.Gdt[c - sz]) + f.Gdt[c - sx]) + Gc) * 0.25;
-        const double am = (((f.Mus[c - sx - sz] + f.Mus[c - sz]) + f.Mus[c - sx]) + Mc) * 0.25;
-        f.txz[c] = tau_s<EL, PERF>(f.txz[c], EL ? f.txz_o[c] : 0.0, ag, am, gdt, n.dz, n._dz, f.Vx[c] - f.Vx[c - sz],
-                                   n.dx, n._dx, f.Vz[c] - f.Vz[c - sx]);
+        const double ag = (((__ldg(&f.Gdt[c - sx - sz]) + __ldg(&f.Gdt[c - sz])) + __ldg(&f.Gdt[c - sx])) + Gc) * 0.25;
+        const double am = (((__ldg(&f.Mus[c - sx - sz]) + __ldg(&f.Mus[c - sz])) + __ldg(&f.Mus[c - sx])) + Mc) * 0.25;
+        f.txz[c] = tau_s<EL, PERF>(f.txz[c], EL ? __ldg(&f.txz_o[c]) : 0.0, ag, am, gdt, n.dz, n._dz, __ldg(&f.Vx[c]) - __ldg(&f.Vx[c - sz]),
+                                   n.dx, n._dx, __ldg(&f.Vz[c]) - __ldg(&f.Vz[c - sx]));
     }
     // τyz on edge (cell i, y-face j, z-face k): i in [1,nx-2], j in [1,ny-1], k in [1,nz-1]
     if (i >= 1 && i <= nx - 2 && j >= 1 && k >= 1) {
-        const double ag = (((f.Gdt[c - sy - sz] + f.Gdt[c - sz]) + f.Gdt[c - sy]) + Gc) * 0.25;
-        const double am = (((f.Mus[c - sy - sz] + f.Mus[c - sz]) + f.Mus[c - sy]) + Mc) * 0.25;
-        f.tyz[c] = tau_s<EL, PERF>(f.tyz[c], EL ? f.tyz_o[c] : 0.0, ag, am, gdt, n.dz, n._dz, f.Vy[c] - f.Vy[c - sz],
-                                   n.dy, n._dy, f.Vz[c] - f.Vz[c - sy]);
+        const double ag = (((__ldg(&f.Gdt[c - sy - sz]) + __ldg(&f.Gdt[c - sz])) + __ldg(&f.Gdt[c - sy])) + Gc) * 0.25;
+        const double am = (((__ldg(&f.Mus[c - sy - sz]) + __ldg(&f.Mus[c - sz])) + __ldg(&f.Mus[c - sy])) + Mc) * 0.25;
+        f.tyz[c] = tau_s<EL, PERF>(f.tyz[c], EL ? __ldg(&f.tyz_o[c]) : 0.0, ag, am, gdt, n.dz, n._dz, __ldg(&f.Vy[c]) - __ldg(&f.Vy[c - sz]),
+                                   n.dy, n._dy, __ldg(&f.Vz[c]) - __ldg(&f.Vz[c - sy]));
     }
 }
 
@@ -125,23 +126,23 @@ __global__ void __launch_bounds__(256) k3_Pt_tau(Geom g, Fields64 f, Num n, int 
 template <bool PERF>
 __device__ __forceinline__ double res3_x(const Fields64& f, const Num& n, idx_t c, idx_t sx, idx_t sy,
                                          idx_t sz) {
-    return ((dsc<PERF>(f.txx[c] - f.txx[c - sx], n.dx, n._dx) + dsc<PERF>(f.txy[c + sy] - f.txy[c], n.dy, n._dy)) +
-            dsc<PERF>(f.txz[c + sz] - f.txz[c], n.dz, n._dz)) -
-           dsc<PERF>(f.Pt[c] - f.Pt[c - sx], n.dx, n._dx);
+    return ((dsc<PERF>(__ldg(&f.txx[c]) - __ldg(&f.txx[c - sx]), n.dx, n._dx) + dsc<PERF>(__ldg(&f.txy[c + sy]) - __ldg(&f.txy[c]), n.dy, n._dy)) +
+            dsc<PERF>(__ldg(&f.txz[c + sz]) - __ldg(&f.txz[c]), n.dz, n._dz)) -
+           dsc<PERF>(__ldg(&f.Pt[c]) - __ldg(&f.Pt[c - sx]), n.dx, n._dx);
 }
 template <bool PERF>
 __device__ __forceinline__ double res3_y(const Fields64& f, const Num& n, idx_t c, idx_t sx, idx_t sy,
                                          idx_t sz) {
-    return ((dsc<PERF>(f.tyy[c] - f.tyy[c - sy], n.dy, n._dy) + dsc<PERF>(f.txy[c + sx] - f.txy[c], n.dx, n._dx)) +
-            dsc<PERF>(f.tyz[c + sz] - f.tyz[c], n.dz, n._dz)) -
-           dsc<PERF>(f.Pt[c] - f.Pt[c - sy], n.dy, n._dy);
+    return ((dsc<PERF>(__ldg(&f.tyy[c]) - __ldg(&f.tyy[c - sy]), n.dy, n._dy) + dsc<PERF>(__ldg(&f.txy[c + sx]) - __ldg(&f.txy[c]), n.dx, n._dx)) +
+            dsc<PERF>(__ldg(&f.tyz[c + sz]) - __ldg(&f.tyz[c]), n.dz, n._dz)) -
+           dsc<PERF>(__ldg(&f.Pt[c]) - __ldg(&f.Pt[c - sy]), n.dy, n._dy);
 }
 template <bool PERF>
 __device__ __forceinline__ double res3_z(const Fields64& f, const Num& n, idx_t c, idx_t sx, idx_t sy,
                                          idx_t sz) {
-    return ((dsc<PERF>(f.tzz[c] - f.tzz[c - sz], n.dz, n._dz) + dsc<PERF>(f.txz[c + sx] - f.txz[c], n.dx, n._dx)) +
-            dsc<PERF>(f.tyz[c + sy] - f.tyz[c], n.dy, n._dy)) -
-           dsc<PERF>(f.Pt[c] - f.Pt[c - sz], n.dz, n._dz);
+    return ((dsc<PERF>(__ldg(&f.tzz[c]) - __ldg(&f.tzz[c - sz]), n.dz, n._dz) + dsc<PERF>(__ldg(&f.txz[c + sx]) - __ldg(&f.txz[c]), n.dx, n._dx)) +
+            dsc<PERF>(__ldg(&f.tyz[c + sy]) - __ldg(&f.tyz[c]), n.dy, n._dy)) -
+           dsc<PERF>(__ldg(&f.Pt[c]) - __ldg(&f.Pt[c - sz]), n.dz, n._dz);
 }
 
 // Residual of the transposed system at an interior face (adjoint mode of 3D_V): the face's
@@ -220,8 +221,8 @@ __global__ void __launch_bounds__(256) k3_V_bc(Geom g, Fields64 f, Num n, int up
         double v = f.Vx[c];
         if (update && i >= 1 && i <= nx - 1) {
             const double R0 = ADJ ? res3_fold<0>(g, f, n, i, j, k) : res3_x<PERF>(f, n, c, sx, sy, sz);
-            const double R = SRC ? R0 + f.Fx[c] : R0;
-            v = v + R * ((f.dtRho[c - sx] + f.dtRho[c]) * 0.5);
+            const double R = SRC ? R0 + __ldg(&f.Fx[c]) : R0;
+            v = v + R * ((__ldg(&f.dtRho[c - sx]) + __ldg(&f.dtRho[c])) * 0.5);
             f.Vx[c] = v;
         }
         if (!ADJ) bc_copies(f.Vx, c, v, j, 1, ny - 2, sy, k, 1, nz - 2, sz);
@@ -231,8 +232,8 @@ __global__ void __launch_bounds__(256) k3_V_bc(Geom g, Fields64 f, Num n, int up
         double v = f.Vy[c];
         if (update && j >= 1 && j <= ny - 1) {
             const double R0 = ADJ ? res3_fold<1>(g, f, n, i, j, k) : res3_y<PERF>(f, n, c, sx, sy, sz);
-            const double R = SRC ? R0 + f.Fy[c] : R0;
-            v = v + R * ((f.dtRho[c - sy] + f.dtRho[c]) * 0.5);
+            const double R = SRC ? R0 + __ldg(&f.Fy[c]) : R0;
+            v = v + R * ((__ldg(&f.dtRho[c - sy]) + __ldg(&f.dtRho[c])) * 0.5);
             f.Vy[c] = v;
         }
         if (!ADJ) bc_copies(f.Vy, c, v, i, 1, nx - 2, sx, k, 1, nz - 2, sz);
@@ -242,8 +243,8 @@ __global__ void __launch_bounds__(256) k3_V_bc(Geom g, Fields64 f, Num n, int up
         double v = f.Vz[c];
         if (update && k >= 1 && k <= nz - 1) {
             const double R0 = ADJ ? res3_fold<2>(g, f, n, i, j, k) : res3_z<PERF>(f, n, c, sx, sy, sz);
-            const double R = SRC ? R0 + f.Fz[c] : R0;
-            v = v + R * ((f.dtRho[c - sz] + f.dtRho[c]) * 0.5);
+            const double R = SRC ? R0 + __ldg(&f.Fz[c]) : R0;
+            v = v + R * ((__ldg(&f.dtRho[c - sz]) + __ldg(&f.dtRho[c])) * 0.5);
             f.Vz[c] = v;
         }
         if (!ADJ) bc_copies(f.Vz, c, v, i, 1, nx - 2, sx, j, 1, ny - 2, sy);

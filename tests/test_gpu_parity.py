@@ -138,6 +138,7 @@ def test_fused_role_pair_bit_exact(gpu_lib, variant, dims):
 
 @pytest.mark.parametrize("variant,dims,kw", [
     ("2d_v", (31, 31), dict(nout=100)),
+    ("2d_v", (127, 127), dict(nout=100)),  # the CPU-runnable configuration: 127², tol 1e-8, check every 100
     ("2d_ve", (31, 27), dict(nout=100, nt=2)),
     ("3d_ve", (15, 15, 13), dict(nout=100, nt=2)),
     ("3d_v", (15, 13, 15), dict(nout=100, nt=1)),
