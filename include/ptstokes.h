@@ -238,7 +238,7 @@ PTS_API const char* pts_batch_last_error(const pts_batch* b);
 /* ICs and smooth! x10 of Mus and ρg for every instance (Stokes2D_param.jl:179-189) */
 PTS_API int pts_batch_setup(pts_batch* b);
 PTS_API int pts_batch_set_tile(pts_batch* b, int32_t tile);
-/* The persistent launch (captured in a CUDA graph when the driver allows it): runs until
+/* The persistent launch (captured in a CUDA graph when the CUDA driver allows it): runs until
  * every instance has converged or passed its iterMax; iter_limit >= 0 is a further ceiling
  * common to all. Synchronous. iters/err/converged (length n, may be NULL) receive each
  * instance's outcome; converged is 0 for an instance stopped by iterMax or by NaN (the call

@@ -71,9 +71,9 @@ template <bool EL, bool PERF>
 __global__ void __launch_bounds__(256) k3_Pt_tau(Geom g, Fields64 f, Num n, int roles, int store_divV) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int k = blockIdx.z;
+    const int k = blockIdx.z * blockDim.z + threadIdx.z;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
-    if (i >= nx || j >= ny) return;
+    if (i >= nx || j >= ny || k >= nz) return;
     const idx_t c = gidx32(g, i, j, k);
     const idx_t sx = 1, sy = g.px, sz = (idx_t)g.pxy;
     const double dvx = __ldg(&f.Vx[c + sx]) - __ldg(&f.Vx[c]);
@@ -1327,13 +1327,24 @@ inline dim3 grid_faces(const Geom& g, bool d3) {
 
 // ------------------------------------------------------------------ launchers
 
+// Block of the 3D compute_Pt_τ! kernel: x-y tile with a short z-extent.
+#ifndef PTS_PT_BX
+#define PTS_PT_BX 32
+#define PTS_PT_BY 8
+#define PTS_PT_BZ 1
+#endif
+inline dim3 blk_pt() { return dim3(PTS_PT_BX, PTS_PT_BY, PTS_PT_BZ); }
+inline dim3 grid_pt(const Geom& g) {
+    return dim3((g.nx + PTS_PT_BX - 1) / PTS_PT_BX, (g.ny + PTS_PT_BY - 1) / PTS_PT_BY, (g.nz + PTS_PT_BZ - 1) / PTS_PT_BZ);
+}
+
 cudaError_t launch_Pt_tau(int v, const Geom& g, const Fields64& f, const Num& n, int roles, bool store_divV,
                           cudaStream_t s) {
     const int sd = store_divV ? 1 : 0;
     switch (v) {
-        case VE3D: k3_Pt_tau<true, false><<<grid_cells(g), blk(), 0, s>>>(g, f, n, roles, sd); break;
-        case VE3D_PERF: k3_Pt_tau<true, true><<<grid_cells(g), blk(), 0, s>>>(g, f, n, roles, sd); break;
-        case V3D: k3_Pt_tau<false, true><<<grid_cells(g), blk(), 0, s>>>(g, f, n, roles, sd); break;
+        case VE3D: k3_Pt_tau<true, false><<<grid_pt(g), blk_pt(), 0, s>>>(g, f, n, roles, sd); break;
+        case VE3D_PERF: k3_Pt_tau<true, true><<<grid_pt(g), blk_pt(), 0, s>>>(g, f, n, roles, sd); break;
+        case V3D: k3_Pt_tau<false, true><<<grid_pt(g), blk_pt(), 0, s>>>(g, f, n, roles, sd); break;
         case V2D: k2_Pt_tau<V2D><<<grid_cells(g), blk(), 0, s>>>(g, f, n, roles, sd); break;
         case VE2D: k2_Pt_tau<VE2D><<<grid_cells(g), blk(), 0, s>>>(g, f, n, roles, sd); break;
         case VE2D_PERF: k2_Pt_tau<VE2D_PERF><<<grid_cells(g), blk(), 0, s>>>(g, f, n, roles, sd); break;
