@@ -182,7 +182,7 @@ def run_ours(args, ws, rank, local, pg):
     nout = args.iters_per_step
     variant = args.variant
     s = ptstokes.Solver(variant, n, n, n, nout=nout, eps=1e-300, iter_max=nout - 1,
-                        single_pass=1 if args.single_pass else 0, precision=args.precision)
+                        single_pass=args.single_pass, precision=args.precision)
     s.setup_inclusion()
     s.assign_tau()
     stream = torch.cuda.ExternalStream(s.stream_handle())
@@ -581,7 +581,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=511)
     ap.add_argument("--variant", default="3d_ve_perf", choices=["3d_ve_perf", "3d_ve", "3d_v"])
-    ap.add_argument("--single-pass", action="store_true", help="use the staged one-launch-per-iteration kernel")
+    ap.add_argument("--single-pass", type=int, nargs="?", const=1, default=0, choices=[0, 1, 2],
+                    help="one launch per PT iteration: 1 staged kernel, 2 direct-load kernel")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--ttt-n", type=int, default=255, help="grid of the time-to-tolerance comparison (0: skip)")
     ap.add_argument("--ttt-nt", type=int, default=5, help="physical steps of the time-to-tolerance comparison")

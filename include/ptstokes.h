@@ -74,7 +74,9 @@ typedef struct pts_desc {
     double eps;         /* tolerance ε on err (Stokes3D_ve_perf.jl:132) */
     double iter_max;    /* `while err > ε && iter <= iterMax` */
     int32_t mixed_inner;    /* MIXED: FP32 sweeps between FP64 corrections; 0 => nout */
-    int32_t single_pass;    /* 3D: 1 = one-launch-per-iteration staged kernel, 0 = two launches */
+    int32_t single_pass;    /* 3D: 0 = two launches per iteration; one launch per iteration with
+                             * 1 = inputs staged in shared memory by bulk copies, 2 = inputs read
+                             * directly (L1/L2) */
     int32_t adjoint;        /* PTS_3D_V / PTS_3D_VE_PERF: 1 = solve the transposed (adjoint) system */
     int32_t reserved[5];
 } pts_desc;

@@ -274,7 +274,8 @@ int enqueue_block(pts_ctx* c, int64_t m, bool store_last) {
     }
     CK(launch_Pt_tau(c->v, c->g, c->f, c->n, ROLE_P | ROLE_TAU, store_last && m == 1 && !c->perf, c->stream));
     for (int64_t q = 1; q < m; ++q) {
-        CK(launch_fused3(c->v, c->g, c->f, c->alt, c->n, store_last && q == m - 1 && !c->perf, c->d_kerr, c->stream));
+        CK(launch_fused3(c->v, c->g, c->f, c->alt, c->n, store_last && q == m - 1 && !c->perf, c->d_kerr, c->stream,
+                         c->d.single_pass == 2));
         swap_buffers(c);
     }
     CK(launch_V_bc(c->v, c->g, c->f, c->n, true, c->stream));

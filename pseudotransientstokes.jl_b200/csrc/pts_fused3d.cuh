@@ -476,4 +476,131 @@ __global__ void __launch_bounds__(256, 1) k3_fused_BA(Geom g, Fused3Args<T> a, N
     }
 }
 
+// The same B-then-A single pass without staging: every iteration-n input is read-only in
+// the launch (the outputs are the other ping-pong buffers), so B and A load them straight
+// from global memory through the read-only data path and let L1/L2 serve the halos. Only
+// V_n of the last three planes stays in shared memory (the ring exchange between B and A).
+template <typename T, bool EL, bool PERF, bool CORR>
+__global__ void __launch_bounds__(256) k3_fused_direct(Geom g, Fused3Args<T> a, NumT<T> n, int zch, int store_divV) {
+    using namespace fused3;
+    constexpr int EX = TX + 2, EY = TY + 2;
+    __shared__ T sVbase[3 * 3 * EY * EX];  // [3 comp][3 planes][EY][EX]
+    auto sV = [&](int comp, int slot, int ey, int ex) -> T& { return sVbase[((comp * 3 + slot) * EY + ey) * EX + ex]; };
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + TX * ty;
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const int k0 = blockIdx.z * zch;
+    const int kB_end = min(k0 + zch, nz + 1);
+    const int kA_end = min(k0 + zch, nz);
+    const int i = x0 + tx, j = y0 + ty;
+    const int s_first = max(k0 - 1, 0), s_last = min(k0 + zch, nz);
+    const idx_t sx = 1, sy = g.px, sz = (idx_t)g.pxy;
+
+    // ring assignment as in k3_fused_BA: 3 components x (TX + TY) faces
+    int rc = -1, rex = 0, rey = 0;
+    if (tid < 3 * (TX + TY)) {
+        rc = tid / (TX + TY);
+        const int q = tid % (TX + TY);
+        if (rc == 0) {
+            if (q < TY) { rex = TX + 1; rey = 1 + q; } else { rex = 1 + (q - TY); rey = 0; }
+        } else if (rc == 1) {
+            if (q < TY) { rex = 0; rey = 1 + q; } else { rex = 1 + (q - TY); rey = TY + 1; }
+        } else {
+            if (q < TY) { rex = 0; rey = 1 + q; } else { rex = 1 + (q - TY); rey = 0; }
+        }
+    }
+    const int ri = x0 - 1 + rex, rj = y0 - 1 + rey;
+    if ((rex == 0 && x0 >= nx) || (rey == 0 && y0 >= ny)) rc = -1;  // read by no point of the tile
+
+    for (int s = s_first; s <= s_last; ++s) {
+        const int slotV = s % 3;
+        // ---------------- B(s): V_n at plane s, owned faces + ring
+        {
+            const bool own = (s >= k0 && s < kB_end);
+            const int64_t c = gidx(g, i, j, s);
+            T v = T(0);
+            if (valid_face(g, 0, i, j, s)) {
+                v = face_global<T, PERF, CORR, 0>(a, n, g, i, j, s);
+                if (own) a.Vx2[c] = v;
+            }
+            sV(0, slotV, ty + 1, tx + 1) = v;
+            v = T(0);
+            if (valid_face(g, 1, i, j, s)) {
+                v = face_global<T, PERF, CORR, 1>(a, n, g, i, j, s);
+                if (own) a.Vy2[c] = v;
+            }
+            sV(1, slotV, ty + 1, tx + 1) = v;
+            v = T(0);
+            if (valid_face(g, 2, i, j, s)) {
+                v = face_global<T, PERF, CORR, 2>(a, n, g, i, j, s);
+                if (own) a.Vz2[c] = v;
+            }
+            sV(2, slotV, ty + 1, tx + 1) = v;
+            if (rc >= 0) {
+                T w = T(0);
+                if (valid_face(g, rc, ri, rj, s))
+                    w = (rc == 0)   ? face_global<T, PERF, CORR, 0>(a, n, g, ri, rj, s)
+                        : (rc == 1) ? face_global<T, PERF, CORR, 1>(a, n, g, ri, rj, s)
+                                    : face_global<T, PERF, CORR, 2>(a, n, g, ri, rj, s);
+                sV(rc, slotV, rey, rex) = w;
+            }
+        }
+        __syncthreads();
+        // ---------------- A(k = s-1): Pt, τ at plane k for the owned point
+        const int k = s - 1;
+        if (k >= k0 && k < kA_end && i < nx && j < ny) {
+            const int sm = (s + 1) % 3, s0 = (s + 2) % 3, sp = slotV;  // V_n planes k-1, k, k+1
+            const int ex = tx + 1, ey = ty + 1;
+            const idx_t c = gidx32(g, i, j, k);
+            const T vx0 = sV(0, s0, ey, ex), vx1 = sV(0, s0, ey, ex + 1);
+            const T vy0 = sV(1, s0, ey, ex), vy1 = sV(1, s0, ey + 1, ex);
+            const T vz0 = sV(2, s0, ey, ex), vz1 = sV(2, sp, ey, ex);
+            const T dvx = vx1 - vx0, dvy = vy1 - vy0, dvz = vz1 - vz0;
+            const T *Gd = a.g3[0], *Mu = a.g3[1];
+            const T Gc = __ldg(Gd + c), Mc = __ldg(Mu + c);
+            {
+                T dv;
+                if (PERF) dv = (n._dx * dvx + n._dy * dvy) + n._dz * dvz;
+                else dv = (dvx / n.dx + dvy / n.dy) + dvz / n.dz;
+                if (!PERF && store_divV && a.divV) a.divV[c] = dv;
+                if (CORR) dv = __ldg(a.g4[6] + c) + dv;
+                a.Pt2[c] = __ldg(a.g1[6] + c) - n.r * Gc * dv;
+            }
+            constexpr bool SRC = EL || CORR;
+            auto src = [&](int f) -> T { return SRC ? __ldg(a.g4[f] + c) : T(0); };
+            auto tau = [&](int f) -> T { return __ldg(a.g1[f] + c); };
+            if (j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2)
+                a.txx2[c] = tau_n<T, EL, PERF, CORR>(tau(0), src(0), Gc, Mc, n, n.dx, n._dx, dvx);
+            if (i >= 1 && i <= nx - 2 && k >= 1 && k <= nz - 2)
+                a.tyy2[c] = tau_n<T, EL, PERF, CORR>(tau(1), src(1), Gc, Mc, n, n.dy, n._dy, dvy);
+            if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2)
+                a.tzz2[c] = tau_n<T, EL, PERF, CORR>(tau(2), src(2), Gc, Mc, n, n.dz, n._dz, dvz);
+            if (i >= 1 && j >= 1 && k >= 1 && k <= nz - 2) {
+                const T ag = (((__ldg(Gd + c - sx - sy) + __ldg(Gd + c - sy)) + __ldg(Gd + c - sx)) + Gc) * n.quarter;
+                const T am = (((__ldg(Mu + c - sx - sy) + __ldg(Mu + c - sy)) + __ldg(Mu + c - sx)) + Mc) * n.quarter;
+                const T d1 = vx0 - sV(0, s0, ey - 1, ex);  // Vx(i,j) - Vx(i,j-1)
+                const T d2 = vy0 - sV(1, s0, ey, ex - 1);  // Vy(i,j) - Vy(i-1,j)
+                a.txy2[c] = tau_s<T, EL, PERF, CORR>(tau(3), src(3), ag, am, n, n.dy, n._dy, d1, n.dx, n._dx, d2);
+            }
+            if (k >= 1) {
+                if (i >= 1 && j >= 1 && j <= ny - 2) {
+                    const T ag = (((__ldg(Gd + c - sx - sz) + __ldg(Gd + c - sz)) + __ldg(Gd + c - sx)) + Gc) * n.quarter;
+                    const T am = (((__ldg(Mu + c - sx - sz) + __ldg(Mu + c - sz)) + __ldg(Mu + c - sx)) + Mc) * n.quarter;
+                    const T d1 = vx0 - sV(0, sm, ey, ex);      // Vx(k) - Vx(k-1)
+                    const T d2 = vz0 - sV(2, s0, ey, ex - 1);  // Vz(i) - Vz(i-1)
+                    a.txz2[c] = tau_s<T, EL, PERF, CORR>(tau(4), src(4), ag, am, n, n.dz, n._dz, d1, n.dx, n._dx, d2);
+                }
+                if (i >= 1 && i <= nx - 2 && j >= 1) {
+                    const T ag = (((__ldg(Gd + c - sy - sz) + __ldg(Gd + c - sz)) + __ldg(Gd + c - sy)) + Gc) * n.quarter;
+                    const T am = (((__ldg(Mu + c - sy - sz) + __ldg(Mu + c - sz)) + __ldg(Mu + c - sy)) + Mc) * n.quarter;
+                    const T d1 = vy0 - sV(1, sm, ey, ex);      // Vy(k) - Vy(k-1)
+                    const T d2 = vz0 - sV(2, s0, ey - 1, ex);  // Vz(j) - Vz(j-1)
+                    a.tyz2[c] = tau_s<T, EL, PERF, CORR>(tau(5), src(5), ag, am, n, n.dz, n._dz, d1, n.dy, n._dy, d2);
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
 }  // namespace pts

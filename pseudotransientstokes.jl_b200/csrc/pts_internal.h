@@ -109,9 +109,11 @@ cudaError_t launch_grad_logmu(const Geom& g, const Fields64& fwd, const Fields64
 // forward and adjoint stresses, written (add = false) or added (add = true) to fwd.grad
 cudaError_t launch_grad_logmu_ve(const Geom& g, const Fields64& fwd, const Fields64& adj, bool add, cudaStream_t s);
 // single-pass 3D kernel: V update of iteration n from `cur`, then Pt/τ of n+1, into `nxt`
-// `err` is a device flag the kernel sets if one of its bounded staging waits timed out.
+// `err` is a device flag the kernel sets if one of its bounded staging waits timed out;
+// `direct` selects the variant that reads its inputs from global memory without staging.
 cudaError_t launch_fused3(int variant, const Geom& g, const Fields64& cur, const Fields64& nxt, const Num& n,
-                          bool store_divV, int* err, cudaStream_t s);
+                          bool store_divV, int* err, cudaStream_t s,
+                          bool direct);
 inline bool variant_fused(int v) { return variant_is3d(v); }
 
 // Message returned by pts_last_error(NULL) (for entry points without a context).

@@ -1582,9 +1582,22 @@ int fused3_zchunk(const Geom& g) {
     return zch;
 }
 
+#ifndef PTS_DIRECT_ZCH
+#define PTS_DIRECT_ZCH 16
+#endif
 template <typename T, bool EL, bool PERF, bool CORR>
-cudaError_t launch_fused3_t(const Geom& g, const Fused3Args<T>& a, const NumT<T>& n, bool store_divV, cudaStream_t s) {
+cudaError_t launch_fused3_t(const Geom& g, const Fused3Args<T>& a, const NumT<T>& n, bool store_divV, cudaStream_t s,
+                            bool direct) {
     using C = fused3::Cfg<T, EL, CORR>;
+    if (direct) {
+        // short z-chunks: many independent blocks; each chunk recomputes one extra B plane
+        const int zch = PTS_DIRECT_ZCH;
+        const dim3 grid((g.nx + 1 + fused3::TX - 1) / fused3::TX, (g.ny + 1 + fused3::TY - 1) / fused3::TY,
+                        (g.nz + 1 + zch - 1) / zch);
+        k3_fused_direct<T, EL, PERF, CORR><<<grid, dim3(fused3::TX, fused3::TY, 1), 0, s>>>(g, a, n, zch,
+                                                                                          store_divV ? 1 : 0);
+        return cudaGetLastError();
+    }
     static bool attr = false;
     if (!attr) {
         cudaError_t e = cudaFuncSetAttribute(k3_fused_BA<T, EL, PERF, CORR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1601,14 +1614,14 @@ cudaError_t launch_fused3_t(const Geom& g, const Fused3Args<T>& a, const NumT<T>
 }
 
 cudaError_t launch_fused3(int v, const Geom& g, const Fields64& cur, const Fields64& nxt, const Num& nm,
-                          bool store_divV, int* err, cudaStream_t s) {
+                          bool store_divV, int* err, cudaStream_t s, bool direct) {
     const Fused3Args<double> a = fused_args(cur, nxt, err);
     NumT<double> n{nm.dx, nm.dy, nm.dz, nm._dx, nm._dy, nm._dz, nm.r, nm.gdt, 2.0, 0.5, 1.0, 0.25,
                    nm.gdt == 1.0 ? 1 : 0};
     switch (v) {
-        case VE3D_PERF: return launch_fused3_t<double, true, true, false>(g, a, n, store_divV, s);
-        case V3D: return launch_fused3_t<double, false, true, false>(g, a, n, store_divV, s);
-        case VE3D: return launch_fused3_t<double, true, false, false>(g, a, n, store_divV, s);
+        case VE3D_PERF: return launch_fused3_t<double, true, true, false>(g, a, n, store_divV, s, direct);
+        case V3D: return launch_fused3_t<double, false, true, false>(g, a, n, store_divV, s, direct);
+        case VE3D: return launch_fused3_t<double, true, false, false>(g, a, n, store_divV, s, direct);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -204,11 +204,13 @@ def test_field_roundtrip_and_shape_errors(gpu_lib):
     g.close()
 
 
+@pytest.mark.parametrize("mode", [1, 2])
 @pytest.mark.parametrize("variant", ["3d_ve_perf", "3d_v", "3d_ve"])
-def test_single_pass_blocks_of_every_length(gpu_lib, variant):
+def test_single_pass_blocks_of_every_length(gpu_lib, variant, mode):
     """The single-pass 3D path runs a block of m iterations as A [BA]^(m-1) B with
-    ping-pong buffers; blocks of odd and even length must leave the same fields."""
-    o, g = make_pair(gpu_lib, variant, (21, 18, 16), single_pass=1)
+    ping-pong buffers (mode 1: staged inputs, 2: direct loads); blocks of odd and even
+    length must leave the same fields."""
+    o, g = make_pair(gpu_lib, variant, (21, 18, 16), single_pass=mode)
     if o.elastic:
         o.assign_tau()
         g.assign_tau()
@@ -221,11 +223,12 @@ def test_single_pass_blocks_of_every_length(gpu_lib, variant):
     g.close()
 
 
+@pytest.mark.parametrize("mode", [1, 2])
 @pytest.mark.parametrize("nout", [50, 51])
-def test_graph_blocks_with_buffer_swaps(gpu_lib, nout):
+def test_graph_blocks_with_buffer_swaps(gpu_lib, nout, mode):
     """Graph-captured check blocks whose swap count is odd (nout=50) or even (nout=51)."""
     o, g = make_pair(gpu_lib, "3d_ve_perf", (15, 14, 13), nout=nout, iter_max=10 * nout + 7, eps=1e-300,
-                     single_pass=1)
+                     single_pass=mode)
     o.assign_tau()
     g.assign_tau()
     info = g.solve()
