@@ -144,6 +144,36 @@ def cpu_sample(n, iters):
     return a_eff(n) * iters / dt / 1e9, nthreads, dt
 
 
+def small_2d_case():
+    """The reference's CPU-runnable case: 2D viscous Stokes (Stokes2D.jl), 127^2, a check every
+    100 iterations, to 1e-8 -- on the host (the oracle, all threads) and on the GPU."""
+    import torch
+
+    import ptstokes
+    from oracle import scripts as S
+    from oracle.binding import lib
+
+    o = S.make("2d_v", 127, 127, nout=100)
+    t0 = time.perf_counter()
+    o.run()
+    cpu_s = time.perf_counter() - t0
+    g = ptstokes.Solver("2d_v", 127, 127, nout=100)
+    g.setup_inclusion()
+    g.sync()
+    st = torch.cuda.ExternalStream(g.stream_handle())
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    r = g.run()
+    b.record(st)
+    b.synchronize()
+    out = {"workload": "2D viscous Stokes2D.jl 127^2, check every 100 iterations, tol 1e-8",
+           "cpu_oracle": {"seconds": round(cpu_s, 4), "iters": o.iters, "threads": lib().ora_num_threads()},
+           "gpu": {"seconds": round(a.elapsed_time(b) / 1e3, 4), "iters": r["iters"]}}
+    g.close()
+    return out
+
+
 def run_reference(args, ws, rank, pg):
     if rank != 0:
         return
@@ -293,7 +323,8 @@ def run_ours(args, ws, rank, local, pg):
         v, thr, dt = cpu_sample(args.cpu_n, args.cpu_iters)
         cpu = {"value": round(v, 3), "unit": "GB/s", "cores": thr, "kind": "port",
                "sample": f"oracle (C++/OpenMP FP64 restatement of Stokes3D_ve_perf.jl) at {args.cpu_n}^3, "
-                         f"{args.cpu_iters} PT iterations, {dt:.1f} s"}
+                         f"{args.cpu_iters} PT iterations, {dt:.1f} s",
+               "time_to_tol_2d_127": small_2d_case()}
 
     launches = args.steps * (2 * nout + 2) if args.precision == "fp64" else args.steps * (2 * nout + 3)
     s.close()
