@@ -73,3 +73,48 @@ def test_no_device_is_an_error_not_a_fallback():
     with pytest.raises(ptstokes.PtsError) as e:
         ptstokes.Solver("3d_ve_perf", 9, 9, 9)
     assert e.value.code == _abi.PTS_E_CUDA
+
+
+def test_adjoint_and_batch_descriptions_are_validated_without_a_device():
+    """The adjoint flag only exists for the 3D explicit-index FP64 two-kernel path; a batch
+    needs instances of at least 3x3 cells, a positive box and a known tile shape."""
+    import ptstokes
+    from ptstokes import _abi
+    lib = ptstokes.load()
+    d = _abi.PtsDesc()
+    d.nx = d.ny = d.nz = 9
+    d.nout, d.lx, d.ly, d.lz = 10, 10.0, 10.0, 10.0
+    ctx = ctypes.c_void_p()
+    d.adjoint = 1
+    for variant, precision, single_pass in ((0, 0, 0), (3, 0, 0), (5, 1, 0), (5, 0, 1), (4, 0, 2)):
+        d.variant, d.precision, d.single_pass = variant, precision, single_pass
+        assert lib.pts_create(ctypes.byref(d), ctypes.byref(ctx)) == _abi.PTS_E_INVAL, (variant, precision)
+        assert b"adjoint" in lib.pts_last_error(None) or b"mixed" in lib.pts_last_error(None)
+
+    bd = _abi.PtsBatchDesc()
+    bd.nout, bd.tile, bd.eps = 100, 0, 1e-8
+    inst = (_abi.PtsBatchInstance * 2)()
+    inst[0] = _abi.PtsBatchInstance(31, 31, 10.0, 10.0, 1e-3, 1.0, 0.0, 1.0)
+    inst[1] = _abi.PtsBatchInstance(2, 31, 10.0, 10.0, 1e-3, 1.0, 0.0, 1.0)
+    b = ctypes.c_void_p()
+    assert lib.pts_batch_create(ctypes.byref(bd), inst, 2, ctypes.byref(b)) == _abi.PTS_E_INVAL
+    inst[1] = _abi.PtsBatchInstance(31, 31, -1.0, 10.0, 1e-3, 1.0, 0.0, 1.0)
+    assert lib.pts_batch_create(ctypes.byref(bd), inst, 2, ctypes.byref(b)) == _abi.PTS_E_INVAL
+    inst[1] = inst[0]
+    bd.tile = 4
+    assert lib.pts_batch_create(ctypes.byref(bd), inst, 2, ctypes.byref(b)) == _abi.PTS_E_INVAL
+    bd.tile, bd.nout = 0, 0
+    assert lib.pts_batch_create(ctypes.byref(bd), inst, 2, ctypes.byref(b)) == _abi.PTS_E_INVAL
+    assert lib.pts_batch_create(ctypes.byref(bd), inst, 0, ctypes.byref(b)) == _abi.PTS_E_INVAL
+
+
+def test_field_table_covers_the_adjoint_fields():
+    """The Python field names follow the header's pts_field enum, new fields included."""
+    from ptstokes import _abi
+    hdr = open(os.path.join(ROOT, "include", "ptstokes.h")).read()
+    enum = hdr[hdr.index("enum pts_field"):]
+    enum = enum[:enum.index("PTS_F_COUNT")]
+    ids = re.findall(r"PTS_F_[A-Z_]+", enum)
+    assert len(ids) == len(_abi.FIELDS)
+    assert ids[-4:] == ["PTS_F_FX", "PTS_F_FY", "PTS_F_FZ", "PTS_F_GRAD"]
+    assert _abi.FIELDS[-4:] == ["Fx", "Fy", "Fz", "grad"]
