@@ -106,8 +106,12 @@ def dist_setup():
         import torch
         import torch.distributed as dist
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        # one process per GPU over NCCL; on a host without GPUs (the reference arm, tests) gloo
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        else:
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
         pg = dist
     return ws, rank, local, pg
 
@@ -117,7 +121,8 @@ def max_over_ranks(x, pg):
         return x
     import torch
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if pg.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
 
