@@ -126,6 +126,57 @@ function run!(ctx::Ctx, nt)
     return per, r[]
 end
 
+# ---- batched 2D sweeps (pts_batch_*): the runme_Stokes2D_*.jl loops in one launch ----
+
+struct BatchInstance
+    nx::Int32; ny::Int32
+    lx::Float64; ly::Float64; μsi::Float64; radius2::Float64; ρgi::Float64; εbg::Float64
+end
+
+struct BatchDesc
+    nout::Int32; tile::Int32
+    ε::Float64; iterMax::Float64; r::Float64; Re::Float64; CFL::Float64
+    reserved::NTuple{4,Int32}
+end
+
+mutable struct Batch
+    ptr::Ptr{Cvoid}
+    n::Int
+end
+
+"""
+    Batch(instances; nout=200, ε=1e-8, iterMax=0.0, tile=1, r=1.0, Re=5π, CFL=0.9/sqrt(2))
+
+A sweep of 2D viscous instances (`Stokes2D_param.jl` numerics); `iterMax <= 0` gives each
+instance iterMax = 100max(nx,ny).
+"""
+function Batch(inst::Vector{BatchInstance}; nout=200, ε=1e-8, iterMax=0.0, tile=1, r=1.0, Re=5π, CFL=0.9/sqrt(2))
+    d = BatchDesc(nout, tile, ε, iterMax, r, Re, CFL, ntuple(_ -> Int32(0), 4))
+    out = Ref{Ptr{Cvoid}}(C_NULL)
+    rc = ccall((:pts_batch_create, libpts), Cint, (Ref{BatchDesc}, Ptr{BatchInstance}, Int32, Ref{Ptr{Cvoid}}),
+               d, inst, length(inst), out)
+    rc == 0 || error("pts_batch_create: ", unsafe_string(ccall((:pts_last_error, libpts), Cstring, (Ptr{Cvoid},), C_NULL)))
+    b = Batch(out[], length(inst))
+    finalizer(x -> ccall((:pts_batch_destroy, libpts), Cint, (Ptr{Cvoid},), x.ptr), b)
+    return b
+end
+
+function batch_check(b::Batch, rc)
+    rc == 0 || error("ptstokes batch error $rc: ", unsafe_string(ccall((:pts_batch_last_error, libpts), Cstring, (Ptr{Cvoid},), b.ptr)))
+    return nothing
+end
+
+setup!(b::Batch) = batch_check(b, ccall((:pts_batch_setup, libpts), Cint, (Ptr{Cvoid},), b.ptr))
+
+"Runs the sweep; returns per-instance iterations, last err and convergence flags."
+function solve!(b::Batch; iter_limit=-1)
+    iters = zeros(Int64, b.n); err = zeros(Float64, b.n); conv = zeros(Int32, b.n); graph = Ref{Int32}(0)
+    batch_check(b, ccall((:pts_batch_solve, libpts), Cint,
+                         (Ptr{Cvoid}, Int64, Ptr{Int64}, Ptr{Float64}, Ptr{Int32}, Ref{Int32}),
+                         b.ptr, iter_limit, iters, err, conv, graph))
+    return iters, err, conv .== 1
+end
+
 # ---- adjoint of the 3D viscous solve (pts_apply_operator, pts_gradient_logmu) ----
 
 "One application of the operator (or of its transpose on an adjoint context)."
