@@ -13,7 +13,6 @@ no data-path collective): value = sum over ranks of the work / max-over-ranks ti
 """
 import argparse
 import json
-import math
 import os
 import subprocess
 import sys

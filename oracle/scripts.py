@@ -13,7 +13,6 @@ Each ``Case`` subclass mirrors one script of PTsolvers/PseudoTransientStokes.jl:
 Arrays are Float64 column-major numpy arrays with the reference's own extents, so the
 oracle state can be compared field by field with the CUDA path (test infrastructure only).
 """
-import ctypes
 import math
 
 import numpy as np
