@@ -632,6 +632,8 @@ def time_to_tol(args, stream_cls):
         fields[prec] = {k: s.get(k) for k in ("Pt", "Vx", "Vy", "Vz", "txx", "tyy", "tzz", "txy", "txz", "tyz")}
         s.close()
     out["speedup_mixed_vs_fp64"] = round(out["fp64"]["seconds"] / out["mixed"]["seconds"], 3)
+    out["T_eff_convention"] = ("the FP64 A_eff (29 arrays x 8 B) per PT iteration for both paths: for the mixed "
+                               "path an FP64-equivalent rate; its FP32 sweeps move 43 arrays x 4 B per iteration")
     out["mixed_rel_err_vs_fp64"] = {
         k: float(np.linalg.norm(fields["mixed"][k] - fields["fp64"][k]) / max(np.linalg.norm(fields["fp64"][k]), 1e-300))
         for k in fields["fp64"]}
