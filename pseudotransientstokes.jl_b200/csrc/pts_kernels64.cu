@@ -984,8 +984,10 @@ __global__ void __launch_bounds__(TX* TY, PTS_SWEEP_THREADS_PER_SM / (TX * TY)) 
     };
     auto first_at = [&](int k) { return in_smem ? s_first[k] : ((volatile const int*)g_first)[k]; };
     auto id_at = [&](int k) { return in_smem ? s_id[k] : ((volatile const int*)g_id)[k]; };
-    // body(P, b, t, i, j) for every point of this block's chunk of the active tiles
-    auto walk = [&](auto&& body) {
+    // body(P, b, t, i, j) for every point of this block's chunk of the active tiles; pre(P, i, j)
+    // is called first with the point of the block's next tile when that tile belongs to the
+    // same instance, so its cache lines can be requested while this tile computes
+    auto walk = [&](auto&& body, auto&& pre) {
         const int chunk = (T + (int)gridDim.x - 1) / (int)gridDim.x;
         const int v0 = (int)blockIdx.x * chunk, v1 = min(T, v0 + chunk);
         if (v0 >= v1) return;
@@ -1004,9 +1006,30 @@ __global__ void __launch_bounds__(TX* TY, PTS_SWEEP_THREADS_PER_SM / (TX * TY)) 
                 P = sweep_params(inst[b], iter_last);
             }
             const int q = v - f0;
+            if (v + 1 < v1 && v + 1 < f1) pre(P, ((q + 1) % P.ntx) * TX + tx, ((q + 1) / P.ntx) * TY + ty);
             body(P, b, P.tile0 + q, (q % P.ntx) * TX + tx, (q / P.ntx) * TY + ty);
         }
     };
+    // L2 prefetches of the lines a point's stencil reads first, at an address clamped into the
+    // instance's own padded arrays (always a valid address)
+    auto pf = [](const double* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); };
+    auto preA = [&](const SweepP& P, int i, int j) {
+        const SweepF f = sweep_at(F, P.off);
+        const int jc = min(j, P.ny);
+        const idx_t c = min(i, P.nx) + P.px * jc;
+        pf(f.Vx + c); pf(f.Vy + c); pf(f.Pt + c); pf(f.Mus + c);
+        pf(f.txx + c); pf(f.tyy + c); pf(f.txy + c);
+        if (jc < P.ny) pf(f.Vy + c + P.px);
+    };
+    auto preB = [&](const SweepP& P, int i, int j) {
+        const SweepF f = sweep_at(F, P.off);
+        const int jc = min(j, P.ny);
+        const idx_t c = min(i, P.nx) + P.px * jc;
+        pf(f.Vx + c); pf(f.Vy + c); pf(f.Pt + c); pf(f.rhog + c);
+        pf(f.txx + c); pf(f.tyy + c); pf(f.txy + c);
+        if (jc < P.ny) pf(f.txy + c + P.px);
+    };
+    auto no_pre = [](const SweepP&, int, int) {};
     if (blockIdx.x == 0) build_active_list(inst, ninst, st, 0, iter_last, s_cnt);
     grid.sync();
     load_list();
@@ -1016,11 +1039,11 @@ __global__ void __launch_bounds__(TX* TY, PTS_SWEEP_THREADS_PER_SM / (TX * TY)) 
         const bool chk = ((iter + 1) % nout == 0);
         walk([&](const SweepP& P, int, int, int i, int j) {
             if (iter <= P.cap) pt_tau_sweep(sweep_at(F, P.off), P, i, j, chk);
-        });
+        }, preA);
         grid.sync();
         walk([&](const SweepP& P, int, int, int i, int j) {
             if (iter <= P.cap) v_bc_sweep(sweep_at(F, P.off), P, i, j);
-        });
+        }, preB);
         // an instance doing its last allowed iteration leaves the active count here
         for (int b = blockIdx.x * TX * TY + tid; b < ninst; b += gridDim.x * TX * TY) {
             const int64_t cap = inst[b].iter_last < iter_last ? inst[b].iter_last : iter_last;
@@ -1059,7 +1082,7 @@ __global__ void __launch_bounds__(TX* TY, PTS_SWEEP_THREADS_PER_SM / (TX * TY)) 
                 a.s[1] = R * R;
             }
             acc_block_store_to(a, st.partials + (int64_t)t * kCheckSlots);
-        });
+        }, no_pre);
         grid.sync();
         // per-instance finalisation: one block per instance, fixed-order reduction
         __shared__ double red[TX * TY][kCheckSlots];
