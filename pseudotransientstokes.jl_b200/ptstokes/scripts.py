@@ -15,6 +15,7 @@ scripts' NX/NY/NZ environment variables (``haskey(ENV, "NX") ? parse(Int, ENV["N
 import os
 import time
 
+from . import output
 from .solver import Solver
 
 
@@ -23,7 +24,12 @@ def _env(name, default):
     return int(v) if v is not None else default
 
 
-def _script(variant, nx, ny, nz, return_solver, verbose, **kw):
+def _flag(name):
+    """`haskey(ENV, name) ? parse(Bool, ENV[name]) : false` of the scripts' headers."""
+    return os.environ.get(name, "false").strip().lower() in ("true", "1")
+
+
+def _script(variant, nx, ny, nz, return_solver, verbose, do_save=None, do_save_viz=None, **kw):
     s = Solver(variant, nx, ny, nz, **kw)
     s.setup_inclusion(musi=kw.get("musi", 1e-3))
     t0 = time.perf_counter()
@@ -33,6 +39,11 @@ def _script(variant, nx, ny, nz, return_solver, verbose, **kw):
     res["wall_s"] = wall
     if verbose:
         print(f"Total iters = {res['ittot']} ({len(res['iters'])} steps), time = {wall:1.3e} sec")
+    if _flag("DO_SAVE") if do_save is None else do_save:  # the scripts' output/out_*.txt line
+        output.save_line(s, res, wall, os.environ.get("PTS_OUTPUT_DIR", "output"))
+    if _flag("DO_SAVE_VIZ") if do_save_viz is None else do_save_viz:  # the scripts' out_visu/*.mat dump
+        if variant in output.MAT_FILES:
+            output.save_visu(s, os.environ.get("PTS_VISU_DIR", "out_visu"))
     out = (*s.centres(), s.get("Pt"))
     if return_solver:
         return out, s, res

@@ -1,0 +1,26 @@
+"""Sample lines of the reference's own output files (printed by Julia's println), kept as a
+fixture for the output writers' number formatting. Run from the repository root:
+
+    python tests/golden/make_output_lines.py /root/reference
+
+The fixture keeps the first and last lines of each output/out_*.txt file.
+"""
+import glob
+import json
+import os
+import sys
+
+
+def main(ref):
+    out = {}
+    for path in sorted(glob.glob(os.path.join(ref, "output", "out_*.txt"))):
+        lines = [ln.rstrip("\n") for ln in open(path) if ln.strip()]
+        if lines:
+            out[os.path.basename(path)] = sorted(set([lines[0], lines[-1]]))
+    dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_output_lines.json")
+    json.dump(out, open(dst, "w"), indent=1)
+    print(dst, sum(len(v) for v in out.values()), "lines")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

@@ -237,3 +237,17 @@ def test_graph_blocks_with_buffer_swaps(gpu_lib, nout, mode):
     assert info["iters"] == 10 * nout + 8 and not info["converged"]
     assert_fields_equal(o, g, fields("3d_ve_perf"))
     g.close()
+
+
+def test_script_mirror_writes_the_reference_outputs(gpu_lib, tmp_path, monkeypatch):
+    """DO_SAVE / DO_SAVE_VIZ as in the scripts: the output line and the MAT dump."""
+    from scipy.io import loadmat
+
+    from ptstokes import scripts
+    monkeypatch.setenv("PTS_OUTPUT_DIR", str(tmp_path / "output"))
+    monkeypatch.setenv("PTS_VISU_DIR", str(tmp_path / "out_visu"))
+    xc, yc, zc, Pt = scripts.Stokes3D_ve_perf(15, 14, 13, do_save=True, do_save_viz=True)
+    row = open(tmp_path / "output" / "out_Stokes3D_ve_perf.txt").read().split()
+    assert row[:5] == ["1", "15", "14", "13", "201"]
+    m = loadmat(str(tmp_path / "out_visu" / "Stokes_3D_ve_perf.mat"))
+    assert np.array_equal(m["Pt_3D"], Pt) and m["Vz_3D"].shape == (15, 14, 14)

@@ -1,0 +1,61 @@
+"""The reference scripts' output files (no GPU): Julia's number printing, the column layout
+the Matlab readers parse, and the MAT dumps."""
+import json
+import os
+
+import numpy as np
+
+from conftest import ROOT
+
+
+def test_numbers_print_as_julia_prints_them():
+    """Every number of the reference's own output files (tests/golden/reference_output_lines.json,
+    made by tests/golden/make_output_lines.py) is reproduced character for character."""
+    from ptstokes.output import jl
+    lines = json.load(open(os.path.join(ROOT, "tests", "golden", "reference_output_lines.json")))
+    n = 0
+    for f, rows in lines.items():
+        for row in rows:
+            for tok in row.split():
+                v = int(tok) if tok.lstrip("-").isdigit() else float(tok)
+                assert jl(v) == tok, (f, tok, jl(v))
+                n += 1
+    assert n > 200
+
+
+def test_result_lines_have_the_columns_of_each_script():
+    from ptstokes.output import result_line
+    assert result_line("2d_v", 127, 127, None, 2200, 1, 0.5) == [127, 127, 2200]
+    assert result_line("2d_ve", 63, 63, None, 4000, 5, 0.5) == [63, 63, 4000, 5]
+    assert len(result_line("2d_ve_perf", 63, 63, None, 101, 1, 0.5)) == 7
+    assert result_line("3d_ve", 31, 31, 31, 3400, 5, 1.0) == [31, 31, 31, 3400, 5]
+    line = result_line("3d_ve_perf", 31, 31, 31, 201, 1, 0.0314)
+    # Stokes3D_ve_perf.jl:229-231: A_eff = 29*n^3*8/1e9, t_it = wtime/(ittot-10), T_eff = A_eff/t_it
+    assert line[:5] == [1, 31, 31, 31, 201]
+    assert abs(line[6] - 29 * 31 ** 3 * 8 / 1e9) < 1e-15
+    assert abs(line[7] - 0.0314 / 191) < 1e-18 and abs(line[8] - line[6] / line[7]) < 1e-9
+
+
+class _FakeSolver:
+    variant, ndim, nx, ny, nz = "3d_ve_perf", 3, 5, 4, 3
+    dx, dy, dz = 2.0, 2.5, 10 / 3
+
+    def get(self, name):
+        shape = {"Vz": (5, 4, 4), "txz": (4, 2, 2)}.get(name, (5, 4, 3))
+        return np.asfortranarray(np.arange(np.prod(shape), dtype=np.float64).reshape(shape, order="F") + len(name))
+
+
+def test_visu_dump_round_trips(tmp_path):
+    from scipy.io import loadmat
+
+    from ptstokes.output import save_line, save_visu
+    s = _FakeSolver()
+    path = save_visu(s, str(tmp_path))
+    m = loadmat(path)
+    assert set(k for k in m if not k.startswith("__")) == {"Pt_3D", "Mus_3D", "Txz_3D", "Vz_3D", "dx_3D", "dy_3D",
+                                                             "dz_3D"}
+    assert np.array_equal(m["Vz_3D"], s.get("Vz")) and float(m["dz_3D"].item()) == s.dz
+    p = save_line(s, {"ittot": 201, "iters": [201]}, 0.5, str(tmp_path))
+    save_line(s, {"ittot": 201, "iters": [201]}, 0.25, str(tmp_path))
+    rows = [r.split() for r in open(p).read().splitlines()]
+    assert len(rows) == 2 and all(len(r) == 9 for r in rows) and rows[0][:5] == ["1", "5", "4", "3", "201"]
