@@ -251,3 +251,19 @@ def test_script_mirror_writes_the_reference_outputs(gpu_lib, tmp_path, monkeypat
     assert row[:5] == ["1", "15", "14", "13", "201"]
     m = loadmat(str(tmp_path / "out_visu" / "Stokes_3D_ve_perf.mat"))
     assert np.array_equal(m["Pt_3D"], Pt) and m["Vz_3D"].shape == (15, 14, 14)
+
+
+@pytest.mark.parametrize("n", [255, 511])
+def test_gpu_reproduces_the_published_2d_ve_iteration_counts(gpu_lib, n):
+    """output/out_Stokes2D_ve.txt: scripts/Stokes2D_ve.jl to 1e-8 over 5 steps takes 22600
+    iterations at 255^2 and 44400 at 511^2; the GPU path takes exactly as many."""
+    import json
+    import os
+
+    from ptstokes import Solver
+    rows = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_output_lines.json")))
+    want = {int(r.split()[0]): int(r.split()[2]) for r in rows["out_Stokes2D_ve.txt"]}
+    g = Solver("2d_ve", n, n, lib=gpu_lib).setup_inclusion()
+    res = g.run()
+    assert res["converged"] and res["ittot"] == want[n], (res["iters"], want[n])
+    g.close()

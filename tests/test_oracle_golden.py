@@ -5,6 +5,9 @@ centres xc of one reference script run on the CPU Threads backend. The oracle mu
 reproduce them within Julia's `isapprox` (the reference's own comparison,
 test/test_2D.jl:14); it in fact reproduces them bit for bit, which is asserted too.
 """
+import json
+import os
+
 import numpy as np
 import pytest
 
@@ -47,3 +50,21 @@ def test_oracle_nan_raises():
     c.f["Pt"][3, 3] = np.nan
     with pytest.raises(FloatingPointError):
         c.run(nt=1)
+
+
+def _published(name):
+    """Rows of one of the reference's output files (tests/golden/reference_output_lines.json)."""
+    d = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_output_lines.json")))
+    return [list(map(int, r.split()[:4])) for r in d[name]]
+
+
+def test_oracle_reproduces_the_published_2d_ve_iteration_counts():
+    """scripts/Stokes2D_ve.jl run to 1e-8 over 5 steps: output/out_Stokes2D_ve.txt lists the total
+    iteration count per grid; the oracle takes exactly as many."""
+    from oracle import scripts as S
+    for nx, ny, ittot, nt in _published("out_Stokes2D_ve.txt"):
+        if nx > 127:
+            continue
+        o = S.make("2d_ve", nx, ny)
+        o.run()
+        assert len(o.iters) == nt and sum(o.iters) == ittot, (nx, o.iters, ittot)
