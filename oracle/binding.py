@@ -79,6 +79,11 @@ _SIGS = {
     "ora3v_res_adj": [Arr] * 10 + [_D] * 3,
     "ora3v_update_V": [Arr] * 10,
     "ora3ve_grad_logmu": [Arr] * 14 + [ctypes.c_int],
+    "ora2d_timesteps": [Arr] * 4 + [_D] * 5,
+    "ora2d_compute_P": [Arr] * 5 + [_D] * 2,
+    "ora2d_compute_tau": [Arr] * 10 + [_D] * 5 + [ctypes.c_int],
+    "ora2d_compute_dV": [Arr] * 8 + [_D] * 4,
+    "ora2d_compute_V": [Arr] * 6,
     "ora3p_compute_Res": [Arr] * 14 + [_D] * 3,
     "ora_stats": [Arr, ctypes.POINTER(_D), ctypes.POINTER(_D), ctypes.POINTER(_D)],
     "ora_num_threads": [],

@@ -395,6 +395,101 @@ void ora2s_compute_dV(oarr Rx_, oarr Ry_, oarr dVx_, oarr dVy_, oarr Pt_, oarr t
         }
 }
 
+// ---------------------------------------------------------------- 2D damped scheme ("accel. 1")
+// scripts/previous_damp/Stokes2D0.jl (viscous) and Stokes2D_ve0.jl (Maxwell visco-elastic):
+// numerical compressibility β_n, a damped velocity rate dV/dτ and per-face pseudo-time steps.
+
+// compute_timesteps! (Stokes2D_ve0.jl:27-32, Stokes2D0.jl:26-31)
+void ora2d_timesteps(oarr dtVx_, oarr dtVy_, oarr dtPt_, oarr Must_, double Vsc, double Ptsc, double min_dxy2,
+                     double beta_n, double max_nxy) {
+    F2 dtVx(dtVx_), dtVy(dtVy_), dtPt(dtPt_), M(Must_);
+#pragma omp parallel for schedule(static)
+    for (int64_t iy = 1; iy <= M.n2; ++iy)
+        for (int64_t ix = 1; ix <= M.n1; ++ix) {
+            if (ix <= dtVx.n1 && iy <= dtVx.n2)
+                dtVx(ix, iy) = 1.0 / 4.1 / Vsc * min_dxy2 / ((M(ix, iy + 1) + M(ix + 1, iy + 1)) * 0.5) / (1.0 + beta_n);
+            if (ix <= dtVy.n1 && iy <= dtVy.n2)
+                dtVy(ix, iy) = 1.0 / 4.1 / Vsc * min_dxy2 / ((M(ix + 1, iy) + M(ix + 1, iy + 1)) * 0.5) / (1.0 + beta_n);
+            dtPt(ix, iy) = 4.1 * (1.0 + beta_n) / Ptsc / max_nxy * M(ix, iy);
+        }
+}
+
+// compute_P! (Stokes2D_ve0.jl:41-45, Stokes2D0.jl:33-37): ∇V, Pt -= dτPt*∇V
+void ora2d_compute_P(oarr divV_, oarr Pt_, oarr Vx_, oarr Vy_, oarr dtPt_, double dx, double dy) {
+    F2 divV(divV_), Pt(Pt_), Vx(Vx_), Vy(Vy_), dtPt(dtPt_);
+#pragma omp parallel for schedule(static)
+    for (int64_t iy = 1; iy <= Pt.n2; ++iy)
+        for (int64_t ix = 1; ix <= Pt.n1; ++ix) {
+            divV(ix, iy) = (Vx(ix + 1, iy) - Vx(ix, iy)) / dx + (Vy(ix, iy + 1) - Vy(ix, iy)) / dy;
+            Pt(ix, iy) = Pt(ix, iy) - dtPt(ix, iy) * divV(ix, iy);
+        }
+}
+
+// compute_τ! viscous (Stokes2D0.jl:39-44) and Maxwell (Stokes2D_ve0.jl:47-54, Xsi = Mus/(G*dt)):
+//   τ = τ_o*Xsi/(Xsi+1) + 2Mus/(Xsi+1)*(ε̇ - ∇V/3 + β_n ∇V)  [elastic]   τ = 2Mus*(ε̇ - ∇V/3 + β_n ∇V)
+void ora2d_compute_tau(oarr txx_, oarr tyy_, oarr txy_, oarr txxo_, oarr tyyo_, oarr txyo_, oarr Vx_, oarr Vy_,
+                       oarr Mus_, oarr divV_, double G, double dt, double beta_n, double dx, double dy, int elastic) {
+    F2 txx(txx_), tyy(tyy_), txy(txy_), Vx(Vx_), Vy(Vy_), M(Mus_), dv(divV_);
+    const bool el = elastic != 0;
+#pragma omp parallel for schedule(static)
+    for (int64_t iy = 1; iy <= txx.n2; ++iy)
+        for (int64_t ix = 1; ix <= txx.n1; ++ix) {
+            const double exx = (Vx(ix + 1, iy) - Vx(ix, iy)) / dx - 1.0 / 3.0 * dv(ix, iy) + beta_n * dv(ix, iy);
+            const double eyy = (Vy(ix, iy + 1) - Vy(ix, iy)) / dy - 1.0 / 3.0 * dv(ix, iy) + beta_n * dv(ix, iy);
+            if (el) {
+                const F2 txxo(txxo_), tyyo(tyyo_);
+                const double X = M(ix, iy) / (G * dt);
+                txx(ix, iy) = txxo(ix, iy) * X / (X + 1.0) + 2.0 * M(ix, iy) / (X + 1.0) * exx;
+                tyy(ix, iy) = tyyo(ix, iy) * X / (X + 1.0) + 2.0 * M(ix, iy) / (X + 1.0) * eyy;
+            } else {
+                txx(ix, iy) = 2.0 * M(ix, iy) * exx;
+                tyy(ix, iy) = 2.0 * M(ix, iy) * eyy;
+            }
+            if (ix <= txy.n1 && iy <= txy.n2) {
+                const double am = (M(ix, iy) + M(ix + 1, iy) + M(ix, iy + 1) + M(ix + 1, iy + 1)) * 0.25;
+                const double exy = 0.5 * ((Vx(ix + 1, iy + 1) - Vx(ix + 1, iy)) / dy + (Vy(ix + 1, iy + 1) - Vy(ix, iy + 1)) / dx);
+                if (el) {
+                    const F2 txyo(txyo_);
+                    const double X = am / (G * dt);
+                    txy(ix, iy) = txyo(ix, iy) * X / (X + 1.0) + 2.0 * am / (X + 1.0) * exy;
+                } else {
+                    txy(ix, iy) = 2.0 * am * exy;
+                }
+            }
+        }
+}
+
+// compute_dV! (Stokes2D_ve0.jl:56-62, Stokes2D0.jl:46-52): R as in Stokes2D.jl, dV/dτ = damp*dV/dτ + R
+void ora2d_compute_dV(oarr Rx_, oarr Ry_, oarr dVx_, oarr dVy_, oarr Pt_, oarr txx_, oarr tyy_, oarr txy_, double dampX,
+                      double dampY, double dx, double dy) {
+    F2 Rx(Rx_), Ry(Ry_), dVx(dVx_), dVy(dVy_), Pt(Pt_), txx(txx_), tyy(tyy_), txy(txy_);
+#pragma omp parallel for schedule(static)
+    for (int64_t iy = 1; iy <= Ry.n2; ++iy)
+        for (int64_t ix = 1; ix <= Rx.n1; ++ix) {
+            if (ix <= Rx.n1 && iy <= Rx.n2) {
+                Rx(ix, iy) = (txx(ix + 1, iy + 1) - txx(ix, iy + 1)) / dx + (txy(ix, iy + 1) - txy(ix, iy)) / dy -
+                             (Pt(ix + 1, iy + 1) - Pt(ix, iy + 1)) / dx;
+                dVx(ix, iy) = dampX * dVx(ix, iy) + Rx(ix, iy);
+            }
+            if (ix <= Ry.n1 && iy <= Ry.n2) {
+                Ry(ix, iy) = (tyy(ix + 1, iy + 1) - tyy(ix + 1, iy)) / dy + (txy(ix + 1, iy) - txy(ix, iy)) / dx -
+                             (Pt(ix + 1, iy + 1) - Pt(ix + 1, iy)) / dy;
+                dVy(ix, iy) = dampY * dVy(ix, iy) + Ry(ix, iy);
+            }
+        }
+}
+
+// compute_V! (Stokes2D_ve0.jl:64-68, Stokes2D0.jl:54-58): @inn(V) += dτV*dV/dτ
+void ora2d_compute_V(oarr Vx_, oarr Vy_, oarr dVx_, oarr dVy_, oarr dtVx_, oarr dtVy_) {
+    F2 Vx(Vx_), Vy(Vy_), dVx(dVx_), dVy(dVy_), dtVx(dtVx_), dtVy(dtVy_);
+#pragma omp parallel for schedule(static)
+    for (int64_t iy = 1; iy <= Vy.n2 - 2; ++iy)
+        for (int64_t ix = 1; ix <= Vx.n1 - 2; ++ix) {
+            if (ix <= dVx.n1 && iy <= dVx.n2) Vx(ix + 1, iy + 1) = Vx(ix + 1, iy + 1) + dtVx(ix, iy) * dVx(ix, iy);
+            if (ix <= dVy.n1 && iy <= dVy.n2) Vy(ix + 1, iy + 1) = Vy(ix + 1, iy + 1) + dtVy(ix, iy) * dVy(ix, iy);
+        }
+}
+
 // ---------------------------------------------------------------- 3D set-up kernels
 
 // smooth! (Stokes3D_ve_perf.jl:24-27): @inn(A2) = @inn(A) + 1.0/6.1/fact*(@d2_xi(A) + @d2_yi(A) + @d2_zi(A))

@@ -7,6 +7,8 @@ Each ``Case`` subclass mirrors one script of PTsolvers/PseudoTransientStokes.jl:
   ``VE2DPerf``   scripts/Stokes2D_ve_perf.jl:80-197     (2D VE, fused explicit-index kernels)
   ``VE3D``       scripts/stokes_3D/Stokes3D_ve_multixpu.jl:118-295 (3D VE, 1 rank)
   ``VE3DPerf``   scripts/stokes_3D/Stokes3D_ve_perf.jl:116-255     (3D VE, fused kernels)
+  ``VE2DDamp``   scripts/previous_damp/Stokes2D_ve0.jl:82-204 (2D VE, damped scheme)
+  ``V2DDamp``    scripts/previous_damp/Stokes2D0.jl:72-173    (2D viscous, damped scheme)
   ``V3D``        3D viscous: no reference script; the 3D perf kernels with the elastic
                  terms removed and the viscous iteration parameters of Stokes2D.jl:27-31.
 
@@ -307,6 +309,53 @@ class VE2DPerf(VE2D):
         return self.norm_err(("Rx", "Ry"), "divV")
 
 
+class VE2DDamp(_Case2D):
+    """scripts/previous_damp/Stokes2D_ve0.jl (2D Maxwell VE, the damped "accel. 1" scheme):
+    numerical compressibility β_n in τ, a damped rate dV/dτ = damp*dV/dτ + R and per-face
+    pseudo-time steps dτV = min(dx,dy)^2/4.1/Vsc/@av(Musτ)/(1+β_n), dτPt = 4.1(1+β_n)/Ptsc/
+    max(nx,ny)*Musτ (:27-32). Set-up and initial conditions are Stokes2D.jl's (:118-145); the
+    check is the same (Vmin/Vmax over Vx, norms scaled by lx, :160-167)."""
+
+    defaults = dict(nt=5, iterMax=2e5, nout=200, eps=1e-8, Vdmp=4.0, beta_n=2.0, Vsc=1.0, Ptsc=3.0, CFL=0.0,
+                    Re=0.0, r=0.0)
+
+    def setup(self):
+        nx, ny = self.nx, self.ny
+        self.dampX, self.dampY = 1.0 - self.Vdmp / nx, 1.0 - self.Vdmp / ny
+        # dVx/dVy hold the damped rates dVxdτ/dVydτ: zero at start, carried across time steps
+        return super().setup()
+
+    def iter_params(self):
+        nx, ny = self.nx, self.ny
+        self.alloc(dtVx=(nx - 1, ny - 2), dtVy=(nx - 2, ny - 1), dtPt=(nx, ny))
+        self.L.ora2d_timesteps(self.A("dtVx"), self.A("dtVy"), self.A("dtPt"), self.A("Must"), self.Vsc, self.Ptsc,
+                               min(self.dx, self.dy) ** 2, self.beta_n, float(max(nx, ny)))
+
+    def iteration(self):
+        L, A = self.L, self.A
+        L.ora2d_compute_P(A("divV"), A("Pt"), A("Vx"), A("Vy"), A("dtPt"), self.dx, self.dy)
+        o = (A("txx_o"), A("tyy_o"), A("txy_o")) if self.elastic else (A("txx"), A("tyy"), A("txy"))
+        L.ora2d_compute_tau(A("txx"), A("tyy"), A("txy"), *o, A("Vx"), A("Vy"), A("Mus"), A("divV"), self.G, self.dt,
+                            self.beta_n, self.dx, self.dy, int(self.elastic))
+        L.ora2d_compute_dV(A("Rx"), A("Ry"), A("dVx"), A("dVy"), A("Pt"), A("txx"), A("tyy"), A("txy"), self.dampX,
+                           self.dampY, self.dx, self.dy)
+        L.ora2d_compute_V(A("Vx"), A("Vy"), A("dVx"), A("dVy"), A("dtVx"), A("dtVy"))
+        self.bc()
+
+    def check(self):
+        # Rx, Ry come from compute_dV! of this iteration (Stokes2D_ve0.jl:160-167)
+        return self.norm_err(("Rx", "Ry"), "divV")
+
+
+class V2DDamp(VE2DDamp):
+    """scripts/previous_damp/Stokes2D0.jl (2D viscous, damped scheme): VE2DDamp without
+    the elastic terms, τ = 2Mus(ε̇ - ∇V/3 + β_n ∇V) (:39-44); one solve, iterMax 1e5,
+    nout 500 (:79-80)."""
+
+    elastic = False
+    defaults = dict(VE2DDamp.defaults, nt=1, iterMax=1e5, nout=500)
+
+
 class _Case3D(Case):
     ndim = 3
     igg_coords = False  # Stokes3D_ve_multixpu.jl builds the ICs through ImplicitGlobalGrid's x_g
@@ -524,6 +573,8 @@ VARIANTS = {
     "3d_ve": VE3D,
     "3d_ve_perf": VE3DPerf,
     "3d_v": V3D,
+    "2d_v_damp": V2DDamp,
+    "2d_ve_damp": VE2DDamp,
 }
 
 

@@ -1,0 +1,51 @@
+"""The damped ("accel. 1") 2D scheme of scripts/previous_damp/Stokes2D0.jl and
+Stokes2D_ve0.jl, restated in the oracle.
+
+The reference holds no fixture for these scripts, and its published iteration totals
+for Stokes2D_ve0 (output/out_Stokes2D_ve0.txt: 2800 iterations at 31^2, 4800 at 63^2)
+are not what the committed script computes: restated line by line it needs 4000 and
+7600 (every other restatement in the oracle reproduces its published totals, so the
+file most likely comes from an earlier version of the script). What pins the
+restatement instead is the fixed point: the damped scheme and the pinned
+Stokes2D.jl / Stokes2D_ve.jl restatements iterate the same discrete Stokes equations
+with different pseudo-time dynamics, so their converged fields must agree to the
+tolerance, step after step.
+"""
+import numpy as np
+import pytest
+
+
+def _rel(a, b, centre=False):
+    if centre:
+        a, b = a - a.mean(), b - b.mean()
+    return np.abs(a - b).max() / np.abs(b).max()
+
+
+@pytest.mark.parametrize("damped,plain", [("2d_v_damp", "2d_v"), ("2d_ve_damp", "2d_ve")])
+def test_damped_scheme_converges_to_the_same_solution(damped, plain):
+    """Same discrete problem, two PT schemes: V and τ agree within 1e-8 relative, Pt within
+    1e-7 up to its constant (free-slip pure shear fixes Pt only up to a constant)."""
+    from oracle import scripts as S
+    a = S.make(damped, 47, 47).run()
+    b = S.make(plain, 47, 47).run()
+    assert len(a.iters) == len(b.iters)
+    for k in ("Vx", "Vy", "txx", "tyy", "txy"):
+        assert _rel(a.f[k], b.f[k]) < 1e-8, k
+    assert _rel(a.f["Pt"], b.f["Pt"], centre=True) < 1e-7
+
+
+def test_damped_ve_iteration_counts():
+    """Regression values of the restated Stokes2D_ve0.jl (5 steps, nout 200, ε 1e-8)."""
+    from oracle import scripts as S
+    c = S.make("2d_ve_damp", 31, 31).run()
+    assert c.iters == [800, 800, 800, 800, 800]
+    assert all(h[2] <= 1e-8 for h in c.err_hist if h[1] == 800)
+
+
+def test_damped_parameters_matter():
+    """Vdmp, β_n, Vsc and Ptsc enter the iteration: other values change the error history."""
+    from oracle import scripts as S
+    base = S.make("2d_v_damp", 31, 31, nout=100).run(iter_max=299).err_hist
+    for kw in (dict(Vdmp=3.0), dict(beta_n=1.0), dict(Vsc=2.0), dict(Ptsc=4.0)):
+        h = S.make("2d_v_damp", 31, 31, nout=100, **kw).run(iter_max=299).err_hist
+        assert [e[2] for e in h] != [e[2] for e in base], kw
