@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define PTS_ABI_VERSION 2
+#define PTS_ABI_VERSION 3
 
 #if defined(__GNUC__)
 #define PTS_API __attribute__((visibility("default")))
@@ -53,7 +53,11 @@ enum pts_variant {
     PTS_2D_VE_PERF = 2,  /* scripts/Stokes2D_ve_perf.jl     2D VE, fused Pt_τ + V, _dx form        */
     PTS_3D_VE = 3,       /* scripts/stokes_3D/Stokes3D_ve_multixpu.jl (one rank), roles P/τ/dV/V */
     PTS_3D_VE_PERF = 4,  /* scripts/stokes_3D/Stokes3D_ve_perf.jl, fused Pt_τ + V             */
-    PTS_3D_V = 5         /* 3D viscous: the 3D fused kernels without elastic terms (no script) */
+    PTS_3D_V = 5,        /* 3D viscous: the 3D fused kernels without elastic terms (no script) */
+    /* The damped ("accel. 1") scheme: numerical compressibility β_n, a damped rate
+     * dV/dτ = damp*dV/dτ + R and per-face pseudo-time steps (pts_set_damping). */
+    PTS_2D_V_DAMP = 6,   /* scripts/previous_damp/Stokes2D0.jl     2D viscous, roles P/τ/dV/V     */
+    PTS_2D_VE_DAMP = 7   /* scripts/previous_damp/Stokes2D_ve0.jl  2D Maxwell VE, roles P/τ/dV/V  */
 };
 
 enum pts_precision {
@@ -99,6 +103,12 @@ enum pts_field {
      * R = ∇·τ − ∇P + F. Absent (zero) until first set; 3D_V and 3D_VE_PERF, FP64 two-kernel path. */
     PTS_F_FX, PTS_F_FY, PTS_F_FZ,
     PTS_F_GRAD,     /* ∂J/∂log μ per cell (nx, ny, nz), written by pts_gradient_logmu */
+    /* Pseudo-time steps of the damped variants, written by pts_compute_iter_params
+     * (compute_timesteps!, Stokes2D_ve0.jl:27-32); the damped rates dVxdτ, dVydτ are
+     * held in the dVx, dVy fields. */
+    PTS_F_DTAU_VX,  /* dτVx (nx-1, ny-2) */
+    PTS_F_DTAU_VY,  /* dτVy (nx-2, ny-1) */
+    PTS_F_DTAU_PT,  /* dτPt (nx, ny)     */
     PTS_F_COUNT
 };
 
@@ -145,8 +155,13 @@ PTS_API int pts_init_inclusion(pts_ctx* ctx, double mus0, double musi, double ra
 PTS_API int pts_smooth(pts_ctx* ctx, int32_t nsweeps, double fact);
 /* Musτ .= Mus; compute_maxloc!(Musτ, Mus); bc_x!/bc_y!/bc_z!(Musτ) (Stokes3D_ve_perf.jl:178-182). */
 PTS_API int pts_compute_maxloc(pts_ctx* ctx);
-/* compute_iter_params! (Stokes3D_ve_perf.jl:34-39; viscous Stokes2D.jl:27-31). */
+/* compute_iter_params! (Stokes3D_ve_perf.jl:34-39; viscous Stokes2D.jl:27-31); for the
+ * damped variants compute_timesteps! (Stokes2D_ve0.jl:27-32). */
 PTS_API int pts_compute_iter_params(pts_ctx* ctx);
+/* Numerics of the damped variants (Stokes2D_ve0.jl:95-98): Vdmp (damp = 1 - Vdmp/n per
+ * direction), β_n, Vsc, Ptsc. A new context has the scripts' 4, 2, 1, 3. Call before
+ * pts_compute_iter_params; PTS_E_INVAL for the other variants or Vsc, Ptsc <= 0. */
+PTS_API int pts_set_damping(pts_ctx* ctx, double Vdmp, double beta_n, double Vsc, double Ptsc);
 
 /* ---- PT iteration roles ---- */
 PTS_API int pts_assign_tau(pts_ctx* ctx);        /* assign_τ!  (Stokes3D_ve_perf.jl:41-49)              */

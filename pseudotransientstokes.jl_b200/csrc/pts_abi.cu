@@ -139,6 +139,10 @@ bool field_info(pts_ctx* c, int id, FInfo* o) {
             if (c->v != PTS_3D_V && c->v != PTS_3D_VE_PERF) return false;
             set(&f.grad, nx, ny, nz, 0, 0, 0);
             break;
+        // pseudo-time steps of the damped variants (Stokes2D_ve0.jl:123-124,106)
+        case PTS_F_DTAU_VX: if (!variant_damped(c->v)) return false; set(&f.dtVx, nx - 1, ny - 2, 1, 1, 1, 0); break;
+        case PTS_F_DTAU_VY: if (!variant_damped(c->v)) return false; set(&f.dtVy, nx - 2, ny - 1, 1, 1, 1, 0); break;
+        case PTS_F_DTAU_PT: if (!variant_damped(c->v)) return false; set(&f.dtPt, nx, ny, 1, 0, 0, 0); break;
         default: return false;
     }
     return true;
@@ -190,6 +194,21 @@ double** iterated(Fields64& f, int q) {
 void swap_buffers(pts_ctx* c) {
     for (int q = 0; q < 10; ++q) std::swap(*iterated(c->f, q), *iterated(c->alt, q));
     c->parity ^= 1;
+}
+
+// Numerics of the damped scheme and what derives from them (Stokes2D_ve0.jl:95-105):
+// dampX = 1.0-Vdmp/nx, dampY = 1.0-Vdmp/ny, min_dxy2 = min(dx,dy)^2, max_nxy = max(nx,ny).
+void set_damping(pts_ctx* c, double Vdmp, double beta_n, double Vsc, double Ptsc) {
+    Num& n = c->n;
+    n.Vdmp = Vdmp;
+    n.beta_n = beta_n;
+    n.Vsc = Vsc;
+    n.Ptsc = Ptsc;
+    n.dampX = 1.0 - Vdmp / (double)c->g.nx;
+    n.dampY = 1.0 - Vdmp / (double)c->g.ny;
+    const double m = std::min(n.dx, n.dy);
+    n.min_dxy2 = m * m;
+    n.max_nxy = (double)std::max(c->g.nx, c->g.ny);
 }
 
 int enter(pts_ctx* c) {
@@ -362,7 +381,7 @@ int pts_create(const pts_desc* d, pts_ctx** out) {
     pts_ctx* c = nullptr;
     if (!d || !out) return fail(nullptr, PTS_E_INVAL, "null argument");
     *out = nullptr;
-    if (d->variant < PTS_2D_V || d->variant > PTS_3D_V) return fail(nullptr, PTS_E_INVAL, "unknown variant");
+    if (d->variant < PTS_2D_V || d->variant > PTS_2D_VE_DAMP) return fail(nullptr, PTS_E_INVAL, "unknown variant");
     if (d->precision != PTS_FP64 && d->precision != PTS_MIXED) return fail(nullptr, PTS_E_INVAL, "unknown precision");
     if (d->precision == PTS_MIXED && d->variant != PTS_3D_VE_PERF && d->variant != PTS_3D_V)
         return fail(nullptr, PTS_E_INVAL, "mixed precision is implemented for PTS_3D_VE_PERF and PTS_3D_V");
@@ -411,6 +430,7 @@ int pts_create(const pts_desc* d, pts_ctx** out) {
     n.Vpdt = (d3 ? std::min(std::min(n.dx, n.dy), n.dz) : std::min(n.dx, n.dy)) * d->CFL;
     n.max_l = d->max_l > 0 ? d->max_l : (d3 ? std::max(std::max(d->lx, d->ly), d->lz) : std::max(d->lx, d->ly));
     n.adjoint = d->adjoint ? 1 : 0;
+    set_damping(c, 4.0, 2.0, 1.0, 3.0);  // Stokes2D_ve0.jl:95-98
     int rc = PTS_OK;
     auto bail = [&](int code) {
         g_create_err = c->err;
@@ -446,6 +466,12 @@ int pts_create(const pts_desc* d, pts_ctx** out) {
             for (double** p : olds3)
                 if ((rc = alloc_field(c, p)) != PTS_OK) return bail(rc);
         }
+    }
+    if (variant_damped(c->v)) {
+        // the damped rates dVxdτ, dVydτ are iteration state (zero at start), and dτV, dτPt
+        double** damp[] = {&f.dVx, &f.dVy, &f.dtVx, &f.dtVy, &f.dtPt};
+        for (double** p : damp)
+            if ((rc = alloc_field(c, p)) != PTS_OK) return bail(rc);
     }
     c->mixed = d->precision == PTS_MIXED;
     c->fused = variant_fused(c->v) && d->single_pass != 0 && !c->mixed;
@@ -593,6 +619,17 @@ int pts_compute_iter_params(pts_ctx* c) {
     int rc = enter(c);
     if (rc) return rc;
     CK(launch_iter_params(c->v, c->g, c->f, c->n, c->stream));
+    return PTS_OK;
+}
+
+int pts_set_damping(pts_ctx* c, double Vdmp, double beta_n, double Vsc, double Ptsc) {
+    int rc = enter(c);
+    if (rc) return rc;
+    if (!variant_damped(c->v)) return fail(c, PTS_E_INVAL, "pts_set_damping needs PTS_2D_V_DAMP or PTS_2D_VE_DAMP");
+    if (!(Vsc > 0) || !(Ptsc > 0) || !std::isfinite(Vdmp) || !std::isfinite(beta_n) || !(beta_n > -1.0))
+        return fail(c, PTS_E_INVAL, "damping numerics: Vsc, Ptsc must be > 0, beta_n > -1, Vdmp finite");
+    set_damping(c, Vdmp, beta_n, Vsc, Ptsc);
+    drop_graph(c);  // the captured launches hold the old numerics
     return PTS_OK;
 }
 

@@ -25,10 +25,13 @@ enum Variant {
     VE3D = PTS_3D_VE,
     VE3D_PERF = PTS_3D_VE_PERF,
     V3D = PTS_3D_V,
+    V2D_DAMP = PTS_2D_V_DAMP,
+    VE2D_DAMP = PTS_2D_VE_DAMP,
 };
 
 inline bool variant_is3d(int v) { return v == VE3D || v == VE3D_PERF || v == V3D; }
-inline bool variant_elastic(int v) { return v != V2D && v != V3D; }
+inline bool variant_elastic(int v) { return v != V2D && v != V3D && v != V2D_DAMP; }
+inline bool variant_damped(int v) { return v == V2D_DAMP || v == VE2D_DAMP; }
 // "perf" variants multiply by _dx = 1/dx (explicit-index kernels); the others divide by dx.
 inline bool variant_perf(int v) { return v == VE2D_PERF || v == VE3D_PERF || v == V3D; }
 // ∇V of the check: from compute_P! before the V update (role variants), or recomputed
@@ -59,6 +62,9 @@ struct Num {
     double Vpdt, max_l, Re;
     double lx, ly, lz;
     int adjoint;  // 3D_V: iterate the transposed (adjoint) system, ghosts folded (pts_abi.cu)
+    // damped variants (Stokes2D_ve0.jl:95-105): Vdmp, β_n, Vsc, Ptsc and the derived
+    // dampX = 1-Vdmp/nx, dampY = 1-Vdmp/ny, min_dxy2 = min(dx,dy)^2, max_nxy = max(nx,ny)
+    double Vdmp, beta_n, Vsc, Ptsc, dampX, dampY, min_dxy2, max_nxy;
 };
 
 template <typename T>
@@ -72,6 +78,7 @@ struct FieldsT {
     T *rhog, *rhog2;  // buoyancy ρg of the batched sweep (Stokes2D_param.jl), else null
     T *Fx, *Fy, *Fz;  // momentum sources on interior faces (adjoint solves), else null
     T *grad;          // ∂J/∂log μ per cell, else null
+    T *dtVx, *dtVy, *dtPt;  // pseudo-time steps dτVx, dτVy, dτPt of the damped variants, else null
 };
 using Fields64 = FieldsT<double>;
 

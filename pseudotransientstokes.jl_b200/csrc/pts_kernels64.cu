@@ -428,6 +428,139 @@ __global__ void k2_add_dV(Geom g, Fields64 f) {
     if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 1) f.Vy[c] = f.Vy[c] + f.dVy[c];
 }
 
+// ------------------------------------------------------------------ 2D damped scheme
+//
+// scripts/previous_damp/Stokes2D0.jl (viscous) and Stokes2D_ve0.jl (Maxwell VE). Unified
+// positions: dτPt on the cells; dτVx and the damped rate dVxdτ (held in dVx) on the x-faces
+// of Rx (i in [1,nx-1], j in [1,ny-2]); dτVy, dVydτ (dVy) on the y-faces of Ry.
+
+// compute_timesteps! (Stokes2D_ve0.jl:27-32, Stokes2D0.jl:26-31)
+__global__ void __launch_bounds__(256) k2d_timesteps(Geom g, Fields64 f, Num n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int nx = g.nx, ny = g.ny;
+    if (i > nx || j > ny) return;
+    const idx_t c = gidx32(g, i, j, 0);
+    const idx_t sx = 1, sy = g.px;
+    if (i < nx && j < ny) f.dtPt[c] = 4.1 * (1.0 + n.beta_n) / n.Ptsc / n.max_nxy * f.Must[c];
+    if (i >= 1 && i <= nx - 1 && j >= 1 && j <= ny - 2)  // @av_xi(Musτ)
+        f.dtVx[c] = 1.0 / 4.1 / n.Vsc * n.min_dxy2 / ((f.Must[c - sx] + f.Must[c]) * 0.5) / (1.0 + n.beta_n);
+    if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 1)  // @av_yi(Musτ)
+        f.dtVy[c] = 1.0 / 4.1 / n.Vsc * n.min_dxy2 / ((f.Must[c - sy] + f.Must[c]) * 0.5) / (1.0 + n.beta_n);
+}
+
+// compute_P! (Stokes2D_ve0.jl:41-45): ∇V, Pt = Pt - dτPt*∇V; then compute_τ! with the
+// numerical compressibility β_n: viscous (Stokes2D0.jl:39-44)
+//   τxx = 2Mus*(d_xa(Vx)/dx - 1/3*∇V + β_n*∇V),  τxy = 2@av(Mus)*(0.5*(d_yi(Vx)/dy + d_xi(Vy)/dx))
+// Maxwell (Stokes2D_ve0.jl:47-54), Xsi = Mus/(G*dt):
+//   τxx = τxx_o*Xsi/(Xsi+1) + 2Mus/(Xsi+1)*(...),  τxy likewise with @av(Mus)
+// With ROLE_TAU alone ∇V is read back from the field compute_P! stored.
+template <bool EL>
+__global__ void __launch_bounds__(256) k2d_Pt_tau(Geom g, Fields64 f, Num n, int roles, int store_divV) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= g.nx || j >= g.ny) return;
+    const idx_t c = gidx32(g, i, j, 0);
+    const idx_t sx = 1, sy = g.px;
+    const double dvx = f.Vx[c + sx] - f.Vx[c];
+    const double dvy = f.Vy[c + sy] - f.Vy[c];
+    double dv;
+    if (roles & ROLE_P) {
+        dv = dvx / n.dx + dvy / n.dy;
+        if (store_divV) f.divV[c] = dv;
+        f.Pt[c] = f.Pt[c] - f.dtPt[c] * dv;
+    } else {
+        dv = f.divV[c];
+    }
+    if (!(roles & ROLE_TAU)) return;
+    const double Mc = f.Mus[c];
+    const double ex = dvx / n.dx - 1.0 / 3.0 * dv + n.beta_n * dv;
+    const double ey = dvy / n.dy - 1.0 / 3.0 * dv + n.beta_n * dv;
+    if (EL) {
+        const double X = Mc / n.gdt;
+        f.txx[c] = f.txx_o[c] * X / (X + 1.0) + 2.0 * Mc / (X + 1.0) * ex;
+        f.tyy[c] = f.tyy_o[c] * X / (X + 1.0) + 2.0 * Mc / (X + 1.0) * ey;
+    } else {
+        f.txx[c] = 2.0 * Mc * ex;
+        f.tyy[c] = 2.0 * Mc * ey;
+    }
+    if (i >= 1 && j >= 1) {  // τxy on the vertex (x-face i, y-face j)
+        const double am = (((f.Mus[c - sx - sy] + f.Mus[c - sy]) + f.Mus[c - sx]) + Mc) * 0.25;
+        const double exy = 0.5 * ((f.Vx[c] - f.Vx[c - sy]) / n.dy + (f.Vy[c] - f.Vy[c - sx]) / n.dx);
+        if (EL) {
+            const double X = am / n.gdt;
+            f.txy[c] = f.txy_o[c] * X / (X + 1.0) + 2.0 * am / (X + 1.0) * exy;
+        } else {
+            f.txy[c] = 2.0 * am * exy;
+        }
+    }
+}
+
+// compute_dV! + compute_V! + bc_y!(Vx), bc_x!(Vy) (Stokes2D_ve0.jl:56-68,156-157):
+//   dVxdτ = dampX*dVxdτ + Rx,  @inn(Vx) = @inn(Vx) + dτVx*dVxdτ
+// With update = 0 only the free-slip copies.
+__global__ void __launch_bounds__(256) k2d_V_bc(Geom g, Fields64 f, Num n, int update) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int nx = g.nx, ny = g.ny;
+    if (i > nx || j > ny) return;
+    const idx_t c = gidx32(g, i, j, 0);
+    const idx_t sx = 1, sy = g.px;
+    if (j >= 1 && j <= ny - 2) {  // Vx source faces (bc_y!)
+        double v = f.Vx[c];
+        if (update && i >= 1 && i <= nx - 1) {
+            const double r = n.dampX * f.dVx[c] + res2_x<false>(f, n, c, sx, sy);
+            f.dVx[c] = r;
+            v = v + f.dtVx[c] * r;
+            f.Vx[c] = v;
+        }
+        if (j == 1) f.Vx[c - sy] = v;
+        if (j == ny - 2) f.Vx[c + sy] = v;
+    }
+    if (i >= 1 && i <= nx - 2) {  // Vy source faces (bc_x!)
+        double v = f.Vy[c];
+        if (update && j >= 1 && j <= ny - 1) {
+            const double r = n.dampY * f.dVy[c] + res2_y<false>(f, n, c, sx, sy);
+            f.dVy[c] = r;
+            v = v + f.dtVy[c] * r;
+            f.Vy[c] = v;
+        }
+        if (i == 1) f.Vy[c - sx] = v;
+        if (i == nx - 2) f.Vy[c + sx] = v;
+    }
+}
+
+// compute_dV! alone (Stokes2D_ve0.jl:56-62): Rx, Ry and the damped rates.
+__global__ void k2d_dV(Geom g, Fields64 f, Num n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int nx = g.nx, ny = g.ny;
+    if (i > nx || j > ny) return;
+    const idx_t c = gidx32(g, i, j, 0);
+    const idx_t sx = 1, sy = g.px;
+    if (i >= 1 && i <= nx - 1 && j >= 1 && j <= ny - 2) {
+        const double R = res2_x<false>(f, n, c, sx, sy);
+        f.Rx[c] = R;
+        f.dVx[c] = n.dampX * f.dVx[c] + R;
+    }
+    if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 1) {
+        const double R = res2_y<false>(f, n, c, sx, sy);
+        f.Ry[c] = R;
+        f.dVy[c] = n.dampY * f.dVy[c] + R;
+    }
+}
+
+// compute_V! alone (Stokes2D_ve0.jl:64-68): @inn(V) = @inn(V) + dτV*dVdτ
+__global__ void k2d_add_dV(Geom g, Fields64 f) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int nx = g.nx, ny = g.ny;
+    if (i > nx || j > ny) return;
+    const idx_t c = gidx32(g, i, j, 0);
+    if (i >= 1 && i <= nx - 1 && j >= 1 && j <= ny - 2) f.Vx[c] = f.Vx[c] + f.dtVx[c] * f.dVx[c];
+    if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 1) f.Vy[c] = f.Vy[c] + f.dtVy[c] * f.dVy[c];
+}
+
 // ------------------------------------------------------------------ convergence check
 
 struct Acc {
@@ -1371,6 +1504,8 @@ cudaError_t launch_Pt_tau(int v, const Geom& g, const Fields64& f, const Num& n,
         case V2D: k2_Pt_tau<V2D><<<grid_cells(g), blk(), 0, s>>>(g, f, n, roles, sd); break;
         case VE2D: k2_Pt_tau<VE2D><<<grid_cells(g), blk(), 0, s>>>(g, f, n, roles, sd); break;
         case VE2D_PERF: k2_Pt_tau<VE2D_PERF><<<grid_cells(g), blk(), 0, s>>>(g, f, n, roles, sd); break;
+        case V2D_DAMP: k2d_Pt_tau<false><<<grid_cells(g), blk(), 0, s>>>(g, f, n, roles, sd); break;
+        case VE2D_DAMP: k2d_Pt_tau<true><<<grid_cells(g), blk(), 0, s>>>(g, f, n, roles, sd); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -1394,6 +1529,8 @@ cudaError_t launch_V_bc(int v, const Geom& g, const Fields64& f, const Num& n, b
         case V2D: k2_V_bc<V2D><<<grid_faces(g, false), blk(), 0, s>>>(g, f, n, u); break;
         case VE2D: k2_V_bc<VE2D><<<grid_faces(g, false), blk(), 0, s>>>(g, f, n, u); break;
         case VE2D_PERF: k2_V_bc<VE2D_PERF><<<grid_faces(g, false), blk(), 0, s>>>(g, f, n, u); break;
+        case V2D_DAMP:
+        case VE2D_DAMP: k2d_V_bc<<<grid_faces(g, false), blk(), 0, s>>>(g, f, n, u); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -1410,6 +1547,8 @@ cudaError_t launch_dV(int v, const Geom& g, const Fields64& f, const Num& n, cud
         case V2D: k2_dV<V2D><<<grid_faces(g, false), blk(), 0, s>>>(g, f, n); break;
         case VE2D: k2_dV<VE2D><<<grid_faces(g, false), blk(), 0, s>>>(g, f, n); break;
         case VE2D_PERF: k2_dV<VE2D_PERF><<<grid_faces(g, false), blk(), 0, s>>>(g, f, n); break;
+        case V2D_DAMP:
+        case VE2D_DAMP: k2d_dV<<<grid_faces(g, false), blk(), 0, s>>>(g, f, n); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -1417,6 +1556,7 @@ cudaError_t launch_dV(int v, const Geom& g, const Fields64& f, const Num& n, cud
 
 cudaError_t launch_add_dV(int v, const Geom& g, const Fields64& f, cudaStream_t s) {
     if (variant_is3d(v)) k3_add_dV<<<grid_faces(g, true), blk(), 0, s>>>(g, f);
+    else if (variant_damped(v)) k2d_add_dV<<<grid_faces(g, false), blk(), 0, s>>>(g, f);
     else k2_add_dV<<<grid_faces(g, false), blk(), 0, s>>>(g, f);
     return cudaGetLastError();
 }
@@ -1452,6 +1592,9 @@ cudaError_t launch_check(int v, const Geom& g, const Fields64& f, const Num& n, 
         case V2D: k2_check<V2D><<<gr, blk(), 0, s>>>(g, f, n, partials); break;
         case VE2D: k2_check<VE2D><<<gr, blk(), 0, s>>>(g, f, n, partials); break;
         case VE2D_PERF: k2_check<VE2D_PERF><<<gr, blk(), 0, s>>>(g, f, n, partials); break;
+        // the damped check is Stokes2D.jl's: ∇V stored by compute_P!, R of the current τ, Pt
+        case V2D_DAMP:
+        case VE2D_DAMP: k2_check<V2D><<<gr, blk(), 0, s>>>(g, f, n, partials); break;
         default: return cudaErrorInvalidValue;
     }
     cudaError_t e = cudaGetLastError();
@@ -1550,7 +1693,8 @@ cudaError_t launch_maxloc(int v, const Geom& g, double* must, const double* mus,
 }
 
 cudaError_t launch_iter_params(int v, const Geom& g, const Fields64& f, const Num& n, cudaStream_t s) {
-    if (variant_elastic(v)) k_iter_params<true><<<grid_cells(g), blk(), 0, s>>>(g, f, n);
+    if (variant_damped(v)) k2d_timesteps<<<grid_faces(g, false), blk(), 0, s>>>(g, f, n);
+    else if (variant_elastic(v)) k_iter_params<true><<<grid_cells(g), blk(), 0, s>>>(g, f, n);
     else k_iter_params<false><<<grid_cells(g), blk(), 0, s>>>(g, f, n);
     return cudaGetLastError();
 }

@@ -23,6 +23,8 @@ VARIANTS = {
     "3d_ve": 3,       # scripts/stokes_3D/Stokes3D_ve_multixpu.jl (one rank)
     "3d_ve_perf": 4,  # scripts/stokes_3D/Stokes3D_ve_perf.jl
     "3d_v": 5,        # 3D viscous (no reference script)
+    "2d_v_damp": 6,   # scripts/previous_damp/Stokes2D0.jl
+    "2d_ve_damp": 7,  # scripts/previous_damp/Stokes2D_ve0.jl
 }
 PRECISIONS = {"fp64": 0, "mixed": 1}
 
@@ -35,6 +37,7 @@ FIELDS = [
     "rhog",
     "Fx", "Fy", "Fz",
     "grad",
+    "dtVx", "dtVy", "dtPt",
 ]
 FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
 
@@ -106,6 +109,7 @@ SIGNATURES = {
     "pts_smooth": ([_P, _I32, _D], ctypes.c_int),
     "pts_compute_maxloc": ([_P], ctypes.c_int),
     "pts_compute_iter_params": ([_P], ctypes.c_int),
+    "pts_set_damping": ([_P] + [ctypes.c_double] * 4, ctypes.c_int),
     "pts_assign_tau": ([_P], ctypes.c_int),
     "pts_compute_P": ([_P], ctypes.c_int),
     "pts_compute_tau": ([_P], ctypes.c_int),

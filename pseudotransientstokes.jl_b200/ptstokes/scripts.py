@@ -11,6 +11,8 @@ scripts' NX/NY/NZ environment variables (``haskey(ENV, "NX") ? parse(Int, ENV["N
     Stokes3D_ve         scripts/stokes_3D/Stokes3D_ve_multixpu.jl (one rank)
     Stokes3D_ve_perf    scripts/stokes_3D/Stokes3D_ve_perf.jl
     Stokes3D_v          3D viscous (no reference script)
+    Stokes2D0           scripts/previous_damp/Stokes2D0.jl    (damped scheme)
+    Stokes2D_ve0        scripts/previous_damp/Stokes2D_ve0.jl (damped scheme)
 """
 import os
 import time
@@ -84,8 +86,17 @@ def Stokes3D_v(nx=None, ny=None, nz=None, return_solver=False, verbose=False, **
                    verbose, **kw)
 
 
+def Stokes2D0(nx=None, ny=None, return_solver=False, verbose=False, **kw):
+    """scripts/previous_damp/Stokes2D0.jl:72-173 (2D viscous, damped scheme; NX, NY default 511)."""
+    return _script("2d_v_damp", nx or _env("NX", 511), ny or _env("NY", 511), None, return_solver, verbose, **kw)
+
+
+def Stokes2D_ve0(nx=None, ny=None, return_solver=False, verbose=False, **kw):
+    """scripts/previous_damp/Stokes2D_ve0.jl:82-204 (2D Maxwell VE, damped scheme, 5 steps)."""
+    return _script("2d_ve_damp", nx or _env("NX", 511), ny or _env("NY", 511), None, return_solver, verbose, **kw)
+
+
 # Effective memory traffic per PT iteration, in bytes, by the reference's own
 # convention (A_eff; Stokes3D_ve_perf.jl:229, Stokes2D_ve_perf.jl:173).
 def a_eff_bytes(variant, nx, ny, nz=1, itemsize=8):
-    arrays = {"3d_ve": 29, "3d_ve_perf": 29, "3d_v": 23, "2d_ve": 18, "2d_ve_perf": 18, "2d_v": 15}[variant]
-    return arrays * nx * ny * (nz if variant.startswith("3d") else 1) * itemsize
+    return output.A_EFF_ARRAYS[variant] * nx * ny * (nz if variant.startswith("3d") else 1) * itemsize

@@ -29,7 +29,14 @@ VARIANT_DEFAULTS = {
     "3d_ve_perf": dict(nt=1, iter_max=200, nout=2000, eps=1e-8, CFL=0.8 / math.sqrt(3), Re=6 * PI, r=1.0),
     # 3D viscous (no script): the 3D numerics, one "time step"
     "3d_v": dict(nt=1, iter_max=2e5, nout=200, eps=1e-8, CFL=0.8 / math.sqrt(3), Re=6 * PI, r=1.0),
+    # scripts/previous_damp/Stokes2D0.jl:76-86 (damped scheme; r, Re, CFL unused)
+    "2d_v_damp": dict(nt=1, iter_max=1e5, nout=500, eps=1e-8, CFL=0.0, Re=0.0, r=0.0, Vdmp=4.0, beta_n=2.0,
+                      Vsc=1.0, Ptsc=3.0),
+    # scripts/previous_damp/Stokes2D_ve0.jl:91-99
+    "2d_ve_damp": dict(nt=5, iter_max=2e5, nout=200, eps=1e-8, CFL=0.0, Re=0.0, r=0.0, Vdmp=4.0, beta_n=2.0,
+                       Vsc=1.0, Ptsc=3.0),
 }
+DAMPING = ("Vdmp", "beta_n", "Vsc", "Ptsc")
 
 
 def linrange(a, b, n):
@@ -41,7 +48,8 @@ def linrange(a, b, n):
 class Solver:
     """A PT Stokes context (``pts_ctx``) with its device fields.
 
-    ``variant`` is one of ``2d_v, 2d_ve, 2d_ve_perf, 3d_ve, 3d_ve_perf, 3d_v``.
+    ``variant`` is one of ``2d_v, 2d_ve, 2d_ve_perf, 3d_ve, 3d_ve_perf, 3d_v, 2d_v_damp,
+    2d_ve_damp``.
     Keyword arguments override the script defaults (``VARIANT_DEFAULTS``) and the
     physics (``lx, ly, lz, G, xi, mus0``: ``dt = mus0/(G*xi)`` as in the scripts).
     """
@@ -73,6 +81,8 @@ class Solver:
         ctx = ctypes.c_void_p()
         check(self.lib, None, self.lib.pts_create(ctypes.byref(d), ctypes.byref(ctx)))
         self.ctx = ctx
+        if variant.endswith("_damp"):
+            self.set_damping(*(p[k] for k in DAMPING))
         self.dx = p["lx"] / nx
         self.dy = p["ly"] / ny
         self.dz = p["lz"] / nz if self.ndim == 3 else 1.0
@@ -134,6 +144,11 @@ class Solver:
 
     def compute_iter_params(self):
         self._ck(self.lib.pts_compute_iter_params(self.ctx))
+
+    def set_damping(self, Vdmp=4.0, beta_n=2.0, Vsc=1.0, Ptsc=3.0):
+        """Numerics of the damped scheme (Stokes2D_ve0.jl:95-98); before compute_iter_params."""
+        self._ck(self.lib.pts_set_damping(self.ctx, Vdmp, beta_n, Vsc, Ptsc))
+        self.p.update(Vdmp=Vdmp, beta_n=beta_n, Vsc=Vsc, Ptsc=Ptsc)
 
     def setup_inclusion(self, musi=1e-3, radius2=1.0, ebg=1.0, nsmooth=10):
         """The scripts' set-up: ICs, 10x smooth!, maxloc + bc, iteration parameters."""

@@ -31,7 +31,7 @@ def test_library_exports_every_declared_symbol():
     lib = ptstokes.load()
     missing = [n for n in declared_symbols() if not hasattr(lib, n)]
     assert not missing, missing
-    assert lib.pts_abi_version() == 2
+    assert lib.pts_abi_version() == 3
 
 
 def test_python_binding_covers_the_header():
@@ -108,7 +108,7 @@ def test_adjoint_and_batch_descriptions_are_validated_without_a_device():
     assert lib.pts_batch_create(ctypes.byref(bd), inst, 0, ctypes.byref(b)) == _abi.PTS_E_INVAL
 
 
-def test_field_table_covers_the_adjoint_fields():
+def test_field_table_covers_the_adjoint_and_damping_fields():
     """The Python field names follow the header's pts_field enum, new fields included."""
     from ptstokes import _abi
     hdr = open(os.path.join(ROOT, "include", "ptstokes.h")).read()
@@ -116,5 +116,29 @@ def test_field_table_covers_the_adjoint_fields():
     enum = enum[:enum.index("PTS_F_COUNT")]
     ids = re.findall(r"PTS_F_[A-Z_]+", enum)
     assert len(ids) == len(_abi.FIELDS)
-    assert ids[-4:] == ["PTS_F_FX", "PTS_F_FY", "PTS_F_FZ", "PTS_F_GRAD"]
-    assert _abi.FIELDS[-4:] == ["Fx", "Fy", "Fz", "grad"]
+    assert ids[-7:] == ["PTS_F_FX", "PTS_F_FY", "PTS_F_FZ", "PTS_F_GRAD", "PTS_F_DTAU_VX", "PTS_F_DTAU_VY",
+                        "PTS_F_DTAU_PT"]
+    assert _abi.FIELDS[-7:] == ["Fx", "Fy", "Fz", "grad", "dtVx", "dtVy", "dtPt"]
+
+
+def test_variant_table_matches_the_header():
+    """pts_variant values, the damped variants included, and their validation without a device."""
+    import ptstokes
+    from ptstokes import _abi
+    hdr = open(os.path.join(ROOT, "include", "ptstokes.h")).read()
+    enum = hdr[hdr.index("enum pts_variant"):]
+    enum = re.sub(r"/\*.*?\*/", "", enum[:enum.index("};")], flags=re.S)
+    vals = {m.group(1): int(m.group(2)) for m in re.finditer(r"(PTS_\w+)\s*=\s*(\d+)", enum)}
+    assert vals["PTS_2D_V_DAMP"] == _abi.VARIANTS["2d_v_damp"] == 6
+    assert vals["PTS_2D_VE_DAMP"] == _abi.VARIANTS["2d_ve_damp"] == 7
+    assert sorted(vals.values()) == sorted(_abi.VARIANTS.values())
+    lib = ptstokes.load()
+    d = _abi.PtsDesc()
+    d.nx = d.ny = d.nz = 9
+    d.nout, d.lx, d.ly, d.lz = 10, 10.0, 10.0, 10.0
+    ctx = ctypes.c_void_p()
+    d.variant = 8
+    assert lib.pts_create(ctypes.byref(d), ctypes.byref(ctx)) == _abi.PTS_E_INVAL
+    d.variant, d.precision = 7, 1
+    assert lib.pts_create(ctypes.byref(d), ctypes.byref(ctx)) == _abi.PTS_E_INVAL
+    assert lib.pts_set_damping(None, 4.0, 2.0, 1.0, 3.0) == _abi.PTS_E_INVAL
