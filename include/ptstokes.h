@@ -57,7 +57,8 @@ enum pts_variant {
     /* The damped ("accel. 1") scheme: numerical compressibility β_n, a damped rate
      * dV/dτ = damp*dV/dτ + R and per-face pseudo-time steps (pts_set_damping). */
     PTS_2D_V_DAMP = 6,   /* scripts/previous_damp/Stokes2D0.jl     2D viscous, roles P/τ/dV/V     */
-    PTS_2D_VE_DAMP = 7   /* scripts/previous_damp/Stokes2D_ve0.jl  2D Maxwell VE, roles P/τ/dV/V  */
+    PTS_2D_VE_DAMP = 7,  /* scripts/previous_damp/Stokes2D_ve0.jl  2D Maxwell VE, roles P/τ/dV/V  */
+    PTS_3D_V_DAMP = 8    /* scripts/stokes_3D/previous_damp/Stokes3D0_multixpu.jl (one rank), 3D viscous */
 };
 
 enum pts_precision {
@@ -106,9 +107,10 @@ enum pts_field {
     /* Pseudo-time steps of the damped variants, written by pts_compute_iter_params
      * (compute_timesteps!, Stokes2D_ve0.jl:27-32); the damped rates dVxdτ, dVydτ are
      * held in the dVx, dVy fields. */
-    PTS_F_DTAU_VX,  /* dτVx (nx-1, ny-2) */
-    PTS_F_DTAU_VY,  /* dτVy (nx-2, ny-1) */
-    PTS_F_DTAU_PT,  /* dτPt (nx, ny)     */
+    PTS_F_DTAU_VX,  /* dτVx, the extent of Rx */
+    PTS_F_DTAU_VY,  /* dτVy, the extent of Ry */
+    PTS_F_DTAU_VZ,  /* dτVz, the extent of Rz (3D) */
+    PTS_F_DTAU_PT,  /* dτPt, one per cell */
     PTS_F_COUNT
 };
 
@@ -158,9 +160,10 @@ PTS_API int pts_compute_maxloc(pts_ctx* ctx);
 /* compute_iter_params! (Stokes3D_ve_perf.jl:34-39; viscous Stokes2D.jl:27-31); for the
  * damped variants compute_timesteps! (Stokes2D_ve0.jl:27-32). */
 PTS_API int pts_compute_iter_params(pts_ctx* ctx);
-/* Numerics of the damped variants (Stokes2D_ve0.jl:95-98): Vdmp (damp = 1 - Vdmp/n per
- * direction), β_n, Vsc, Ptsc. A new context has the scripts' 4, 2, 1, 3. Call before
- * pts_compute_iter_params; PTS_E_INVAL for the other variants or Vsc, Ptsc <= 0. */
+/* Numerics of the damped variants (Stokes2D_ve0.jl:95-98, Stokes3D0_multixpu.jl:105-108):
+ * Vdmp (damp = 1 - Vdmp/n per direction), β_n, Vsc, Ptsc. A new context has the scripts'
+ * values: 4, 2, 1, 3 in 2D and 4, 3, 1, 5 in 3D. Call before pts_compute_iter_params;
+ * PTS_E_INVAL for the other variants, Vsc or Ptsc <= 0, or β_n <= -1. */
 PTS_API int pts_set_damping(pts_ctx* ctx, double Vdmp, double beta_n, double Vsc, double Ptsc);
 
 /* ---- PT iteration roles ---- */

@@ -84,6 +84,11 @@ _SIGS = {
     "ora2d_compute_tau": [Arr] * 10 + [_D] * 5 + [ctypes.c_int],
     "ora2d_compute_dV": [Arr] * 8 + [_D] * 4,
     "ora2d_compute_V": [Arr] * 6,
+    "ora3d_timesteps": [Arr] * 5 + [_D] * 5,
+    "ora3d_compute_P": [Arr] * 6 + [_D] * 3,
+    "ora3d_compute_tau": [Arr] * 11 + [_D] * 4,
+    "ora3d_compute_dV": [Arr] * 13 + [_D] * 6,
+    "ora3d_compute_V": [Arr] * 9,
     "ora3p_compute_Res": [Arr] * 14 + [_D] * 3,
     "ora_stats": [Arr, ctypes.POINTER(_D), ctypes.POINTER(_D), ctypes.POINTER(_D)],
     "ora_num_threads": [],

@@ -693,6 +693,120 @@ void ora3_compute_V(oarr Vx_, oarr Vy_, oarr Vz_, oarr dVx_, oarr dVy_, oarr dVz
             }
 }
 
+// ---------------------------------------------------------------- 3D damped scheme (viscous)
+// scripts/stokes_3D/previous_damp/Stokes3D0_multixpu.jl on one rank: the "accel. 1" scheme
+// of the 2D damped scripts in 3D.
+
+// compute_timesteps! (Stokes3D0_multixpu.jl:37-43); note the 3D order 1/6.1/(1+β_n)/Vsc*…
+void ora3d_timesteps(oarr dtVx_, oarr dtVy_, oarr dtVz_, oarr dtPt_, oarr Must_, double Vsc, double Ptsc,
+                     double min_dxyz2, double beta_n, double max_nxyz) {
+    F3 dtVx(dtVx_), dtVy(dtVy_), dtVz(dtVz_), dtPt(dtPt_), M(Must_);
+#pragma omp parallel for schedule(static)
+    for (int64_t iz = 1; iz <= M.n3; ++iz)
+        for (int64_t iy = 1; iy <= M.n2; ++iy)
+            for (int64_t ix = 1; ix <= M.n1; ++ix) {
+                const double c = 1.0 / 6.1 / (1.0 + beta_n) / Vsc * min_dxyz2;
+                if (ix <= dtVx.n1 && iy <= dtVx.n2 && iz <= dtVx.n3)
+                    dtVx(ix, iy, iz) = c / ((M(ix, iy + 1, iz + 1) + M(ix + 1, iy + 1, iz + 1)) * 0.5);
+                if (ix <= dtVy.n1 && iy <= dtVy.n2 && iz <= dtVy.n3)
+                    dtVy(ix, iy, iz) = c / ((M(ix + 1, iy, iz + 1) + M(ix + 1, iy + 1, iz + 1)) * 0.5);
+                if (ix <= dtVz.n1 && iy <= dtVz.n2 && iz <= dtVz.n3)
+                    dtVz(ix, iy, iz) = c / ((M(ix + 1, iy + 1, iz) + M(ix + 1, iy + 1, iz + 1)) * 0.5);
+                dtPt(ix, iy, iz) = 6.1 * (1.0 + beta_n) / Ptsc / max_nxyz * M(ix, iy, iz);
+            }
+}
+
+// compute_P! (Stokes3D0_multixpu.jl:45-49): ∇V, Pt = Pt - dτPt*∇V
+void ora3d_compute_P(oarr divV_, oarr Pt_, oarr Vx_, oarr Vy_, oarr Vz_, oarr dtPt_, double dx, double dy, double dz) {
+    F3 divV(divV_), Pt(Pt_), Vx(Vx_), Vy(Vy_), Vz(Vz_), dtPt(dtPt_);
+#pragma omp parallel for schedule(static)
+    for (int64_t iz = 1; iz <= Pt.n3; ++iz)
+        for (int64_t iy = 1; iy <= Pt.n2; ++iy)
+            for (int64_t ix = 1; ix <= Pt.n1; ++ix) {
+                divV(ix, iy, iz) = (Vx(ix + 1, iy, iz) - Vx(ix, iy, iz)) / dx + (Vy(ix, iy + 1, iz) - Vy(ix, iy, iz)) / dy +
+                                   (Vz(ix, iy, iz + 1) - Vz(ix, iy, iz)) / dz;
+                Pt(ix, iy, iz) = Pt(ix, iy, iz) - dtPt(ix, iy, iz) * divV(ix, iy, iz);
+            }
+}
+
+// compute_τ! (Stokes3D0_multixpu.jl:51-59):
+//   τxx = 2@inn_yz(Mus)*(@d_xi(Vx)/dx - 1/3*@inn_yz(∇V) + β_n*@inn_yz(∇V)),
+//   τxy = 2@av_xyi(Mus)*(0.5*(@d_yi(Vx)/dy + @d_xi(Vy)/dx)), ...
+void ora3d_compute_tau(oarr divV_, oarr txx_, oarr tyy_, oarr tzz_, oarr txy_, oarr txz_, oarr tyz_, oarr Vx_,
+                       oarr Vy_, oarr Vz_, oarr Mus_, double beta_n, double dx, double dy, double dz) {
+    F3 dv(divV_), txx(txx_), tyy(tyy_), tzz(tzz_), txy(txy_), txz(txz_), tyz(tyz_), Vx(Vx_), Vy(Vy_), Vz(Vz_), M(Mus_);
+    const int64_t nx = M.n1, ny = M.n2, nz = M.n3;
+#pragma omp parallel for schedule(static)
+    for (int64_t iz = 1; iz <= nz; ++iz)
+        for (int64_t iy = 1; iy <= ny; ++iy)
+            for (int64_t ix = 1; ix <= nx; ++ix) {
+                const int64_t ixi = ix + 1, iyi = iy + 1, izi = iz + 1;
+                if (ix <= txx.n1 && iy <= txx.n2 && iz <= txx.n3) {
+                    const double d = dv(ix, iyi, izi);
+                    txx(ix, iy, iz) = 2.0 * M(ix, iyi, izi) *
+                                      ((Vx(ix + 1, iyi, izi) - Vx(ix, iyi, izi)) / dx - 1.0 / 3.0 * d + beta_n * d);
+                }
+                if (ix <= tyy.n1 && iy <= tyy.n2 && iz <= tyy.n3) {
+                    const double d = dv(ixi, iy, izi);
+                    tyy(ix, iy, iz) = 2.0 * M(ixi, iy, izi) *
+                                      ((Vy(ixi, iy + 1, izi) - Vy(ixi, iy, izi)) / dy - 1.0 / 3.0 * d + beta_n * d);
+                }
+                if (ix <= tzz.n1 && iy <= tzz.n2 && iz <= tzz.n3) {
+                    const double d = dv(ixi, iyi, iz);
+                    tzz(ix, iy, iz) = 2.0 * M(ixi, iyi, iz) *
+                                      ((Vz(ixi, iyi, iz + 1) - Vz(ixi, iyi, iz)) / dz - 1.0 / 3.0 * d + beta_n * d);
+                }
+                if (ix <= txy.n1 && iy <= txy.n2 && iz <= txy.n3) {
+                    const double am = (M(ix, iy, izi) + M(ix + 1, iy, izi) + M(ix, iy + 1, izi) + M(ix + 1, iy + 1, izi)) * 0.25;
+                    txy(ix, iy, iz) = 2.0 * am * (0.5 * ((Vx(ixi, iy + 1, izi) - Vx(ixi, iy, izi)) / dy +
+                                                         (Vy(ix + 1, iyi, izi) - Vy(ix, iyi, izi)) / dx));
+                }
+                if (ix <= txz.n1 && iy <= txz.n2 && iz <= txz.n3) {
+                    const double am = (M(ix, iyi, iz) + M(ix + 1, iyi, iz) + M(ix, iyi, iz + 1) + M(ix + 1, iyi, iz + 1)) * 0.25;
+                    txz(ix, iy, iz) = 2.0 * am * (0.5 * ((Vx(ixi, iyi, iz + 1) - Vx(ixi, iyi, iz)) / dz +
+                                                         (Vz(ix + 1, iyi, izi) - Vz(ix, iyi, izi)) / dx));
+                }
+                if (ix <= tyz.n1 && iy <= tyz.n2 && iz <= tyz.n3) {
+                    const double am = (M(ixi, iy, iz) + M(ixi, iy + 1, iz) + M(ixi, iy, iz + 1) + M(ixi, iy + 1, iz + 1)) * 0.25;
+                    tyz(ix, iy, iz) = 2.0 * am * (0.5 * ((Vy(ixi, iyi, iz + 1) - Vy(ixi, iyi, iz)) / dz +
+                                                         (Vz(ixi, iy + 1, izi) - Vz(ixi, iy, izi)) / dy));
+                }
+            }
+}
+
+// compute_dV! (Stokes3D0_multixpu.jl:61-69): R as compute_dV! of Stokes3D_ve_multixpu.jl,
+// dV/dτ = damp*dV/dτ + R
+void ora3d_compute_dV(oarr Rx_, oarr Ry_, oarr Rz_, oarr dVx_, oarr dVy_, oarr dVz_, oarr Pt_, oarr txx_, oarr tyy_,
+                      oarr tzz_, oarr txy_, oarr txz_, oarr tyz_, double dampX, double dampY, double dampZ, double dx,
+                      double dy, double dz) {
+    ora3m_compute_dV(Rx_, Ry_, Rz_, Pt_, txx_, tyy_, tzz_, txy_, txz_, tyz_, oarr{nullptr, 0, 0, 0}, dx, dy, dz, 1);
+    F3 Rx(Rx_), Ry(Ry_), Rz(Rz_), dVx(dVx_), dVy(dVy_), dVz(dVz_);
+    const int64_t n = Rx.n1 * Rx.n2 * Rx.n3, m = Ry.n1 * Ry.n2 * Ry.n3, l = Rz.n1 * Rz.n2 * Rz.n3;
+#pragma omp parallel for schedule(static)
+    for (int64_t q = 0; q < n; ++q) dVx.p[q] = dampX * dVx.p[q] + Rx.p[q];
+#pragma omp parallel for schedule(static)
+    for (int64_t q = 0; q < m; ++q) dVy.p[q] = dampY * dVy.p[q] + Ry.p[q];
+#pragma omp parallel for schedule(static)
+    for (int64_t q = 0; q < l; ++q) dVz.p[q] = dampZ * dVz.p[q] + Rz.p[q];
+}
+
+// compute_V! (Stokes3D0_multixpu.jl:71-76): @inn(V) = @inn(V) + dτV*dV/dτ
+void ora3d_compute_V(oarr Vx_, oarr Vy_, oarr Vz_, oarr dVx_, oarr dVy_, oarr dVz_, oarr dtVx_, oarr dtVy_,
+                     oarr dtVz_) {
+    F3 Vx(Vx_), Vy(Vy_), Vz(Vz_), dVx(dVx_), dVy(dVy_), dVz(dVz_), tx(dtVx_), ty(dtVy_), tz(dtVz_);
+#pragma omp parallel for schedule(static)
+    for (int64_t iz = 1; iz <= std::max(dVx.n3, dVz.n3); ++iz)
+        for (int64_t iy = 1; iy <= std::max(dVx.n2, dVy.n2); ++iy)
+            for (int64_t ix = 1; ix <= std::max(dVx.n1, dVy.n1); ++ix) {
+                if (ix <= dVx.n1 && iy <= dVx.n2 && iz <= dVx.n3)
+                    Vx(ix + 1, iy + 1, iz + 1) = Vx(ix + 1, iy + 1, iz + 1) + tx(ix, iy, iz) * dVx(ix, iy, iz);
+                if (ix <= dVy.n1 && iy <= dVy.n2 && iz <= dVy.n3)
+                    Vy(ix + 1, iy + 1, iz + 1) = Vy(ix + 1, iy + 1, iz + 1) + ty(ix, iy, iz) * dVy(ix, iy, iz);
+                if (ix <= dVz.n1 && iy <= dVz.n2 && iz <= dVz.n3)
+                    Vz(ix + 1, iy + 1, iz + 1) = Vz(ix + 1, iy + 1, iz + 1) + tz(ix, iy, iz) * dVz(ix, iy, iz);
+            }
+}
+
 // ---------------------------------------------------------------- 3D VE explicit-index (Stokes3D_ve_perf.jl)
 
 static inline double tau_normal_mul(double t, double to, double g, double m, double gdt, double _h, double d,

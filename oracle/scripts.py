@@ -9,6 +9,7 @@ Each ``Case`` subclass mirrors one script of PTsolvers/PseudoTransientStokes.jl:
   ``VE3DPerf``   scripts/stokes_3D/Stokes3D_ve_perf.jl:116-255     (3D VE, fused kernels)
   ``VE2DDamp``   scripts/previous_damp/Stokes2D_ve0.jl:82-204 (2D VE, damped scheme)
   ``V2DDamp``    scripts/previous_damp/Stokes2D0.jl:72-173    (2D viscous, damped scheme)
+  ``V3DDamp``    scripts/stokes_3D/previous_damp/Stokes3D0_multixpu.jl:96-248 (3D viscous, damped, 1 rank)
   ``V3D``        3D viscous: no reference script; the 3D perf kernels with the elastic
                  terms removed and the viscous iteration parameters of Stokes2D.jl:27-31.
 
@@ -479,6 +480,42 @@ class VE3D(_Case3D):
         return self.norm_err(("Rx", "Ry", "Rz"), "divV")
 
 
+class V3DDamp(_Case3D):
+    """scripts/stokes_3D/previous_damp/Stokes3D0_multixpu.jl on one rank (3D viscous, the damped
+    "accel. 1" scheme): β_n in τ, a damped rate dV/dτ = damp*dV/dτ + R, per-face pseudo-time
+    steps (:37-43); ICs through ImplicitGlobalGrid's x_g as Stokes3D_ve_multixpu.jl
+    (:144-166); one solve, iterMax 6e4, nout 500, Vdmp 4, β_n 3, Vsc 1, Ptsc 5 (:102-109);
+    the check of Stokes3D_ve_multixpu.jl on one rank (:206-216)."""
+
+    elastic = False
+    unfused = True
+    igg_coords = True
+    defaults = dict(nt=1, iterMax=6e4, nout=500, eps=1e-8, Vdmp=4.0, beta_n=3.0, Vsc=1.0, Ptsc=5.0, CFL=0.0,
+                    Re=0.0, r=0.0)
+
+    def iter_params(self):
+        nx, ny, nz = self.nx, self.ny, self.nz
+        self.dampX, self.dampY, self.dampZ = 1.0 - self.Vdmp / nx, 1.0 - self.Vdmp / ny, 1.0 - self.Vdmp / nz
+        self.alloc(dtVx=self.f["Rx"].shape, dtVy=self.f["Ry"].shape, dtVz=self.f["Rz"].shape, dtPt=(nx, ny, nz))
+        self.L.ora3d_timesteps(self.A("dtVx"), self.A("dtVy"), self.A("dtVz"), self.A("dtPt"), self.A("Must"),
+                               self.Vsc, self.Ptsc, min(self.dx, self.dy, self.dz) ** 2, self.beta_n,
+                               float(max(nx, ny, nz)))
+
+    def iteration(self):
+        L, A = self.L, self.A
+        L.ora3d_compute_P(A("divV"), A("Pt"), A("Vx"), A("Vy"), A("Vz"), A("dtPt"), self.dx, self.dy, self.dz)
+        L.ora3d_compute_tau(A("divV"), *self._tau(), A("Vx"), A("Vy"), A("Vz"), A("Mus"), self.beta_n, self.dx,
+                            self.dy, self.dz)
+        L.ora3d_compute_dV(A("Rx"), A("Ry"), A("Rz"), A("dVx"), A("dVy"), A("dVz"), A("Pt"), *self._tau(),
+                           self.dampX, self.dampY, self.dampZ, self.dx, self.dy, self.dz)
+        L.ora3d_compute_V(A("Vx"), A("Vy"), A("Vz"), A("dVx"), A("dVy"), A("dVz"), A("dtVx"), A("dtVy"), A("dtVz"))
+        self.bc()
+
+    def check(self):
+        # Rx, Ry, Rz from compute_dV! of this iteration (Stokes3D0_multixpu.jl:206-213)
+        return self.norm_err(("Rx", "Ry", "Rz"), "divV")
+
+
 class VE3DPerf(_Case3D):
     """scripts/stokes_3D/Stokes3D_ve_perf.jl (fused explicit-index kernels, _dx form).
 
@@ -575,6 +612,7 @@ VARIANTS = {
     "3d_v": V3D,
     "2d_v_damp": V2DDamp,
     "2d_ve_damp": VE2DDamp,
+    "3d_v_damp": V3DDamp,
 }
 
 

@@ -140,9 +140,21 @@ bool field_info(pts_ctx* c, int id, FInfo* o) {
             set(&f.grad, nx, ny, nz, 0, 0, 0);
             break;
         // pseudo-time steps of the damped variants (Stokes2D_ve0.jl:123-124,106)
-        case PTS_F_DTAU_VX: if (!variant_damped(c->v)) return false; set(&f.dtVx, nx - 1, ny - 2, 1, 1, 1, 0); break;
-        case PTS_F_DTAU_VY: if (!variant_damped(c->v)) return false; set(&f.dtVy, nx - 2, ny - 1, 1, 1, 1, 0); break;
-        case PTS_F_DTAU_PT: if (!variant_damped(c->v)) return false; set(&f.dtPt, nx, ny, 1, 0, 0, 0); break;
+        // pseudo-time steps of the damped variants: the extents of Rx, Ry, Rz and of the cells
+        // (Stokes2D_ve0.jl:106,123-124; Stokes3D0_multixpu.jl:123,138-140)
+        case PTS_F_DTAU_VX:
+            if (!variant_damped(c->v)) return false;
+            set(&f.dtVx, nx - 1, ny - 2, d3 ? nz - 2 : 1, 1, 1, d3 ? 1 : 0);
+            break;
+        case PTS_F_DTAU_VY:
+            if (!variant_damped(c->v)) return false;
+            set(&f.dtVy, nx - 2, ny - 1, d3 ? nz - 2 : 1, 1, 1, d3 ? 1 : 0);
+            break;
+        case PTS_F_DTAU_VZ:
+            if (!variant_damped(c->v) || !d3) return false;
+            set(&f.dtVz, nx - 2, ny - 2, nz - 1, 1, 1, 1);
+            break;
+        case PTS_F_DTAU_PT: if (!variant_damped(c->v)) return false; set(&f.dtPt, nx, ny, nz, 0, 0, 0); break;
         default: return false;
     }
     return true;
@@ -196,8 +208,9 @@ void swap_buffers(pts_ctx* c) {
     c->parity ^= 1;
 }
 
-// Numerics of the damped scheme and what derives from them (Stokes2D_ve0.jl:95-105):
-// dampX = 1.0-Vdmp/nx, dampY = 1.0-Vdmp/ny, min_dxy2 = min(dx,dy)^2, max_nxy = max(nx,ny).
+// Numerics of the damped scheme and what derives from them (Stokes2D_ve0.jl:95-105,
+// Stokes3D0_multixpu.jl:105-120): dampX = 1.0-Vdmp/nx (Y, Z alike), min_dxy2 =
+// min(dx,dy[,dz])^2, max_nxy = max(nx,ny[,nz]).
 void set_damping(pts_ctx* c, double Vdmp, double beta_n, double Vsc, double Ptsc) {
     Num& n = c->n;
     n.Vdmp = Vdmp;
@@ -206,9 +219,10 @@ void set_damping(pts_ctx* c, double Vdmp, double beta_n, double Vsc, double Ptsc
     n.Ptsc = Ptsc;
     n.dampX = 1.0 - Vdmp / (double)c->g.nx;
     n.dampY = 1.0 - Vdmp / (double)c->g.ny;
-    const double m = std::min(n.dx, n.dy);
+    n.dampZ = 1.0 - Vdmp / (double)c->g.nz;
+    const double m = c->d3 ? std::min(std::min(n.dx, n.dy), n.dz) : std::min(n.dx, n.dy);
     n.min_dxy2 = m * m;
-    n.max_nxy = (double)std::max(c->g.nx, c->g.ny);
+    n.max_nxy = (double)(c->d3 ? std::max(std::max(c->g.nx, c->g.ny), c->g.nz) : std::max(c->g.nx, c->g.ny));
 }
 
 int enter(pts_ctx* c) {
@@ -381,7 +395,7 @@ int pts_create(const pts_desc* d, pts_ctx** out) {
     pts_ctx* c = nullptr;
     if (!d || !out) return fail(nullptr, PTS_E_INVAL, "null argument");
     *out = nullptr;
-    if (d->variant < PTS_2D_V || d->variant > PTS_2D_VE_DAMP) return fail(nullptr, PTS_E_INVAL, "unknown variant");
+    if (d->variant < PTS_2D_V || d->variant > PTS_3D_V_DAMP) return fail(nullptr, PTS_E_INVAL, "unknown variant");
     if (d->precision != PTS_FP64 && d->precision != PTS_MIXED) return fail(nullptr, PTS_E_INVAL, "unknown precision");
     if (d->precision == PTS_MIXED && d->variant != PTS_3D_VE_PERF && d->variant != PTS_3D_V)
         return fail(nullptr, PTS_E_INVAL, "mixed precision is implemented for PTS_3D_VE_PERF and PTS_3D_V");
@@ -430,7 +444,8 @@ int pts_create(const pts_desc* d, pts_ctx** out) {
     n.Vpdt = (d3 ? std::min(std::min(n.dx, n.dy), n.dz) : std::min(n.dx, n.dy)) * d->CFL;
     n.max_l = d->max_l > 0 ? d->max_l : (d3 ? std::max(std::max(d->lx, d->ly), d->lz) : std::max(d->lx, d->ly));
     n.adjoint = d->adjoint ? 1 : 0;
-    set_damping(c, 4.0, 2.0, 1.0, 3.0);  // Stokes2D_ve0.jl:95-98
+    if (d3) set_damping(c, 4.0, 3.0, 1.0, 5.0);  // Stokes3D0_multixpu.jl:105-108
+    else set_damping(c, 4.0, 2.0, 1.0, 3.0);     // Stokes2D_ve0.jl:95-98
     int rc = PTS_OK;
     auto bail = [&](int code) {
         g_create_err = c->err;
@@ -472,6 +487,11 @@ int pts_create(const pts_desc* d, pts_ctx** out) {
         double** damp[] = {&f.dVx, &f.dVy, &f.dtVx, &f.dtVy, &f.dtPt};
         for (double** p : damp)
             if ((rc = alloc_field(c, p)) != PTS_OK) return bail(rc);
+        if (d3) {
+            double** damp3[] = {&f.dVz, &f.dtVz};
+            for (double** p : damp3)
+                if ((rc = alloc_field(c, p)) != PTS_OK) return bail(rc);
+        }
     }
     c->mixed = d->precision == PTS_MIXED;
     c->fused = variant_fused(c->v) && d->single_pass != 0 && !c->mixed;
@@ -625,7 +645,8 @@ int pts_compute_iter_params(pts_ctx* c) {
 int pts_set_damping(pts_ctx* c, double Vdmp, double beta_n, double Vsc, double Ptsc) {
     int rc = enter(c);
     if (rc) return rc;
-    if (!variant_damped(c->v)) return fail(c, PTS_E_INVAL, "pts_set_damping needs PTS_2D_V_DAMP or PTS_2D_VE_DAMP");
+    if (!variant_damped(c->v))
+        return fail(c, PTS_E_INVAL, "pts_set_damping needs PTS_2D_V_DAMP, PTS_2D_VE_DAMP or PTS_3D_V_DAMP");
     if (!(Vsc > 0) || !(Ptsc > 0) || !std::isfinite(Vdmp) || !std::isfinite(beta_n) || !(beta_n > -1.0))
         return fail(c, PTS_E_INVAL, "damping numerics: Vsc, Ptsc must be > 0, beta_n > -1, Vdmp finite");
     set_damping(c, Vdmp, beta_n, Vsc, Ptsc);

@@ -27,11 +27,12 @@ enum Variant {
     V3D = PTS_3D_V,
     V2D_DAMP = PTS_2D_V_DAMP,
     VE2D_DAMP = PTS_2D_VE_DAMP,
+    V3D_DAMP = PTS_3D_V_DAMP,
 };
 
-inline bool variant_is3d(int v) { return v == VE3D || v == VE3D_PERF || v == V3D; }
-inline bool variant_elastic(int v) { return v != V2D && v != V3D && v != V2D_DAMP; }
-inline bool variant_damped(int v) { return v == V2D_DAMP || v == VE2D_DAMP; }
+inline bool variant_is3d(int v) { return v == VE3D || v == VE3D_PERF || v == V3D || v == V3D_DAMP; }
+inline bool variant_elastic(int v) { return v != V2D && v != V3D && v != V2D_DAMP && v != V3D_DAMP; }
+inline bool variant_damped(int v) { return v == V2D_DAMP || v == VE2D_DAMP || v == V3D_DAMP; }
 // "perf" variants multiply by _dx = 1/dx (explicit-index kernels); the others divide by dx.
 inline bool variant_perf(int v) { return v == VE2D_PERF || v == VE3D_PERF || v == V3D; }
 // ∇V of the check: from compute_P! before the V update (role variants), or recomputed
@@ -62,9 +63,10 @@ struct Num {
     double Vpdt, max_l, Re;
     double lx, ly, lz;
     int adjoint;  // 3D_V: iterate the transposed (adjoint) system, ghosts folded (pts_abi.cu)
-    // damped variants (Stokes2D_ve0.jl:95-105): Vdmp, β_n, Vsc, Ptsc and the derived
-    // dampX = 1-Vdmp/nx, dampY = 1-Vdmp/ny, min_dxy2 = min(dx,dy)^2, max_nxy = max(nx,ny)
-    double Vdmp, beta_n, Vsc, Ptsc, dampX, dampY, min_dxy2, max_nxy;
+    // damped variants (Stokes2D_ve0.jl:95-105, Stokes3D0_multixpu.jl:105-120): Vdmp, β_n,
+    // Vsc, Ptsc and the derived dampX = 1-Vdmp/nx (Y, Z alike), min_dxy2 = min(dx,dy[,dz])^2,
+    // max_nxy = max(nx,ny[,nz])
+    double Vdmp, beta_n, Vsc, Ptsc, dampX, dampY, dampZ, min_dxy2, max_nxy;
 };
 
 template <typename T>
@@ -78,7 +80,7 @@ struct FieldsT {
     T *rhog, *rhog2;  // buoyancy ρg of the batched sweep (Stokes2D_param.jl), else null
     T *Fx, *Fy, *Fz;  // momentum sources on interior faces (adjoint solves), else null
     T *grad;          // ∂J/∂log μ per cell, else null
-    T *dtVx, *dtVy, *dtPt;  // pseudo-time steps dτVx, dτVy, dτPt of the damped variants, else null
+    T *dtVx, *dtVy, *dtVz, *dtPt;  // pseudo-time steps of the damped variants, else null
 };
 using Fields64 = FieldsT<double>;
 
@@ -121,7 +123,7 @@ cudaError_t launch_grad_logmu_ve(const Geom& g, const Fields64& fwd, const Field
 cudaError_t launch_fused3(int variant, const Geom& g, const Fields64& cur, const Fields64& nxt, const Num& n,
                           bool store_divV, int* err, cudaStream_t s,
                           bool direct);
-inline bool variant_fused(int v) { return variant_is3d(v); }
+inline bool variant_fused(int v) { return variant_is3d(v) && !variant_damped(v); }
 
 // Message returned by pts_last_error(NULL) (for entry points without a context).
 void set_global_error(const char* msg);

@@ -286,6 +286,155 @@ __global__ void k3_add_dV(Geom g, Fields64 f) {
     if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 1) f.Vz[c] = f.Vz[c] + f.dVz[c];
 }
 
+// ------------------------------------------------------------------ 3D damped scheme (viscous)
+//
+// scripts/stokes_3D/previous_damp/Stokes3D0_multixpu.jl on one rank. Unified positions as
+// in 2D: dτPt on the cells; dτVx and dVxdτ (held in dVx) on the x-faces of Rx, and so on.
+
+// compute_timesteps! (Stokes3D0_multixpu.jl:37-43), one thread per face/cell point
+__global__ void __launch_bounds__(256) k3d_timesteps(Geom g, Fields64 f, Num n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    if (i > nx || j > ny) return;
+    const idx_t c = gidx32(g, i, j, k);
+    const idx_t sx = 1, sy = g.px, sz = (idx_t)g.pxy;
+    const double t = 1.0 / 6.1 / (1.0 + n.beta_n) / n.Vsc * n.min_dxy2;
+    if (i < nx && j < ny && k < nz) f.dtPt[c] = 6.1 * (1.0 + n.beta_n) / n.Ptsc / n.max_nxy * f.Must[c];
+    if (i >= 1 && i <= nx - 1 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2)  // @av_xi(Musτ)
+        f.dtVx[c] = t / ((f.Must[c - sx] + f.Must[c]) * 0.5);
+    if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 1 && k >= 1 && k <= nz - 2)  // @av_yi(Musτ)
+        f.dtVy[c] = t / ((f.Must[c - sy] + f.Must[c]) * 0.5);
+    if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 1)  // @av_zi(Musτ)
+        f.dtVz[c] = t / ((f.Must[c - sz] + f.Must[c]) * 0.5);
+}
+
+// compute_P! (Stokes3D0_multixpu.jl:45-49) and compute_τ! (:51-59):
+//   τxx = 2@inn_yz(Mus)*(@d_xi(Vx)/dx - 1/3*∇V + β_n*∇V),  τxy = 2@av_xyi(Mus)*(0.5*(@d_yi(Vx)/dy + @d_xi(Vy)/dx))
+// With ROLE_TAU alone ∇V is read back from the field compute_P! stored.
+__global__ void __launch_bounds__(256) k3d_Pt_tau(Geom g, Fields64 f, Num n, int roles, int store_divV) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z * blockDim.z + threadIdx.z;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    if (i >= nx || j >= ny || k >= nz) return;
+    const idx_t c = gidx32(g, i, j, k);
+    const idx_t sx = 1, sy = g.px, sz = (idx_t)g.pxy;
+    const double dvx = f.Vx[c + sx] - f.Vx[c];
+    const double dvy = f.Vy[c + sy] - f.Vy[c];
+    const double dvz = f.Vz[c + sz] - f.Vz[c];
+    double dv;
+    if (roles & ROLE_P) {
+        dv = (dvx / n.dx + dvy / n.dy) + dvz / n.dz;
+        if (store_divV) f.divV[c] = dv;
+        f.Pt[c] = f.Pt[c] - f.dtPt[c] * dv;
+    } else {
+        dv = f.divV[c];
+    }
+    if (!(roles & ROLE_TAU)) return;
+    const double Mc = f.Mus[c];
+    if (j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2)
+        f.txx[c] = 2.0 * Mc * (dvx / n.dx - 1.0 / 3.0 * dv + n.beta_n * dv);
+    if (i >= 1 && i <= nx - 2 && k >= 1 && k <= nz - 2)
+        f.tyy[c] = 2.0 * Mc * (dvy / n.dy - 1.0 / 3.0 * dv + n.beta_n * dv);
+    if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2)
+        f.tzz[c] = 2.0 * Mc * (dvz / n.dz - 1.0 / 3.0 * dv + n.beta_n * dv);
+    if (i >= 1 && j >= 1 && k >= 1 && k <= nz - 2) {  // τxy edge
+        const double am = (((f.Mus[c - sx - sy] + f.Mus[c - sy]) + f.Mus[c - sx]) + Mc) * 0.25;
+        f.txy[c] = 2.0 * am * (0.5 * ((f.Vx[c] - f.Vx[c - sy]) / n.dy + (f.Vy[c] - f.Vy[c - sx]) / n.dx));
+    }
+    if (i >= 1 && j >= 1 && j <= ny - 2 && k >= 1) {  // τxz edge
+        const double am = (((f.Mus[c - sx - sz] + f.Mus[c - sz]) + f.Mus[c - sx]) + Mc) * 0.25;
+        f.txz[c] = 2.0 * am * (0.5 * ((f.Vx[c] - f.Vx[c - sz]) / n.dz + (f.Vz[c] - f.Vz[c - sx]) / n.dx));
+    }
+    if (i >= 1 && i <= nx - 2 && j >= 1 && k >= 1) {  // τyz edge
+        const double am = (((f.Mus[c - sy - sz] + f.Mus[c - sz]) + f.Mus[c - sy]) + Mc) * 0.25;
+        f.tyz[c] = 2.0 * am * (0.5 * ((f.Vy[c] - f.Vy[c - sz]) / n.dz + (f.Vz[c] - f.Vz[c - sy]) / n.dy));
+    }
+}
+
+// compute_dV! + compute_V! + the six bc copies (Stokes3D0_multixpu.jl:61-76,186-193):
+//   dVxdτ = dampX*dVxdτ + Rx,  @inn(Vx) = @inn(Vx) + dτVx*dVxdτ.  update = 0: copies only.
+__global__ void __launch_bounds__(256) k3d_V_bc(Geom g, Fields64 f, Num n, int update) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    if (i > nx || j > ny) return;
+    const idx_t c = gidx32(g, i, j, k);
+    const idx_t sx = 1, sy = g.px, sz = (idx_t)g.pxy;
+    if (j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2) {
+        double v = f.Vx[c];
+        if (update && i >= 1 && i <= nx - 1) {
+            const double r = n.dampX * f.dVx[c] + res3_x<false>(f, n, c, sx, sy, sz);
+            f.dVx[c] = r;
+            v = v + f.dtVx[c] * r;
+            f.Vx[c] = v;
+        }
+        bc_copies(f.Vx, c, v, j, 1, ny - 2, sy, k, 1, nz - 2, sz);
+    }
+    if (i >= 1 && i <= nx - 2 && k >= 1 && k <= nz - 2) {
+        double v = f.Vy[c];
+        if (update && j >= 1 && j <= ny - 1) {
+            const double r = n.dampY * f.dVy[c] + res3_y<false>(f, n, c, sx, sy, sz);
+            f.dVy[c] = r;
+            v = v + f.dtVy[c] * r;
+            f.Vy[c] = v;
+        }
+        bc_copies(f.Vy, c, v, i, 1, nx - 2, sx, k, 1, nz - 2, sz);
+    }
+    if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2) {
+        double v = f.Vz[c];
+        if (update && k >= 1 && k <= nz - 1) {
+            const double r = n.dampZ * f.dVz[c] + res3_z<false>(f, n, c, sx, sy, sz);
+            f.dVz[c] = r;
+            v = v + f.dtVz[c] * r;
+            f.Vz[c] = v;
+        }
+        bc_copies(f.Vz, c, v, i, 1, nx - 2, sx, j, 1, ny - 2, sy);
+    }
+}
+
+// compute_dV! alone (Stokes3D0_multixpu.jl:61-69): R and the damped rates.
+__global__ void k3d_dV(Geom g, Fields64 f, Num n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    if (i > nx || j > ny) return;
+    const idx_t c = gidx32(g, i, j, k);
+    const idx_t sx = 1, sy = g.px, sz = (idx_t)g.pxy;
+    if (i >= 1 && i <= nx - 1 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2) {
+        const double R = res3_x<false>(f, n, c, sx, sy, sz);
+        f.Rx[c] = R;
+        f.dVx[c] = n.dampX * f.dVx[c] + R;
+    }
+    if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 1 && k >= 1 && k <= nz - 2) {
+        const double R = res3_y<false>(f, n, c, sx, sy, sz);
+        f.Ry[c] = R;
+        f.dVy[c] = n.dampY * f.dVy[c] + R;
+    }
+    if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 1) {
+        const double R = res3_z<false>(f, n, c, sx, sy, sz);
+        f.Rz[c] = R;
+        f.dVz[c] = n.dampZ * f.dVz[c] + R;
+    }
+}
+
+// compute_V! alone (Stokes3D0_multixpu.jl:71-76): @inn(V) = @inn(V) + dτV*dVdτ
+__global__ void k3d_add_dV(Geom g, Fields64 f) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    if (i > nx || j > ny) return;
+    const idx_t c = gidx32(g, i, j, k);
+    if (i >= 1 && i <= nx - 1 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2) f.Vx[c] = f.Vx[c] + f.dtVx[c] * f.dVx[c];
+    if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 1 && k >= 1 && k <= nz - 2) f.Vy[c] = f.Vy[c] + f.dtVy[c] * f.dVy[c];
+    if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 1) f.Vz[c] = f.Vz[c] + f.dtVz[c] * f.dVz[c];
+}
+
 // ------------------------------------------------------------------ 2D kernels
 
 // compute_P! + compute_τ! for the three 2D scripts:
@@ -1501,6 +1650,7 @@ cudaError_t launch_Pt_tau(int v, const Geom& g, const Fields64& f, const Num& n,
         case VE3D: k3_Pt_tau<true, false><<<grid_pt(g), blk_pt(), 0, s>>>(g, f, n, roles, sd); break;
         case VE3D_PERF: k3_Pt_tau<true, true><<<grid_pt(g), blk_pt(), 0, s>>>(g, f, n, roles, sd); break;
         case V3D: k3_Pt_tau<false, true><<<grid_pt(g), blk_pt(), 0, s>>>(g, f, n, roles, sd); break;
+        case V3D_DAMP: k3d_Pt_tau<<<grid_pt(g), blk_pt(), 0, s>>>(g, f, n, roles, sd); break;
         case V2D: k2_Pt_tau<V2D><<<grid_cells(g), blk(), 0, s>>>(g, f, n, roles, sd); break;
         case VE2D: k2_Pt_tau<VE2D><<<grid_cells(g), blk(), 0, s>>>(g, f, n, roles, sd); break;
         case VE2D_PERF: k2_Pt_tau<VE2D_PERF><<<grid_cells(g), blk(), 0, s>>>(g, f, n, roles, sd); break;
@@ -1515,6 +1665,7 @@ cudaError_t launch_V_bc(int v, const Geom& g, const Fields64& f, const Num& n, b
     const int u = update ? 1 : 0;
     switch (v) {
         case VE3D: k3_V_bc<false><<<grid_faces(g, true), blk(), 0, s>>>(g, f, n, u); break;
+        case V3D_DAMP: k3d_V_bc<<<grid_faces(g, true), blk(), 0, s>>>(g, f, n, u); break;
         case VE3D_PERF:
         case V3D:
             if (n.adjoint) {
@@ -1539,6 +1690,7 @@ cudaError_t launch_V_bc(int v, const Geom& g, const Fields64& f, const Num& n, b
 cudaError_t launch_dV(int v, const Geom& g, const Fields64& f, const Num& n, cudaStream_t s) {
     switch (v) {
         case VE3D: k3_dV<false><<<grid_faces(g, true), blk(), 0, s>>>(g, f, n); break;
+        case V3D_DAMP: k3d_dV<<<grid_faces(g, true), blk(), 0, s>>>(g, f, n); break;
         case VE3D_PERF:
         case V3D:
             if (f.Fx) k3_dV<true, true><<<grid_faces(g, true), blk(), 0, s>>>(g, f, n);
@@ -1555,7 +1707,8 @@ cudaError_t launch_dV(int v, const Geom& g, const Fields64& f, const Num& n, cud
 }
 
 cudaError_t launch_add_dV(int v, const Geom& g, const Fields64& f, cudaStream_t s) {
-    if (variant_is3d(v)) k3_add_dV<<<grid_faces(g, true), blk(), 0, s>>>(g, f);
+    if (v == V3D_DAMP) k3d_add_dV<<<grid_faces(g, true), blk(), 0, s>>>(g, f);
+    else if (variant_is3d(v)) k3_add_dV<<<grid_faces(g, true), blk(), 0, s>>>(g, f);
     else if (variant_damped(v)) k2d_add_dV<<<grid_faces(g, false), blk(), 0, s>>>(g, f);
     else k2_add_dV<<<grid_faces(g, false), blk(), 0, s>>>(g, f);
     return cudaGetLastError();
@@ -1577,7 +1730,8 @@ cudaError_t launch_check(int v, const Geom& g, const Fields64& f, const Num& n, 
     const int nb = (int)(gr.x * gr.y * gr.z);
     if (nb > nblocks_cap) return cudaErrorInvalidValue;
     switch (v) {
-        case VE3D: k3_check<false><<<gr, blk(), 0, s>>>(g, f, n, partials); break;
+        case VE3D:
+        case V3D_DAMP: k3_check<false><<<gr, blk(), 0, s>>>(g, f, n, partials); break;
         case VE3D_PERF:
         case V3D:
             if (n.adjoint) {
@@ -1674,7 +1828,8 @@ cudaError_t launch_init_inclusion(int v, const Geom& g, const Fields64& f, const
                                   double radius2, double ebg, cudaStream_t s) {
     const bool d3 = variant_is3d(v);
     const dim3 gr = grid_faces(g, d3);
-    if (v == VE3D) k_init_inclusion<true, true><<<gr, blk(), 0, s>>>(g, f, n, mus0, musi, radius2, ebg);
+    // the multi-XPU scripts build their ICs through ImplicitGlobalGrid's x_g
+    if (v == VE3D || v == V3D_DAMP) k_init_inclusion<true, true><<<gr, blk(), 0, s>>>(g, f, n, mus0, musi, radius2, ebg);
     else if (d3) k_init_inclusion<true, false><<<gr, blk(), 0, s>>>(g, f, n, mus0, musi, radius2, ebg);
     else k_init_inclusion<false, false><<<gr, blk(), 0, s>>>(g, f, n, mus0, musi, radius2, ebg);
     return cudaGetLastError();
@@ -1693,7 +1848,8 @@ cudaError_t launch_maxloc(int v, const Geom& g, double* must, const double* mus,
 }
 
 cudaError_t launch_iter_params(int v, const Geom& g, const Fields64& f, const Num& n, cudaStream_t s) {
-    if (variant_damped(v)) k2d_timesteps<<<grid_faces(g, false), blk(), 0, s>>>(g, f, n);
+    if (v == V3D_DAMP) k3d_timesteps<<<grid_faces(g, true), blk(), 0, s>>>(g, f, n);
+    else if (variant_damped(v)) k2d_timesteps<<<grid_faces(g, false), blk(), 0, s>>>(g, f, n);
     else if (variant_elastic(v)) k_iter_params<true><<<grid_cells(g), blk(), 0, s>>>(g, f, n);
     else k_iter_params<false><<<grid_cells(g), blk(), 0, s>>>(g, f, n);
     return cudaGetLastError();

@@ -13,11 +13,11 @@ module PTStokesB200
 const libpts = get(ENV, "PTSTOKES_LIB", joinpath(@__DIR__, "..", "lib", "libptstokes.so"))
 
 const PTS_OK = Cint(0)
-@enum Variant::Int32 V2D = 0 VE2D = 1 VE2D_PERF = 2 VE3D = 3 VE3D_PERF = 4 V3D = 5 V2D_DAMP = 6 VE2D_DAMP = 7
+@enum Variant::Int32 V2D = 0 VE2D = 1 VE2D_PERF = 2 VE3D = 3 VE3D_PERF = 4 V3D = 5 V2D_DAMP = 6 VE2D_DAMP = 7 V3D_DAMP = 8
 const FIELDS = (:Pt, :Vx, :Vy, :Vz, :τxx, :τyy, :τzz, :τxy, :τxz, :τyz,
                 :τxx_o, :τyy_o, :τzz_o, :τxy_o, :τxz_o, :τyz_o,
                 :Mus, :Musτ, :Gdτ, :dτ_Rho, :∇V, :Rx, :Ry, :Rz, :dVx, :dVy, :dVz,
-                :ρg, :Fx, :Fy, :Fz, :grad, :dτVx, :dτVy, :dτPt)
+                :ρg, :Fx, :Fy, :Fz, :grad, :dτVx, :dτVy, :dτVz, :dτPt)
 field_id(s::Symbol) = Int32(findfirst(==(s), FIELDS) - 1)
 
 # pts_desc (include/ptstokes.h)
@@ -93,7 +93,8 @@ for (jl, c) in ((:init_inclusion!, :pts_init_inclusion),)
     @eval $jl(ctx::Ctx; μs0=1.0, μsi=1e-3, radius2=1.0, εbg=1.0) =
         check(ctx, ccall(($(QuoteNode(c)), libpts), Cint, (Ptr{Cvoid}, Float64, Float64, Float64, Float64), ctx.ptr, μs0, μsi, radius2, εbg))
 end
-# numerics of the damped variants (previous_damp/Stokes2D_ve0.jl:95-98), before compute_iter_params!
+# numerics of the damped variants (previous_damp/Stokes2D_ve0.jl:95-98; the 3D script's are
+# Vdmp=4, β_n=3, Vsc=1, Ptsc=5, Stokes3D0_multixpu.jl:105-108), before compute_iter_params!
 set_damping!(ctx::Ctx; Vdmp=4.0, β_n=2.0, Vsc=1.0, Ptsc=3.0) =
     check(ctx, ccall((:pts_set_damping, libpts), Cint, (Ptr{Cvoid}, Float64, Float64, Float64, Float64),
                      ctx.ptr, Vdmp, β_n, Vsc, Ptsc))

@@ -25,6 +25,7 @@ VARIANTS = {
     "3d_v": 5,        # 3D viscous (no reference script)
     "2d_v_damp": 6,   # scripts/previous_damp/Stokes2D0.jl
     "2d_ve_damp": 7,  # scripts/previous_damp/Stokes2D_ve0.jl
+    "3d_v_damp": 8,   # scripts/stokes_3D/previous_damp/Stokes3D0_multixpu.jl (one rank)
 }
 PRECISIONS = {"fp64": 0, "mixed": 1}
 
@@ -37,7 +38,7 @@ FIELDS = [
     "rhog",
     "Fx", "Fy", "Fz",
     "grad",
-    "dtVx", "dtVy", "dtPt",
+    "dtVx", "dtVy", "dtVz", "dtPt",
 ]
 FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
 

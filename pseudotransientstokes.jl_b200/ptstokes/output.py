@@ -12,6 +12,7 @@ and, with DO_SAVE_VIZ, dumps a few fields to ``out_visu/<name>.mat``:
     Stokes3D_ve_perf.jl        1 nx ny nz ittot wtime A_eff wtime_it T_eff (:244-247) same as the multi-XPU script (:250)
     previous_damp/Stokes2D0.jl     nx ny iter (:168-169)                            --
     previous_damp/Stokes2D_ve0.jl  nx ny ittot nt (:195-196)                        same as Stokes2D_ve.jl (:199-200)
+    stokes_3D/previous_damp/Stokes3D0_multixpu.jl  nx ny nz iter (:241-243)         --
 
 Numbers are printed as Julia prints them (``println`` of an Int or a Float64: shortest
 round-trip digits, scientific below 1e-4 and from 1e6 upward), so the lines read like the
@@ -26,7 +27,7 @@ import numpy as np
 
 # A_eff arrays per PT iteration of each script (the scripts' own conventions)
 A_EFF_ARRAYS = {"2d_v": 6, "2d_ve": 13, "2d_ve_perf": 18, "3d_ve": 21, "3d_ve_perf": 29, "3d_v": 23,
-                "2d_v_damp": 6, "2d_ve_damp": 13}
+                "2d_v_damp": 6, "2d_ve_damp": 13, "3d_v_damp": 8}
 
 
 def jl(x):
@@ -64,7 +65,7 @@ def _append(path, values):
 
 LINE_FILES = {"2d_v": "out_Stokes2D.txt", "2d_ve": "out_Stokes2D_ve.txt", "2d_ve_perf": "out_Stokes2D_ve_perf.txt",
               "3d_ve": "out_Stokes3D_ve.txt", "3d_ve_perf": "out_Stokes3D_ve_perf.txt", "3d_v": "out_Stokes3D_v.txt",
-              "2d_v_damp": "out_Stokes2D0.txt", "2d_ve_damp": "out_Stokes2D_ve0.txt"}
+              "2d_v_damp": "out_Stokes2D0.txt", "2d_ve_damp": "out_Stokes2D_ve0.txt", "3d_v_damp": "out_Stokes3D0.txt"}
 MAT_FILES = {"2d_ve": "Stokes_2D_ve.mat", "2d_ve_perf": "Stokes_2D_ve_perf.mat", "3d_ve": "Stokes_3D_ve.mat",
              "3d_ve_perf": "Stokes_3D_ve_perf.mat", "3d_v": "Stokes_3D_v.mat", "2d_ve_damp": "Stokes_2D_ve0.mat"}
 
@@ -83,6 +84,8 @@ def result_line(variant, nx, ny, nz, ittot, nt, wtime):
         return [nx, ny, ittot, wtime, a_eff, t_it, t_eff]
     if variant == "3d_ve":
         return [nx, ny, nz, ittot, nt]
+    if variant == "3d_v_damp":
+        return [nx, ny, nz, ittot]
     return [1, nx, ny, nz, ittot, wtime, a_eff, t_it, t_eff]
 
 

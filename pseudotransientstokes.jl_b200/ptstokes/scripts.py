@@ -13,6 +13,7 @@ scripts' NX/NY/NZ environment variables (``haskey(ENV, "NX") ? parse(Int, ENV["N
     Stokes3D_v          3D viscous (no reference script)
     Stokes2D0           scripts/previous_damp/Stokes2D0.jl    (damped scheme)
     Stokes2D_ve0        scripts/previous_damp/Stokes2D_ve0.jl (damped scheme)
+    Stokes3D0           scripts/stokes_3D/previous_damp/Stokes3D0_multixpu.jl (one rank, damped scheme)
 """
 import os
 import time
@@ -94,6 +95,13 @@ def Stokes2D0(nx=None, ny=None, return_solver=False, verbose=False, **kw):
 def Stokes2D_ve0(nx=None, ny=None, return_solver=False, verbose=False, **kw):
     """scripts/previous_damp/Stokes2D_ve0.jl:82-204 (2D Maxwell VE, damped scheme, 5 steps)."""
     return _script("2d_ve_damp", nx or _env("NX", 511), ny or _env("NY", 511), None, return_solver, verbose, **kw)
+
+
+def Stokes3D0(nx=None, ny=None, nz=None, return_solver=False, verbose=False, **kw):
+    """scripts/stokes_3D/previous_damp/Stokes3D0_multixpu.jl:96-248 on one rank (3D viscous,
+    damped scheme; NX, NY, NZ default 63)."""
+    return _script("3d_v_damp", nx or _env("NX", 63), ny or _env("NY", 63), nz or _env("NZ", 63), return_solver,
+                   verbose, **kw)
 
 
 # Effective memory traffic per PT iteration, in bytes, by the reference's own

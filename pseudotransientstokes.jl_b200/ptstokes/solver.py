@@ -35,6 +35,9 @@ VARIANT_DEFAULTS = {
     # scripts/previous_damp/Stokes2D_ve0.jl:91-99
     "2d_ve_damp": dict(nt=5, iter_max=2e5, nout=200, eps=1e-8, CFL=0.0, Re=0.0, r=0.0, Vdmp=4.0, beta_n=2.0,
                        Vsc=1.0, Ptsc=3.0),
+    # scripts/stokes_3D/previous_damp/Stokes3D0_multixpu.jl:102-109 (one solve)
+    "3d_v_damp": dict(nt=1, iter_max=6e4, nout=500, eps=1e-8, CFL=0.0, Re=0.0, r=0.0, Vdmp=4.0, beta_n=3.0,
+                      Vsc=1.0, Ptsc=5.0),
 }
 DAMPING = ("Vdmp", "beta_n", "Vsc", "Ptsc")
 
@@ -49,7 +52,7 @@ class Solver:
     """A PT Stokes context (``pts_ctx``) with its device fields.
 
     ``variant`` is one of ``2d_v, 2d_ve, 2d_ve_perf, 3d_ve, 3d_ve_perf, 3d_v, 2d_v_damp,
-    2d_ve_damp``.
+    2d_ve_damp, 3d_v_damp``.
     Keyword arguments override the script defaults (``VARIANT_DEFAULTS``) and the
     physics (``lx, ly, lz, G, xi, mus0``: ``dt = mus0/(G*xi)`` as in the scripts).
     """
@@ -145,8 +148,13 @@ class Solver:
     def compute_iter_params(self):
         self._ck(self.lib.pts_compute_iter_params(self.ctx))
 
-    def set_damping(self, Vdmp=4.0, beta_n=2.0, Vsc=1.0, Ptsc=3.0):
-        """Numerics of the damped scheme (Stokes2D_ve0.jl:95-98); before compute_iter_params."""
+    def set_damping(self, Vdmp=4.0, beta_n=None, Vsc=1.0, Ptsc=None):
+        """Numerics of the damped scheme (Stokes2D_ve0.jl:95-98, Stokes3D0_multixpu.jl:105-108);
+        before compute_iter_params. β_n and Ptsc default to the script's (2, 3 in 2D; 3, 5 in 3D)."""
+        if beta_n is None:
+            beta_n = 3.0 if self.ndim == 3 else 2.0
+        if Ptsc is None:
+            Ptsc = 5.0 if self.ndim == 3 else 3.0
         self._ck(self.lib.pts_set_damping(self.ctx, Vdmp, beta_n, Vsc, Ptsc))
         self.p.update(Vdmp=Vdmp, beta_n=beta_n, Vsc=Vsc, Ptsc=Ptsc)
 

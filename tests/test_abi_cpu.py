@@ -116,9 +116,9 @@ def test_field_table_covers_the_adjoint_and_damping_fields():
     enum = enum[:enum.index("PTS_F_COUNT")]
     ids = re.findall(r"PTS_F_[A-Z_]+", enum)
     assert len(ids) == len(_abi.FIELDS)
-    assert ids[-7:] == ["PTS_F_FX", "PTS_F_FY", "PTS_F_FZ", "PTS_F_GRAD", "PTS_F_DTAU_VX", "PTS_F_DTAU_VY",
-                        "PTS_F_DTAU_PT"]
-    assert _abi.FIELDS[-7:] == ["Fx", "Fy", "Fz", "grad", "dtVx", "dtVy", "dtPt"]
+    assert ids[-8:] == ["PTS_F_FX", "PTS_F_FY", "PTS_F_FZ", "PTS_F_GRAD", "PTS_F_DTAU_VX", "PTS_F_DTAU_VY",
+                        "PTS_F_DTAU_VZ", "PTS_F_DTAU_PT"]
+    assert _abi.FIELDS[-8:] == ["Fx", "Fy", "Fz", "grad", "dtVx", "dtVy", "dtVz", "dtPt"]
 
 
 def test_variant_table_matches_the_header():
@@ -131,14 +131,19 @@ def test_variant_table_matches_the_header():
     vals = {m.group(1): int(m.group(2)) for m in re.finditer(r"(PTS_\w+)\s*=\s*(\d+)", enum)}
     assert vals["PTS_2D_V_DAMP"] == _abi.VARIANTS["2d_v_damp"] == 6
     assert vals["PTS_2D_VE_DAMP"] == _abi.VARIANTS["2d_ve_damp"] == 7
+    assert vals["PTS_3D_V_DAMP"] == _abi.VARIANTS["3d_v_damp"] == 8
     assert sorted(vals.values()) == sorted(_abi.VARIANTS.values())
     lib = ptstokes.load()
     d = _abi.PtsDesc()
     d.nx = d.ny = d.nz = 9
     d.nout, d.lx, d.ly, d.lz = 10, 10.0, 10.0, 10.0
     ctx = ctypes.c_void_p()
-    d.variant = 8
+    d.variant = 9
     assert lib.pts_create(ctypes.byref(d), ctypes.byref(ctx)) == _abi.PTS_E_INVAL
-    d.variant, d.precision = 7, 1
-    assert lib.pts_create(ctypes.byref(d), ctypes.byref(ctx)) == _abi.PTS_E_INVAL
+    for v in (7, 8):
+        d.variant, d.precision, d.adjoint = v, 1, 0
+        assert lib.pts_create(ctypes.byref(d), ctypes.byref(ctx)) == _abi.PTS_E_INVAL
+        d.precision, d.adjoint = 0, 1
+        assert lib.pts_create(ctypes.byref(d), ctypes.byref(ctx)) == _abi.PTS_E_INVAL
+    d.adjoint = 0
     assert lib.pts_set_damping(None, 4.0, 2.0, 1.0, 3.0) == _abi.PTS_E_INVAL

@@ -34,6 +34,18 @@ def test_damped_scheme_converges_to_the_same_solution(damped, plain):
     assert _rel(a.f["Pt"], b.f["Pt"], centre=True) < 1e-7
 
 
+def test_damped_3d_scheme_converges_to_the_3d_viscous_solution():
+    """Stokes3D0_multixpu.jl (one rank) against the 3D viscous restatement at 31^3: same
+    discrete equations (the explicit-index form differs only in rounding), same fixed point."""
+    from oracle import scripts as S
+    a = S.make("3d_v_damp", 31, 31, 31).run()
+    b = S.make("3d_v", 31, 31, 31).run()
+    assert a.iters == [1000] and b.iters == [800]
+    for k in ("Vx", "Vy", "Vz", "txx", "tyy", "tzz", "txy", "txz", "tyz"):
+        assert _rel(a.f[k], b.f[k]) < 1e-8, k
+    assert _rel(a.f["Pt"], b.f["Pt"], centre=True) < 1e-7
+
+
 def test_damped_ve_iteration_counts():
     """Regression values of the restated Stokes2D_ve0.jl (5 steps, nout 200, ε 1e-8)."""
     from oracle import scripts as S
