@@ -601,6 +601,74 @@ def run_inclusions(args, ws, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_damped(args, ws, rank, local):
+    """The damped ("accel. 1") scheme of scripts/previous_damp against the current one, on
+    the reference's own problems: PT iterations and device time to err <= 1e-8 for 2D
+    Maxwell VE (Stokes2D_ve0.jl vs Stokes2D_ve.jl, 5 physical steps) at each of
+    `--damp-n2`, and for 3D viscous (Stokes3D0_multixpu.jl on one rank vs the 3D viscous
+    variant) at each of `--damp-n3`. The reference's published 2D VE totals of both schemes
+    (its output/ files, kept in tests/golden) are listed beside ours."""
+    import torch
+
+    import ptstokes
+
+    torch.cuda.set_device(local)
+    pub = {}
+    try:
+        with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden",
+                               "reference_output_lines.json")) as fh:
+            lines = json.load(fh)
+        for key, name in (("2d_ve", "out_Stokes2D_ve.txt"), ("2d_ve_damp", "out_Stokes2D_ve0.txt")):
+            pub[key] = {int(r.split()[0]): int(r.split()[2]) for r in lines.get(name, [])}
+    except OSError:
+        pass
+
+    def solve(variant, dims):
+        s = ptstokes.Solver(variant, *dims)
+        s.setup_inclusion()
+        s.sync()
+        st = torch.cuda.ExternalStream(s.stream_handle())
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        res = s.run()
+        b.record(st)
+        b.synchronize()
+        s.close()
+        return {"ittot": res["ittot"], "iters": res["iters"], "converged": res["converged"],
+                "seconds": round(a.elapsed_time(b) / 1e3, 4)}
+
+    clk = ClockSampler(local)
+    clk.start()
+    rows = []
+    for n in args.damp_n2:
+        row = {"problem": f"2D Maxwell VE {n}^2, 5 steps"}
+        for v in ("2d_ve", "2d_ve_damp"):
+            row[v] = solve(v, (n, n))
+            if n in pub.get(v, {}):
+                row[v]["published_ittot"] = pub[v][n]
+        rows.append(row)
+    for n in args.damp_n3:
+        row = {"problem": f"3D viscous {n}^3, one solve"}
+        for v in ("3d_v", "3d_v_damp"):
+            row[v] = solve(v, (n, n, n))
+        rows.append(row)
+    clocks = clk.stop()
+    big = [r for r in rows if "2d_ve" in r][-1]
+    line = {
+        "metric": "PT iterations to err <= 1e-8: damped scheme (scripts/previous_damp) / current scheme, 2D VE",
+        "value": round(big["2d_ve_damp"]["ittot"] / big["2d_ve"]["ittot"], 3), "unit": "iteration ratio",
+        "n_gpus": ws, "higher_is_better": False, "scaling": "weak", "dtype": "f64",
+        "data": "the reference's inclusion problem (synthetic, deterministic)",
+        "config": {"workload": big["problem"], "eps": 1e-8, "nout": "the scripts' (200 VE, 500 viscous)"},
+        "rows": rows, "clocks": clocks,
+        "note": ("published_ittot: the reference's output files; its Stokes2D_ve0 totals do not match what "
+                 "the committed Stokes2D_ve0.jl computes (the oracle's restatement agrees with the GPU)"),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def time_to_tol(args, stream_cls):
     """Time to tolerance of the converged problem of the metric: `nt` physical steps of
     3D VE, each PT loop run to err <= 1e-8 with a check every 200 iterations
@@ -664,6 +732,10 @@ def main():
                     help="inclusion log10 viscosity drawn from U[-L, L] (adjoint and inclusion modes)")
     ap.add_argument("--batch-iter-max", type=float, default=0,
                     help="common iterMax of the sweep (0: 100*max(nx,ny) per instance)")
+    ap.add_argument("--damped", action="store_true",
+                    help="compare iterations to tolerance of the damped scheme (scripts/previous_damp)")
+    ap.add_argument("--damp-n2", type=int, nargs="*", default=[63, 127, 255, 511])
+    ap.add_argument("--damp-n3", type=int, nargs="*", default=[63, 127])
     ap.add_argument("--iters-per-step", type=int, default=200)
     ap.add_argument("--cpu-n", type=int, default=511)
     ap.add_argument("--cpu-iters", type=int, default=25)
@@ -682,6 +754,8 @@ def main():
             run_adjoint(args, ws, rank, local)
         elif args.inclusions:
             run_inclusions(args, ws, rank, local)
+        elif args.damped:
+            run_damped(args, ws, rank, local)
         else:
             run_ours(args, ws, rank, local, pg)
     finally:
