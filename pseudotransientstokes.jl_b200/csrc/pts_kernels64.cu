@@ -58,6 +58,17 @@ __device__ __forceinline__ double tau_s(double t, double to, double ag, double a
     return (t + (2.0 * ag) * (0.5 * s)) / (1.0 + ag / am);
 }
 
+// Normal stress update with the denominator computed once per cell: τxx, τyy, τzz share
+// Gdτ and Mus at the cell centre, so (1.0 + Gdτ/Mus + Gr) and Gr are the same three times
+// (same operations, same bits as tau_n).
+template <bool EL, bool PERF>
+__device__ __forceinline__ double tau_n_den(double t, double to, double g, double Gr, double den, double h, double ih,
+                                            double d) {
+    const double e = PERF ? (ih * d) : (d / h);
+    if (EL) return ((t + to * Gr) + (2.0 * g) * e) / den;
+    return (t + (2.0 * g) * e) / den;
+}
+
 template <bool PERF>
 __device__ __forceinline__ double dsc(double d, double h, double ih) {
     return PERF ? (ih * d) : (d / h);
@@ -92,12 +103,16 @@ __global__ void __launch_bounds__(256) k3_Pt_tau(Geom g, Fields64 f, Num n, int 
     if (!(roles & ROLE_TAU)) return;
     const double Mc = __ldg(&f.Mus[c]);
     const double gdt = n.gdt;
-    if (j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2)
-        f.txx[c] = tau_n<EL, PERF>(f.txx[c], EL ? __ldg(&f.txx_o[c]) : 0.0, Gc, Mc, gdt, n.dx, n._dx, dvx);
-    if (i >= 1 && i <= nx - 2 && k >= 1 && k <= nz - 2)
-        f.tyy[c] = tau_n<EL, PERF>(f.tyy[c], EL ? __ldg(&f.tyy_o[c]) : 0.0, Gc, Mc, gdt, n.dy, n._dy, dvy);
-    if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2)
-        f.tzz[c] = tau_n<EL, PERF>(f.tzz[c], EL ? __ldg(&f.tzz_o[c]) : 0.0, Gc, Mc, gdt, n.dz, n._dz, dvz);
+    const bool nx_ = j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2;
+    const bool ny_ = i >= 1 && i <= nx - 2 && k >= 1 && k <= nz - 2;
+    const bool nz_ = i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2;
+    if (nx_ || ny_ || nz_) {
+        const double Gr = EL ? gr_of(Gc, gdt) : 0.0;
+        const double den = EL ? ((1.0 + Gc / Mc) + Gr) : (1.0 + Gc / Mc);
+        if (nx_) f.txx[c] = tau_n_den<EL, PERF>(f.txx[c], EL ? __ldg(&f.txx_o[c]) : 0.0, Gc, Gr, den, n.dx, n._dx, dvx);
+        if (ny_) f.tyy[c] = tau_n_den<EL, PERF>(f.tyy[c], EL ? __ldg(&f.tyy_o[c]) : 0.0, Gc, Gr, den, n.dy, n._dy, dvy);
+        if (nz_) f.tzz[c] = tau_n_den<EL, PERF>(f.tzz[c], EL ? __ldg(&f.tzz_o[c]) : 0.0, Gc, Gr, den, n.dz, n._dz, dvz);
+    }
     // τxy on edge (x-face i, y-face j, cell k): i in [1,nx-1], j in [1,ny-1], k in [1,nz-2]
     if (i >= 1 && j >= 1 && k >= 1 && k <= nz - 2) {
         const double ag = (((__ldg(&f.Gdt[c - sx - sy]) + __ldg(&f.Gdt[c - sy])) + __ldg(&f.Gdt[c - sx])) + Gc) * 0.25;
