@@ -34,8 +34,10 @@
 // whole-plane bc copies leaves there. Vx/Vy on the first and last interior z-planes
 // (whose clamped source is another plane) are computed from global memory.
 //
-// CORR selects the defect-correction form used by the mixed-precision inner sweeps: the
-// state is a correction δ and the FP64 residuals of the current iterate enter as sources
+// CORR selects a defect-correction form with stress sources (no instantiation is launched:
+// the mixed-precision sweeps are the two FP32 kernels of pts_kernels32.cu, which carry
+// the stresses source-free): the state is a correction δ and the FP64 residuals of the
+// current iterate enter as sources
 //   δPt' = δPt - r*Gdτ*(aP + ∇·δV),   δτ' = (δτ + aτ + 2Gdτ*ε̇(δV)) / D,
 //   δV'  = δV + (R(δτ', δPt') + aV) * av(dτ_Rho)
 // which is the same PT iteration applied to (FP64 iterate + δ).

@@ -129,8 +129,9 @@ inline bool variant_fused(int v) { return variant_is3d(v) && !variant_damped(v);
 void set_global_error(const char* msg);
 
 // ---- mixed precision (3D explicit-index variants) ----
-// FP32 fields of the inner sweeps: the correction δ of the ten iterated fields, the FP64
-// residual sources of the current iterate (rounded once), and FP32 copies of the
+// FP32 fields of the inner sweeps: the correction δ of the ten iterated fields (the six
+// stresses carried as u = δτ - w), the sources of the current FP64 iterate (aP, aV, and
+// w = aτ/(D - 1) in the aτ arrays; pts_kernels32.cu), and FP32 copies of the
 // coefficients. Same unified layout and extents as the FP64 fields.
 struct Mixed32 {
     float *dPt, *dVx, *dVy, *dVz, *dtxx, *dtyy, *dtzz, *dtxy, *dtxz, *dtyz;

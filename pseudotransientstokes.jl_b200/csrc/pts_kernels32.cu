@@ -2,16 +2,21 @@
 //
 // The state of the sweeps is a correction δ to the FP64 iterate X (Pt, τ, V). The FP64
 // residuals of X enter as sources, computed once per outer step (pts_kernels64.cu):
-//   aP = ∇·V_X,  aτ = τ_o*Gr + 2Gdτ*ε̇(V_X) - τ_X*(Gdτ/Mus + Gr),  aV = R(τ_X, Pt_X)
+//   aP = ∇·V_X,  aτ = τ_o*Gr + 2Gdτ*ε̇(V_X) - τ_X*(D - 1),  D = 1 + Gdτ/Mus + Gr
 // and the sweep is the reference's PT iteration (compute_Pt_τ!, compute_V! + bc,
 // Stokes3D_ve_perf.jl:69-88,202-207) written for X + δ with X held fixed:
 //   δPt' = δPt - r*Gdτ*(aP + ∇·δV)
-//   δτ'  = (δτ + aτ + 2Gdτ*ε̇(δV)) / (1 + Gdτ/Mus + Gr)
-//   δV'  = δV + (R(δτ', δPt') + aV) * av(dτ_Rho)
-// In exact arithmetic X + δ follows the FP64 iteration step for step; in FP32 the
-// rounding is relative to the size of δ, which the outer step folds into X (in FP64)
-// and resets every nout sweeps. The stress and velocity fields move half the bytes of
-// the FP64 kernels. Compiled with FMA contraction (no bit-exact target here).
+//   δτ'  = (δτ + aτ + 2Gdτ*ε̇(δV)) / D
+//   δV'  = δV + (R(δτ', δPt') + R(τ_X, Pt_X)) * av(dτ_Rho)
+// The stress corrections are carried as u = δτ - w with w = aτ/(D - 1), which turns the
+// stress update into u' = (u + 2Gdτ*ε̇(δV)) / D with no source, and the momentum update
+// into δV' = δV + (R(u', δPt') + aV) * av(dτ_Rho) with aV = R(τ_X, Pt_X) + R_τ(w) (the
+// stress part of R); w, aV and the start u = -w come from the outer step, which folds
+// δτ = u + w into X. In exact arithmetic X + δ follows the FP64 iteration step for step;
+// in FP32 the rounding is relative to the size of δ and w, which the outer step folds
+// into X (in FP64) every nout sweeps. The sweeps read no stress source, and the stress
+// and velocity fields move half the bytes of the FP64 kernels. Compiled with FMA
+// contraction (no bit-exact target here).
 #include <cuda_runtime.h>
 
 #include "pts_internal.h"
@@ -26,7 +31,7 @@ struct Num32 {
 
 __device__ __forceinline__ float gr32(float g, const Num32& n) { return n.gdt_one ? g : __fdividef(g, n.gdt); }
 
-// δ-form compute_Pt_τ!, one thread per cell (arrays it only reads go through the read-only
+// δ-form compute_Pt_τ! (stresses as u = δτ - w), one thread per cell (arrays it only reads go through the read-only
 // data path).
 template <bool EL>
 __global__ void __launch_bounds__(256) k3_corrA(Geom g, Mixed32 m, Num32 n) {
@@ -46,28 +51,28 @@ __global__ void __launch_bounds__(256) k3_corrA(Geom g, Mixed32 m, Num32 n) {
     const float G2 = 2.0f * Gc;
     const float rDn = __fdividef(1.0f, Dn);
     if (j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2)
-        m.dtxx[c] = ((m.dtxx[c] + __ldg(&m.atxx[c])) + G2 * (n._dx * dvx)) * rDn;
+        m.dtxx[c] = (m.dtxx[c] + G2 * (n._dx * dvx)) * rDn;
     if (i >= 1 && i <= nx - 2 && k >= 1 && k <= nz - 2)
-        m.dtyy[c] = ((m.dtyy[c] + __ldg(&m.atyy[c])) + G2 * (n._dy * dvy)) * rDn;
+        m.dtyy[c] = (m.dtyy[c] + G2 * (n._dy * dvy)) * rDn;
     if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2)
-        m.dtzz[c] = ((m.dtzz[c] + __ldg(&m.atzz[c])) + G2 * (n._dz * dvz)) * rDn;
+        m.dtzz[c] = (m.dtzz[c] + G2 * (n._dz * dvz)) * rDn;
     if (i >= 1 && j >= 1 && k >= 1 && k <= nz - 2) {
         const float ag = (((__ldg(&m.Gdt[c - sx - sy]) + __ldg(&m.Gdt[c - sy])) + __ldg(&m.Gdt[c - sx])) + Gc) * 0.25f;
         const float am = (((__ldg(&m.Mus[c - sx - sy]) + __ldg(&m.Mus[c - sy])) + __ldg(&m.Mus[c - sx])) + Mc) * 0.25f;
         const float s = 0.5f * (n._dy * (__ldg(&m.dVx[c]) - __ldg(&m.dVx[c - sy])) + n._dx * (__ldg(&m.dVy[c]) - __ldg(&m.dVy[c - sx])));
-        m.dtxy[c] = __fdividef((m.dtxy[c] + __ldg(&m.atxy[c])) + (2.0f * ag) * s, (1.0f + __fdividef(ag, am)) + (EL ? gr32(ag, n) : 0.0f));
+        m.dtxy[c] = __fdividef(m.dtxy[c] + (2.0f * ag) * s, (1.0f + __fdividef(ag, am)) + (EL ? gr32(ag, n) : 0.0f));
     }
     if (i >= 1 && j >= 1 && j <= ny - 2 && k >= 1) {
         const float ag = (((__ldg(&m.Gdt[c - sx - sz]) + __ldg(&m.Gdt[c - sz])) + __ldg(&m.Gdt[c - sx])) + Gc) * 0.25f;
         const float am = (((__ldg(&m.Mus[c - sx - sz]) + __ldg(&m.Mus[c - sz])) + __ldg(&m.Mus[c - sx])) + Mc) * 0.25f;
         const float s = 0.5f * (n._dz * (__ldg(&m.dVx[c]) - __ldg(&m.dVx[c - sz])) + n._dx * (__ldg(&m.dVz[c]) - __ldg(&m.dVz[c - sx])));
-        m.dtxz[c] = __fdividef((m.dtxz[c] + __ldg(&m.atxz[c])) + (2.0f * ag) * s, (1.0f + __fdividef(ag, am)) + (EL ? gr32(ag, n) : 0.0f));
+        m.dtxz[c] = __fdividef(m.dtxz[c] + (2.0f * ag) * s, (1.0f + __fdividef(ag, am)) + (EL ? gr32(ag, n) : 0.0f));
     }
     if (i >= 1 && i <= nx - 2 && j >= 1 && k >= 1) {
         const float ag = (((__ldg(&m.Gdt[c - sy - sz]) + __ldg(&m.Gdt[c - sz])) + __ldg(&m.Gdt[c - sy])) + Gc) * 0.25f;
         const float am = (((__ldg(&m.Mus[c - sy - sz]) + __ldg(&m.Mus[c - sz])) + __ldg(&m.Mus[c - sy])) + Mc) * 0.25f;
         const float s = 0.5f * (n._dz * (__ldg(&m.dVy[c]) - __ldg(&m.dVy[c - sz])) + n._dy * (__ldg(&m.dVz[c]) - __ldg(&m.dVz[c - sy])));
-        m.dtyz[c] = __fdividef((m.dtyz[c] + __ldg(&m.atyz[c])) + (2.0f * ag) * s, (1.0f + __fdividef(ag, am)) + (EL ? gr32(ag, n) : 0.0f));
+        m.dtyz[c] = __fdividef(m.dtyz[c] + (2.0f * ag) * s, (1.0f + __fdividef(ag, am)) + (EL ? gr32(ag, n) : 0.0f));
     }
 }
 

@@ -1436,14 +1436,22 @@ __global__ void __launch_bounds__(TX* TY, PTS_SWEEP_THREADS_PER_SM / (TX * TY)) 
 
 // ------------------------------------------------------------------ mixed precision: FP64 outer step
 
-// X += δ for the ten iterated fields, then δ = 0 (elementwise over the padded arrays).
+// X += δ for the ten iterated fields, then the corrections are cleared (elementwise over
+// the padded arrays). The sweeps carry the stress corrections as u = δτ - w (w in the aτ
+// arrays, see k3_sources), so δτ = u + w.
 __global__ void k_fold(int64_t n, Fields64 f, Mixed32 m) {
     double* X[10] = {f.Pt, f.Vx, f.Vy, f.Vz, f.txx, f.tyy, f.tzz, f.txy, f.txz, f.tyz};
     float* D[10] = {m.dPt, m.dVx, m.dVy, m.dVz, m.dtxx, m.dtyy, m.dtzz, m.dtxy, m.dtxz, m.dtyz};
+    const float* W[6] = {m.atxx, m.atyy, m.atzz, m.atxy, m.atxz, m.atyz};
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
 #pragma unroll
-        for (int q = 0; q < 10; ++q) {
+        for (int q = 0; q < 4; ++q) {
             X[q][e] = X[q][e] + (double)D[q][e];
+            D[q][e] = 0.0f;
+        }
+#pragma unroll
+        for (int q = 4; q < 10; ++q) {
+            X[q][e] = X[q][e] + ((double)D[q][e] + (double)W[q - 4][e]);
             D[q][e] = 0.0f;
         }
     }
@@ -1451,8 +1459,12 @@ __global__ void k_fold(int64_t n, Fields64 f, Mixed32 m) {
 
 // Residual sources of the FP64 iterate for the FP32 sweeps, and the convergence check of
 // that iterate (compute_Res! + norms, Stokes3D_ve_perf.jl:90-96,210-218) in one pass:
-//   aP = ∇·V (the check's ∇V), aV = R (the check's Rx, Ry, Rz),
-//   aτ = τ_o*Gr + 2Gdτ*ε̇(V) - τ*(Gdτ/Mus + Gr)   (zero when τ satisfies its PT update)
+//   aP = ∇·V (the check's ∇V), R (the check's Rx, Ry, Rz, FP64, for k3_srcw),
+//   w = aτ/(D - 1) into the aτ arrays, where aτ = τ_o*Gr + 2Gdτ*ε̇(V) - τ*(D - 1) is the
+//   constitutive residual (zero when τ satisfies its PT update) and D = 1 + Gdτ/Mus + Gr.
+// With the stress corrections carried as u = δτ - w the sweeps' stress update
+// δτ' = (δτ + aτ + 2Gdτ*ε̇(δV))/D becomes u' = (u + 2Gdτ*ε̇(δV))/D exactly: no stress
+// source is read by the sweeps, and w joins the momentum source instead (k3_srcw).
 template <bool EL>
 __global__ void __launch_bounds__(256) k3_sources(Geom g, Fields64 f, Mixed32 m, Num n, double* partials) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1480,7 +1492,7 @@ __global__ void __launch_bounds__(256) k3_sources(Geom g, Fields64 f, Mixed32 m,
                 const double Gr = EL ? gr_of(Gc, n.gdt) : 0.0;
                 const double Dm = Gc / Mc + Gr;  // D - 1
                 auto a_n = [&](const double* t, const double* to, double e) {
-                    return ((EL ? to[c] * Gr : 0.0) + (2.0 * Gc) * e) - t[c] * Dm;
+                    return (((EL ? to[c] * Gr : 0.0) + (2.0 * Gc) * e) - t[c] * Dm) / Dm;
                 };
                 if (j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2) m.atxx[c] = (float)a_n(f.txx, f.txx_o, n._dx * dvx);
                 if (i >= 1 && i <= nx - 2 && k >= 1 && k <= nz - 2) m.atyy[c] = (float)a_n(f.tyy, f.tyy_o, n._dy * dvy);
@@ -1491,7 +1503,8 @@ __global__ void __launch_bounds__(256) k3_sources(Geom g, Fields64 f, Mixed32 m,
                     const double ag = (((f.Gdt[c - o1 - o2] + f.Gdt[c - o2]) + f.Gdt[c - o1]) + f.Gdt[c]) * 0.25;
                     const double am = (((f.Mus[c - o1 - o2] + f.Mus[c - o2]) + f.Mus[c - o1]) + f.Mus[c]) * 0.25;
                     const double Gr = EL ? gr_of(ag, n.gdt) : 0.0;
-                    return ((EL ? to[c] * Gr : 0.0) + (2.0 * ag) * (0.5 * s)) - t[c] * (ag / am + Gr);
+                    const double dm = ag / am + Gr;
+                    return (((EL ? to[c] * Gr : 0.0) + (2.0 * ag) * (0.5 * s)) - t[c] * dm) / dm;
                 };
                 if (i >= 1 && j >= 1 && k >= 1 && k <= nz - 2)
                     m.atxy[c] = (float)a_s(f.txy, f.txy_o, sx, sy,
@@ -1506,24 +1519,51 @@ __global__ void __launch_bounds__(256) k3_sources(Geom g, Fields64 f, Mixed32 m,
             if (i >= 1 && i <= nx - 1 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2) {
                 const double R = res3_x<true>(f, n, c, sx, sy, sz);
                 f.Rx[c] = R;
-                m.aVx[c] = (float)R;
                 a.s[0] += R * R;
             }
             if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 1 && k >= 1 && k <= nz - 2) {
                 const double R = res3_y<true>(f, n, c, sx, sy, sz);
                 f.Ry[c] = R;
-                m.aVy[c] = (float)R;
                 a.s[1] += R * R;
             }
             if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 1) {
                 const double R = res3_z<true>(f, n, c, sx, sy, sz);
                 f.Rz[c] = R;
-                m.aVz[c] = (float)R;
                 a.s[2] += R * R;
             }
         }
     }
     acc_block_store(a, partials);
+}
+
+// Momentum sources and the sweeps' starting stress corrections, after k3_sources:
+//   aV = R(τ, Pt) of the FP64 iterate + the stress part of R applied to w (FP64 sums of the
+//   FP32 w, so the sweeps and the fold see the same w), and u = -w (δτ = 0).
+// One thread per unified face point.
+__global__ void __launch_bounds__(256) k3_srcw(Geom g, Fields64 f, Mixed32 m, Num n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    if (i > nx || j > ny) return;
+    const idx_t c = gidx32(g, i, j, k);
+    const idx_t sx = 1, sy = g.px, sz = (idx_t)g.pxy;
+    auto W = [&](const float* w, idx_t o) -> double { return (double)w[o]; };
+    if (i >= 1 && i <= nx - 1 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2)
+        m.aVx[c] = (float)(f.Rx[c] + ((n._dx * (W(m.atxx, c) - W(m.atxx, c - sx)) + n._dy * (W(m.atxy, c + sy) - W(m.atxy, c))) +
+                                      n._dz * (W(m.atxz, c + sz) - W(m.atxz, c))));
+    if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 1 && k >= 1 && k <= nz - 2)
+        m.aVy[c] = (float)(f.Ry[c] + ((n._dy * (W(m.atyy, c) - W(m.atyy, c - sy)) + n._dx * (W(m.atxy, c + sx) - W(m.atxy, c))) +
+                                      n._dz * (W(m.atyz, c + sz) - W(m.atyz, c))));
+    if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 1)
+        m.aVz[c] = (float)(f.Rz[c] + ((n._dz * (W(m.atzz, c) - W(m.atzz, c - sz)) + n._dx * (W(m.atxz, c + sx) - W(m.atxz, c))) +
+                                      n._dy * (W(m.atyz, c + sy) - W(m.atyz, c))));
+    m.dtxx[c] = -m.atxx[c];
+    m.dtyy[c] = -m.atyy[c];
+    m.dtzz[c] = -m.atzz[c];
+    m.dtxy[c] = -m.atxy[c];
+    m.dtxz[c] = -m.atxz[c];
+    m.dtyz[c] = -m.atyz[c];
 }
 
 __global__ void k_coef32(int64_t n, const double* Gdt, const double* Mus, const double* dtRho, float* G32, float* M32,
@@ -1831,6 +1871,8 @@ cudaError_t launch_sources(int v, const Geom& g, const Fields64& f, const Mixed3
     const double nx = g.nx, ny = g.ny, nz = g.nz;
     k_check_finalize<<<1, 256, 0, s>>>(partials, nb, n.lx, (nx - 1) * (ny - 2) * (nz - 2), (nx - 2) * (ny - 1) * (nz - 2),
                                        (nx - 2) * (ny - 2) * (nz - 1), nx * ny * nz, 3, result);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    k3_srcw<<<grid_faces(g, true), blk(), 0, s>>>(g, f, m, n);
     return cudaGetLastError();
 }
 
