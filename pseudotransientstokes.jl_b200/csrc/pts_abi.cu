@@ -498,7 +498,7 @@ int pts_create(const pts_desc* d, pts_ctx** out) {
     if (c->mixed) {
         float** p32[] = {&c->m.dPt, &c->m.dVx, &c->m.dVy, &c->m.dVz, &c->m.dtxx, &c->m.dtyy, &c->m.dtzz, &c->m.dtxy,
                          &c->m.dtxz, &c->m.dtyz, &c->m.aP, &c->m.atxx, &c->m.atyy, &c->m.atzz, &c->m.atxy,
-                         &c->m.atxz, &c->m.atyz, &c->m.aVx, &c->m.aVy, &c->m.aVz, &c->m.Gdt, &c->m.Mus, &c->m.dtRho};
+                         &c->m.atxz, &c->m.atyz, &c->m.aVx, &c->m.aVy, &c->m.aVz, &c->m.dtRho};
         for (float** p : p32) {
             void* q = nullptr;
             if (cudaMalloc(&q, (size_t)g.n * sizeof(float)) != cudaSuccess ||
@@ -510,6 +510,15 @@ int pts_create(const pts_desc* d, pts_ctx** out) {
             *p = (float*)q;
             c->owned32.push_back(*p);
         }
+        void* q = nullptr;
+        if (cudaMalloc(&q, (size_t)g.n * sizeof(float2)) != cudaSuccess ||
+            cudaMemsetAsync(q, 0, (size_t)g.n * sizeof(float2), c->stream) != cudaSuccess) {
+            cudaGetLastError();
+            c->err = "allocation of the FP32 fields failed";
+            return bail(PTS_E_NOMEM);
+        }
+        c->m.GM = (float2*)q;
+        c->owned32.push_back((float*)q);
     }
     if (c->fused) {
         for (int q = 0; q < 10; ++q)

@@ -136,7 +136,8 @@ void set_global_error(const char* msg);
 struct Mixed32 {
     float *dPt, *dVx, *dVy, *dVz, *dtxx, *dtyy, *dtzz, *dtxy, *dtxz, *dtyz;
     float *aP, *atxx, *atyy, *atzz, *atxy, *atxz, *atyz, *aVx, *aVy, *aVz;
-    float *Gdt, *Mus, *dtRho;
+    float2* GM;    // Gdτ and Mus interleaved: one 8-byte load gives both at a point
+    float* dtRho;
 };
 // FP32 inner sweep (pts_kernels32.cu): δ-form compute_Pt_τ! and compute_V! + bc.
 cudaError_t launch_corr_A32(int variant, const Geom& g, const Mixed32& m, const Num& n, cudaStream_t s);

@@ -45,7 +45,14 @@ __global__ void __launch_bounds__(256) k3_corrA(Geom g, Mixed32 m, Num32 n) {
     const float dvx = __ldg(&m.dVx[c + sx]) - __ldg(&m.dVx[c]);
     const float dvy = __ldg(&m.dVy[c + sy]) - __ldg(&m.dVy[c]);
     const float dvz = __ldg(&m.dVz[c + sz]) - __ldg(&m.dVz[c]);
-    const float Gc = __ldg(&m.Gdt[c]), Mc = __ldg(&m.Mus[c]);
+    const float2 gmc = __ldg(&m.GM[c]);
+    const float Gc = gmc.x, Mc = gmc.y;
+    // 4-point averages of Gdτ and Mus on an edge from the interleaved pairs at c-o1-o2, c-o2, c-o1, c
+    auto avg = [&](idx_t o1, idx_t o2, float* ag, float* am) {
+        const float2 a = __ldg(&m.GM[c - o1 - o2]), b = __ldg(&m.GM[c - o2]), d = __ldg(&m.GM[c - o1]);
+        *ag = (((a.x + b.x) + d.x) + Gc) * 0.25f;
+        *am = (((a.y + b.y) + d.y) + Mc) * 0.25f;
+    };
     m.dPt[c] = m.dPt[c] - n.r * Gc * (__ldg(&m.aP[c]) + ((n._dx * dvx + n._dy * dvy) + n._dz * dvz));
     const float Dn = (1.0f + __fdividef(Gc, Mc)) + (EL ? gr32(Gc, n) : 0.0f);
     const float G2 = 2.0f * Gc;
@@ -57,20 +64,20 @@ __global__ void __launch_bounds__(256) k3_corrA(Geom g, Mixed32 m, Num32 n) {
     if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2)
         m.dtzz[c] = (m.dtzz[c] + G2 * (n._dz * dvz)) * rDn;
     if (i >= 1 && j >= 1 && k >= 1 && k <= nz - 2) {
-        const float ag = (((__ldg(&m.Gdt[c - sx - sy]) + __ldg(&m.Gdt[c - sy])) + __ldg(&m.Gdt[c - sx])) + Gc) * 0.25f;
-        const float am = (((__ldg(&m.Mus[c - sx - sy]) + __ldg(&m.Mus[c - sy])) + __ldg(&m.Mus[c - sx])) + Mc) * 0.25f;
+        float ag, am;
+        avg(sx, sy, &ag, &am);
         const float s = 0.5f * (n._dy * (__ldg(&m.dVx[c]) - __ldg(&m.dVx[c - sy])) + n._dx * (__ldg(&m.dVy[c]) - __ldg(&m.dVy[c - sx])));
         m.dtxy[c] = __fdividef(m.dtxy[c] + (2.0f * ag) * s, (1.0f + __fdividef(ag, am)) + (EL ? gr32(ag, n) : 0.0f));
     }
     if (i >= 1 && j >= 1 && j <= ny - 2 && k >= 1) {
-        const float ag = (((__ldg(&m.Gdt[c - sx - sz]) + __ldg(&m.Gdt[c - sz])) + __ldg(&m.Gdt[c - sx])) + Gc) * 0.25f;
-        const float am = (((__ldg(&m.Mus[c - sx - sz]) + __ldg(&m.Mus[c - sz])) + __ldg(&m.Mus[c - sx])) + Mc) * 0.25f;
+        float ag, am;
+        avg(sx, sz, &ag, &am);
         const float s = 0.5f * (n._dz * (__ldg(&m.dVx[c]) - __ldg(&m.dVx[c - sz])) + n._dx * (__ldg(&m.dVz[c]) - __ldg(&m.dVz[c - sx])));
         m.dtxz[c] = __fdividef(m.dtxz[c] + (2.0f * ag) * s, (1.0f + __fdividef(ag, am)) + (EL ? gr32(ag, n) : 0.0f));
     }
     if (i >= 1 && i <= nx - 2 && j >= 1 && k >= 1) {
-        const float ag = (((__ldg(&m.Gdt[c - sy - sz]) + __ldg(&m.Gdt[c - sz])) + __ldg(&m.Gdt[c - sy])) + Gc) * 0.25f;
-        const float am = (((__ldg(&m.Mus[c - sy - sz]) + __ldg(&m.Mus[c - sz])) + __ldg(&m.Mus[c - sy])) + Mc) * 0.25f;
+        float ag, am;
+        avg(sy, sz, &ag, &am);
         const float s = 0.5f * (n._dz * (__ldg(&m.dVy[c]) - __ldg(&m.dVy[c - sz])) + n._dy * (__ldg(&m.dVz[c]) - __ldg(&m.dVz[c - sy])));
         m.dtyz[c] = __fdividef(m.dtyz[c] + (2.0f * ag) * s, (1.0f + __fdividef(ag, am)) + (EL ? gr32(ag, n) : 0.0f));
     }

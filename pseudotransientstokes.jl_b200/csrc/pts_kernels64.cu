@@ -1566,11 +1566,10 @@ __global__ void __launch_bounds__(256) k3_srcw(Geom g, Fields64 f, Mixed32 m, Nu
     m.dtyz[c] = -m.atyz[c];
 }
 
-__global__ void k_coef32(int64_t n, const double* Gdt, const double* Mus, const double* dtRho, float* G32, float* M32,
+__global__ void k_coef32(int64_t n, const double* Gdt, const double* Mus, const double* dtRho, float2* GM32,
                          float* R32) {
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
-        G32[e] = (float)Gdt[e];
-        M32[e] = (float)Mus[e];
+        GM32[e] = make_float2((float)Gdt[e], (float)Mus[e]);
         R32[e] = (float)dtRho[e];
     }
 }
@@ -1877,7 +1876,7 @@ cudaError_t launch_sources(int v, const Geom& g, const Fields64& f, const Mixed3
 }
 
 cudaError_t launch_coef32(const Geom& g, const Fields64& f, const Mixed32& m, cudaStream_t s) {
-    k_coef32<<<148 * 8, 256, 0, s>>>(g.n, f.Gdt, f.Mus, f.dtRho, m.Gdt, m.Mus, m.dtRho);
+    k_coef32<<<148 * 8, 256, 0, s>>>(g.n, f.Gdt, f.Mus, f.dtRho, m.GM, m.dtRho);
     return cudaGetLastError();
 }
 
