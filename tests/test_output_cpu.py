@@ -36,6 +36,23 @@ def test_result_lines_have_the_columns_of_each_script():
     assert abs(line[7] - 0.0314 / 191) < 1e-18 and abs(line[8] - line[6] / line[7]) < 1e-9
 
 
+def test_damped_scripts_lines_and_files():
+    """Stokes2D0.jl:168-169 "nx ny iter", Stokes2D_ve0.jl:195-196 "nx ny ittot nt" (the
+    columns of the reference's out_Stokes2D_ve0.txt), Stokes3D0_multixpu.jl:242-243
+    "nx ny nz iter"; only Stokes2D_ve0.jl writes a MAT file (:199-200)."""
+    from ptstokes.output import A_EFF_ARRAYS, LINE_FILES, MAT_FILES, result_line
+    assert result_line("2d_v_damp", 511, 511, None, 9000, 1, 0.5) == [511, 511, 9000]
+    assert result_line("2d_ve_damp", 31, 31, None, 4000, 5, 0.5) == [31, 31, 4000, 5]
+    assert result_line("3d_v_damp", 63, 63, 63, 1500, 1, 0.5) == [63, 63, 63, 1500]
+    lines = json.load(open(os.path.join(ROOT, "tests", "golden", "reference_output_lines.json")))
+    assert all(len(r.split()) == 4 for r in lines["out_Stokes2D_ve0.txt"])
+    assert LINE_FILES["2d_ve_damp"] == "out_Stokes2D_ve0.txt" and LINE_FILES["3d_v_damp"] == "out_Stokes3D0.txt"
+    assert set(MAT_FILES) & {"2d_v_damp", "2d_ve_damp", "3d_v_damp"} == {"2d_ve_damp"}
+    # A_eff of the scripts: (3*2), (6*2 + 1), (4*2) arrays (Stokes2D0.jl:153, Stokes2D_ve0.jl:178,
+    # Stokes3D0_multixpu.jl:222)
+    assert (A_EFF_ARRAYS["2d_v_damp"], A_EFF_ARRAYS["2d_ve_damp"], A_EFF_ARRAYS["3d_v_damp"]) == (6, 13, 8)
+
+
 class _FakeSolver:
     variant, ndim, nx, ny, nz = "3d_ve_perf", 3, 5, 4, 3
     dx, dy, dz = 2.0, 2.5, 10 / 3
