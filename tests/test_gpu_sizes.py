@@ -1,8 +1,9 @@
 """Edge sizes on the GPU, through the C ABI.
 
 * The smallest grids the stencils allow (3 cells along an axis, where each stress and
-  velocity interior is a single plane) and ragged shapes whose padded row length differs
-  from the cell count by 0, 1 and 15, for every variant: every field bit for bit against
+  velocity interior is a single plane) and ragged shapes whose x-faces fill the padded row
+  exactly (nx + 1 = 16 or 32) or spill one face into the next 16-element group (nx = 16),
+  for every variant: every field bit for bit against
   the oracle after a few PT iterations (NaN where the oracle has NaN).
 * A full-size case: 3D VE (Stokes3D_ve_perf.jl kernels) at 255^3, three iterations, bit for
   bit against the oracle.
