@@ -78,7 +78,8 @@ typedef struct pts_desc {
     double max_l;       /* length in dτ_Rho = Vpdτ*max_l/Re/μ_eff; 0 => max(lx,ly[,lz]) */
     double eps;         /* tolerance ε on err (Stokes3D_ve_perf.jl:132) */
     double iter_max;    /* `while err > ε && iter <= iterMax` */
-    int32_t mixed_inner;    /* MIXED: FP32 sweeps between FP64 corrections; 0 => nout */
+    int32_t mixed_inner;    /* MIXED: FP32 sweeps between FP64 corrections. The correction runs
+                             * with every check, so this must be 0 or nout (others: PTS_E_INVAL) */
     int32_t single_pass;    /* 3D: 0 = two launches per iteration; one launch per iteration with
                              * 1 = inputs staged in shared memory by bulk copies, 2 = inputs read
                              * directly (L1/L2) */

@@ -404,6 +404,8 @@ int pts_create(const pts_desc* d, pts_ctx** out) {
     if ((int64_t)d->nx + 1 > (1 << 20) || (int64_t)d->ny + 1 > (1 << 20) || (d3 && (int64_t)d->nz + 1 > (1 << 20)))
         return fail(nullptr, PTS_E_INVAL, "grid extent too large");
     if (d->nout < 1) return fail(nullptr, PTS_E_INVAL, "nout must be >= 1");
+    if (d->mixed_inner != 0 && d->mixed_inner != d->nout)
+        return fail(nullptr, PTS_E_INVAL, "mixed_inner: the FP64 correction runs with every check, so it must be 0 or nout");
     if (!(d->lx > 0) || !(d->ly > 0) || (d3 && !(d->lz > 0))) return fail(nullptr, PTS_E_INVAL, "domain extents must be > 0");
     if (d->adjoint && ((d->variant != PTS_3D_V && d->variant != PTS_3D_VE_PERF) || d->precision != PTS_FP64 ||
                        d->single_pass))

@@ -61,6 +61,10 @@ def test_create_rejects_bad_descriptions_without_a_device():
     assert lib.pts_create(ctypes.byref(d), ctypes.byref(ctx)) == _abi.PTS_E_INVAL
     d.variant, d.nout = 4, 0
     assert lib.pts_create(ctypes.byref(d), ctypes.byref(ctx)) == _abi.PTS_E_INVAL
+    d.nout, d.precision, d.mixed_inner = 10, 1, 7
+    assert lib.pts_create(ctypes.byref(d), ctypes.byref(ctx)) == _abi.PTS_E_INVAL
+    assert b"mixed_inner" in lib.pts_last_error(None)
+    d.precision, d.mixed_inner, d.nout = 0, 0, 0
     assert lib.pts_create(None, ctypes.byref(ctx)) == _abi.PTS_E_INVAL
 
 
