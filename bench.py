@@ -148,6 +148,22 @@ def cpu_sample(n, iters):
     return a_eff(n) * iters / dt / 1e9, nthreads, dt
 
 
+def cpu_sample_2d(n, iters):
+    """The oracle's OpenMP FP64 restatement of Stokes2D_ve_perf.jl on the host cores:
+    T_eff with the script's A_eff = 18*nx*ny*8 bytes per PT iteration."""
+    from oracle import scripts as S
+    from oracle.binding import lib
+
+    c = S.make("2d_ve_perf", n, n)
+    c.assign_tau()
+    c.iteration()
+    t0 = time.perf_counter()
+    for _ in range(iters):
+        c.iteration()
+    dt = time.perf_counter() - t0
+    return 18 * n * n * 8 * iters / dt / 1e9, lib().ora_num_threads(), dt
+
+
 def small_2d_case():
     """The reference's CPU-runnable case: 2D viscous Stokes (Stokes2D.jl), 127^2, a check every
     100 iterations, to 1e-8 -- on the host (the oracle, all threads) and on the GPU."""
@@ -389,6 +405,85 @@ def run_ours(args, ws, rank, local, pg):
         print(json.dumps(line), flush=True)
 
 
+def run_2d(args, ws, rank, local, pg):
+    """The 2D visco-elastic perf script (Stokes2D_ve_perf.jl) at `--n2`^2: T_eff = A_eff/t_it
+    with the script's A_eff = 18*nx*ny*8 bytes (Stokes2D_ve_perf.jl:173), a step being one
+    check block of `--iters-per-step` PT iterations (two kernels each) + one check."""
+    import torch
+
+    import ptstokes
+
+    torch.cuda.set_device(local)
+    n, nout = args.n2, args.iters_per_step
+    s = ptstokes.Solver("2d_ve_perf", n, n, nout=nout, eps=1e-300, iter_max=nout - 1)
+    s.setup_inclusion()
+    s.assign_tau()
+    stream = torch.cuda.ExternalStream(s.stream_handle())
+    for _ in range(args.warmup):
+        s.solve()
+    s.sync()
+    barrier(pg)
+    clk = ClockSampler(local)
+    clk.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        s.solve()
+    e1.record(stream)
+    e1.synchronize()
+    barrier(pg)
+    clocks = clk.stop()
+    t_ms = max_over_ranks(e0.elapsed_time(e1), pg)
+    t_it = t_ms / 1e3 / (args.steps * nout)
+    aeff = 18 * n * n * 8
+
+    def time_kernel(fn, reps=20):
+        for _ in range(3):
+            fn()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        b.record(stream)
+        b.synchronize()
+        return a.elapsed_time(b) / reps
+
+    ms_A = time_kernel(s.compute_Pt_tau)
+    ms_B = time_kernel(s.compute_V_bc)
+    peak, peak_kind = hbm_peak()
+    bytes_A = 15 * n * n * 8  # Vx Vy Gdτ Mus Pt τ(3) τ_o(3) read, Pt τ(3) written
+    s.close()
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        v, thr, dt = cpu_sample_2d(args.cpu_n2, args.cpu_iters2)
+        cpu = {"value": round(v, 3), "unit": "GB/s", "cores": thr, "kind": "port",
+               "sample": f"oracle (C++/OpenMP FP64 restatement of Stokes2D_ve_perf.jl) at {args.cpu_n2}^2, "
+                         f"{args.cpu_iters2} PT iterations, {dt:.1f} s"}
+    if rank == 0:
+        line = {
+            "metric": "T_eff GB/s, 2D VE perf (Stokes2D_ve_perf.jl), FP64, 1 B200", "value": round(ws * aeff / t_it / 1e9, 3),
+            "unit": "GB/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(t_ms / args.steps, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (the script's circular inclusion r=1 mu=1e-3, pure shear, G=1, dt=1)",
+            "config": {"workload": f"2D VE Stokes (Stokes2D_ve_perf.jl kernels), FP64, {n}^2, box 10^2", "nx": n,
+                       "ny": n, "iters_per_step": nout, "t_it_ms": round(t_it * 1e3, 5),
+                       "A_eff": "18 arrays x 8 B per cell (Stokes2D_ve_perf.jl:173)",
+                       "l2": f"inputs larger than L2 ({n * n * 8 / 1e6:.0f} MB per field)"},
+            "reference_published": {"value": 932.8, "unit": "GB/s", "hardware": "A100 SXM4",
+                                    "source": "output/out_Stokes2D_ve_perf_ampere.txt:45 (8191^2)"},
+            "roofline": {"bound": "hbm", "achieved": round(bytes_A / (ms_A / 1e3) / 1e9, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(bytes_A / (ms_A / 1e3) / 1e9 / peak, 4), "traffic": None, "kernel": "k2_Pt_tau",
+                         "peak_kind": peak_kind, "kernel_ms": round(ms_A, 4), "algorithmic_bytes": bytes_A,
+                         "other_kernel": {"name": "k2_V_bc", "ms": round(ms_B, 4),
+                                          "achieved": round(9 * n * n * 8 / (ms_B / 1e3) / 1e9, 1)}},
+            "cpu_baseline": cpu, "gpu_launches": args.steps * (2 * nout + 2), "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+
+
 def run_batch(args, ws, rank, local):
     """The batched 2D viscous sweep: `--batch-n` seeded instances (nx in {63,127,255,511},
     lx/ly ~ U[1,4], log10 contrast ~ U[-6,-1], buoyancy or pure shear), each to err <= 1e-8
@@ -449,13 +544,16 @@ def run_adjoint(args, ws, rank, local):
     torch.cuda.set_device(local)
     n = args.adj_n
     L = args.log10_range
-    mus = viscosity_field(n, n, n, inclusion_set(seed=1855 + rank, log10_mu=(-L, L)))
+    incl = inclusion_set(seed=1855 + rank, log10_mu=(-L, L))
     pert = lognormal_factor((n, n, n), sigma=0.5, corr=8.0, seed=1856 + rank)
     p = ViscousAdjoint(n, n, n, eps=1e-8, nout=200, iter_max=2e5)
-    p.set_viscosity(mus * pert)
+    # the synthetic observations: the inclusion field times the log-normal perturbation
+    p.set_viscosity(viscosity_field(n, n, n, incl) * pert)
     obs = p.forward()
     vobs = p.top_vz()
-    p.set_viscosity(mus)
+    # the field whose gradient is taken is built on the device (pts_init_inclusions + smooth!)
+    p.set_inclusions(incl)
+    mus = viscosity_field(n, n, n, incl)
     st = torch.cuda.ExternalStream(p.fwd.stream_handle())
     clk = ClockSampler(local)
     clk.start()
@@ -499,12 +597,12 @@ def run_adjoint(args, ws, rank, local):
     }
     p.close()
     if args.adj_ve_steps > 0:
-        line["visco_elastic"] = adjoint_ve(args, n, mus, pert, delta, rank)
+        line["visco_elastic"] = adjoint_ve(args, n, mus, incl, pert, delta, rank)
     if rank == 0:
         print(json.dumps(line), flush=True)
 
 
-def adjoint_ve(args, n, mus, pert, delta, rank):
+def adjoint_ve(args, n, mus, incl, pert, delta, rank):
     """The visco-elastic variant: `--adj-ve-steps` Maxwell steps (G = 1, dt = 1), each to 1e-8,
     per-step stress checkpoints, the backward adjoint time loop; J on the last step."""
     import numpy as np
@@ -517,7 +615,7 @@ def adjoint_ve(args, n, mus, pert, delta, rank):
     p.set_viscosity(mus * pert)
     p.forward()
     vobs = p.top_vz()
-    p.set_viscosity(mus)
+    p.set_inclusions(incl)
     st = torch.cuda.ExternalStream(p.fwd.stream_handle())
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -552,18 +650,17 @@ def run_inclusions(args, ws, rank, local):
     import torch
 
     import ptstokes
-    from ptstokes.adjoint import inclusion_set, viscosity_field
+    from ptstokes.adjoint import inclusion_array, inclusion_set
 
     torch.cuda.set_device(local)
     n, L = args.incl_n, args.log10_range
-    mus = viscosity_field(n, n, n, inclusion_set(seed=1855 + rank, log10_mu=(-L, L)))
+    rows = inclusion_array(inclusion_set(seed=1855 + rank, log10_mu=(-L, L)))
     out, fields = {}, {}
     clk = ClockSampler(local)
     clk.start()
     for prec in ("fp64", "mixed"):
         s = ptstokes.Solver("3d_v", n, n, n, precision=prec, eps=1e-8, nout=200, iter_max=4e5)
-        s.init_inclusion(1.0, 1.0, 0.0, 1.0)
-        s.set("Mus", mus)
+        s.init_inclusions(rows, mus0=1.0, ebg=1.0)  # the 20-sphere field, built on the device
         s.smooth(10, 1.0)
         s.compute_maxloc()
         s.compute_iter_params()
@@ -715,7 +812,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=511)
-    ap.add_argument("--variant", default="3d_ve_perf", choices=["3d_ve_perf", "3d_ve", "3d_v"])
+    ap.add_argument("--variant", default="3d_ve_perf", choices=["3d_ve_perf", "3d_ve", "3d_v", "2d_ve_perf"],
+                    help="2d_ve_perf: the 2D perf script at --n2 (its own JSON line)")
+    ap.add_argument("--n2", type=int, default=8191)
+    ap.add_argument("--cpu-n2", type=int, default=2047)
+    ap.add_argument("--cpu-iters2", type=int, default=101)
     ap.add_argument("--single-pass", type=int, nargs="?", const=1, default=0, choices=[0, 1, 2],
                     help="one launch per PT iteration: 1 staged kernel, 2 direct-load kernel")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
@@ -756,6 +857,8 @@ def main():
             run_inclusions(args, ws, rank, local)
         elif args.damped:
             run_damped(args, ws, rank, local)
+        elif args.variant == "2d_ve_perf":
+            run_2d(args, ws, rank, local, pg)
         else:
             run_ours(args, ws, rank, local, pg)
     finally:

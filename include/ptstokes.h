@@ -84,7 +84,13 @@ typedef struct pts_desc {
                              * 1 = inputs staged in shared memory by bulk copies, 2 = inputs read
                              * directly (L1/L2) */
     int32_t adjoint;        /* PTS_3D_V / PTS_3D_VE_PERF: 1 = solve the transposed (adjoint) system */
-    int32_t reserved[5];
+    int32_t stencil;        /* 3D FP64 two-kernel path, compute_Pt_τ!: 0 = z-marching kernel whose
+                             * input planes the tensor-memory accelerator stages in shared memory;
+                             * 1 = one thread per cell, operands read directly. Same bits. */
+    int32_t stencil_tile;   /* z-marching kernel: tile configuration 0 .. pts_stencil_tiles()-1
+                             * (0 = default; chosen by timing, e.g. ptstokes.tune_stencil) */
+    int32_t stencil_kz;     /* z-marching kernel: z-planes per thread block (0 = default 32) */
+    int32_t reserved[2];
 } pts_desc;
 
 /* Fields, by the reference's names. Extents are the reference's (pts_field_shape). */
@@ -138,6 +144,12 @@ PTS_API int pts_destroy(pts_ctx* ctx);
 PTS_API const char* pts_last_error(const pts_ctx* ctx);        /* ctx may be NULL (creation errors) */
 PTS_API int pts_abi_version(void);
 PTS_API int pts_sync(pts_ctx* ctx);                            /* wait for the context's stream */
+/* Tile configurations of the z-marching compute_Pt_τ! (pts_desc.stencil_tile): their count,
+ * and per configuration the tile height in cells (the width is 32) and the number of
+ * shared-memory plane slots. No reference counterpart (ParallelStencil picks its launch
+ * shape itself). */
+PTS_API int pts_stencil_tiles(void);
+PTS_API int pts_stencil_tile_info(int32_t tile, int32_t* tile_y, int32_t* ring_slots);
 /* The context's cudaStream_t (as void*), to order or time the caller's own work with it. */
 PTS_API int pts_stream(pts_ctx* ctx, void** stream);
 
@@ -154,6 +166,19 @@ PTS_API int pts_get_field_device(pts_ctx* ctx, int32_t field, double* dev, int64
  * the cell centre from the box centre is < radius2, pure-shear V with strain rate ebg,
  * every other field zero (Stokes3D_ve_perf.jl:164-172, Stokes2D.jl:106-114). */
 PTS_API int pts_init_inclusion(pts_ctx* ctx, double mus0, double musi, double radius2, double ebg);
+/* One inclusion of pts_init_inclusions: a circle (2D) or sphere (3D). */
+typedef struct pts_inclusion {
+    double x, y, z;  /* centre, relative to the domain centre (the scripts' Xi, Yi); z unused in 2D */
+    double r2;       /* squared radius */
+    double mus;      /* viscosity inside */
+} pts_inclusion;
+/* create_inclusions! (scripts/Stokes2D_param.jl:83-99) over a list of `count` inclusions
+ * (0 <= count <= PTS_MAX_INCLUSIONS), each with its own radius and viscosity, in 2D or 3D:
+ * Mus = the viscosity of the first inclusion whose squared distance from the cell centre is
+ * below its r2, else mus0; pure-shear V with strain rate ebg; every other field zero (as
+ * pts_init_inclusion). The list is read before the call returns. */
+#define PTS_MAX_INCLUSIONS 65536
+PTS_API int pts_init_inclusions(pts_ctx* ctx, const pts_inclusion* list, int32_t count, double mus0, double ebg);
 /* smooth!(Mus2, Mus, fact) nsweeps times with the Mus/Mus2 swap (Stokes3D_ve_perf.jl:173-177). */
 PTS_API int pts_smooth(pts_ctx* ctx, int32_t nsweeps, double fact);
 /* Musτ .= Mus; compute_maxloc!(Musτ, Mus); bc_x!/bc_y!/bc_z!(Musτ) (Stokes3D_ve_perf.jl:178-182). */

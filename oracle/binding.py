@@ -60,6 +60,7 @@ _SIGS = {
     "ora2p_compute_V": [Arr] * 7 + [_D, _D, _L, _L, _L, _L],
     "ora2p_compute_Res": [Arr] * 9 + [_D, _D],
     "ora2_create_inclusions": [Arr, Arr, ctypes.c_void_p, ctypes.c_void_p, _L] + [_D] * 9,
+    "ora_create_inclusions_list": [Arr] + [ctypes.c_void_p] * 5 + [_L] + [_D] * 7 + [ctypes.c_int],
     "ora2s_compute_tau": [Arr] * 7 + [_D, _D],
     "ora2s_compute_dV": [Arr] * 10 + [_D, _D],
     "ora3_smooth": [Arr, Arr, _D],

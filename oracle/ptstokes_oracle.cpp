@@ -354,6 +354,39 @@ void ora2_create_inclusions(oarr Mus_, oarr rhog_, const double* Xi, const doubl
         }
 }
 
+// create_inclusions! (Stokes2D_param.jl:83-99) over a list of inclusions, each with its own
+// squared radius r2[q] and viscosity musi[q], in 2D (Zi unused, n3 = 1) or 3D (the same
+// test with the z term added last): Mus = musi of the first inclusion the cell centre is
+// inside (the reference's loop breaks at the first hit), else mus0. Centres are in the
+// reference's centred frame: x = (ix-1)*dx + 0.5*dx - 0.5*lx.
+void ora_create_inclusions_list(oarr Mus_, const double* Xi, const double* Yi, const double* Zi, const double* r2,
+                                const double* musi, int64_t ni, double mus0, double dx, double dy, double dz,
+                                double lx, double ly, double lz, int d3) {
+    F3 Mus(Mus_);
+#pragma omp parallel for schedule(static)
+    for (int64_t iz = 1; iz <= Mus.n3; ++iz)
+        for (int64_t iy = 1; iy <= Mus.n2; ++iy)
+            for (int64_t ix = 1; ix <= Mus.n1; ++ix) {
+                const double x = (ix - 1) * dx + 0.5 * dx - 0.5 * lx;
+                const double y = (iy - 1) * dy + 0.5 * dy - 0.5 * ly;
+                const double z = (iz - 1) * dz + 0.5 * dz - 0.5 * lz;
+                double mu = mus0;
+                for (int64_t q = 0; q < ni; ++q) {
+                    const double ax = x - Xi[q], ay = y - Yi[q];
+                    double rad2 = ax * ax + ay * ay;
+                    if (d3) {
+                        const double az = z - Zi[q];
+                        rad2 = rad2 + az * az;
+                    }
+                    if (rad2 < r2[q]) {
+                        mu = musi[q];
+                        break;
+                    }
+                }
+                Mus(ix, iy, iz) = mu;
+            }
+}
+
 // compute_τ! (Stokes2D_param.jl:48-55): τ = 2μ_veτ(ε̇ + τ/Gdτ/2), μ_veτ = 1/(1/Gdτ + 1/Mus)
 void ora2s_compute_tau(oarr txx_, oarr tyy_, oarr txy_, oarr Vx_, oarr Vy_, oarr Mus_, oarr Gdt_, double dx,
                        double dy) {

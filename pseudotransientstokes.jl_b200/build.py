@@ -27,6 +27,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hi
 UNITS = {
     "pts_kernels64.cu": ["--fmad=false"],
     "pts_noalloc.cu": ["--fmad=false"],
+    "pts_zstage.cu": ["--fmad=false"],
     "pts_kernels32.cu": [],
     "pts_abi.cu": [],
     "pts_batch.cu": [],

@@ -35,6 +35,7 @@ struct pts_ctx {
     Fields64 f{};    // current fields
     Fields64 alt{};  // second buffers of the ten iterated fields (single-pass 3D path)
     bool fused = false;
+    bool zs = false;         // compute_Pt_τ! by the z-marching TMA-staged kernel
     bool mixed = false;      // FP32 inner sweeps + FP64 defect correction
     Mixed32 m{};
     std::vector<float*> owned32;
@@ -46,6 +47,8 @@ struct pts_ctx {
     CheckResult* h_result = nullptr;  // pinned
     cudaGraphExec_t chunk[2] = {nullptr, nullptr};  // nout iterations + check, per starting parity
     int* d_kerr = nullptr;  // set by a kernel whose bounded wait timed out
+    pts_inclusion* d_incl = nullptr;  // inclusion list of pts_init_inclusions
+    int incl_cap = 0;
     std::string err;
 };
 
@@ -239,7 +242,7 @@ int synced(pts_ctx* c) {
     CK(cudaMemcpy(&flag, c->d_kerr, sizeof(int), cudaMemcpyDeviceToHost));
     if (flag) {
         CK(cudaMemset(c->d_kerr, 0, sizeof(int)));
-        return fail(c, PTS_E_CUDA, "a shared-memory staging wait in the single-pass kernel timed out");
+        return fail(c, PTS_E_CUDA, "a bounded shared-memory staging wait in a z-marching kernel timed out");
     }
     return PTS_OK;
 }
@@ -275,9 +278,21 @@ int copy3d(pts_ctx* c, int id, const double* src_dense, double* dst_dense, int64
     return PTS_OK;
 }
 
+// compute_Pt_τ! (both roles) on the context's fields: the z-marching TMA-staged kernel
+// unless the context asked for the one-thread-per-cell form (same bits either way).
+int Pt_tau(pts_ctx* c, bool store_divV) {
+    if (c->zs)
+        CK(launch_Pt_tau_zs(c->v, c->d.stencil_tile, c->g, c->f, c->n, c->d.stencil_kz, store_divV && !c->perf,
+                            c->d_kerr, c->stream));
+    else
+        CK(launch_Pt_tau(c->v, c->g, c->f, c->n, ROLE_P | ROLE_TAU, store_divV && !c->perf, c->stream));
+    return PTS_OK;
+}
+
 // One PT iteration with the two-kernel path: compute_Pt_τ! then compute_V! + bc.
 int iteration(pts_ctx* c, bool store_divV) {
-    CK(launch_Pt_tau(c->v, c->g, c->f, c->n, ROLE_P | ROLE_TAU, store_divV && !c->perf, c->stream));
+    int rc = Pt_tau(c, store_divV);
+    if (rc) return rc;
     CK(launch_V_bc(c->v, c->g, c->f, c->n, true, c->stream));
     return PTS_OK;
 }
@@ -389,6 +404,16 @@ extern "C" {
 
 int pts_abi_version(void) { return PTS_ABI_VERSION; }
 
+int pts_stencil_tiles(void) { return zstage_num_configs(); }
+
+int pts_stencil_tile_info(int32_t tile, int32_t* tile_y, int32_t* ring_slots) {
+    int ty = 0, r = 0;
+    if (!zstage_tile_info(tile, &ty, &r)) return fail(nullptr, PTS_E_INVAL, "no such stencil tile");
+    if (tile_y) *tile_y = ty;
+    if (ring_slots) *ring_slots = r;
+    return PTS_OK;
+}
+
 const char* pts_last_error(const pts_ctx* c) { return c ? c->err.c_str() : g_create_err.c_str(); }
 
 int pts_create(const pts_desc* d, pts_ctx** out) {
@@ -407,6 +432,10 @@ int pts_create(const pts_desc* d, pts_ctx** out) {
     if (d->mixed_inner != 0 && d->mixed_inner != d->nout)
         return fail(nullptr, PTS_E_INVAL, "mixed_inner: the FP64 correction runs with every check, so it must be 0 or nout");
     if (!(d->lx > 0) || !(d->ly > 0) || (d3 && !(d->lz > 0))) return fail(nullptr, PTS_E_INVAL, "domain extents must be > 0");
+    if (d->stencil != 0 && d->stencil != 1) return fail(nullptr, PTS_E_INVAL, "stencil must be 0 or 1");
+    if (d->stencil_tile < 0 || d->stencil_tile >= zstage_num_configs())
+        return fail(nullptr, PTS_E_INVAL, "stencil_tile out of range (pts_stencil_tiles)");
+    if (d->stencil_kz < 0) return fail(nullptr, PTS_E_INVAL, "stencil_kz must be >= 0");
     if (d->adjoint && ((d->variant != PTS_3D_V && d->variant != PTS_3D_VE_PERF) || d->precision != PTS_FP64 ||
                        d->single_pass))
         return fail(nullptr, PTS_E_INVAL,
@@ -497,6 +526,7 @@ int pts_create(const pts_desc* d, pts_ctx** out) {
     }
     c->mixed = d->precision == PTS_MIXED;
     c->fused = variant_fused(c->v) && d->single_pass != 0 && !c->mixed;
+    c->zs = (c->v == VE3D || c->v == VE3D_PERF || c->v == V3D) && !c->fused && !c->mixed && d->stencil == 0;
     if (c->mixed) {
         float** p32[] = {&c->m.dPt, &c->m.dVx, &c->m.dVy, &c->m.dVz, &c->m.dtxx, &c->m.dtyy, &c->m.dtzz, &c->m.dtxy,
                          &c->m.dtxz, &c->m.dtyz, &c->m.aP, &c->m.atxx, &c->m.atyy, &c->m.atzz, &c->m.atxy,
@@ -554,6 +584,7 @@ int pts_destroy(pts_ctx* c) {
     if (c->partials) cudaFree(c->partials);
     if (c->d_result) cudaFree(c->d_result);
     if (c->d_kerr) cudaFree(c->d_kerr);
+    if (c->d_incl) cudaFree(c->d_incl);
     if (c->h_result) cudaFreeHost(c->h_result);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -622,6 +653,39 @@ int pts_init_inclusion(pts_ctx* c, double mus0, double musi, double radius2, dou
     if (rc) return rc;
     for (double* p : c->owned) CK(cudaMemsetAsync(p, 0, (size_t)c->g.n * sizeof(double), c->stream));
     CK(launch_init_inclusion(c->v, c->g, c->f, c->n, mus0, musi, radius2, ebg, c->stream));
+    return PTS_OK;
+}
+
+int pts_init_inclusions(pts_ctx* c, const pts_inclusion* list, int32_t count, double mus0, double ebg) {
+    int rc = enter(c);
+    if (rc) return rc;
+    if (count < 0 || count > PTS_MAX_INCLUSIONS) return fail(c, PTS_E_INVAL, "inclusion count out of range");
+    if (count > 0 && !list) return fail(c, PTS_E_INVAL, "null inclusion list");
+    for (int32_t q = 0; q < count; ++q)
+        if (!std::isfinite(list[q].x) || !std::isfinite(list[q].y) || !std::isfinite(list[q].z) ||
+            !std::isfinite(list[q].r2))
+            return fail(c, PTS_E_INVAL, "inclusion " + std::to_string(q) + ": centre and r2 must be finite");
+    if (count > c->incl_cap) {
+        if (c->d_incl) {
+            CK(cudaStreamSynchronize(c->stream));
+            cudaFree(c->d_incl);
+            c->d_incl = nullptr;
+            c->incl_cap = 0;
+        }
+        if (cudaMalloc((void**)&c->d_incl, (size_t)count * sizeof(pts_inclusion)) != cudaSuccess) {
+            cudaGetLastError();
+            c->d_incl = nullptr;
+            return fail(c, PTS_E_NOMEM, "allocation of the inclusion list failed");
+        }
+        c->incl_cap = count;
+    }
+    if (count > 0) {
+        CK(cudaMemcpyAsync(c->d_incl, list, (size_t)count * sizeof(pts_inclusion), cudaMemcpyHostToDevice, c->stream));
+    }
+    for (double* p : c->owned) CK(cudaMemsetAsync(p, 0, (size_t)c->g.n * sizeof(double), c->stream));
+    CK(launch_init_inclusions(c->v, c->g, c->f, c->n, c->d_incl, count, mus0, ebg, c->stream));
+    // the caller's list is borrowed for the call only
+    CK(cudaStreamSynchronize(c->stream));
     return PTS_OK;
 }
 
@@ -722,8 +786,7 @@ int pts_apply_bc(pts_ctx* c) {
 int pts_compute_Pt_tau(pts_ctx* c) {
     int rc = enter(c);
     if (rc) return rc;
-    CK(launch_Pt_tau(c->v, c->g, c->f, c->n, ROLE_P | ROLE_TAU, !c->perf, c->stream));
-    return PTS_OK;
+    return Pt_tau(c, true);
 }
 
 int pts_compute_V_bc(pts_ctx* c) {

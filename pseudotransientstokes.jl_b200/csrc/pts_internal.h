@@ -106,6 +106,8 @@ cudaError_t launch_check(int variant, const Geom& g, const Fields64& f, const Nu
 int check_num_blocks(int variant, const Geom& g);
 cudaError_t launch_init_inclusion(int variant, const Geom& g, const Fields64& f, const Num& n, double mus0,
                                   double musi, double radius2, double ebg, cudaStream_t s);
+cudaError_t launch_init_inclusions(int variant, const Geom& g, const Fields64& f, const Num& n,
+                                   const pts_inclusion* d_inc, int count, double mus0, double ebg, cudaStream_t s);
 cudaError_t launch_smooth(int variant, const Geom& g, double* dst, const double* src, double fact, cudaStream_t s);
 cudaError_t launch_maxloc(int variant, const Geom& g, double* must, const double* mus, cudaStream_t s);
 cudaError_t launch_iter_params(int variant, const Geom& g, const Fields64& f, const Num& n, cudaStream_t s);
@@ -124,6 +126,14 @@ cudaError_t launch_fused3(int variant, const Geom& g, const Fields64& cur, const
                           bool store_divV, int* err, cudaStream_t s,
                           bool direct);
 inline bool variant_fused(int v) { return variant_is3d(v) && !variant_damped(v); }
+
+// ---- z-marching compute_Pt_τ! with TMA-staged planes (pts_zstage.cu): 3D_VE, 3D_VE_PERF,
+// 3D_V. `tile` selects a tile configuration (zstage_tile_info), `kz` the z-planes per
+// thread block; `err` is set if one of the kernel's bounded waits gave up.
+int zstage_num_configs();
+bool zstage_tile_info(int tile, int* ty, int* ring);
+cudaError_t launch_Pt_tau_zs(int variant, int tile, const Geom& g, const Fields64& f, const Num& n, int kz,
+                             bool store_divV, int* err, cudaStream_t s);
 
 // Message returned by pts_last_error(NULL) (for entry points without a context).
 void set_global_error(const char* msg);

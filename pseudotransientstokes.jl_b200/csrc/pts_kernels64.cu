@@ -7,7 +7,8 @@
 //
 // Kernels here are the straightforward one-thread-per-point forms (two launches per PT
 // iteration: compute_Pt_τ! and compute_V! + bc); the 3D visco-elastic hot path also has
-// the single-pass z-streaming kernel in pts_fused3d.cu.
+// the single-pass z-streaming kernel in pts_fused3d.cuh and the z-staged compute_Pt_τ! in
+// pts_zstage.cu.
 #include <cooperative_groups.h>
 
 #include <cfloat>
@@ -15,6 +16,7 @@
 #include <cstdlib>
 
 #include "pts_internal.h"
+#include "pts_expr64.cuh"
 
 namespace pts {
 namespace {
@@ -23,56 +25,9 @@ constexpr unsigned kFull = 0xffffffffu;
 
 // ------------------------------------------------------------------ expression helpers
 
-// Gr = Gdτ/(G*dt). When G*dt is exactly 1.0 the quotient is Gdτ itself (IEEE division by
-// one is exact), so the division is skipped; the result is the same bits either way.
-__device__ __forceinline__ double gr_of(double g, double gdt) {
-    if (gdt == 1.0) return g;
-    return g / gdt;
-}
-
-// Normal stress update. Perf form (Stokes3D_ve_perf.jl:71-73):
-//   (τ + τ_o*Gr + 2.0*Gdτ*(_dx*d)) / (1.0 + Gdτ/Mus + Gr),  Gr = Gdτ/(G*dt)
-// Role form (Stokes3D_ve_multixpu.jl:70-72): the same with (d/dx).
-// Viscous: the τ_o and Gr terms are absent.
-template <bool EL, bool PERF>
-__device__ __forceinline__ double tau_n(double t, double to, double g, double m, double gdt, double h, double ih,
-                                        double d) {
-    const double e = PERF ? (ih * d) : (d / h);
-    if (EL) {
-        const double Gr = gr_of(g, gdt);
-        return ((t + to * Gr) + (2.0 * g) * e) / ((1.0 + g / m) + Gr);
-    }
-    return (t + (2.0 * g) * e) / (1.0 + g / m);
-}
-
-// Shear stress update (Stokes3D_ve_perf.jl:74-76, Stokes3D_ve_multixpu.jl:73-75):
-//   (τ + τ_o*av_Gr + 2.0*av_Gdτ*(0.5*(_h1*d1 + _h2*d2))) / (1.0 + av_Gdτ/av_Mus + av_Gr)
-template <bool EL, bool PERF>
-__device__ __forceinline__ double tau_s(double t, double to, double ag, double am, double gdt, double h1, double ih1,
-                                        double d1, double h2, double ih2, double d2) {
-    const double s = PERF ? (ih1 * d1 + ih2 * d2) : (d1 / h1 + d2 / h2);
-    if (EL) {
-        const double Gr = gr_of(ag, gdt);
-        return ((t + to * Gr) + (2.0 * ag) * (0.5 * s)) / ((1.0 + ag / am) + Gr);
-    }
-    return (t + (2.0 * ag) * (0.5 * s)) / (1.0 + ag / am);
-}
-
-// Normal stress update with the denominator computed once per cell: τxx, τyy, τzz share
-// Gdτ and Mus at the cell centre, so (1.0 + Gdτ/Mus + Gr) and Gr are the same three times
-// (same operations, same bits as tau_n).
-template <bool EL, bool PERF>
-__device__ __forceinline__ double tau_n_den(double t, double to, double g, double Gr, double den, double h, double ih,
-                                            double d) {
-    const double e = PERF ? (ih * d) : (d / h);
-    if (EL) return ((t + to * Gr) + (2.0 * g) * e) / den;
-    return (t + (2.0 * g) * e) / den;
-}
-
-template <bool PERF>
-__device__ __forceinline__ double dsc(double d, double h, double ih) {
-    return PERF ? (ih * d) : (d / h);
-}
+// The stress expressions (gr_of, tau_n, tau_s, tau_n_den, dsc) live in pts_expr64.cuh,
+// shared with the z-staged kernels of pts_zstage.cu.
+using namespace expr;
 
 // ------------------------------------------------------------------ 3D kernels
 
@@ -1609,6 +1564,52 @@ __global__ void k_init_inclusion(Geom g, Fields64 f, Num n, double mus0, double 
     }
 }
 
+// create_inclusions! (Stokes2D_param.jl:83-99) for a list of circles (2D) or spheres (3D),
+// each with its own squared radius and viscosity: at each cell centre
+//   x = (ix-1)*dx + 0.5*dx - 0.5*lx   (y, z alike; inclusion centres in the same centred frame)
+//   rad2 = (x - Xi)^2 + (y - Yi)^2 [+ (z - Zi)^2],  inside when rad2 < r2,
+// Mus = the viscosity of the first inclusion the cell is inside, else mus0 (the reference's
+// loop breaks at the first hit). Velocities get the pure-shear ICs of k_init_inclusion.
+template <bool D3, bool IGG>
+__global__ void k_init_inclusions(Geom g, Fields64 f, Num n, const pts_inclusion* __restrict__ inc, int count,
+                                  double mus0, double ebg) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    if (i > nx || j > ny) return;
+    const idx_t c = gidx32(g, i, j, k);
+    if (i < nx && j < ny && k < (D3 ? nz : 1)) {
+        const double X = ((double)i * n.dx + 0.5 * n.dx) - 0.5 * n.lx;
+        const double Y = ((double)j * n.dy + 0.5 * n.dy) - 0.5 * n.ly;
+        const double Z = D3 ? ((double)k * n.dz + 0.5 * n.dz) - 0.5 * n.lz : 0.0;
+        double mu = mus0;
+        for (int q = 0; q < count; ++q) {
+            const double ax = X - __ldg(&inc[q].x), ay = Y - __ldg(&inc[q].y);
+            double rad2 = ax * ax + ay * ay;
+            if (D3) {
+                const double az = Z - __ldg(&inc[q].z);
+                rad2 = rad2 + az * az;
+            }
+            if (rad2 < __ldg(&inc[q].r2)) {
+                mu = __ldg(&inc[q].mus);
+                break;
+            }
+        }
+        f.Mus[c] = mu;
+    }
+    const double xv = IGG ? ((((double)i * n.dx + (-0.5 * n.dx)) + 0.5 * n.dx) - 0.5 * n.lx)
+                          : ((double)i * n.dx - 0.5 * n.lx);
+    if (j < ny && k < (D3 ? nz : 1)) f.Vx[c] = (-ebg) * xv;
+    if (D3) {
+        const double zv = IGG ? ((((double)k * n.dz + (-0.5 * n.dz)) + 0.5 * n.dz) - 0.5 * n.lz)
+                              : ((double)k * n.dz - 0.5 * n.lz);
+        if (i < nx && j < ny) f.Vz[c] = ebg * zv;
+    } else {
+        if (i < nx) f.Vy[c] = ebg * ((double)j * n.dy - 0.5 * n.ly);
+    }
+}
+
 // ICs of one batched-sweep instance (Stokes2D_param.jl:176-181 with one centred inclusion;
 // the box lx x ly of Stokes2D_ve_param.jl:99-102): the same operations as the oracle.
 __global__ void k2_init_sweep(Geom g, Fields64 f, Num n, double musi, double radius2, double rhogi, double ebg) {
@@ -1888,6 +1889,16 @@ cudaError_t launch_init_inclusion(int v, const Geom& g, const Fields64& f, const
     if (v == VE3D || v == V3D_DAMP) k_init_inclusion<true, true><<<gr, blk(), 0, s>>>(g, f, n, mus0, musi, radius2, ebg);
     else if (d3) k_init_inclusion<true, false><<<gr, blk(), 0, s>>>(g, f, n, mus0, musi, radius2, ebg);
     else k_init_inclusion<false, false><<<gr, blk(), 0, s>>>(g, f, n, mus0, musi, radius2, ebg);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_init_inclusions(int v, const Geom& g, const Fields64& f, const Num& n, const pts_inclusion* d_inc,
+                                   int count, double mus0, double ebg, cudaStream_t s) {
+    const bool d3 = variant_is3d(v);
+    const dim3 gr = grid_faces(g, d3);
+    if (v == VE3D || v == V3D_DAMP) k_init_inclusions<true, true><<<gr, blk(), 0, s>>>(g, f, n, d_inc, count, mus0, ebg);
+    else if (d3) k_init_inclusions<true, false><<<gr, blk(), 0, s>>>(g, f, n, d_inc, count, mus0, ebg);
+    else k_init_inclusions<false, false><<<gr, blk(), 0, s>>>(g, f, n, d_inc, count, mus0, ebg);
     return cudaGetLastError();
 }
 

@@ -217,6 +217,8 @@ int pts_check_noalloc(const pts_desc* d, const double* const fields[10], pts_che
         return fail(PTS_E_INVAL, "pts_check_noalloc supports the explicit-index variants (2D VE perf, 3D VE perf, 3D viscous)");
     const int nx = d->nx, ny = d->ny, nz = d3 ? d->nz : 1;
     if (nx < 3 || ny < 3 || (d3 && nz < 3)) return fail(PTS_E_INVAL, "each of nx, ny(, nz) must be >= 3");
+    if (!(d->lx > 0) || !(d->ly > 0) || (d3 && !(d->lz > 0)))
+        return fail(PTS_E_INVAL, "domain extents must be > 0");
     const int gx = (nx + 1 + 31) / 32, gy = (ny + 7) / 8;
     if ((int64_t)gx * gy > kMaxBlocks) {
         snprintf(msg, sizeof(msg),

@@ -1,0 +1,370 @@
+// pts_zstage.cu -- compute_Pt_τ! (3D) as a z-marching kernel whose input planes are
+// staged in shared memory by the tensor-memory accelerator (TMA).
+//
+// Reference: compute_Pt_τ! (scripts/stokes_3D/Stokes3D_ve_perf.jl:51-78) and the role
+// pair compute_P! + compute_τ! (Stokes3D_ve_multixpu.jl:57-77). The arithmetic is the
+// one-thread-per-point kernel's (pts_expr64.cuh, --fmad=false), operand for operand, so
+// the result is the same bits; only the way the operands reach the threads differs.
+//
+// Why: the one-thread-per-point kernel issues ~870 instructions per cell, half of them
+// address, bounds and constant-bank work around its ~50 scalar loads, and its memory
+// parallelism is capped by its registers. Here
+//  * a CTA owns a 32 x TY tile of cells (one warp per y-row, one cell per lane) and marches
+//    through a chunk of z-planes;
+//  * one producer warp issues, per plane, one 3D tensor copy per input array into a ring of
+//    R shared-memory slots (completion on an mbarrier per slot), so the bytes in flight do
+//    not depend on registers;
+//  * consumers read their operands from shared memory at compile-time offsets and carry
+//    the values of the previous plane (the -z neighbours) in registers, so each input value
+//    crosses HBM once and each cell reads 30 shared-memory words;
+//  * results go straight to global memory (every cell writes only its own Pt and τ, which
+//    no other CTA reads in this launch, so the update is in place).
+//
+// Slot layout of plane s (one tensor copy per array, zero fill outside the array):
+//   halo group, box (TX+4) x (TY+2) at (i0-2, j0-1):  Vx(s), Vy(s), Gdτ(s), Mus(s), Vz(s+1)
+//   point group, box TX x TY at (i0, j0):             Pt, τxx..τyz [, τxx_o..τyz_o] at s
+// The halo box starts two columns left of the tile so that its x offset stays a multiple
+// of 16 bytes (the TMA rule); the columns i0-1 .. i0+TX and rows j0-1 .. j0+TY are used.
+// The chunk's first stage is plane kb-1, halo group only: it primes the carried registers.
+//
+// Waits are bounded (2 s of %globaltimer): a wait that gives up sets the context's error
+// flag, the producer still waits (bounded) for every copy it issued, and the kernel ends.
+// No copy uses cluster multicast; every tensor map covers this GPU's own fields.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <cstring>
+
+#include "pts_expr64.cuh"
+#include "pts_internal.h"
+
+namespace pts {
+namespace zs {
+
+using namespace expr;
+
+constexpr int TX = 32;           // tile width: one lane per cell
+constexpr int NH = 5;            // halo-group arrays
+constexpr int NPMAX = 13;        // point-group arrays (visco-elastic)
+constexpr uint64_t kWaitNs = 2000000000ull;
+
+struct alignas(64) Maps {
+    CUtensorMap h[NH];     // Vx Vy Gdτ Mus Vz
+    CUtensorMap p[NPMAX];  // Pt τxx τyy τzz τxy τxz τyz [τ_o x6]
+};
+
+template <int TY, bool EL>
+struct Cfg {
+    static constexpr int HW = TX + 4;  // halo box width (elements)
+    static constexpr int HH = TY + 2;  // halo box rows
+    static constexpr int HBOX = HW * HH * 8;
+    static constexpr int HSTRIDE = (HBOX + 127) / 128 * 128;
+    static constexpr int NP = EL ? 13 : 7;
+    static constexpr int PBOX = TX * TY * 8;
+    static constexpr int SLOT = NH * HSTRIDE + NP * PBOX;
+};
+
+// ---- TMA / mbarrier primitives (no cluster multicast anywhere) ----
+__device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(saddr(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(saddr(b)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(saddr(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ uint64_t gtimer() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Bounded wait for the completion of the phase of parity `parity`; false if it gave up.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity) {
+    if (mbar_try(b, parity)) return true;
+    const uint64_t t0 = gtimer();
+    while (!mbar_try(b, parity))
+        if (gtimer() - t0 > kWaitNs) return false;
+    return true;
+}
+// One 3D tile of a tensor into shared memory, completion counted on mbarrier `b`.
+__device__ __forceinline__ void tma_load3(void* dst, const CUtensorMap* m, int x, int y, int z, uint64_t* b) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];" ::"r"(saddr(dst)),
+        "l"(m), "r"(x), "r"(y), "r"(z), "r"(saddr(b))
+        : "memory");
+}
+__device__ __forceinline__ void prefetch_map(const CUtensorMap* m) {
+    asm volatile("prefetch.tensormap [%0];" ::"l"(m) : "memory");
+}
+
+// compute_Pt_τ! over a 32 x TY tile and planes [kb, ke). Block: TY consumer warps + one
+// producer warp. R = slots in the shared-memory ring.
+template <bool EL, bool PERF, int TY, int R>
+__global__ void __launch_bounds__(32 * (TY + 1)) k3_Pt_tau_zs(const __grid_constant__ Maps maps, Geom g, Fields64 f,
+                                                               Num n, int kz, int store_divV, int* err) {
+    using C = Cfg<TY, EL>;
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+    uint64_t* full = (uint64_t*)(smem + (size_t)R * C::SLOT);
+    uint64_t* empty = full + R;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
+    const int kb = blockIdx.z * kz;
+    const int ke = min(kb + kz, g.nz);
+    const int nst = ke - kb + 1;  // stages: plane kb-1 (halo only), then kb .. ke-1
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < R; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], TY);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    if (warp == TY) {
+        // ---------------- producer: one elected lane issues every copy
+        if (lane != 0) return;
+        for (int q = 0; q < NH; ++q) prefetch_map(&maps.h[q]);
+        for (int q = 0; q < C::NP; ++q) prefetch_map(&maps.p[q]);
+        bool ok = true;
+        int issued = 0;
+        for (int t = 0; t < nst && ok; ++t) {
+            const int slot = t % R, use = t / R;
+            if (use > 0 && !mbar_wait(&empty[slot], (use - 1) & 1)) {
+                ok = false;
+                break;
+            }
+            const int s = kb - 1 + t;
+            unsigned char* base = smem + (size_t)slot * C::SLOT;
+            const uint32_t bytes = NH * C::HBOX + (t > 0 ? C::NP * C::PBOX : 0);
+            mbar_expect_tx(&full[slot], bytes);
+            tma_load3(base + 0 * C::HSTRIDE, &maps.h[0], i0 - 2, j0 - 1, s, &full[slot]);
+            tma_load3(base + 1 * C::HSTRIDE, &maps.h[1], i0 - 2, j0 - 1, s, &full[slot]);
+            tma_load3(base + 2 * C::HSTRIDE, &maps.h[2], i0 - 2, j0 - 1, s, &full[slot]);
+            tma_load3(base + 3 * C::HSTRIDE, &maps.h[3], i0 - 2, j0 - 1, s, &full[slot]);
+            tma_load3(base + 4 * C::HSTRIDE, &maps.h[4], i0 - 2, j0 - 1, s + 1, &full[slot]);
+            if (t > 0) {
+                unsigned char* pb = base + NH * C::HSTRIDE;
+#pragma unroll
+                for (int q = 0; q < C::NP; ++q) tma_load3(pb + q * C::PBOX, &maps.p[q], i0, j0, s, &full[slot]);
+            }
+            issued = t + 1;
+        }
+        if (!ok) atomicExch(err, 1);
+        // every copy issued must have landed before the CTA may end (bounded)
+        for (int t = (issued > R ? issued - R : 0); t < issued; ++t)
+            if (!mbar_wait(&full[t % R], (t / R) & 1)) {
+                atomicExch(err, 1);
+                break;
+            }
+        return;
+    }
+
+    // ---------------- consumers: warp = tile row, lane = tile column
+    const int i = i0 + lane, j = j0 + warp;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const bool in = i < nx && j < ny;
+    // tangential conditions of each stress point that do not depend on k
+    const bool jI = j >= 1 && j <= ny - 2, iI = i >= 1 && i <= nx - 2;
+    const bool cx = in && jI, cy = in && iI, czz = in && iI && jI;                   // τxx, τyy, τzz
+    const bool cxy = in && i >= 1 && j >= 1, cxz = in && i >= 1 && jI, cyz = in && iI && j >= 1;
+    const double gdt = n.gdt;
+
+    // halo-box offsets (elements) of this cell and its -x / -y neighbours
+    const int hc = (warp + 1) * C::HW + (lane + 2);
+    const int hxm = hc - 1, hym = hc - C::HW, hxp = hc + 1, hyp = hc + C::HW, hxym = hc - C::HW - 1;
+    const int pc = warp * TX + lane;
+
+    // registers carried from the previous plane (the -z neighbours)
+    double vx_m, vy_m, g_m, gx_m, gy_m, m_m, mx_m, my_m;  // plane k-1
+    double vz_c, vz_x, vz_y;                               // Vz at plane k: c, c-sx, c-sy
+
+    idx_t c = gidx32(g, i, j, kb);
+    const idx_t sz = (idx_t)g.pxy;
+    for (int t = 0; t < nst; ++t) {
+        const int slot = t % R;
+        if (!mbar_wait(&full[slot], (t / R) & 1)) {
+            atomicExch(err, 1);
+            return;
+        }
+        const double* H = (const double*)(smem + (size_t)slot * C::SLOT);
+        const double* hVx = H;
+        const double* hVy = H + C::HSTRIDE / 8;
+        const double* hG = H + 2 * (C::HSTRIDE / 8);
+        const double* hM = H + 3 * (C::HSTRIDE / 8);
+        const double* hVz = H + 4 * (C::HSTRIDE / 8);  // Vz of plane s+1
+        const double vx = hVx[hc], vy = hVy[hc], Gc = hG[hc], Mc = hM[hc];
+        const double Gx = hG[hxm], Gy = hG[hym], Mx = hM[hxm], My = hM[hym];
+        const double vzn = hVz[hc], vznx = hVz[hxm], vzny = hVz[hym];
+        if (t > 0 && in) {
+            const int k = kb + t - 1;
+            const double* P = H + NH * (C::HSTRIDE / 8);
+            const double dvx = hVx[hxp] - vx;
+            const double dvy = hVy[hyp] - vy;
+            const double dvz = vzn - vz_c;
+            if (PERF) {
+                f.Pt[c] = P[pc] - n.r * Gc * ((n._dx * dvx + n._dy * dvy) + n._dz * dvz);
+            } else {
+                const double dv = (dvx / n.dx + dvy / n.dy) + dvz / n.dz;
+                if (store_divV) f.divV[c] = dv;
+                f.Pt[c] = P[pc] - n.r * Gc * dv;
+            }
+            const bool kI = k >= 1 && k <= nz - 2, k1 = k >= 1;
+            const double* Po = P + 7 * (C::PBOX / 8);  // τ_o
+            constexpr int PS = C::PBOX / 8;
+            if ((cx && kI) || (cy && kI) || czz) {
+                const double Gr = EL ? gr_of(Gc, gdt) : 0.0;
+                const double den = EL ? ((1.0 + Gc / Mc) + Gr) : (1.0 + Gc / Mc);
+                if (cx && kI)
+                    f.txx[c] = tau_n_den<EL, PERF>(P[1 * PS + pc], EL ? Po[0 * PS + pc] : 0.0, Gc, Gr, den, n.dx,
+                                                   n._dx, dvx);
+                if (cy && kI)
+                    f.tyy[c] = tau_n_den<EL, PERF>(P[2 * PS + pc], EL ? Po[1 * PS + pc] : 0.0, Gc, Gr, den, n.dy,
+                                                   n._dy, dvy);
+                if (czz)
+                    f.tzz[c] = tau_n_den<EL, PERF>(P[3 * PS + pc], EL ? Po[2 * PS + pc] : 0.0, Gc, Gr, den, n.dz,
+                                                   n._dz, dvz);
+            }
+            // τxy on edge (x-face i, y-face j, cell k): i in [1,nx-1], j in [1,ny-1], k in [1,nz-2]
+            if (cxy && kI) {
+                const double ag = (((hG[hxym] + Gy) + Gx) + Gc) * 0.25;
+                const double am = (((hM[hxym] + My) + Mx) + Mc) * 0.25;
+                f.txy[c] = tau_s<EL, PERF>(P[4 * PS + pc], EL ? Po[3 * PS + pc] : 0.0, ag, am, gdt, n.dy, n._dy,
+                                           vx - hVx[hym], n.dx, n._dx, vy - hVy[hxm]);
+            }
+            // τxz on edge (x-face i, cell j, z-face k): i in [1,nx-1], j in [1,ny-2], k in [1,nz-1]
+            if (cxz && k1) {
+                const double ag = (((gx_m + g_m) + Gx) + Gc) * 0.25;
+                const double am = (((mx_m + m_m) + Mx) + Mc) * 0.25;
+                f.txz[c] = tau_s<EL, PERF>(P[5 * PS + pc], EL ? Po[4 * PS + pc] : 0.0, ag, am, gdt, n.dz, n._dz,
+                                           vx - vx_m, n.dx, n._dx, vz_c - vz_x);
+            }
+            // τyz on edge (cell i, y-face j, z-face k): i in [1,nx-2], j in [1,ny-1], k in [1,nz-1]
+            if (cyz && k1) {
+                const double ag = (((gy_m + g_m) + Gy) + Gc) * 0.25;
+                const double am = (((my_m + m_m) + My) + Mc) * 0.25;
+                f.tyz[c] = tau_s<EL, PERF>(P[6 * PS + pc], EL ? Po[5 * PS + pc] : 0.0, ag, am, gdt, n.dz, n._dz,
+                                           vy - vy_m, n.dy, n._dy, vz_c - vz_y);
+            }
+            c += sz;
+        }
+        // this plane becomes the -z neighbour of the next
+        vx_m = vx, vy_m = vy, g_m = Gc, gx_m = Gx, gy_m = Gy, m_m = Mc, mx_m = Mx, my_m = My;
+        vz_c = vzn, vz_x = vznx, vz_y = vzny;
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[slot]);
+    }
+}
+
+// ---- host side ----
+
+PFN_cuTensorMapEncodeTiled_v12000 encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
+// A field of the unified layout as a px x py x pz FP64 tensor, copied in bw x bh x 1 boxes.
+bool encode(CUtensorMap* m, const double* base, const Geom& g, int bw, int bh) {
+    auto fn = encoder();
+    if (!fn || !base) return false;
+    cuuint64_t dims[3] = {(cuuint64_t)g.px, (cuuint64_t)g.py, (cuuint64_t)g.pz};
+    cuuint64_t strides[2] = {(cuuint64_t)g.px * 8, (cuuint64_t)g.pxy * 8};
+    cuuint32_t box[3] = {(cuuint32_t)bw, (cuuint32_t)bh, 1};
+    cuuint32_t es[3] = {1, 1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void*)base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <bool EL, bool PERF, int TY, int R>
+cudaError_t launch_cfg(const Geom& g, const Fields64& f, const Num& n, int kz, bool store_divV, int* err,
+                       cudaStream_t s) {
+    using C = Cfg<TY, EL>;
+    Maps maps;
+    memset(&maps, 0, sizeof(maps));
+    const double* hsrc[NH] = {f.Vx, f.Vy, f.Gdt, f.Mus, f.Vz};
+    for (int q = 0; q < NH; ++q)
+        if (!encode(&maps.h[q], hsrc[q], g, C::HW, C::HH)) return cudaErrorInvalidValue;
+    const double* psrc[NPMAX] = {f.Pt,    f.txx,   f.tyy,   f.tzz,   f.txy,   f.txz,  f.tyz,
+                                 f.txx_o, f.tyy_o, f.tzz_o, f.txy_o, f.txz_o, f.tyz_o};
+    for (int q = 0; q < C::NP; ++q)
+        if (!encode(&maps.p[q], psrc[q], g, TX, TY)) return cudaErrorInvalidValue;
+    const size_t smem = 128 + (size_t)R * C::SLOT + 2 * R * sizeof(uint64_t);
+    static bool attr[64] = {};  // per device: the opt-in to more than 48 KB of shared memory
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!attr[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(k3_Pt_tau_zs<EL, PERF, TY, R>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr[dev] = true;
+    }
+    const dim3 grid((g.nx + TX - 1) / TX, (g.ny + TY - 1) / TY, (g.nz + kz - 1) / kz);
+    k3_Pt_tau_zs<EL, PERF, TY, R><<<grid, 32 * (TY + 1), smem, s>>>(maps, g, f, n, kz, store_divV ? 1 : 0, err);
+    return cudaGetLastError();
+}
+
+// Tile configurations: (tile height TY, ring slots R). Shared memory per block for the
+// visco-elastic form: 8x2 83 KB (2 blocks/SM), 4x2 45 KB (5), 4x3 67 KB (3), 8x3 124 KB (1).
+constexpr int kTiles[][2] = {{8, 2}, {4, 2}, {4, 3}, {8, 3}};
+constexpr int kNumTiles = (int)(sizeof(kTiles) / sizeof(kTiles[0]));
+
+template <bool EL, bool PERF>
+cudaError_t launch_form(int cfg, const Geom& g, const Fields64& f, const Num& n, int kz, bool sd, int* err,
+                        cudaStream_t s) {
+    switch (cfg) {
+        case 0: return launch_cfg<EL, PERF, kTiles[0][0], kTiles[0][1]>(g, f, n, kz, sd, err, s);
+        case 1: return launch_cfg<EL, PERF, kTiles[1][0], kTiles[1][1]>(g, f, n, kz, sd, err, s);
+        case 2: return launch_cfg<EL, PERF, kTiles[2][0], kTiles[2][1]>(g, f, n, kz, sd, err, s);
+        case 3: return launch_cfg<EL, PERF, kTiles[3][0], kTiles[3][1]>(g, f, n, kz, sd, err, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace zs
+
+int zstage_num_configs() { return zs::kNumTiles; }
+
+bool zstage_tile_info(int tile, int* ty, int* ring) {
+    if (tile < 0 || tile >= zs::kNumTiles) return false;
+    if (ty) *ty = zs::kTiles[tile][0];
+    if (ring) *ring = zs::kTiles[tile][1];
+    return true;
+}
+
+cudaError_t launch_Pt_tau_zs(int variant, int cfg, const Geom& g, const Fields64& f, const Num& n, int kz,
+                             bool store_divV, int* err, cudaStream_t s) {
+    if (kz <= 0) kz = 32;
+    switch (variant) {
+        case VE3D_PERF: return zs::launch_form<true, true>(cfg, g, f, n, kz, false, err, s);
+        case V3D: return zs::launch_form<false, true>(cfg, g, f, n, kz, false, err, s);
+        case VE3D: return zs::launch_form<true, false>(cfg, g, f, n, kz, store_divV, err, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace pts

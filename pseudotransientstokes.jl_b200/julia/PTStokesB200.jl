@@ -29,7 +29,8 @@ struct Desc
     r::Float64; Re::Float64; CFL::Float64
     max_l::Float64; eps::Float64; iter_max::Float64
     mixed_inner::Int32; single_pass::Int32; adjoint::Int32
-    reserved::NTuple{5,Int32}
+    stencil::Int32; stencil_tile::Int32; stencil_kz::Int32
+    reserved::NTuple{2,Int32}
 end
 
 struct Check
@@ -59,9 +60,10 @@ end
 A device context for one problem (the scripts' `Stokes2D_()`/`Stokes3D_()` state).
 """
 function Ctx(variant::Variant, nx, ny, nz=1; lx=10.0, ly=10.0, lz=10.0, G=1.0, dt=1.0, r=1.0, Re, CFL,
-             nout=200, ε=1e-8, iterMax=2e5, max_l=0.0, precision=0, single_pass=0, adjoint=0)
+             nout=200, ε=1e-8, iterMax=2e5, max_l=0.0, precision=0, single_pass=0, adjoint=0, stencil=0,
+             stencil_tile=0, stencil_kz=0)
     d = Desc(Int32(variant), Int32(precision), nx, ny, nz, nout, lx, ly, lz, G, dt, r, Re, CFL, max_l, ε, iterMax,
-             0, single_pass, adjoint, ntuple(_ -> Int32(0), 5))
+             0, single_pass, adjoint, stencil, stencil_tile, stencil_kz, ntuple(_ -> Int32(0), 2))
     out = Ref{Ptr{Cvoid}}(C_NULL)
     check(nothing, ccall((:pts_create, libpts), Cint, (Ref{Desc}, Ref{Ptr{Cvoid}}), d, out))
     ctx = Ctx(out[])
@@ -211,20 +213,7 @@ function top_vz(logμ::Array{Float64,3}, fwd::Ctx, adj::Ctx, Vwall)
     return Vz[2:end-1, 2:end-1, end-1]
 end
 
-# The ChainRulesCore rule a maintainer would add next to the shim (ChainRulesCore is not a
-# dependency of this file):
-#
-#   function ChainRulesCore.rrule(::typeof(top_vz), logμ, fwd, adj, Vwall)
-#       v = top_vz(logμ, fwd, adj, Vwall)
-#       function top_vz_pullback(v̄)
-#           init_inclusion!(adj; μs0=1.0, μsi=1.0, radius2=0.0, εbg=0.0)    # zero state
-#           set_field!(adj, :Mus, exp.(logμ)); compute_maxloc!(adj); compute_iter_params!(adj)
-#           Fz = zeros(field_shape(adj, :Fz)...); Fz[:, :, end] .= unthunk(v̄)
-#           set_field!(adj, :Fz, Fz); solve!(adj)
-#           gradient_logmu!(fwd, adj)
-#           return NoTangent(), get_field(fwd, :grad), NoTangent(), NoTangent(), NoTangent()
-#       end
-#       return v, top_vz_pullback
-#   end
+# Reverse rules for top_vz (and its visco-elastic time-loop twin top_vz_ve) are the
+# ChainRulesCore.rrule methods of PTStokesB200ChainRules.jl, next to this file.
 
 end # module

@@ -53,7 +53,8 @@ class PtsDesc(ctypes.Structure):
         ("r", ctypes.c_double), ("Re", ctypes.c_double), ("CFL", ctypes.c_double),
         ("max_l", ctypes.c_double), ("eps", ctypes.c_double), ("iter_max", ctypes.c_double),
         ("mixed_inner", ctypes.c_int32), ("single_pass", ctypes.c_int32), ("adjoint", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 5),
+        ("stencil", ctypes.c_int32), ("stencil_tile", ctypes.c_int32), ("stencil_kz", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 2),
     ]
 
 
@@ -68,6 +69,11 @@ class PtsCheck(ctypes.Structure):
 class PtsSolveInfo(ctypes.Structure):
     _fields_ = [("iters", ctypes.c_int64), ("converged", ctypes.c_int32), ("nchecks", ctypes.c_int32),
                 ("last", PtsCheck)]
+
+
+class PtsInclusion(ctypes.Structure):
+    _fields_ = [("x", ctypes.c_double), ("y", ctypes.c_double), ("z", ctypes.c_double), ("r2", ctypes.c_double),
+                ("mus", ctypes.c_double)]
 
 
 class PtsBatchInstance(ctypes.Structure):
@@ -96,6 +102,8 @@ _DP = ctypes.c_void_p  # double* (host or device), passed as an address
 
 SIGNATURES = {
     "pts_abi_version": ([], ctypes.c_int),
+    "pts_stencil_tiles": ([], ctypes.c_int),
+    "pts_stencil_tile_info": ([_I32, ctypes.POINTER(_I32), ctypes.POINTER(_I32)], ctypes.c_int),
     "pts_last_error": ([_P], ctypes.c_char_p),
     "pts_create": ([ctypes.POINTER(PtsDesc), ctypes.POINTER(_P)], ctypes.c_int),
     "pts_destroy": ([_P], ctypes.c_int),
@@ -107,6 +115,7 @@ SIGNATURES = {
     "pts_set_field_device": ([_P, _I32, _DP, _I64], ctypes.c_int),
     "pts_get_field_device": ([_P, _I32, _DP, _I64], ctypes.c_int),
     "pts_init_inclusion": ([_P, _D, _D, _D, _D], ctypes.c_int),
+    "pts_init_inclusions": ([_P, ctypes.POINTER(PtsInclusion), _I32, _D, _D], ctypes.c_int),
     "pts_smooth": ([_P, _I32, _D], ctypes.c_int),
     "pts_compute_maxloc": ([_P], ctypes.c_int),
     "pts_compute_iter_params": ([_P], ctypes.c_int),

@@ -8,8 +8,10 @@ J = ½‖Vz(top) − Vobs‖². ``ViscousAdjoint`` runs the forward solve, the t
 all on the device (``pts_gradient_logmu`` in include/ptstokes.h); ``ViscoElasticAdjoint``
 does the same for nt Maxwell visco-elastic steps with per-step checkpoints. ``TopVz`` wraps the
 same steps as a ``torch.autograd.Function`` of log μ (the viscosity the solver uses, after
-any smoothing). ``inclusion_set``, ``viscosity_field`` and ``lognormal_factor`` draw the
-seeded 20-inclusion field and its log-normal perturbation.
+any smoothing). ``inclusion_set`` draws the seeded 20-inclusion set, which
+``Solver.init_inclusions`` turns into the viscosity field on the device (``viscosity_field``
+is the same field computed on the host); ``lognormal_factor`` draws the log-normal
+perturbation of the synthetic observations.
 """
 import numpy as np
 
@@ -27,22 +29,37 @@ def inclusion_set(count=20, seed=1855, box=(10.0, 10.0, 10.0), radius=(0.3, 0.8)
     return out
 
 
+def inclusion_array(inclusions, box=(10.0, 10.0, 10.0)):
+    """The (count, 5) float64 rows [x, y, z, r2, mus] of pts_init_inclusions: centres in the
+    scripts' centred frame (x - lx/2, as Stokes2D_param.jl's Xi, Yi), squared radii and
+    viscosities 10**log10_mu."""
+    out = np.zeros((len(inclusions), 5), dtype=np.float64)
+    for q, inc in enumerate(inclusions):
+        c = inc["centre"]
+        out[q, 0:3] = [c[0] - 0.5 * box[0], c[1] - 0.5 * box[1], (c[2] if len(c) > 2 else 0.5 * box[2]) - 0.5 * box[2]]
+        out[q, 3] = inc["radius"] * inc["radius"]
+        out[q, 4] = 10.0 ** inc["log10_mu"]
+    return out
+
+
 def viscosity_field(nx, ny, nz, inclusions, box=(10.0, 10.0, 10.0), mus0=1.0):
-    """Cell-centred viscosity (nx, ny, nz), column-major: mus0, and 10**log10_mu inside each
-    sphere (cell centre strictly inside; a later sphere overwrites an earlier one)."""
+    """Cell-centred viscosity (nx, ny, nz), column-major, on the host: the same operations as
+    pts_init_inclusions (create_inclusions!, Stokes2D_param.jl:83-99, in 3D): at the cell
+    centre x = (ix-1)*dx + 0.5*dx - 0.5*lx, the first inclusion with
+    (x-Xi)^2 + (y-Yi)^2 + (z-Zi)^2 < r2 gives 10**log10_mu, else mus0."""
     lx, ly, lz = box
     dx, dy, dz = lx / nx, ly / ny, lz / nz
+    rows = inclusion_array(inclusions, box)
+    x = (np.arange(nx) * dx + 0.5 * dx) - 0.5 * lx
+    y = (np.arange(ny) * dy + 0.5 * dy) - 0.5 * ly
+    z = (np.arange(nz) * dz + 0.5 * dz) - 0.5 * lz
     mus = np.full((nx, ny, nz), mus0, dtype=np.float64, order="F")
-    for inc in inclusions:
-        (cx, cy, cz), r = inc["centre"], inc["radius"]
-        lo = [max(0, int(np.floor((c - r) / h)) - 1) for c, h in ((cx, dx), (cy, dy), (cz, dz))]
-        hi = [min(n, int(np.ceil((c + r) / h)) + 1) for c, h, n in ((cx, dx, nx), (cy, dy, ny), (cz, dz, nz))]
-        x = (np.arange(lo[0], hi[0]) + 0.5) * dx - cx
-        y = (np.arange(lo[1], hi[1]) + 0.5) * dy - cy
-        z = (np.arange(lo[2], hi[2]) + 0.5) * dz - cz
-        inside = (x[:, None, None] ** 2 + y[None, :, None] ** 2 + z[None, None, :] ** 2) < r * r
-        sub = mus[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]]
-        sub[inside] = 10.0 ** inc["log10_mu"]
+    # the first hit wins: apply the list backwards, each inclusion overwriting the later ones
+    for xi, yi, zi, r2, mu in rows[::-1]:
+        ax, ay, az = x - xi, y - yi, z - zi
+        rad2 = (ax * ax)[:, None, None] + (ay * ay)[None, :, None]
+        rad2 = rad2 + (az * az)[None, None, :]
+        mus[rad2 < r2] = mu
     return mus
 
 
@@ -88,12 +105,39 @@ class ViscousAdjoint:
         self.mus = f.get("Mus")
         return self
 
+    def set_inclusions(self, inclusions, nsmooth=10, box=(10.0, 10.0, 10.0)):
+        """Mus built on the device from a list of spheres (``inclusion_set`` dicts; the first
+        sphere a cell centre is inside gives its viscosity, else 1), then smoothed nsmooth
+        times there: no host-built field crosses to the device. ``self.mus`` is a host copy."""
+        import torch
+
+        f = self.fwd
+        f.init_inclusions(inclusion_array(inclusions, box), mus0=1.0, ebg=self.ebg)
+        if nsmooth:
+            f.smooth(nsmooth, 1.0)
+        self.mus = f.get("Mus")
+        t = torch.empty(self.mus.size, dtype=torch.float64, device="cuda")
+        f.get_device("Mus", t.data_ptr(), t.numel())
+        self._mus_dev, self._mus_src = t, self.mus
+        return self
+
+    def _load_mus(self, s):
+        """Mus of context s = the current viscosity: a device-to-device copy while ``self.mus``
+        is the field the device copy was made from, else an upload of ``self.mus``."""
+        import torch
+
+        if getattr(self, "_mus_src", None) is not self.mus:
+            self._mus_dev = torch.from_numpy(np.ascontiguousarray(self.mus.ravel(order="F"))).to("cuda")
+            self._mus_src = self.mus
+        torch.cuda.synchronize()
+        s.set_device("Mus", self._mus_dev.data_ptr(), self._mus_dev.numel())
+
     def forward(self):
         """The forward PT solve from the pure-shear initial state (walls and ICs, Mus, the
         local-max viscosity and the iteration parameters); returns its outcome (pts_solve)."""
         f = self.fwd
         f.init_inclusion(1.0, 1.0, 0.0, self.ebg)
-        f.set("Mus", self.mus)
+        self._load_mus(f)
         f.compute_maxloc()
         f.compute_iter_params()
         return f.solve()
@@ -105,7 +149,7 @@ class ViscousAdjoint:
         """The transposed solve with the momentum source dJ/dVz on the top interior plane."""
         a = self.adj
         a.init_inclusion(1.0, 1.0, 0.0, 0.0)  # every field zero; walls and ghosts zero
-        a.set("Mus", self.mus)
+        self._load_mus(a)
         a.compute_maxloc()
         a.compute_iter_params()
         Fz = np.zeros(a.shape("Fz"), order="F")
@@ -154,11 +198,14 @@ class ViscoElasticAdjoint:
         self.adj.close()
 
     set_viscosity = ViscousAdjoint.set_viscosity
+    set_inclusions = ViscousAdjoint.set_inclusions
     top_vz = ViscousAdjoint.top_vz
+
+    _load_mus = ViscousAdjoint._load_mus
 
     def _prepare(self, s, ebg):
         s.init_inclusion(1.0, 1.0, 0.0, ebg)
-        s.set("Mus", self.mus)
+        self._load_mus(s)
         s.compute_maxloc()
         s.compute_iter_params()
 

@@ -62,7 +62,7 @@ class Solver:
         self.variant = variant
         self.ndim = 3 if variant.startswith("3d") else 2
         p = dict(lx=10.0, ly=10.0, lz=10.0, xi=1.0, mus0=1.0, G=1.0, max_l=0.0, mixed_inner=0, single_pass=0,
-                 adjoint=0)
+                 adjoint=0, stencil=0, stencil_tile=0, stencil_kz=0)
         p.update(VARIANT_DEFAULTS[variant])
         p.update(kw)
         self.p = p
@@ -80,6 +80,9 @@ class Solver:
         d.mixed_inner = int(p["mixed_inner"])
         d.single_pass = int(p["single_pass"])
         d.adjoint = int(p["adjoint"])
+        d.stencil = int(p["stencil"])
+        d.stencil_tile = int(p["stencil_tile"])
+        d.stencil_kz = int(p["stencil_kz"])
         self.desc = d
         ctx = ctypes.c_void_p()
         check(self.lib, None, self.lib.pts_create(ctypes.byref(d), ctypes.byref(ctx)))
@@ -138,6 +141,17 @@ class Solver:
     # ---------------------------------------------------------------- set-up
     def init_inclusion(self, mus0=1.0, musi=1e-3, radius2=1.0, ebg=1.0):
         self._ck(self.lib.pts_init_inclusion(self.ctx, mus0, musi, radius2, ebg))
+
+    def init_inclusions(self, rows, mus0=1.0, ebg=1.0):
+        """create_inclusions! (Stokes2D_param.jl:83-99) on the device for a list of inclusions:
+        ``rows`` is (count, 5) [x, y, z, r2, mus], centres relative to the domain centre
+        (``ptstokes.adjoint.inclusion_array``); the first inclusion a cell centre is inside
+        gives its viscosity, else mus0. Velocities get the pure-shear ICs, the rest zero."""
+        rows = np.asarray(rows, dtype=np.float64).reshape(-1, 5)
+        arr = (_abi.PtsInclusion * max(len(rows), 1))()
+        for q, (x, y, z, r2, mu) in enumerate(rows):
+            arr[q] = _abi.PtsInclusion(x, y, z, r2, mu)
+        self._ck(self.lib.pts_init_inclusions(self.ctx, arr, len(rows), mus0, ebg))
 
     def smooth(self, nsweeps=10, fact=1.0):
         self._ck(self.lib.pts_smooth(self.ctx, nsweeps, fact))

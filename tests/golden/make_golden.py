@@ -12,7 +12,7 @@ column-major bytes) and writes each as JSON with exact hex floats, plus the run
 that produced it. It reads the reference checkout, so it runs only where that
 checkout exists; the JSON files it writes are committed.
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py /path/to/reference   (or set PTS_REFERENCE_DIR)
 """
 import hashlib
 import json
@@ -111,5 +111,13 @@ def main(ref_root):
         print("wrote", dst)
 
 
+def reference_dir():
+    """The reference checkout: the first argument, else $PTS_REFERENCE_DIR."""
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PTS_REFERENCE_DIR")
+    if not ref:
+        sys.exit("usage: python tests/golden/make_golden.py /path/to/reference  (or set PTS_REFERENCE_DIR)")
+    return ref
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    main(reference_dir())

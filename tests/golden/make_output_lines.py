@@ -1,7 +1,7 @@
 """Sample lines of the reference's own output files (printed by Julia's println), kept as a
 fixture for the output writers' number formatting. Run from the repository root:
 
-    python tests/golden/make_output_lines.py /root/reference
+    python tests/golden/make_output_lines.py /path/to/reference   (or set PTS_REFERENCE_DIR)
 
 The fixture keeps every line of the short files (the iteration counts to tolerance per grid
 size) and the first and last lines of the long ones.
@@ -23,5 +23,13 @@ def main(ref):
     print(dst, sum(len(v) for v in out.values()), "lines")
 
 
+def reference_dir():
+    """The reference checkout: the first argument, else $PTS_REFERENCE_DIR."""
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PTS_REFERENCE_DIR")
+    if not ref:
+        sys.exit("usage: python tests/golden/make_output_lines.py /path/to/reference  (or set PTS_REFERENCE_DIR)")
+    return ref
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    main(reference_dir())

@@ -131,12 +131,13 @@ def test_visco_elastic_gradient_kernel_equals_the_oracle(gpu_lib, add):
 def test_visco_elastic_gradient_matches_central_differences(gpu_lib):
     from ptstokes.adjoint import ViscoElasticAdjoint, inclusion_set, lognormal_factor, viscosity_field
     n = (18, 17, 16)
-    mus = viscosity_field(*n, inclusion_set(seed=1855, log10_mu=(-2.0, 2.0)))
+    incl = inclusion_set(seed=1855, log10_mu=(-2.0, 2.0))
+    mus = viscosity_field(*n, incl)
     p = ViscoElasticAdjoint(*n, nt=3, lib=gpu_lib, eps=1e-12, nout=100, iter_max=1e6)
     p.set_viscosity(mus * lognormal_factor(n, seed=1856), nsmooth=10)
     p.forward()
     vobs = p.top_vz()
-    p.set_viscosity(mus, nsmooth=10)
+    p.set_inclusions(incl, nsmooth=10)  # the same field, built on the device
     J0, g, fo, ao = p.misfit_gradient(vobs)
     assert all(r["converged"] for r in fo + ao)
     mus0 = p.mus.copy()
@@ -197,12 +198,18 @@ def test_transposed_system_dot_product_on_the_gpu(gpu_lib):
 
 def _problem(gpu_lib, n, seed=1855):
     from ptstokes.adjoint import ViscousAdjoint, inclusion_set, lognormal_factor, viscosity_field
-    mus = viscosity_field(*n, inclusion_set(seed=seed))
+    incl = inclusion_set(seed=seed)
+    mus = viscosity_field(*n, incl)
     p = ViscousAdjoint(*n, lib=gpu_lib, eps=1e-12, nout=100, iter_max=1e6)
     p.set_viscosity(mus * lognormal_factor(n, seed=seed + 1), nsmooth=10)
     p.forward()
     vobs = p.top_vz()
+    # the field of the gradient is built on the device; the host path gives the same bits
+    p.set_inclusions(incl, nsmooth=10)
+    dev = p.mus.copy()
     p.set_viscosity(mus, nsmooth=10)
+    assert np.array_equal(p.mus, dev)
+    p.set_inclusions(incl, nsmooth=10)
     return p, vobs
 
 

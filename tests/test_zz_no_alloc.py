@@ -18,7 +18,10 @@ CHECK_KEYS = ("err", "norm_Rx", "norm_Ry", "norm_Rz", "norm_divV", "Vmin", "Vmax
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("variant,dims", [("3d_ve_perf", (41, 37, 33)), ("3d_v", (35, 33, 31)),
-                                          ("2d_ve_perf", (63, 47))])
+                                          ("2d_ve_perf", (63, 47)),
+                                          # 2 x 32 tiles per plane: 64 z-blocks for 200 planes, so each
+                                          # block reduces several strided planes
+                                          ("3d_v", (63, 255, 200))])
 def test_noalloc_check_matches_the_context_check(gpu_lib, variant, dims):
     import torch
 
@@ -71,3 +74,9 @@ def test_noalloc_rejects_sizes_beyond_its_fixed_scratch():
     d.variant = _abi.VARIANTS["3d_ve"]
     d.nx = d.ny = 63
     assert lib.pts_check_noalloc(ctypes.byref(d), ptrs, ctypes.c_void_p(16), None) == _abi.PTS_E_INVAL
+    # domain extents that would make the 1/dx factors infinite or NaN
+    d.variant = _abi.VARIANTS["3d_ve_perf"]
+    for lx, lz in ((0.0, 10.0), (-1.0, 10.0), (float("nan"), 10.0), (10.0, 0.0)):
+        d.lx, d.lz = lx, lz
+        assert lib.pts_check_noalloc(ctypes.byref(d), ptrs, ctypes.c_void_p(16), None) == _abi.PTS_E_INVAL
+        assert b"extents" in lib.pts_last_error(None)
