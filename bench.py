@@ -378,9 +378,13 @@ def run_ours(args, ws, rank, local, pg):
 
     launches = args.steps * (2 * nout + 2) if args.precision == "fp64" else args.steps * (2 * nout + 3)
     s.close()
-    ttt = None
+    ttt = ttt2 = incl = None
     if args.ttt_n > 0:
-        ttt = time_to_tol(args, stream_cls=torch.cuda.ExternalStream)
+        ttt = time_to_tol(args, args.ttt_n, stream_cls=torch.cuda.ExternalStream)
+    if args.ttt_n2 > 0:
+        ttt2 = time_to_tol(args, args.ttt_n2, stream_cls=torch.cuda.ExternalStream)
+    if args.incl_default_n > 0:
+        incl = inclusions_block(args.incl_default_n, args.log10_range, rank, clocks_too=False)
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": ws, "steps": args.steps,
@@ -400,7 +404,7 @@ def run_ours(args, ws, rank, local, pg):
                          "other_kernel": {"name": "k3_V_bc", "ms": round(ms_B, 4),
                                           "achieved": round(14 * n ** 3 * 8 / (ms_B / 1e3) / 1e9, 1)}},
             "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clocks,
-            "time_to_tol": ttt,
+            "time_to_tol": ttt, "time_to_tol_small": ttt2, "inclusions_20": incl,
         }
         print(json.dumps(line), flush=True)
 
@@ -640,23 +644,20 @@ def adjoint_ve(args, n, mus, incl, pert, delta, rank):
                                   "rel_err": abs(dd_adj - dd_fd) / max(abs(dd_fd), 1e-300)}}
 
 
-def run_inclusions(args, ws, rank, local):
-    """Mixed precision on the 20-inclusion 3D viscous problem at `--incl-n`³ (viscosity =
-    matrix 1 plus 20 seeded spheres, radii U[0.3,0.8], log10 μ U[-L,L], smoothed 10x):
-    time to err <= 1e-8 in plain FP64 and with FP32 inner sweeps + FP64 defect correction,
-    same problem and check; per-field L2 and max errors of the mixed solution against the
-    FP64 one."""
-    import numpy as np
+def inclusions_block(n, L, rank, clocks_too=True):
+    """Mixed precision on the 20-inclusion 3D viscous problem at n^3 (viscosity = matrix 1
+    plus 20 seeded spheres, radii U[0.3,0.8], log10 μ U[-L,L], built on the device by
+    pts_init_inclusions and smoothed 10x there): time to err <= 1e-8 in plain FP64 and with
+    FP32 inner sweeps + FP64 defect correction, same problem and check; per-field L2 and max
+    errors of the mixed solution against the FP64 one."""
     import torch
 
     import ptstokes
     from ptstokes.adjoint import inclusion_array, inclusion_set
 
-    torch.cuda.set_device(local)
-    n, L = args.incl_n, args.log10_range
     rows = inclusion_array(inclusion_set(seed=1855 + rank, log10_mu=(-L, L)))
     out, fields = {}, {}
-    clk = ClockSampler(local)
+    clk = ClockSampler(torch.cuda.current_device())
     clk.start()
     for prec in ("fp64", "mixed"):
         s = ptstokes.Solver("3d_v", n, n, n, precision=prec, eps=1e-8, nout=200, iter_max=4e5)
@@ -673,26 +674,41 @@ def run_inclusions(args, ws, rank, local):
         b.record(st)
         b.synchronize()
         sec = a.elapsed_time(b) / 1e3
-        out[prec] = {"seconds": round(sec, 3), "iters": r["iters"], "converged": r["converged"], "err": r["last"]["err"]}
-        fields[prec] = {k: s.get(k) for k in ("Pt", "Vx", "Vy", "Vz", "txx", "tyy", "tzz", "txy", "txz", "tyz")}
+        out[prec] = {"seconds": round(sec, 3), "iters": r["iters"], "converged": r["converged"], "err": r["last"]["err"],
+                     "T_eff_GBs": round(23 * n ** 3 * 8 * r["iters"] / sec / 1e9, 1)}
+        fields[prec] = device_fields(s)
         s.close()
     clocks = clk.stop()
-    errs = {}
-    for k, ref in fields["fp64"].items():
-        d = fields["mixed"][k] - ref
-        errs[k] = {"l2_rel": float(np.linalg.norm(d) / max(np.linalg.norm(ref), 1e-300)),
-                   "max_rel": float(np.abs(d).max() / max(np.abs(ref).max(), 1e-300))}
+    blk = {"grid": n, "workload": f"3D viscous Stokes {n}^3, 20 seeded inclusions (set-up on the device)",
+           "inclusions": 20, "log10_mu_range": [-L, L], "eps": 1e-8, "nout": 200,
+           "fp64": out["fp64"], "mixed": out["mixed"],
+           "speedup_mixed_vs_fp64": round(out["fp64"]["seconds"] / out["mixed"]["seconds"], 3),
+           "mixed_error_vs_fp64": field_errors(fields["mixed"], fields["fp64"]),
+           "T_eff_convention": "23 arrays x 8 B per cell and PT iteration (3D viscous, FP64 bytes for both)",
+           "deviation": "log10 mu in [-2, 2], not [-4, 4]: with the reference's 3D numerics the +-4 field "
+                        "diverges or stalls in plain FP64 too" if L < 4 else None}
+    if clocks_too:
+        blk["clocks"] = clocks
+    return blk
+
+
+def run_inclusions(args, ws, rank, local):
+    """The 20-inclusion mixed-vs-FP64 comparison (``inclusions_block``) as its own JSON line."""
+    import torch
+
+    torch.cuda.set_device(local)
+    n, L = args.incl_n, args.log10_range
+    blk = inclusions_block(n, L, rank)
     line = {
         "metric": f"time to err <= 1e-8, 3D viscous {n}^3 with 20 inclusions: FP32 inner sweeps + FP64 correction vs FP64",
-        "value": round(out["fp64"]["seconds"] / out["mixed"]["seconds"], 3), "unit": "speed-up (x)", "n_gpus": ws,
+        "value": blk["speedup_mixed_vs_fp64"], "unit": "speed-up (x)", "n_gpus": ws,
         "higher_is_better": True, "scaling": "weak", "dtype": "f32 sweeps, f64 correction",
         "data": "synthetic seeded 20-inclusion field",
-        "config": {"workload": f"3D viscous Stokes {n}^3", "inclusions": 20, "log10_mu_range": [-L, L], "eps": 1e-8,
+        "config": {"workload": blk["workload"], "inclusions": 20, "log10_mu_range": [-L, L], "eps": 1e-8,
                    "nout": 200},
-        "fp64": out["fp64"], "mixed": out["mixed"], "mixed_error_vs_fp64": errs,
-        "T_eff_GBs": {p: round(23 * n ** 3 * 8 * out[p]["iters"] / out[p]["seconds"] / 1e9, 1) for p in out},
-        "T_eff_convention": "23 arrays x 8 B per cell and PT iteration (3D viscous, FP64 bytes for both)",
-        "clocks": clocks,
+        "fp64": blk["fp64"], "mixed": blk["mixed"], "mixed_error_vs_fp64": blk["mixed_error_vs_fp64"],
+        "T_eff_GBs": {p: blk[p]["T_eff_GBs"] for p in ("fp64", "mixed")},
+        "T_eff_convention": blk["T_eff_convention"], "deviation": blk["deviation"], "clocks": blk["clocks"],
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -766,17 +782,15 @@ def run_damped(args, ws, rank, local):
         print(json.dumps(line), flush=True)
 
 
-def time_to_tol(args, stream_cls):
+def time_to_tol(args, n, stream_cls):
     """Time to tolerance of the converged problem of the metric: `nt` physical steps of
     3D VE, each PT loop run to err <= 1e-8 with a check every 200 iterations
     (Stokes3D_ve_multixpu.jl:128-134 numerics on the Stokes3D_ve_perf.jl kernels), plain
     FP64 vs FP32 sweeps + FP64 defect correction, same problem, same check."""
-    import numpy as np
     import torch
 
     import ptstokes
 
-    n = args.ttt_n
     out = {"grid": n, "nt": args.ttt_nt, "eps": 1e-8, "nout": 200}
     fields = {}
     for prec in ("fp64", "mixed"):
@@ -794,14 +808,39 @@ def time_to_tol(args, stream_cls):
         out[prec] = {"seconds": round(sec, 3), "iters": res["iters"], "ittot": res["ittot"],
                      "converged": res["converged"], "err": res["last"]["err"],
                      "T_eff_GBs": round(a_eff(n) * res["ittot"] / sec / 1e9, 1)}
-        fields[prec] = {k: s.get(k) for k in ("Pt", "Vx", "Vy", "Vz", "txx", "tyy", "tzz", "txy", "txz", "tyz")}
+        fields[prec] = device_fields(s)
         s.close()
     out["speedup_mixed_vs_fp64"] = round(out["fp64"]["seconds"] / out["mixed"]["seconds"], 3)
     out["T_eff_convention"] = ("the FP64 A_eff (29 arrays x 8 B) per PT iteration for both paths: for the mixed "
                                "path an FP64-equivalent rate; its FP32 sweeps move 43 arrays x 4 B per iteration")
-    out["mixed_rel_err_vs_fp64"] = {
-        k: float(np.linalg.norm(fields["mixed"][k] - fields["fp64"][k]) / max(np.linalg.norm(fields["fp64"][k]), 1e-300))
-        for k in fields["fp64"]}
+    out["mixed_error_vs_fp64"] = field_errors(fields["mixed"], fields["fp64"])
+    return out
+
+
+ITERATED = ("Pt", "Vx", "Vy", "Vz", "txx", "tyy", "tzz", "txy", "txz", "tyz")
+
+
+def device_fields(s):
+    """The ten iterated fields of a context, copied into dense device tensors."""
+    import numpy as np
+    import torch
+
+    out = {}
+    for k in ITERATED:
+        t = torch.empty(int(np.prod(s.shape(k))), dtype=torch.float64, device="cuda")
+        s.get_device(k, t.data_ptr(), t.numel())
+        out[k] = t
+    torch.cuda.synchronize()
+    return out
+
+
+def field_errors(got, ref):
+    """Per field: ||got-ref||_2/||ref||_2 and max|got-ref|/max|ref| (computed on the device)."""
+    out = {}
+    for k, r in ref.items():
+        d = got[k] - r
+        out[k] = {"l2_rel": float(d.norm() / max(float(r.norm()), 1e-300)),
+                  "max_rel": float(d.abs().max() / max(float(r.abs().max()), 1e-300))}
     return out
 
 
@@ -820,7 +859,10 @@ def main():
     ap.add_argument("--single-pass", type=int, nargs="?", const=1, default=0, choices=[0, 1, 2],
                     help="one launch per PT iteration: 1 staged kernel, 2 direct-load kernel")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
-    ap.add_argument("--ttt-n", type=int, default=255, help="grid of the time-to-tolerance comparison (0: skip)")
+    ap.add_argument("--ttt-n", type=int, default=511, help="grid of the time-to-tolerance comparison (0: skip)")
+    ap.add_argument("--ttt-n2", type=int, default=255, help="a second, smaller time-to-tolerance grid (0: skip)")
+    ap.add_argument("--incl-default-n", type=int, default=255,
+                    help="grid of the 20-inclusion mixed-vs-FP64 block of the default line (0: skip)")
     ap.add_argument("--ttt-nt", type=int, default=5, help="physical steps of the time-to-tolerance comparison")
     ap.add_argument("--batch", action="store_true", help="run the batched 2D sweep instead")
     ap.add_argument("--batch-n", type=int, default=256)

@@ -84,11 +84,12 @@ typedef struct pts_desc {
                              * 1 = inputs staged in shared memory by bulk copies, 2 = inputs read
                              * directly (L1/L2) */
     int32_t adjoint;        /* PTS_3D_V / PTS_3D_VE_PERF: 1 = solve the transposed (adjoint) system */
-    int32_t stencil;        /* 3D FP64 two-kernel path, compute_Pt_τ!: 0 = z-marching kernel whose
-                             * input planes the tensor-memory accelerator stages in shared memory;
-                             * 1 = one thread per cell, operands read directly. Same bits. */
-    int32_t stencil_tile;   /* z-marching kernel: tile configuration 0 .. pts_stencil_tiles()-1
-                             * (0 = default; chosen by timing, e.g. ptstokes.tune_stencil) */
+    int32_t stencil;        /* 3D compute_Pt_τ! (FP64 two-kernel path, and the FP32 sweeps of MIXED):
+                             * 0 = z-marching kernel whose input planes the tensor-memory
+                             * accelerator stages in shared memory; 1 = one thread per cell,
+                             * operands read directly. Same arithmetic (FP64: same bits). */
+    int32_t stencil_tile;   /* z-marching kernel: tile configuration 0 .. pts_stencil_tiles(precision)-1
+                             * (0 = default; see pts_stencil_tile_info) */
     int32_t stencil_kz;     /* z-marching kernel: z-planes per thread block (0 = default 32) */
     int32_t reserved[2];
 } pts_desc;
@@ -144,12 +145,16 @@ PTS_API int pts_destroy(pts_ctx* ctx);
 PTS_API const char* pts_last_error(const pts_ctx* ctx);        /* ctx may be NULL (creation errors) */
 PTS_API int pts_abi_version(void);
 PTS_API int pts_sync(pts_ctx* ctx);                            /* wait for the context's stream */
-/* Tile configurations of the z-marching compute_Pt_τ! (pts_desc.stencil_tile): their count,
- * and per configuration the tile height in cells (the width is 32) and the number of
- * shared-memory plane slots. No reference counterpart (ParallelStencil picks its launch
- * shape itself). */
-PTS_API int pts_stencil_tiles(void);
-PTS_API int pts_stencil_tile_info(int32_t tile, int32_t* tile_y, int32_t* ring_slots);
+/* Tile configurations of the z-marching compute_Pt_τ! (pts_desc.stencil_tile) for a
+ * precision (PTS_FP64 kernel, or the FP32 sweep of PTS_MIXED): their count, and per
+ * configuration the tile height in cells (the width is 32) and the number of shared-memory
+ * plane slots. No reference counterpart (ParallelStencil picks its launch shape itself). */
+PTS_API int pts_stencil_tiles(int32_t precision);
+/* Change a context's pts_desc.stencil, stencil_tile and stencil_kz (same meaning) without
+ * re-creating it, e.g. to time the tile configurations on the problem itself. Results do
+ * not depend on the choice (FP64: bit for bit). No reference counterpart. */
+PTS_API int pts_set_stencil(pts_ctx* ctx, int32_t stencil, int32_t tile, int32_t kz);
+PTS_API int pts_stencil_tile_info(int32_t precision, int32_t tile, int32_t* tile_y, int32_t* ring_slots);
 /* The context's cudaStream_t (as void*), to order or time the caller's own work with it. */
 PTS_API int pts_stream(pts_ctx* ctx, void** stream);
 

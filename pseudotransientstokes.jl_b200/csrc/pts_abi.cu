@@ -307,7 +307,10 @@ int enqueue_block(pts_ctx* c, int64_t m, bool store_last) {
         // m FP32 sweeps on the correction, then the FP64 fold X += δ (δ = 0 again). The
         // sources must already describe the current X (mixed_prepare or a previous check).
         for (int64_t q = 0; q < m; ++q) {
-            CK(launch_corr_A32(c->v, c->g, c->m, c->n, c->stream));
+            if (c->zs)
+                CK(launch_corr_A32_zs(c->v, c->d.stencil_tile, c->g, c->m, c->n, c->d.stencil_kz, c->d_kerr, c->stream));
+            else
+                CK(launch_corr_A32(c->v, c->g, c->m, c->n, c->stream));
             CK(launch_corr_B32(c->v, c->g, c->m, c->n, c->stream));
         }
         CK(launch_fold(c->g, c->f, c->m, c->stream));
@@ -404,11 +407,30 @@ extern "C" {
 
 int pts_abi_version(void) { return PTS_ABI_VERSION; }
 
-int pts_stencil_tiles(void) { return zstage_num_configs(); }
+int pts_set_stencil(pts_ctx* c, int32_t stencil, int32_t tile, int32_t kz) {
+    int rc = enter(c);
+    if (rc) return rc;
+    if (stencil != 0 && stencil != 1) return fail(c, PTS_E_INVAL, "stencil must be 0 or 1");
+    if (tile < 0 || tile >= (c->mixed ? zstage32_num_configs() : zstage_num_configs()))
+        return fail(c, PTS_E_INVAL, "stencil_tile out of range (pts_stencil_tiles)");
+    if (kz < 0) return fail(c, PTS_E_INVAL, "stencil_kz must be >= 0");
+    c->d.stencil = stencil;
+    c->d.stencil_tile = tile;
+    c->d.stencil_kz = kz;
+    c->zs = (c->v == VE3D || c->v == VE3D_PERF || c->v == V3D) && !c->fused && stencil == 0;
+    CK(cudaStreamSynchronize(c->stream));
+    drop_graph(c);  // the captured check blocks hold the previous kernels
+    return PTS_OK;
+}
 
-int pts_stencil_tile_info(int32_t tile, int32_t* tile_y, int32_t* ring_slots) {
+int pts_stencil_tiles(int32_t precision) {
+    return precision == PTS_MIXED ? zstage32_num_configs() : zstage_num_configs();
+}
+
+int pts_stencil_tile_info(int32_t precision, int32_t tile, int32_t* tile_y, int32_t* ring_slots) {
     int ty = 0, r = 0;
-    if (!zstage_tile_info(tile, &ty, &r)) return fail(nullptr, PTS_E_INVAL, "no such stencil tile");
+    const bool ok = precision == PTS_MIXED ? zstage32_tile_info(tile, &ty, &r) : zstage_tile_info(tile, &ty, &r);
+    if (!ok) return fail(nullptr, PTS_E_INVAL, "no such stencil tile");
     if (tile_y) *tile_y = ty;
     if (ring_slots) *ring_slots = r;
     return PTS_OK;
@@ -433,7 +455,8 @@ int pts_create(const pts_desc* d, pts_ctx** out) {
         return fail(nullptr, PTS_E_INVAL, "mixed_inner: the FP64 correction runs with every check, so it must be 0 or nout");
     if (!(d->lx > 0) || !(d->ly > 0) || (d3 && !(d->lz > 0))) return fail(nullptr, PTS_E_INVAL, "domain extents must be > 0");
     if (d->stencil != 0 && d->stencil != 1) return fail(nullptr, PTS_E_INVAL, "stencil must be 0 or 1");
-    if (d->stencil_tile < 0 || d->stencil_tile >= zstage_num_configs())
+    if (d->stencil_tile < 0 ||
+        d->stencil_tile >= (d->precision == PTS_MIXED ? zstage32_num_configs() : zstage_num_configs()))
         return fail(nullptr, PTS_E_INVAL, "stencil_tile out of range (pts_stencil_tiles)");
     if (d->stencil_kz < 0) return fail(nullptr, PTS_E_INVAL, "stencil_kz must be >= 0");
     if (d->adjoint && ((d->variant != PTS_3D_V && d->variant != PTS_3D_VE_PERF) || d->precision != PTS_FP64 ||
@@ -526,7 +549,8 @@ int pts_create(const pts_desc* d, pts_ctx** out) {
     }
     c->mixed = d->precision == PTS_MIXED;
     c->fused = variant_fused(c->v) && d->single_pass != 0 && !c->mixed;
-    c->zs = (c->v == VE3D || c->v == VE3D_PERF || c->v == V3D) && !c->fused && !c->mixed && d->stencil == 0;
+    // z-marching TMA-staged compute_Pt_τ!: the FP64 two-kernel path, and the FP32 sweeps
+    c->zs = (c->v == VE3D || c->v == VE3D_PERF || c->v == V3D) && !c->fused && d->stencil == 0;
     if (c->mixed) {
         float** p32[] = {&c->m.dPt, &c->m.dVx, &c->m.dVy, &c->m.dVz, &c->m.dtxx, &c->m.dtyy, &c->m.dtzz, &c->m.dtxy,
                          &c->m.dtxz, &c->m.dtyz, &c->m.aP, &c->m.atxx, &c->m.atyy, &c->m.atzz, &c->m.atxy,

@@ -152,6 +152,12 @@ struct Mixed32 {
 // FP32 inner sweep (pts_kernels32.cu): δ-form compute_Pt_τ! and compute_V! + bc.
 cudaError_t launch_corr_A32(int variant, const Geom& g, const Mixed32& m, const Num& n, cudaStream_t s);
 cudaError_t launch_corr_B32(int variant, const Geom& g, const Mixed32& m, const Num& n, cudaStream_t s);
+// The δ-form compute_Pt_τ! as a z-marching kernel with TMA-staged planes (same arithmetic as
+// launch_corr_A32); `tile` < zstage32_num_configs(), `kz` planes per block (0: 32).
+cudaError_t launch_corr_A32_zs(int variant, int tile, const Geom& g, const Mixed32& m, const Num& n, int kz, int* err,
+                               cudaStream_t s);
+int zstage32_num_configs();
+bool zstage32_tile_info(int tile, int* ty, int* ring);
 // FP64 outer step (pts_kernels64.cu): fold X += δ and clear δ; residual sources of X
 // (aP = ∇·V, aτ = constitutive residual, aV = momentum residual R) with the check
 // partials and its finaliser; FP32 copies of the coefficients.

@@ -30,23 +30,21 @@
 // Waits are bounded (2 s of %globaltimer): a wait that gives up sets the context's error
 // flag, the producer still waits (bounded) for every copy it issued, and the kernel ends.
 // No copy uses cluster multicast; every tensor map covers this GPU's own fields.
-#include <cuda.h>
-#include <cudaTypedefs.h>
-
 #include <cstring>
 
 #include "pts_expr64.cuh"
 #include "pts_internal.h"
+#include "pts_tma.cuh"
 
 namespace pts {
 namespace zs {
 
 using namespace expr;
+using namespace tma;
 
 constexpr int TX = 32;           // tile width: one lane per cell
 constexpr int NH = 5;            // halo-group arrays
 constexpr int NPMAX = 13;        // point-group arrays (visco-elastic)
-constexpr uint64_t kWaitNs = 2000000000ull;
 
 struct alignas(64) Maps {
     CUtensorMap h[NH];     // Vx Vy Gdτ Mus Vz
@@ -64,56 +62,45 @@ struct Cfg {
     static constexpr int SLOT = NH * HSTRIDE + NP * PBOX;
 };
 
-// ---- TMA / mbarrier primitives (no cluster multicast anywhere) ----
-__device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(saddr(b)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr(b)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(saddr(b)) : "memory");
-}
-__device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(saddr(b)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-__device__ __forceinline__ uint64_t gtimer() {
-    uint64_t t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-// Bounded wait for the completion of the phase of parity `parity`; false if it gave up.
-__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity) {
-    if (mbar_try(b, parity)) return true;
-    const uint64_t t0 = gtimer();
-    while (!mbar_try(b, parity))
-        if (gtimer() - t0 > kWaitNs) return false;
-    return true;
-}
-// One 3D tile of a tensor into shared memory, completion counted on mbarrier `b`.
-__device__ __forceinline__ void tma_load3(void* dst, const CUtensorMap* m, int x, int y, int z, uint64_t* b) {
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
-        "[%5];" ::"r"(saddr(dst)),
-        "l"(m), "r"(x), "r"(y), "r"(z), "r"(saddr(b))
-        : "memory");
-}
-__device__ __forceinline__ void prefetch_map(const CUtensorMap* m) {
-    asm volatile("prefetch.tensormap [%0];" ::"l"(m) : "memory");
+// The copies of stage t (plane kb-1+t) into its ring slot, completion on full[slot]; one
+// thread issues them. Stage 0 brings the halo group only (it primes the carried registers).
+template <bool EL, int TY, int R>
+__device__ __forceinline__ void issue_stage(const Maps& maps, unsigned char* smem, uint64_t* full, int t, int i0,
+                                            int j0, int kb) {
+    using C = Cfg<TY, EL>;
+    const int slot = t % R, s = kb - 1 + t;
+    unsigned char* base = smem + (size_t)slot * C::SLOT;
+    mbar_expect_tx(&full[slot], NH * C::HBOX + (t > 0 ? C::NP * C::PBOX : 0));
+    tma_load3(base + 0 * C::HSTRIDE, &maps.h[0], i0 - 2, j0 - 1, s, &full[slot]);
+    tma_load3(base + 1 * C::HSTRIDE, &maps.h[1], i0 - 2, j0 - 1, s, &full[slot]);
+    tma_load3(base + 2 * C::HSTRIDE, &maps.h[2], i0 - 2, j0 - 1, s, &full[slot]);
+    tma_load3(base + 3 * C::HSTRIDE, &maps.h[3], i0 - 2, j0 - 1, s, &full[slot]);
+    tma_load3(base + 4 * C::HSTRIDE, &maps.h[4], i0 - 2, j0 - 1, s + 1, &full[slot]);
+    if (t > 0) {
+        unsigned char* pb = base + NH * C::HSTRIDE;
+#pragma unroll
+        for (int q = 0; q < C::NP; ++q) tma_load3(pb + q * C::PBOX, &maps.p[q], i0, j0, s, &full[slot]);
+    }
 }
 
-// compute_Pt_τ! over a 32 x TY tile and planes [kb, ke). Block: TY consumer warps + one
-// producer warp. R = slots in the shared-memory ring.
-template <bool EL, bool PERF, int TY, int R>
-__global__ void __launch_bounds__(32 * (TY + 1)) k3_Pt_tau_zs(const __grid_constant__ Maps maps, Geom g, Fields64 f,
-                                                               Num n, int kz, int store_divV, int* err) {
+// Bounded wait for every copy of stages [from, issued) to land (the CTA may not end while
+// a copy into its shared memory is in flight).
+template <int R>
+__device__ __forceinline__ void drain(uint64_t* full, int from, int issued, int* err) {
+    for (int t = (from > issued - R ? from : issued - R); t < issued; ++t)
+        if (t >= 0 && !mbar_wait(&full[t % R], (t / R) & 1)) {
+            atomicExch(err, 1);
+            return;
+        }
+}
+
+// compute_Pt_τ! over a 32 x TY tile and planes [kb, ke): TY consumer warps, and either one
+// extra producer warp (PW) or thread 0 issuing the copies between its own steps (a warp's
+// registers saved). R = slots in the shared-memory ring; MINB = blocks per SM the register
+// allocation must allow.
+template <bool EL, bool PERF, int TY, int R, bool PW, int MINB>
+__global__ void __launch_bounds__(32 * (TY + (PW ? 1 : 0)), MINB)
+    k3_Pt_tau_zs(const __grid_constant__ Maps maps, Geom g, Fields64 f, Num n, int kz, int store_divV, int* err) {
     using C = Cfg<TY, EL>;
     extern __shared__ unsigned char smem_raw[];
     unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
@@ -135,43 +122,32 @@ __global__ void __launch_bounds__(32 * (TY + 1)) k3_Pt_tau_zs(const __grid_const
     }
     __syncthreads();
 
-    if (warp == TY) {
-        // ---------------- producer: one elected lane issues every copy
+    if (PW && warp == TY) {
+        // ---------------- producer warp: one lane issues every copy, R stages ahead
         if (lane != 0) return;
         for (int q = 0; q < NH; ++q) prefetch_map(&maps.h[q]);
         for (int q = 0; q < C::NP; ++q) prefetch_map(&maps.p[q]);
-        bool ok = true;
         int issued = 0;
-        for (int t = 0; t < nst && ok; ++t) {
-            const int slot = t % R, use = t / R;
-            if (use > 0 && !mbar_wait(&empty[slot], (use - 1) & 1)) {
-                ok = false;
-                break;
-            }
-            const int s = kb - 1 + t;
-            unsigned char* base = smem + (size_t)slot * C::SLOT;
-            const uint32_t bytes = NH * C::HBOX + (t > 0 ? C::NP * C::PBOX : 0);
-            mbar_expect_tx(&full[slot], bytes);
-            tma_load3(base + 0 * C::HSTRIDE, &maps.h[0], i0 - 2, j0 - 1, s, &full[slot]);
-            tma_load3(base + 1 * C::HSTRIDE, &maps.h[1], i0 - 2, j0 - 1, s, &full[slot]);
-            tma_load3(base + 2 * C::HSTRIDE, &maps.h[2], i0 - 2, j0 - 1, s, &full[slot]);
-            tma_load3(base + 3 * C::HSTRIDE, &maps.h[3], i0 - 2, j0 - 1, s, &full[slot]);
-            tma_load3(base + 4 * C::HSTRIDE, &maps.h[4], i0 - 2, j0 - 1, s + 1, &full[slot]);
-            if (t > 0) {
-                unsigned char* pb = base + NH * C::HSTRIDE;
-#pragma unroll
-                for (int q = 0; q < C::NP; ++q) tma_load3(pb + q * C::PBOX, &maps.p[q], i0, j0, s, &full[slot]);
-            }
-            issued = t + 1;
-        }
-        if (!ok) atomicExch(err, 1);
-        // every copy issued must have landed before the CTA may end (bounded)
-        for (int t = (issued > R ? issued - R : 0); t < issued; ++t)
-            if (!mbar_wait(&full[t % R], (t / R) & 1)) {
+        for (int t = 0; t < nst; ++t) {
+            const int use = t / R;
+            if (use > 0 && !mbar_wait(&empty[t % R], (use - 1) & 1)) {
                 atomicExch(err, 1);
                 break;
             }
+            issue_stage<EL, TY, R>(maps, smem, full, t, i0, j0, kb);
+            issued = t + 1;
+        }
+        drain<R>(full, 0, issued, err);
         return;
+    }
+    // without a producer warp, thread 0 keeps R-1 stages in flight: before its step t it
+    // refills the slot of stage t-1 once every warp has left that stage
+    const bool prod = !PW && threadIdx.x == 0;
+    int issued = 0;
+    if (prod) {
+        for (int q = 0; q < NH; ++q) prefetch_map(&maps.h[q]);
+        for (int q = 0; q < C::NP; ++q) prefetch_map(&maps.p[q]);
+        for (; issued < R - 1 && issued < nst; ++issued) issue_stage<EL, TY, R>(maps, smem, full, issued, i0, j0, kb);
     }
 
     // ---------------- consumers: warp = tile row, lane = tile column
@@ -195,11 +171,20 @@ __global__ void __launch_bounds__(32 * (TY + 1)) k3_Pt_tau_zs(const __grid_const
 
     idx_t c = gidx32(g, i, j, kb);
     const idx_t sz = (idx_t)g.pxy;
-    for (int t = 0; t < nst; ++t) {
+    int t = 0;
+    for (; t < nst; ++t) {
         const int slot = t % R;
+        if (prod && issued < nst) {  // stage t+R-1 into the slot stage t-1 leaves
+            if (issued >= R && !mbar_wait(&empty[issued % R], (issued / R - 1) & 1)) {
+                atomicExch(err, 1);
+                break;
+            }
+            issue_stage<EL, TY, R>(maps, smem, full, issued, i0, j0, kb);
+            ++issued;
+        }
         if (!mbar_wait(&full[slot], (t / R) & 1)) {
             atomicExch(err, 1);
-            return;
+            break;
         }
         const double* H = (const double*)(smem + (size_t)slot * C::SLOT);
         const double* hVx = H;
@@ -268,39 +253,12 @@ __global__ void __launch_bounds__(32 * (TY + 1)) k3_Pt_tau_zs(const __grid_const
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[slot]);
     }
+    if (prod) drain<R>(full, t, issued, err);  // copies this thread issued and nobody consumed
 }
 
 // ---- host side ----
 
-PFN_cuTensorMapEncodeTiled_v12000 encoder() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    if (!fn) {
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
-                cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
-        else
-            cudaGetLastError();
-    }
-    return fn;
-}
-
-// A field of the unified layout as a px x py x pz FP64 tensor, copied in bw x bh x 1 boxes.
-bool encode(CUtensorMap* m, const double* base, const Geom& g, int bw, int bh) {
-    auto fn = encoder();
-    if (!fn || !base) return false;
-    cuuint64_t dims[3] = {(cuuint64_t)g.px, (cuuint64_t)g.py, (cuuint64_t)g.pz};
-    cuuint64_t strides[2] = {(cuuint64_t)g.px * 8, (cuuint64_t)g.pxy * 8};
-    cuuint32_t box[3] = {(cuuint32_t)bw, (cuuint32_t)bh, 1};
-    cuuint32_t es[3] = {1, 1, 1};
-    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void*)base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
-}
-
-template <bool EL, bool PERF, int TY, int R>
+template <bool EL, bool PERF, int TY, int R, bool PW, int MINB>
 cudaError_t launch_cfg(const Geom& g, const Fields64& f, const Num& n, int kz, bool store_divV, int* err,
                        cudaStream_t s) {
     using C = Cfg<TY, EL>;
@@ -308,39 +266,52 @@ cudaError_t launch_cfg(const Geom& g, const Fields64& f, const Num& n, int kz, b
     memset(&maps, 0, sizeof(maps));
     const double* hsrc[NH] = {f.Vx, f.Vy, f.Gdt, f.Mus, f.Vz};
     for (int q = 0; q < NH; ++q)
-        if (!encode(&maps.h[q], hsrc[q], g, C::HW, C::HH)) return cudaErrorInvalidValue;
+        if (!encode_field(&maps.h[q], hsrc[q], g, 8, C::HW, C::HH)) return cudaErrorInvalidValue;
     const double* psrc[NPMAX] = {f.Pt,    f.txx,   f.tyy,   f.tzz,   f.txy,   f.txz,  f.tyz,
                                  f.txx_o, f.tyy_o, f.tzz_o, f.txy_o, f.txz_o, f.tyz_o};
     for (int q = 0; q < C::NP; ++q)
-        if (!encode(&maps.p[q], psrc[q], g, TX, TY)) return cudaErrorInvalidValue;
+        if (!encode_field(&maps.p[q], psrc[q], g, 8, TX, TY)) return cudaErrorInvalidValue;
     const size_t smem = 128 + (size_t)R * C::SLOT + 2 * R * sizeof(uint64_t);
     static bool attr[64] = {};  // per device: the opt-in to more than 48 KB of shared memory
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
     if (!attr[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(k3_Pt_tau_zs<EL, PERF, TY, R>,
+        cudaError_t e = cudaFuncSetAttribute(k3_Pt_tau_zs<EL, PERF, TY, R, PW, MINB>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         attr[dev] = true;
     }
     const dim3 grid((g.nx + TX - 1) / TX, (g.ny + TY - 1) / TY, (g.nz + kz - 1) / kz);
-    k3_Pt_tau_zs<EL, PERF, TY, R><<<grid, 32 * (TY + 1), smem, s>>>(maps, g, f, n, kz, store_divV ? 1 : 0, err);
+    k3_Pt_tau_zs<EL, PERF, TY, R, PW, MINB>
+        <<<grid, 32 * (TY + (PW ? 1 : 0)), smem, s>>>(maps, g, f, n, kz, store_divV ? 1 : 0, err);
     return cudaGetLastError();
 }
 
-// Tile configurations: (tile height TY, ring slots R). Shared memory per block for the
-// visco-elastic form: 8x2 83 KB (2 blocks/SM), 4x2 45 KB (5), 4x3 67 KB (3), 8x3 124 KB (1).
-constexpr int kTiles[][2] = {{8, 2}, {4, 2}, {4, 3}, {8, 3}};
+// Tile configurations: tile height TY, ring slots R, producer warp PW, blocks per SM MINB
+// the registers must allow. Shared memory per block for the visco-elastic form: 32x4 with 2
+// slots 45 KB (5 blocks/SM), 32x8 83 KB (2), 32x6 63 KB (3), 32x2 25 KB (9).
+struct TileCfg {
+    int ty, r, pw, minb;
+};
+constexpr TileCfg kTiles[] = {{4, 2, 0, 5}, {4, 2, 1, 4}, {4, 2, 1, 5}, {8, 2, 0, 2}, {6, 2, 0, 3}, {2, 2, 0, 9}};
 constexpr int kNumTiles = (int)(sizeof(kTiles) / sizeof(kTiles[0]));
+
+template <bool EL, bool PERF, int Q>
+cudaError_t launch_q(const Geom& g, const Fields64& f, const Num& n, int kz, bool sd, int* err, cudaStream_t s) {
+    constexpr TileCfg c = kTiles[Q];
+    return launch_cfg<EL, PERF, c.ty, c.r, c.pw != 0, c.minb>(g, f, n, kz, sd, err, s);
+}
 
 template <bool EL, bool PERF>
 cudaError_t launch_form(int cfg, const Geom& g, const Fields64& f, const Num& n, int kz, bool sd, int* err,
                         cudaStream_t s) {
     switch (cfg) {
-        case 0: return launch_cfg<EL, PERF, kTiles[0][0], kTiles[0][1]>(g, f, n, kz, sd, err, s);
-        case 1: return launch_cfg<EL, PERF, kTiles[1][0], kTiles[1][1]>(g, f, n, kz, sd, err, s);
-        case 2: return launch_cfg<EL, PERF, kTiles[2][0], kTiles[2][1]>(g, f, n, kz, sd, err, s);
-        case 3: return launch_cfg<EL, PERF, kTiles[3][0], kTiles[3][1]>(g, f, n, kz, sd, err, s);
+        case 0: return launch_q<EL, PERF, 0>(g, f, n, kz, sd, err, s);
+        case 1: return launch_q<EL, PERF, 1>(g, f, n, kz, sd, err, s);
+        case 2: return launch_q<EL, PERF, 2>(g, f, n, kz, sd, err, s);
+        case 3: return launch_q<EL, PERF, 3>(g, f, n, kz, sd, err, s);
+        case 4: return launch_q<EL, PERF, 4>(g, f, n, kz, sd, err, s);
+        case 5: return launch_q<EL, PERF, 5>(g, f, n, kz, sd, err, s);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -351,8 +322,8 @@ int zstage_num_configs() { return zs::kNumTiles; }
 
 bool zstage_tile_info(int tile, int* ty, int* ring) {
     if (tile < 0 || tile >= zs::kNumTiles) return false;
-    if (ty) *ty = zs::kTiles[tile][0];
-    if (ring) *ring = zs::kTiles[tile][1];
+    if (ty) *ty = zs::kTiles[tile].ty;
+    if (ring) *ring = zs::kTiles[tile].r;
     return true;
 }
 

@@ -95,6 +95,15 @@ for (jl, c) in ((:init_inclusion!, :pts_init_inclusion),)
     @eval $jl(ctx::Ctx; μs0=1.0, μsi=1e-3, radius2=1.0, εbg=1.0) =
         check(ctx, ccall(($(QuoteNode(c)), libpts), Cint, (Ptr{Cvoid}, Float64, Float64, Float64, Float64), ctx.ptr, μs0, μsi, radius2, εbg))
 end
+# create_inclusions! (Stokes2D_param.jl:83-99) for a list of circles/spheres (pts_inclusion)
+struct Inclusion
+    x::Float64; y::Float64; z::Float64   # centre relative to the domain centre (the script's Xi, Yi)
+    r2::Float64                          # squared radius
+    μs::Float64                          # viscosity inside
+end
+init_inclusions!(ctx::Ctx, list::Vector{Inclusion}; μs0=1.0, εbg=1.0) =
+    check(ctx, ccall((:pts_init_inclusions, libpts), Cint, (Ptr{Cvoid}, Ptr{Inclusion}, Int32, Float64, Float64),
+                     ctx.ptr, list, length(list), μs0, εbg))
 # numerics of the damped variants (previous_damp/Stokes2D_ve0.jl:95-98; the 3D script's are
 # Vdmp=4, β_n=3, Vsc=1, Ptsc=5, Stokes3D0_multixpu.jl:105-108), before compute_iter_params!
 set_damping!(ctx::Ctx; Vdmp=4.0, β_n=2.0, Vsc=1.0, Ptsc=3.0) =

@@ -102,8 +102,9 @@ _DP = ctypes.c_void_p  # double* (host or device), passed as an address
 
 SIGNATURES = {
     "pts_abi_version": ([], ctypes.c_int),
-    "pts_stencil_tiles": ([], ctypes.c_int),
-    "pts_stencil_tile_info": ([_I32, ctypes.POINTER(_I32), ctypes.POINTER(_I32)], ctypes.c_int),
+    "pts_stencil_tiles": ([_I32], ctypes.c_int),
+    "pts_set_stencil": ([_P, _I32, _I32, _I32], ctypes.c_int),
+    "pts_stencil_tile_info": ([_I32, _I32, ctypes.POINTER(_I32), ctypes.POINTER(_I32)], ctypes.c_int),
     "pts_last_error": ([_P], ctypes.c_char_p),
     "pts_create": ([ctypes.POINTER(PtsDesc), ctypes.POINTER(_P)], ctypes.c_int),
     "pts_destroy": ([_P], ctypes.c_int),

@@ -224,6 +224,62 @@ class Solver:
         fn = self.lib.pts_gradient_logmu_add if add else self.lib.pts_gradient_logmu
         self._ck(fn(self.ctx, adj.ctx))
 
+    # ---------------------------------------------------------------- kernel form
+    def set_stencil(self, stencil=0, tile=0, kz=0):
+        """compute_Pt_τ! kernel form (pts_set_stencil): 0 = z-marching with TMA-staged planes
+        (tile configuration `tile`, `kz` planes per block), 1 = one thread per cell."""
+        self._ck(self.lib.pts_set_stencil(self.ctx, int(stencil), int(tile), int(kz)))
+        self.desc.stencil, self.desc.stencil_tile, self.desc.stencil_kz = int(stencil), int(tile), int(kz)
+
+    def tune_stencil(self, iters=20, kzs=(16, 32, 64), use_cache=True):
+        """Time every z-marching tile configuration x planes-per-block in `kzs` on this problem
+        (`iters` PT iterations each, CUDA events on the context's stream), keep the fastest,
+        and cache the choice per (variant, precision, grid) in ~/.cache/ptstokes/stencil.json.
+        The iterations advance the fields; results do not depend on the configuration."""
+        import json
+        import os
+        import time
+
+        import torch
+
+        key = f"{self.variant}/{self.desc.precision}/{self.nx}x{self.ny}x{self.nz}"
+        path = os.path.join(os.path.expanduser("~"), ".cache", "ptstokes", "stencil.json")
+        cache = {}
+        if use_cache and os.path.exists(path):
+            try:
+                cache = json.load(open(path))
+            except Exception:
+                cache = {}
+        if use_cache and key in cache:
+            e = cache[key]
+            self.set_stencil(0, e["tile"], e["kz"])
+            return e
+        stream = torch.cuda.ExternalStream(self.stream_handle())
+        ms = {}
+        for tile in range(self.lib.pts_stencil_tiles(self.desc.precision)):
+            for kz in kzs:
+                self.set_stencil(0, tile, kz)
+                self.iterate(2)
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                self.iterate(iters)
+                b.record(stream)
+                b.synchronize()
+                ms[f"{tile}:{kz}"] = a.elapsed_time(b) / iters
+        best = min(ms, key=ms.get)
+        tile, kz = map(int, best.split(":"))
+        self.set_stencil(0, tile, kz)
+        entry = {"tile": tile, "kz": kz, "ms_per_iteration": ms, "when": time.time()}
+        if use_cache:
+            try:
+                os.makedirs(os.path.dirname(path), exist_ok=True)
+                cache[key] = entry
+                json.dump(cache, open(path, "w"), indent=1)
+            except OSError:
+                pass
+        return entry
+
     # ---------------------------------------------------------------- drivers
     def iterate(self, n):
         self._ck(self.lib.pts_iterate(self.ctx, int(n)))

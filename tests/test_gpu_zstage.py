@@ -1,0 +1,80 @@
+"""The z-marching compute_Pt_τ! with TMA-staged planes against the one-thread-per-cell kernel.
+
+FP64: every tile configuration and several z-chunk lengths give the same bits as the direct
+kernel after iterations (so the oracle parity of tests/test_gpu_parity.py carries over to
+both), on ragged grids whose tiles, z-chunks and halos fall off every edge. The FP32 sweeps
+of the mixed path: both kernel forms agree to FP32 rounding. The kernel form can be switched
+on a live context.
+"""
+import numpy as np
+import pytest
+
+ITERATED = ("Pt", "Vx", "Vy", "Vz", "txx", "tyy", "tzz", "txy", "txz", "tyz")
+
+
+def run(gpu_lib, variant, dims, it=12, precision="fp64", **kw):
+    import ptstokes
+
+    s = ptstokes.Solver(variant, *dims, lib=gpu_lib, nout=it, eps=1e-300, iter_max=10 ** 9, precision=precision,
+                        **kw)
+    s.setup_inclusion()
+    if variant != "3d_v":
+        s.assign_tau()
+    s.iterate(it)
+    if variant != "3d_v":
+        s.assign_tau()
+    s.iterate(it)
+    chk = s.compute_res()
+    out = {k: s.get(k) for k in ITERATED}
+    s.close()
+    return out, chk
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("variant", ["3d_ve_perf", "3d_v", "3d_ve"])
+@pytest.mark.parametrize("dims", [(37, 29, 23), (33, 7, 40), (4, 3, 5)])
+def test_every_tile_is_bit_exact(gpu_lib, variant, dims):
+    ref, cref = run(gpu_lib, variant, dims, stencil=1)
+    for tile in range(gpu_lib.pts_stencil_tiles(0)):
+        for kz in (0, 7, 1):
+            got, c = run(gpu_lib, variant, dims, stencil=0, stencil_tile=tile, stencil_kz=kz)
+            for k in ITERATED:
+                assert np.array_equal(got[k], ref[k]), (tile, kz, k)
+            assert c == cref
+
+
+@pytest.mark.gpu
+def test_switching_on_a_live_context(gpu_lib):
+    import ptstokes
+
+    dims = (41, 35, 29)
+    ref, _ = run(gpu_lib, "3d_ve_perf", dims, stencil=1)
+    # iter_max = 11: one solve() is exactly one captured block of nout = 12 iterations
+    s = ptstokes.Solver("3d_ve_perf", *dims, lib=gpu_lib, nout=12, eps=1e-300, iter_max=11)
+    s.setup_inclusion()
+    s.assign_tau()
+    s.set_stencil(0, gpu_lib.pts_stencil_tiles(0) - 1, 5)
+    s.iterate(5)
+    s.set_stencil(1)
+    s.iterate(7)
+    s.assign_tau()
+    s.set_stencil(0, 0, 0)
+    assert s.solve()["iters"] == 12  # a captured block after the switch
+    for k in ITERATED:
+        assert np.array_equal(s.get(k), ref[k]), k
+    with pytest.raises(ptstokes.PtsError):
+        s.set_stencil(0, gpu_lib.pts_stencil_tiles(0), 0)
+    s.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("variant", ["3d_ve_perf", "3d_v"])
+def test_fp32_sweep_forms_agree(gpu_lib, variant):
+    dims = (45, 38, 31)
+    ref, _ = run(gpu_lib, variant, dims, it=40, precision="mixed", stencil=1)
+    for tile in range(gpu_lib.pts_stencil_tiles(1)):
+        got, _ = run(gpu_lib, variant, dims, it=40, precision="mixed", stencil=0, stencil_tile=tile)
+        for k in ITERATED:
+            scale = max(float(np.abs(ref[k]).max()), 1e-300)
+            # same FP32 arithmetic up to the compiler's multiply-add contraction
+            assert float(np.abs(got[k] - ref[k]).max()) <= 1e-5 * scale, (tile, k)
