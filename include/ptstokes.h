@@ -84,14 +84,17 @@ typedef struct pts_desc {
                              * 1 = inputs staged in shared memory by bulk copies, 2 = inputs read
                              * directly (L1/L2) */
     int32_t adjoint;        /* PTS_3D_V / PTS_3D_VE_PERF: 1 = solve the transposed (adjoint) system */
-    int32_t stencil;        /* 3D compute_Pt_τ! (FP64 two-kernel path, and the FP32 sweeps of MIXED):
-                             * 0 = z-marching kernel whose input planes the tensor-memory
-                             * accelerator stages in shared memory; 1 = one thread per cell,
-                             * operands read directly. Same arithmetic (FP64: same bits). */
+    int32_t stencil;        /* 3D compute_Pt_τ! and compute_V! + bc (FP64 two-kernel path, and the
+                             * FP32 sweeps of MIXED): 0 = z-marching kernels whose input planes
+                             * the tensor-memory accelerator stages in shared memory; 1 = one
+                             * thread per cell or face, operands read directly. Same arithmetic
+                             * (FP64: same bits). */
     int32_t stencil_tile;   /* z-marching kernel: tile configuration 0 .. pts_stencil_tiles(precision)-1
                              * (0 = default; see pts_stencil_tile_info) */
-    int32_t stencil_kz;     /* z-marching kernel: z-planes per thread block (0 = default 32) */
-    int32_t reserved[2];
+    int32_t stencil_kz;     /* z-marching kernels: z-planes per thread block (0 = default 32) */
+    int32_t stencil_vtile;  /* z-marching compute_V! + bc: tile configuration
+                             * 0 .. pts_stencil_vtiles(precision)-1 (0 = default) */
+    int32_t reserved[1];
 } pts_desc;
 
 /* Fields, by the reference's names. Extents are the reference's (pts_field_shape). */
@@ -150,10 +153,12 @@ PTS_API int pts_sync(pts_ctx* ctx);                            /* wait for the c
  * configuration the tile height in cells (the width is 32) and the number of shared-memory
  * plane slots. No reference counterpart (ParallelStencil picks its launch shape itself). */
 PTS_API int pts_stencil_tiles(int32_t precision);
-/* Change a context's pts_desc.stencil, stencil_tile and stencil_kz (same meaning) without
- * re-creating it, e.g. to time the tile configurations on the problem itself. Results do
- * not depend on the choice (FP64: bit for bit). No reference counterpart. */
-PTS_API int pts_set_stencil(pts_ctx* ctx, int32_t stencil, int32_t tile, int32_t kz);
+/* The number of tile configurations of the z-marching compute_V! + bc (pts_desc.stencil_vtile). */
+PTS_API int pts_stencil_vtiles(int32_t precision);
+/* Change a context's pts_desc.stencil, stencil_tile, stencil_kz and stencil_vtile (same
+ * meaning) without re-creating it, e.g. to time the tile configurations on the problem
+ * itself. Results do not depend on the choice (FP64: bit for bit). No reference counterpart. */
+PTS_API int pts_set_stencil(pts_ctx* ctx, int32_t stencil, int32_t tile, int32_t kz, int32_t vtile);
 PTS_API int pts_stencil_tile_info(int32_t precision, int32_t tile, int32_t* tile_y, int32_t* ring_slots);
 /* The context's cudaStream_t (as void*), to order or time the caller's own work with it. */
 PTS_API int pts_stream(pts_ctx* ctx, void** stream);

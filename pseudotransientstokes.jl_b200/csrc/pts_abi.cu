@@ -289,11 +289,22 @@ int Pt_tau(pts_ctx* c, bool store_divV) {
     return PTS_OK;
 }
 
+// compute_V! + bc: the z-marching TMA-staged kernel on the plain path (no momentum sources,
+// no adjoint folding), else the one-thread-per-face kernel (same bits either way).
+int V_bc(pts_ctx* c, bool update) {
+    if (c->zs && update && !c->f.Fx && !c->n.adjoint)
+        CK(launch_V_bc_zs(c->v, c->d.stencil_vtile, c->g, c->f, c->n, c->d.stencil_kz, c->d_kerr, c->stream));
+    else
+        CK(launch_V_bc(c->v, c->g, c->f, c->n, update, c->stream));
+    return PTS_OK;
+}
+
 // One PT iteration with the two-kernel path: compute_Pt_τ! then compute_V! + bc.
 int iteration(pts_ctx* c, bool store_divV) {
     int rc = Pt_tau(c, store_divV);
     if (rc) return rc;
-    CK(launch_V_bc(c->v, c->g, c->f, c->n, true, c->stream));
+    rc = V_bc(c, true);
+    if (rc) return rc;
     return PTS_OK;
 }
 
@@ -311,7 +322,11 @@ int enqueue_block(pts_ctx* c, int64_t m, bool store_last) {
                 CK(launch_corr_A32_zs(c->v, c->d.stencil_tile, c->g, c->m, c->n, c->d.stencil_kz, c->d_kerr, c->stream));
             else
                 CK(launch_corr_A32(c->v, c->g, c->m, c->n, c->stream));
-            CK(launch_corr_B32(c->v, c->g, c->m, c->n, c->stream));
+            if (c->zs)
+                CK(launch_corr_B32_zs(c->v, c->d.stencil_vtile, c->g, c->m, c->n, c->d.stencil_kz, c->d_kerr,
+                                      c->stream));
+            else
+                CK(launch_corr_B32(c->v, c->g, c->m, c->n, c->stream));
         }
         CK(launch_fold(c->g, c->f, c->m, c->stream));
         return PTS_OK;
@@ -407,16 +422,19 @@ extern "C" {
 
 int pts_abi_version(void) { return PTS_ABI_VERSION; }
 
-int pts_set_stencil(pts_ctx* c, int32_t stencil, int32_t tile, int32_t kz) {
+int pts_set_stencil(pts_ctx* c, int32_t stencil, int32_t tile, int32_t kz, int32_t vtile) {
     int rc = enter(c);
     if (rc) return rc;
     if (stencil != 0 && stencil != 1) return fail(c, PTS_E_INVAL, "stencil must be 0 or 1");
     if (tile < 0 || tile >= (c->mixed ? zstage32_num_configs() : zstage_num_configs()))
         return fail(c, PTS_E_INVAL, "stencil_tile out of range (pts_stencil_tiles)");
+    if (vtile < 0 || vtile >= (c->mixed ? zvbc32_num_configs() : zvbc_num_configs()))
+        return fail(c, PTS_E_INVAL, "stencil_vtile out of range (pts_stencil_vtiles)");
     if (kz < 0) return fail(c, PTS_E_INVAL, "stencil_kz must be >= 0");
     c->d.stencil = stencil;
     c->d.stencil_tile = tile;
     c->d.stencil_kz = kz;
+    c->d.stencil_vtile = vtile;
     c->zs = (c->v == VE3D || c->v == VE3D_PERF || c->v == V3D) && !c->fused && stencil == 0;
     CK(cudaStreamSynchronize(c->stream));
     drop_graph(c);  // the captured check blocks hold the previous kernels
@@ -425,6 +443,10 @@ int pts_set_stencil(pts_ctx* c, int32_t stencil, int32_t tile, int32_t kz) {
 
 int pts_stencil_tiles(int32_t precision) {
     return precision == PTS_MIXED ? zstage32_num_configs() : zstage_num_configs();
+}
+
+int pts_stencil_vtiles(int32_t precision) {
+    return precision == PTS_MIXED ? zvbc32_num_configs() : zvbc_num_configs();
 }
 
 int pts_stencil_tile_info(int32_t precision, int32_t tile, int32_t* tile_y, int32_t* ring_slots) {
@@ -459,6 +481,9 @@ int pts_create(const pts_desc* d, pts_ctx** out) {
         d->stencil_tile >= (d->precision == PTS_MIXED ? zstage32_num_configs() : zstage_num_configs()))
         return fail(nullptr, PTS_E_INVAL, "stencil_tile out of range (pts_stencil_tiles)");
     if (d->stencil_kz < 0) return fail(nullptr, PTS_E_INVAL, "stencil_kz must be >= 0");
+    if (d->stencil_vtile < 0 ||
+        d->stencil_vtile >= (d->precision == PTS_MIXED ? zvbc32_num_configs() : zvbc_num_configs()))
+        return fail(nullptr, PTS_E_INVAL, "stencil_vtile out of range (pts_stencil_vtiles)");
     if (d->adjoint && ((d->variant != PTS_3D_V && d->variant != PTS_3D_VE_PERF) || d->precision != PTS_FP64 ||
                        d->single_pass))
         return fail(nullptr, PTS_E_INVAL,
@@ -816,8 +841,7 @@ int pts_compute_Pt_tau(pts_ctx* c) {
 int pts_compute_V_bc(pts_ctx* c) {
     int rc = enter(c);
     if (rc) return rc;
-    CK(launch_V_bc(c->v, c->g, c->f, c->n, true, c->stream));
-    return PTS_OK;
+    return V_bc(c, true);
 }
 
 int pts_compute_res(pts_ctx* c, pts_check* out) {

@@ -157,6 +157,15 @@ cudaError_t launch_corr_B32(int variant, const Geom& g, const Mixed32& m, const 
 cudaError_t launch_corr_A32_zs(int variant, int tile, const Geom& g, const Mixed32& m, const Num& n, int kz, int* err,
                                cudaStream_t s);
 int zstage32_num_configs();
+// compute_V! + bc as a z-marching kernel with TMA-staged planes (pts_zvbc.cuh): FP64 (same
+// bits as launch_V_bc, without momentum sources or adjoint folding) and the FP32 δ-form sweep
+// (same arithmetic as launch_corr_B32). `tile` < zvbc_num_configs() / zvbc32_num_configs().
+cudaError_t launch_V_bc_zs(int variant, int tile, const Geom& g, const Fields64& f, const Num& n, int kz, int* err,
+                           cudaStream_t s);
+cudaError_t launch_corr_B32_zs(int variant, int tile, const Geom& g, const Mixed32& m, const Num& n, int kz, int* err,
+                               cudaStream_t s);
+int zvbc_num_configs();
+int zvbc32_num_configs();
 bool zstage32_tile_info(int tile, int* ty, int* ring);
 // FP64 outer step (pts_kernels64.cu): fold X += δ and clear δ; residual sources of X
 // (aP = ∇·V, aτ = constitutive residual, aV = momentum residual R) with the check

@@ -23,6 +23,7 @@
 
 #include "pts_internal.h"
 #include "pts_tma.cuh"
+#include "pts_zvbc.cuh"
 
 namespace pts {
 namespace {
@@ -384,6 +385,42 @@ bool zstage32_tile_info(int tile, int* ty, int* ring) {
     if (ring) *ring = zs32::kTiles[tile][1];
     return true;
 }
+
+// The δ-form compute_V! + bc as the z-staged template of pts_zvbc.cuh (FP32, sources aV).
+namespace zvbc32 {
+using namespace zvbc;
+struct VTile {
+    int ty, r, minb;
+};
+constexpr VTile kVTiles[] = {{8, 2, 4}, {4, 2, 8}, {8, 3, 3}};
+constexpr int kNumVTiles = (int)(sizeof(kVTiles) / sizeof(kVTiles[0]));
+
+template <int Q>
+cudaError_t launch32(const Geom& g, const Mixed32& m, const Num& n, int kz, int* err, cudaStream_t s) {
+    constexpr VTile c = kVTiles[Q];
+    MapsV maps;
+    memset(&maps, 0, sizeof(maps));
+    const void* hsrc[NHV] = {m.dtxx, m.dtyy, m.dtxy, m.dPt, m.dtRho, m.dtxz, m.dtyz};
+    const void* psrc[9] = {m.dVx, m.dVy, m.dVz, m.dtzz, m.dPt, m.dtRho, m.aVx, m.aVy, m.aVz};
+    if (!make_maps<float, c.ty, true>(&maps, g, hsrc, psrc)) return cudaErrorInvalidValue;
+    ArgsV<float> a{m.dVx, m.dVy, m.dVz, {m.aVx, m.aVy, m.aVz}};
+    NumV<float> nv{(float)n.dx, (float)n.dy, (float)n.dz, (float)n._dx, (float)n._dy, (float)n._dz, 0.5f};
+    return launch_v<float, true, true, c.ty, c.r, c.minb>(g, maps, a, nv, kz, err, s);
+}
+}  // namespace zvbc32
+
+cudaError_t launch_corr_B32_zs(int v, int tile, const Geom& g, const Mixed32& m, const Num& n, int kz, int* err,
+                               cudaStream_t s) {
+    if (v != VE3D_PERF && v != V3D) return cudaErrorInvalidValue;
+    switch (tile) {
+        case 0: return zvbc32::launch32<0>(g, m, n, kz, err, s);
+        case 1: return zvbc32::launch32<1>(g, m, n, kz, err, s);
+        case 2: return zvbc32::launch32<2>(g, m, n, kz, err, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+int zvbc32_num_configs() { return zvbc32::kNumVTiles; }
 
 cudaError_t launch_corr_B32(int v, const Geom& g, const Mixed32& m, const Num& n, cudaStream_t s) {
     if (v != VE3D_PERF && v != V3D) return cudaErrorInvalidValue;

@@ -291,19 +291,19 @@ __global__ void __launch_bounds__(256) k3d_Pt_tau(Geom g, Fields64 f, Num n, int
     if (i >= nx || j >= ny || k >= nz) return;
     const idx_t c = gidx32(g, i, j, k);
     const idx_t sx = 1, sy = g.px, sz = (idx_t)g.pxy;
-    const double dvx = f.Vx[c + sx] - f.Vx[c];
-    const double dvy = f.Vy[c + sy] - f.Vy[c];
-    const double dvz = f.Vz[c + sz] - f.Vz[c];
+    const double dvx = __ldg(&f.Vx[c + sx]) - __ldg(&f.Vx[c]);
+    const double dvy = __ldg(&f.Vy[c + sy]) - __ldg(&f.Vy[c]);
+    const double dvz = __ldg(&f.Vz[c + sz]) - __ldg(&f.Vz[c]);
     double dv;
     if (roles & ROLE_P) {
         dv = (dvx / n.dx + dvy / n.dy) + dvz / n.dz;
         if (store_divV) f.divV[c] = dv;
-        f.Pt[c] = f.Pt[c] - f.dtPt[c] * dv;
+        f.Pt[c] = f.Pt[c] - __ldg(&f.dtPt[c]) * dv;
     } else {
         dv = f.divV[c];
     }
     if (!(roles & ROLE_TAU)) return;
-    const double Mc = f.Mus[c];
+    const double Mc = __ldg(&f.Mus[c]);
     if (j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2)
         f.txx[c] = 2.0 * Mc * (dvx / n.dx - 1.0 / 3.0 * dv + n.beta_n * dv);
     if (i >= 1 && i <= nx - 2 && k >= 1 && k <= nz - 2)
@@ -311,16 +311,16 @@ __global__ void __launch_bounds__(256) k3d_Pt_tau(Geom g, Fields64 f, Num n, int
     if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2)
         f.tzz[c] = 2.0 * Mc * (dvz / n.dz - 1.0 / 3.0 * dv + n.beta_n * dv);
     if (i >= 1 && j >= 1 && k >= 1 && k <= nz - 2) {  // τxy edge
-        const double am = (((f.Mus[c - sx - sy] + f.Mus[c - sy]) + f.Mus[c - sx]) + Mc) * 0.25;
-        f.txy[c] = 2.0 * am * (0.5 * ((f.Vx[c] - f.Vx[c - sy]) / n.dy + (f.Vy[c] - f.Vy[c - sx]) / n.dx));
+        const double am = (((__ldg(&f.Mus[c - sx - sy]) + __ldg(&f.Mus[c - sy])) + __ldg(&f.Mus[c - sx])) + Mc) * 0.25;
+        f.txy[c] = 2.0 * am * (0.5 * ((__ldg(&f.Vx[c]) - __ldg(&f.Vx[c - sy])) / n.dy + (__ldg(&f.Vy[c]) - __ldg(&f.Vy[c - sx])) / n.dx));
     }
     if (i >= 1 && j >= 1 && j <= ny - 2 && k >= 1) {  // τxz edge
-        const double am = (((f.Mus[c - sx - sz] + f.Mus[c - sz]) + f.Mus[c - sx]) + Mc) * 0.25;
-        f.txz[c] = 2.0 * am * (0.5 * ((f.Vx[c] - f.Vx[c - sz]) / n.dz + (f.Vz[c] - f.Vz[c - sx]) / n.dx));
+        const double am = (((__ldg(&f.Mus[c - sx - sz]) + __ldg(&f.Mus[c - sz])) + __ldg(&f.Mus[c - sx])) + Mc) * 0.25;
+        f.txz[c] = 2.0 * am * (0.5 * ((__ldg(&f.Vx[c]) - __ldg(&f.Vx[c - sz])) / n.dz + (__ldg(&f.Vz[c]) - __ldg(&f.Vz[c - sx])) / n.dx));
     }
     if (i >= 1 && i <= nx - 2 && j >= 1 && k >= 1) {  // τyz edge
-        const double am = (((f.Mus[c - sy - sz] + f.Mus[c - sz]) + f.Mus[c - sy]) + Mc) * 0.25;
-        f.tyz[c] = 2.0 * am * (0.5 * ((f.Vy[c] - f.Vy[c - sz]) / n.dz + (f.Vz[c] - f.Vz[c - sy]) / n.dy));
+        const double am = (((__ldg(&f.Mus[c - sy - sz]) + __ldg(&f.Mus[c - sz])) + __ldg(&f.Mus[c - sy])) + Mc) * 0.25;
+        f.tyz[c] = 2.0 * am * (0.5 * ((__ldg(&f.Vy[c]) - __ldg(&f.Vy[c - sz])) / n.dz + (__ldg(&f.Vz[c]) - __ldg(&f.Vz[c - sy])) / n.dy));
     }
 }
 
@@ -339,7 +339,7 @@ __global__ void __launch_bounds__(256) k3d_V_bc(Geom g, Fields64 f, Num n, int u
         if (update && i >= 1 && i <= nx - 1) {
             const double r = n.dampX * f.dVx[c] + res3_x<false>(f, n, c, sx, sy, sz);
             f.dVx[c] = r;
-            v = v + f.dtVx[c] * r;
+            v = v + __ldg(&f.dtVx[c]) * r;
             f.Vx[c] = v;
         }
         bc_copies(f.Vx, c, v, j, 1, ny - 2, sy, k, 1, nz - 2, sz);
@@ -349,7 +349,7 @@ __global__ void __launch_bounds__(256) k3d_V_bc(Geom g, Fields64 f, Num n, int u
         if (update && j >= 1 && j <= ny - 1) {
             const double r = n.dampY * f.dVy[c] + res3_y<false>(f, n, c, sx, sy, sz);
             f.dVy[c] = r;
-            v = v + f.dtVy[c] * r;
+            v = v + __ldg(&f.dtVy[c]) * r;
             f.Vy[c] = v;
         }
         bc_copies(f.Vy, c, v, i, 1, nx - 2, sx, k, 1, nz - 2, sz);
@@ -359,7 +359,7 @@ __global__ void __launch_bounds__(256) k3d_V_bc(Geom g, Fields64 f, Num n, int u
         if (update && k >= 1 && k <= nz - 1) {
             const double r = n.dampZ * f.dVz[c] + res3_z<false>(f, n, c, sx, sy, sz);
             f.dVz[c] = r;
-            v = v + f.dtVz[c] * r;
+            v = v + __ldg(&f.dtVz[c]) * r;
             f.Vz[c] = v;
         }
         bc_copies(f.Vz, c, v, i, 1, nx - 2, sx, j, 1, ny - 2, sy);
@@ -630,7 +630,7 @@ __global__ void __launch_bounds__(256) k2d_V_bc(Geom g, Fields64 f, Num n, int u
         if (update && i >= 1 && i <= nx - 1) {
             const double r = n.dampX * f.dVx[c] + res2_x<false>(f, n, c, sx, sy);
             f.dVx[c] = r;
-            v = v + f.dtVx[c] * r;
+            v = v + __ldg(&f.dtVx[c]) * r;
             f.Vx[c] = v;
         }
         if (j == 1) f.Vx[c - sy] = v;
@@ -641,7 +641,7 @@ __global__ void __launch_bounds__(256) k2d_V_bc(Geom g, Fields64 f, Num n, int u
         if (update && j >= 1 && j <= ny - 1) {
             const double r = n.dampY * f.dVy[c] + res2_y<false>(f, n, c, sx, sy);
             f.dVy[c] = r;
-            v = v + f.dtVy[c] * r;
+            v = v + __ldg(&f.dtVy[c]) * r;
             f.Vy[c] = v;
         }
         if (i == 1) f.Vy[c - sx] = v;

@@ -35,6 +35,7 @@
 #include "pts_expr64.cuh"
 #include "pts_internal.h"
 #include "pts_tma.cuh"
+#include "pts_zvbc.cuh"
 
 namespace pts {
 namespace zs {
@@ -325,6 +326,52 @@ bool zstage_tile_info(int tile, int* ty, int* ring) {
     if (ty) *ty = zs::kTiles[tile].ty;
     if (ring) *ring = zs::kTiles[tile].r;
     return true;
+}
+
+// ---- compute_V! + bc, z-staged (pts_zvbc.cuh), FP64 ----
+namespace zvbc {
+// Tile configurations (TY, R, MINB): shared memory per block 66 KB for 32x8 (3 blocks/SM),
+// 37 KB for 32x4 (6).
+struct VTile {
+    int ty, r, minb;
+};
+constexpr VTile kVTiles[] = {{8, 2, 3}, {4, 2, 6}, {8, 2, 2}};
+constexpr int kNumVTiles = (int)(sizeof(kVTiles) / sizeof(kVTiles[0]));
+
+template <bool PERF, int Q>
+cudaError_t launch64(const Geom& g, const Fields64& f, const Num& n, int kz, int* err, cudaStream_t s) {
+    constexpr VTile c = kVTiles[Q];
+    MapsV maps;
+    memset(&maps, 0, sizeof(maps));
+    const void* hsrc[NHV] = {f.txx, f.tyy, f.txy, f.Pt, f.dtRho, f.txz, f.tyz};
+    const void* psrc[9] = {f.Vx, f.Vy, f.Vz, f.tzz, f.Pt, f.dtRho, nullptr, nullptr, nullptr};
+    if (!make_maps<double, c.ty, false>(&maps, g, hsrc, psrc)) return cudaErrorInvalidValue;
+    ArgsV<double> a{f.Vx, f.Vy, f.Vz, {nullptr, nullptr, nullptr}};
+    NumV<double> nv{n.dx, n.dy, n.dz, n._dx, n._dy, n._dz, 0.5};
+    return launch_v<double, PERF, false, c.ty, c.r, c.minb>(g, maps, a, nv, kz, err, s);
+}
+
+template <bool PERF>
+cudaError_t launch64_form(int tile, const Geom& g, const Fields64& f, const Num& n, int kz, int* err, cudaStream_t s) {
+    switch (tile) {
+        case 0: return launch64<PERF, 0>(g, f, n, kz, err, s);
+        case 1: return launch64<PERF, 1>(g, f, n, kz, err, s);
+        case 2: return launch64<PERF, 2>(g, f, n, kz, err, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+}  // namespace zvbc
+
+int zvbc_num_configs() { return zvbc::kNumVTiles; }
+
+cudaError_t launch_V_bc_zs(int variant, int tile, const Geom& g, const Fields64& f, const Num& n, int kz, int* err,
+                           cudaStream_t s) {
+    switch (variant) {
+        case VE3D_PERF:
+        case V3D: return zvbc::launch64_form<true>(tile, g, f, n, kz, err, s);
+        case VE3D: return zvbc::launch64_form<false>(tile, g, f, n, kz, err, s);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 cudaError_t launch_Pt_tau_zs(int variant, int cfg, const Geom& g, const Fields64& f, const Num& n, int kz,

@@ -54,7 +54,7 @@ class PtsDesc(ctypes.Structure):
         ("max_l", ctypes.c_double), ("eps", ctypes.c_double), ("iter_max", ctypes.c_double),
         ("mixed_inner", ctypes.c_int32), ("single_pass", ctypes.c_int32), ("adjoint", ctypes.c_int32),
         ("stencil", ctypes.c_int32), ("stencil_tile", ctypes.c_int32), ("stencil_kz", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 2),
+        ("stencil_vtile", ctypes.c_int32), ("reserved", ctypes.c_int32 * 1),
     ]
 
 
@@ -103,7 +103,8 @@ _DP = ctypes.c_void_p  # double* (host or device), passed as an address
 SIGNATURES = {
     "pts_abi_version": ([], ctypes.c_int),
     "pts_stencil_tiles": ([_I32], ctypes.c_int),
-    "pts_set_stencil": ([_P, _I32, _I32, _I32], ctypes.c_int),
+    "pts_stencil_vtiles": ([_I32], ctypes.c_int),
+    "pts_set_stencil": ([_P, _I32, _I32, _I32, _I32], ctypes.c_int),
     "pts_stencil_tile_info": ([_I32, _I32, ctypes.POINTER(_I32), ctypes.POINTER(_I32)], ctypes.c_int),
     "pts_last_error": ([_P], ctypes.c_char_p),
     "pts_create": ([ctypes.POINTER(PtsDesc), ctypes.POINTER(_P)], ctypes.c_int),

@@ -62,7 +62,7 @@ class Solver:
         self.variant = variant
         self.ndim = 3 if variant.startswith("3d") else 2
         p = dict(lx=10.0, ly=10.0, lz=10.0, xi=1.0, mus0=1.0, G=1.0, max_l=0.0, mixed_inner=0, single_pass=0,
-                 adjoint=0, stencil=0, stencil_tile=0, stencil_kz=0)
+                 adjoint=0, stencil=0, stencil_tile=0, stencil_kz=0, stencil_vtile=0)
         p.update(VARIANT_DEFAULTS[variant])
         p.update(kw)
         self.p = p
@@ -83,6 +83,7 @@ class Solver:
         d.stencil = int(p["stencil"])
         d.stencil_tile = int(p["stencil_tile"])
         d.stencil_kz = int(p["stencil_kz"])
+        d.stencil_vtile = int(p["stencil_vtile"])
         self.desc = d
         ctx = ctypes.c_void_p()
         check(self.lib, None, self.lib.pts_create(ctypes.byref(d), ctypes.byref(ctx)))
@@ -225,11 +226,13 @@ class Solver:
         self._ck(fn(self.ctx, adj.ctx))
 
     # ---------------------------------------------------------------- kernel form
-    def set_stencil(self, stencil=0, tile=0, kz=0):
-        """compute_Pt_τ! kernel form (pts_set_stencil): 0 = z-marching with TMA-staged planes
-        (tile configuration `tile`, `kz` planes per block), 1 = one thread per cell."""
-        self._ck(self.lib.pts_set_stencil(self.ctx, int(stencil), int(tile), int(kz)))
-        self.desc.stencil, self.desc.stencil_tile, self.desc.stencil_kz = int(stencil), int(tile), int(kz)
+    def set_stencil(self, stencil=0, tile=0, kz=0, vtile=0):
+        """Kernel form of compute_Pt_τ! and compute_V! + bc (pts_set_stencil): 0 = z-marching
+        with TMA-staged planes (tile configurations `tile` and `vtile`, `kz` planes per block),
+        1 = one thread per cell or face."""
+        self._ck(self.lib.pts_set_stencil(self.ctx, int(stencil), int(tile), int(kz), int(vtile)))
+        d = self.desc
+        d.stencil, d.stencil_tile, d.stencil_kz, d.stencil_vtile = int(stencil), int(tile), int(kz), int(vtile)
 
     def tune_stencil(self, iters=20, kzs=(16, 32, 64), use_cache=True):
         """Time every z-marching tile configuration x planes-per-block in `kzs` on this problem
@@ -252,25 +255,30 @@ class Solver:
                 cache = {}
         if use_cache and key in cache:
             e = cache[key]
-            self.set_stencil(0, e["tile"], e["kz"])
+            self.set_stencil(0, e["tile"], e["kz"], e.get("vtile", 0))
             return e
         stream = torch.cuda.ExternalStream(self.stream_handle())
-        ms = {}
-        for tile in range(self.lib.pts_stencil_tiles(self.desc.precision)):
-            for kz in kzs:
-                self.set_stencil(0, tile, kz)
-                self.iterate(2)
-                a = torch.cuda.Event(enable_timing=True)
-                b = torch.cuda.Event(enable_timing=True)
-                a.record(stream)
-                self.iterate(iters)
-                b.record(stream)
-                b.synchronize()
-                ms[f"{tile}:{kz}"] = a.elapsed_time(b) / iters
-        best = min(ms, key=ms.get)
-        tile, kz = map(int, best.split(":"))
-        self.set_stencil(0, tile, kz)
-        entry = {"tile": tile, "kz": kz, "ms_per_iteration": ms, "when": time.time()}
+
+        def timed(tile, kz, vtile):
+            self.set_stencil(0, tile, kz, vtile)
+            self.iterate(2)
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            self.iterate(iters)
+            b.record(stream)
+            b.synchronize()
+            return a.elapsed_time(b) / iters
+
+        # compute_Pt_τ! tiles x z-chunks with the default compute_V! tile, then the V tiles
+        ms = {f"{t}:{kz}:0": timed(t, kz, 0) for t in range(self.lib.pts_stencil_tiles(self.desc.precision))
+              for kz in kzs}
+        tile, kz, _ = map(int, min(ms, key=ms.get).split(":"))
+        for v in range(1, self.lib.pts_stencil_vtiles(self.desc.precision)):
+            ms[f"{tile}:{kz}:{v}"] = timed(tile, kz, v)
+        tile, kz, vtile = map(int, min(ms, key=ms.get).split(":"))
+        self.set_stencil(0, tile, kz, vtile)
+        entry = {"tile": tile, "kz": kz, "vtile": vtile, "ms_per_iteration": ms, "when": time.time()}
         if use_cache:
             try:
                 os.makedirs(os.path.dirname(path), exist_ok=True)

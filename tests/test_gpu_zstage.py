@@ -1,7 +1,8 @@
-"""The z-marching compute_Pt_τ! with TMA-staged planes against the one-thread-per-cell kernel.
+"""The z-marching compute_Pt_τ! and compute_V! + bc with TMA-staged planes against the
+one-thread-per-point kernels.
 
 FP64: every tile configuration and several z-chunk lengths give the same bits as the direct
-kernel after iterations (so the oracle parity of tests/test_gpu_parity.py carries over to
+kernels after iterations (so the oracle parity of tests/test_gpu_parity.py carries over to
 both), on ragged grids whose tiles, z-chunks and halos fall off every edge. The FP32 sweeps
 of the mixed path: both kernel forms agree to FP32 rounding. The kernel form can be switched
 on a live context.
@@ -35,12 +36,13 @@ def run(gpu_lib, variant, dims, it=12, precision="fp64", **kw):
 @pytest.mark.parametrize("dims", [(37, 29, 23), (33, 7, 40), (4, 3, 5)])
 def test_every_tile_is_bit_exact(gpu_lib, variant, dims):
     ref, cref = run(gpu_lib, variant, dims, stencil=1)
-    for tile in range(gpu_lib.pts_stencil_tiles(0)):
-        for kz in (0, 7, 1):
-            got, c = run(gpu_lib, variant, dims, stencil=0, stencil_tile=tile, stencil_kz=kz)
-            for k in ITERATED:
-                assert np.array_equal(got[k], ref[k]), (tile, kz, k)
-            assert c == cref
+    cfgs = [(t, kz, 0) for t in range(gpu_lib.pts_stencil_tiles(0)) for kz in (0, 7, 1)]
+    cfgs += [(0, kz, v) for v in range(1, gpu_lib.pts_stencil_vtiles(0)) for kz in (0, 3)]
+    for tile, kz, vtile in cfgs:
+        got, c = run(gpu_lib, variant, dims, stencil=0, stencil_tile=tile, stencil_kz=kz, stencil_vtile=vtile)
+        for k in ITERATED:
+            assert np.array_equal(got[k], ref[k]), (tile, kz, vtile, k)
+        assert c == cref
 
 
 @pytest.mark.gpu
@@ -53,7 +55,7 @@ def test_switching_on_a_live_context(gpu_lib):
     s = ptstokes.Solver("3d_ve_perf", *dims, lib=gpu_lib, nout=12, eps=1e-300, iter_max=11)
     s.setup_inclusion()
     s.assign_tau()
-    s.set_stencil(0, gpu_lib.pts_stencil_tiles(0) - 1, 5)
+    s.set_stencil(0, gpu_lib.pts_stencil_tiles(0) - 1, 5, gpu_lib.pts_stencil_vtiles(0) - 1)
     s.iterate(5)
     s.set_stencil(1)
     s.iterate(7)
@@ -72,8 +74,11 @@ def test_switching_on_a_live_context(gpu_lib):
 def test_fp32_sweep_forms_agree(gpu_lib, variant):
     dims = (45, 38, 31)
     ref, _ = run(gpu_lib, variant, dims, it=40, precision="mixed", stencil=1)
-    for tile in range(gpu_lib.pts_stencil_tiles(1)):
-        got, _ = run(gpu_lib, variant, dims, it=40, precision="mixed", stencil=0, stencil_tile=tile)
+    cfgs = [(t, 0) for t in range(gpu_lib.pts_stencil_tiles(1))]
+    cfgs += [(0, v) for v in range(1, gpu_lib.pts_stencil_vtiles(1))]
+    for tile, vtile in cfgs:
+        got, _ = run(gpu_lib, variant, dims, it=40, precision="mixed", stencil=0, stencil_tile=tile,
+                     stencil_vtile=vtile)
         for k in ITERATED:
             scale = max(float(np.abs(ref[k]).max()), 1e-300)
             # same FP32 arithmetic up to the compiler's multiply-add contraction
