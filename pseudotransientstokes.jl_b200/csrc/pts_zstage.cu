@@ -290,11 +290,12 @@ cudaError_t launch_cfg(const Geom& g, const Fields64& f, const Num& n, int kz, b
 
 // Tile configurations: tile height TY, ring slots R, producer warp PW, blocks per SM MINB
 // the registers must allow. Shared memory per block for the visco-elastic form: 32x4 with 2
-// slots 45 KB (5 blocks/SM), 32x8 83 KB (2), 32x6 63 KB (3), 32x2 25 KB (9).
+// slots 45 KB (4 blocks/SM by registers), 32x8 83 KB (2), 32x6 63 KB (3). The first is the
+// fastest measured at 511^3 on a B200 (5.01 ms; without the producer warp 5.07, 32x8 5.12).
 struct TileCfg {
     int ty, r, pw, minb;
 };
-constexpr TileCfg kTiles[] = {{4, 2, 0, 5}, {4, 2, 1, 4}, {4, 2, 1, 5}, {8, 2, 0, 2}, {6, 2, 0, 3}, {2, 2, 0, 9}};
+constexpr TileCfg kTiles[] = {{4, 2, 1, 4}, {4, 2, 0, 5}, {8, 2, 1, 2}, {6, 2, 1, 3}, {8, 2, 0, 2}};
 constexpr int kNumTiles = (int)(sizeof(kTiles) / sizeof(kTiles[0]));
 
 template <bool EL, bool PERF, int Q>
@@ -312,7 +313,6 @@ cudaError_t launch_form(int cfg, const Geom& g, const Fields64& f, const Num& n,
         case 2: return launch_q<EL, PERF, 2>(g, f, n, kz, sd, err, s);
         case 3: return launch_q<EL, PERF, 3>(g, f, n, kz, sd, err, s);
         case 4: return launch_q<EL, PERF, 4>(g, f, n, kz, sd, err, s);
-        case 5: return launch_q<EL, PERF, 5>(g, f, n, kz, sd, err, s);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -330,12 +330,12 @@ bool zstage_tile_info(int tile, int* ty, int* ring) {
 
 // ---- compute_V! + bc, z-staged (pts_zvbc.cuh), FP64 ----
 namespace zvbc {
-// Tile configurations (TY, R, MINB): shared memory per block 66 KB for 32x8 (3 blocks/SM),
-// 37 KB for 32x4 (6).
+// Tile configurations (TY, R, producer warp PW, MINB): shared memory per block 66 KB for
+// 32x8 (3 blocks/SM), 37 KB for 32x4 (6).
 struct VTile {
-    int ty, r, minb;
+    int ty, r, pw, minb;
 };
-constexpr VTile kVTiles[] = {{8, 2, 3}, {4, 2, 6}, {8, 2, 2}};
+constexpr VTile kVTiles[] = {{8, 2, 1, 3}, {8, 2, 0, 3}, {4, 2, 1, 5}, {4, 2, 0, 6}};
 constexpr int kNumVTiles = (int)(sizeof(kVTiles) / sizeof(kVTiles[0]));
 
 template <bool PERF, int Q>
@@ -348,7 +348,7 @@ cudaError_t launch64(const Geom& g, const Fields64& f, const Num& n, int kz, int
     if (!make_maps<double, c.ty, false>(&maps, g, hsrc, psrc)) return cudaErrorInvalidValue;
     ArgsV<double> a{f.Vx, f.Vy, f.Vz, {nullptr, nullptr, nullptr}};
     NumV<double> nv{n.dx, n.dy, n.dz, n._dx, n._dy, n._dz, 0.5};
-    return launch_v<double, PERF, false, c.ty, c.r, c.minb>(g, maps, a, nv, kz, err, s);
+    return launch_v<double, PERF, false, c.ty, c.r, c.pw != 0, c.minb>(g, maps, a, nv, kz, err, s);
 }
 
 template <bool PERF>
@@ -357,6 +357,7 @@ cudaError_t launch64_form(int tile, const Geom& g, const Fields64& f, const Num&
         case 0: return launch64<PERF, 0>(g, f, n, kz, err, s);
         case 1: return launch64<PERF, 1>(g, f, n, kz, err, s);
         case 2: return launch64<PERF, 2>(g, f, n, kz, err, s);
+        case 3: return launch64<PERF, 3>(g, f, n, kz, err, s);
         default: return cudaErrorInvalidValue;
     }
 }

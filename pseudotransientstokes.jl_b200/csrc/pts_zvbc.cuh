@@ -15,7 +15,7 @@
 // plane s that stage s does not hold (τxz, τyz, τzz, Pt, dτ_Rho at its own face) it carries
 // in registers from stage s-1, where it came as "s+1". Every face is written only by its
 // own thread and the bc copies write faces no thread reads, so the update is in place.
-// Thread 0 keeps R-1 stages in flight; waits are bounded (pts_tma.cuh).
+// A producer warp (PW) or thread 0 keeps R-1 stages in flight; waits are bounded (pts_tma.cuh).
 #pragma once
 #include "pts_internal.h"
 #include "pts_tma.cuh"
@@ -103,8 +103,8 @@ __device__ __forceinline__ void copies(T* A, idx_t c, T v, int a, int alo, int a
     if (ua && ub) A[c + sa + sb] = v;
 }
 
-template <typename T, bool PERF, bool SRC, int TY, int R, int MINB>
-__global__ void __launch_bounds__(32 * TY, MINB)
+template <typename T, bool PERF, bool SRC, int TY, int R, bool PW, int MINB>
+__global__ void __launch_bounds__(32 * (TY + (PW ? 1 : 0)), MINB)
     k3_V_bc_zs(const __grid_constant__ MapsV maps, Geom g, ArgsV<T> a, NumV<T> n, int kz, int* err) {
     using C = CfgV<T, TY, SRC>;
     extern __shared__ unsigned char smem_raw[];
@@ -124,7 +124,24 @@ __global__ void __launch_bounds__(32 * TY, MINB)
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    const bool prod = threadIdx.x == 0;
+    if (PW && warp == TY) {  // producer warp: one lane issues every copy, R stages ahead
+        if (lane != 0) return;
+        for (int q = 0; q < NHV; ++q) prefetch_map(&maps.h[q]);
+        for (int q = 0; q < C::NP; ++q) prefetch_map(&maps.p[q]);
+        int issued = 0;
+        for (int t = 0; t < nst; ++t) {
+            if (t >= R && !mbar_wait(&empty[t % R], (t / R - 1) & 1)) {
+                atomicExch(err, 1);
+                break;
+            }
+            issue_v<T, TY, SRC, R>(maps, smem, full, t, i0, j0, kb);
+            issued = t + 1;
+        }
+        drain_v<R>(full, 0, issued, err);
+        return;
+    }
+    // without a producer warp, thread 0 issues the copies between its own steps
+    const bool prod = !PW && threadIdx.x == 0;
     int issued = 0;
     if (prod) {
         for (int q = 0; q < NHV; ++q) prefetch_map(&maps.h[q]);
@@ -237,7 +254,7 @@ bool make_maps(MapsV* m, const Geom& g, const void* const hsrc[NHV], const void*
     return true;
 }
 
-template <typename T, bool PERF, bool SRC, int TY, int R, int MINB>
+template <typename T, bool PERF, bool SRC, int TY, int R, bool PW, int MINB>
 cudaError_t launch_v(const Geom& g, const MapsV& maps, const ArgsV<T>& a, const NumV<T>& n, int kz, int* err,
                      cudaStream_t s) {
     using C = CfgV<T, TY, SRC>;
@@ -246,14 +263,14 @@ cudaError_t launch_v(const Geom& g, const MapsV& maps, const ArgsV<T>& a, const 
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
     if (!attr[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(k3_V_bc_zs<T, PERF, SRC, TY, R, MINB>,
+        cudaError_t e = cudaFuncSetAttribute(k3_V_bc_zs<T, PERF, SRC, TY, R, PW, MINB>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         attr[dev] = true;
     }
     if (kz <= 0) kz = 32;
     const dim3 grid((g.nx + 1 + TX - 1) / TX, (g.ny + 1 + TY - 1) / TY, (g.nz + kz - 1) / kz);
-    k3_V_bc_zs<T, PERF, SRC, TY, R, MINB><<<grid, 32 * TY, smem, s>>>(maps, g, a, n, kz, err);
+    k3_V_bc_zs<T, PERF, SRC, TY, R, PW, MINB><<<grid, 32 * (TY + (PW ? 1 : 0)), smem, s>>>(maps, g, a, n, kz, err);
     return cudaGetLastError();
 }
 

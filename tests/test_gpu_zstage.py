@@ -14,7 +14,12 @@ ITERATED = ("Pt", "Vx", "Vy", "Vz", "txx", "tyy", "tzz", "txy", "txz", "tyz")
 
 
 def run(gpu_lib, variant, dims, it=12, precision="fp64", **kw):
+    """Fields after `it` iterations, assign_τ!, `it` more, and the residual check (its return
+    code and result: the smallest grids may go NaN, identically in both kernel forms)."""
+    import ctypes
+
     import ptstokes
+    from ptstokes._abi import PtsCheck
 
     s = ptstokes.Solver(variant, *dims, lib=gpu_lib, nout=it, eps=1e-300, iter_max=10 ** 9, precision=precision,
                         **kw)
@@ -25,10 +30,15 @@ def run(gpu_lib, variant, dims, it=12, precision="fp64", **kw):
     if variant != "3d_v":
         s.assign_tau()
     s.iterate(it)
-    chk = s.compute_res()
+    c = PtsCheck()
+    rc = gpu_lib.pts_compute_res(s.ctx, ctypes.byref(c))
     out = {k: s.get(k) for k in ITERATED}
     s.close()
-    return out, chk
+    return out, (rc, bytes(c))
+
+
+def same_bits(a, b):
+    return a.shape == b.shape and np.array_equal(a.view(np.uint64), b.view(np.uint64))
 
 
 @pytest.mark.gpu
@@ -41,7 +51,7 @@ def test_every_tile_is_bit_exact(gpu_lib, variant, dims):
     for tile, kz, vtile in cfgs:
         got, c = run(gpu_lib, variant, dims, stencil=0, stencil_tile=tile, stencil_kz=kz, stencil_vtile=vtile)
         for k in ITERATED:
-            assert np.array_equal(got[k], ref[k]), (tile, kz, vtile, k)
+            assert same_bits(got[k], ref[k]), (tile, kz, vtile, k)
         assert c == cref
 
 
@@ -63,7 +73,7 @@ def test_switching_on_a_live_context(gpu_lib):
     s.set_stencil(0, 0, 0)
     assert s.solve()["iters"] == 12  # a captured block after the switch
     for k in ITERATED:
-        assert np.array_equal(s.get(k), ref[k]), k
+        assert same_bits(s.get(k), ref[k]), k
     with pytest.raises(ptstokes.PtsError):
         s.set_stencil(0, gpu_lib.pts_stencil_tiles(0), 0)
     s.close()
