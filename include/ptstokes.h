@@ -189,6 +189,23 @@ typedef struct pts_inclusion {
  * pts_init_inclusion). The list is read before the call returns. */
 #define PTS_MAX_INCLUSIONS 65536
 PTS_API int pts_init_inclusions(pts_ctx* ctx, const pts_inclusion* list, int32_t count, double mus0, double ebg);
+/* ---- z-slab decomposition over several GPUs (the ImplicitGlobalGrid part of
+ * scripts/stokes_3D/Stokes3D_ve_multixpu.jl, along z): each rank holds nz local planes that
+ * overlap its neighbours by two (nz_g = P*(nz-2) + 2, init_global_grid, :138), and the host
+ * exchanges the halo planes of V after every PT iteration (update_halo!(Vx, Vy, Vz), :238)
+ * and of Mus, Musτ during set-up (:182-195), and reduces the check over ranks (:243-248).
+ * ptstokes.multi drives it over torch.distributed. */
+/* Before the set-up: this context is the slab [zoff, zoff+nz) of a global grid of nz_global
+ * z-cells: dz = lz/nz_global, and the initial conditions use the global z coordinate
+ * (z_g(iz, dz, A), :174-176). */
+PTS_API int pts_set_decomposition(pts_ctx* ctx, int32_t zoff, int32_t nz_global);
+/* Copy z-plane k (0-based, the field's reference extents) of a 3D field to or from a dense
+ * device buffer of extent(1)*extent(2) doubles; synchronous. */
+PTS_API int pts_get_plane_device(pts_ctx* ctx, int32_t id, int32_t k, double* dev, int64_t n);
+PTS_API int pts_set_plane_device(pts_ctx* ctx, int32_t id, int32_t k, const double* dev, int64_t n);
+/* The local pieces of the check, to be reduced over ranks (norm_g, minimum_g, maximum_g,
+ * :243-248): {Σ Rx², Σ Ry², Σ Rz², Σ ∇V², min Vx, max Vx, min Pt, max Pt}; synchronous. */
+PTS_API int pts_check_partials(pts_ctx* ctx, double out[8]);
 /* smooth!(Mus2, Mus, fact) nsweeps times with the Mus/Mus2 swap (Stokes3D_ve_perf.jl:173-177). */
 PTS_API int pts_smooth(pts_ctx* ctx, int32_t nsweeps, double fact);
 /* Musτ .= Mus; compute_maxloc!(Musτ, Mus); bc_x!/bc_y!/bc_z!(Musτ) (Stokes3D_ve_perf.jl:178-182). */

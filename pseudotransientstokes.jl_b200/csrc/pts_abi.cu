@@ -738,6 +738,64 @@ int pts_init_inclusions(pts_ctx* c, const pts_inclusion* list, int32_t count, do
     return PTS_OK;
 }
 
+int pts_set_decomposition(pts_ctx* c, int32_t zoff, int32_t nz_global) {
+    int rc = enter(c);
+    if (rc) return rc;
+    if (!c->d3) return fail(c, PTS_E_STATE, "a z-slab decomposition needs a 3D variant");
+    if (zoff < 0 || nz_global < c->g.nz || zoff + c->g.nz > nz_global)
+        return fail(c, PTS_E_INVAL, "the slab [zoff, zoff+nz) must lie in [0, nz_global)");
+    Num& n = c->n;
+    n.zoff = zoff;
+    n.dz = c->d.lz / nz_global;  // dz = lz/nz_g() (Stokes3D_ve_multixpu.jl:139)
+    n._dz = 1.0 / n.dz;
+    n.Vpdt = std::min(std::min(n.dx, n.dy), n.dz) * c->d.CFL;
+    set_damping(c, n.Vdmp, n.beta_n, n.Vsc, n.Ptsc);
+    CK(cudaStreamSynchronize(c->stream));
+    drop_graph(c);  // captured launches hold the previous numerics
+    return PTS_OK;
+}
+
+// One z-plane k of a 3D field (the reference's extents) to or from a dense device buffer.
+int plane_copy(pts_ctx* c, int32_t id, int32_t k, double* dev, int64_t n, bool to_field) {
+    int rc = enter(c);
+    if (rc) return rc;
+    FInfo fi;
+    if (!c->d3) return fail(c, PTS_E_STATE, "plane copies are for 3D fields");
+    if (!field_info(c, id, &fi)) return fail(c, PTS_E_INVAL, "field not present for this variant: " + std::to_string(id));
+    if (*fi.ptr == nullptr) return fail(c, PTS_E_STATE, "field not allocated: " + std::to_string(id));
+    if (!dev) return fail(c, PTS_E_INVAL, "null device pointer");
+    if (k < 0 || k >= fi.e[2]) return fail(c, PTS_E_INVAL, "plane index out of range");
+    if (n != fi.e[0] * fi.e[1]) return fail(c, PTS_E_INVAL, "a plane of this field has " + std::to_string(fi.e[0] * fi.e[1]) + " elements");
+    double* p = *fi.ptr + gidx(c->g, fi.s[0], fi.s[1], fi.s[2] + k);
+    const size_t pitch = (size_t)c->g.px * sizeof(double), w = (size_t)fi.e[0] * sizeof(double);
+    if (to_field)
+        CK(cudaMemcpy2DAsync(p, pitch, dev, w, w, (size_t)fi.e[1], cudaMemcpyDeviceToDevice, c->stream));
+    else
+        CK(cudaMemcpy2DAsync(dev, w, p, pitch, w, (size_t)fi.e[1], cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return PTS_OK;
+}
+
+int pts_get_plane_device(pts_ctx* c, int32_t id, int32_t k, double* dev, int64_t n) {
+    return plane_copy(c, id, k, dev, n, false);
+}
+
+int pts_set_plane_device(pts_ctx* c, int32_t id, int32_t k, const double* dev, int64_t n) {
+    return plane_copy(c, id, k, const_cast<double*>(dev), n, true);
+}
+
+int pts_check_partials(pts_ctx* c, double out[8]) {
+    int rc = enter(c);
+    if (rc) return rc;
+    if (!out) return fail(c, PTS_E_INVAL, "null argument");
+    if ((rc = enqueue_check(c)) != PTS_OK) return rc;
+    if ((rc = synced(c)) != PTS_OK) return rc;
+    const CheckResult& r = *c->h_result;
+    const double v[8] = {r.sRx, r.sRy, r.sRz, r.sdiv, r.vmin, r.vmax, r.pmin, r.pmax};
+    for (int q = 0; q < 8; ++q) out[q] = v[q];
+    return PTS_OK;
+}
+
 int pts_smooth(pts_ctx* c, int32_t nsweeps, double fact) {
     int rc = enter(c);
     if (rc) return rc;

@@ -63,6 +63,7 @@ struct Num {
     double Vpdt, max_l, Re;
     double lx, ly, lz;
     int adjoint;  // 3D_V: iterate the transposed (adjoint) system, ghosts folded (pts_abi.cu)
+    int zoff;     // z-slab decomposition: global index of this context's first z-plane (ICs)
     // damped variants (Stokes2D_ve0.jl:95-105, Stokes3D0_multixpu.jl:105-120): Vdmp, β_n,
     // Vsc, Ptsc and the derived dampX = 1-Vdmp/nx (Y, Z alike), min_dxy2 = min(dx,dy[,dz])^2,
     // max_nxy = max(nx,ny[,nz])
@@ -91,6 +92,7 @@ constexpr int kCheckSlots = 8;
 struct CheckResult {
     double err, nRx, nRy, nRz, ndiv, vmin, vmax, pmin, pmax;
     double flag_nan;
+    double sRx, sRy, sRz, sdiv;  // the sums of squares the norms come from
 };
 
 // ---- launchers implemented in pts_kernels64.cu (FP64, no FMA contraction) ----

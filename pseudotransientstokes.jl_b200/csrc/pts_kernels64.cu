@@ -848,6 +848,7 @@ __global__ void k_check_finalize(const double* partials, int nblocks, double lx,
         c.nRz = (ndim == 3) ? sqrt(sm[0][2]) / dP * lx / sqrt(lenRz) : 0.0;
         c.ndiv = sqrt(sm[0][3]) / dV * lx / sqrt(lenDiv);
         c.vmin = sm[0][4]; c.vmax = sm[0][5]; c.pmin = sm[0][6]; c.pmax = sm[0][7];
+        c.sRx = sm[0][0]; c.sRy = sm[0][1]; c.sRz = sm[0][2]; c.sdiv = sm[0][3];
         const bool bad = isnan(c.nRx) || isnan(c.nRy) || isnan(c.nRz) || isnan(c.ndiv);
         c.err = bad ? NAN : fmax(fmax(c.nRx, c.nRy), fmax(c.nRz, c.ndiv));
         c.flag_nan = bad ? 1.0 : 0.0;
@@ -1547,7 +1548,7 @@ __global__ void k_init_inclusion(Geom g, Fields64 f, Num n, double mus0, double 
     if (i < nx && j < ny && k < (D3 ? nz : 1)) {
         double rad2 = X * X + Y * Y;
         if (D3) {
-            const double Z = ((double)k * n.dz + 0.5 * n.dz) - 0.5 * n.lz;
+            const double Z = ((double)(k + n.zoff) * n.dz + 0.5 * n.dz) - 0.5 * n.lz;
             rad2 = rad2 + Z * Z;
         }
         f.Mus[c] = (rad2 < radius2) ? musi : mus0;
@@ -1556,8 +1557,8 @@ __global__ void k_init_inclusion(Geom g, Fields64 f, Num n, double mus0, double 
                           : ((double)i * n.dx - 0.5 * n.lx);
     if (j < ny && k < (D3 ? nz : 1)) f.Vx[c] = (-ebg) * xv;
     if (D3) {
-        const double zv = IGG ? ((((double)k * n.dz + (-0.5 * n.dz)) + 0.5 * n.dz) - 0.5 * n.lz)
-                              : ((double)k * n.dz - 0.5 * n.lz);
+        const double zv = IGG ? ((((double)(k + n.zoff) * n.dz + (-0.5 * n.dz)) + 0.5 * n.dz) - 0.5 * n.lz)
+                              : ((double)(k + n.zoff) * n.dz - 0.5 * n.lz);
         if (i < nx && j < ny) f.Vz[c] = ebg * zv;
     } else {
         if (i < nx) f.Vy[c] = ebg * ((double)j * n.dy - 0.5 * n.ly);
@@ -1582,7 +1583,7 @@ __global__ void k_init_inclusions(Geom g, Fields64 f, Num n, const pts_inclusion
     if (i < nx && j < ny && k < (D3 ? nz : 1)) {
         const double X = ((double)i * n.dx + 0.5 * n.dx) - 0.5 * n.lx;
         const double Y = ((double)j * n.dy + 0.5 * n.dy) - 0.5 * n.ly;
-        const double Z = D3 ? ((double)k * n.dz + 0.5 * n.dz) - 0.5 * n.lz : 0.0;
+        const double Z = D3 ? ((double)(k + n.zoff) * n.dz + 0.5 * n.dz) - 0.5 * n.lz : 0.0;
         double mu = mus0;
         for (int q = 0; q < count; ++q) {
             const double ax = X - __ldg(&inc[q].x), ay = Y - __ldg(&inc[q].y);
@@ -1602,8 +1603,8 @@ __global__ void k_init_inclusions(Geom g, Fields64 f, Num n, const pts_inclusion
                           : ((double)i * n.dx - 0.5 * n.lx);
     if (j < ny && k < (D3 ? nz : 1)) f.Vx[c] = (-ebg) * xv;
     if (D3) {
-        const double zv = IGG ? ((((double)k * n.dz + (-0.5 * n.dz)) + 0.5 * n.dz) - 0.5 * n.lz)
-                              : ((double)k * n.dz - 0.5 * n.lz);
+        const double zv = IGG ? ((((double)(k + n.zoff) * n.dz + (-0.5 * n.dz)) + 0.5 * n.dz) - 0.5 * n.lz)
+                              : ((double)(k + n.zoff) * n.dz - 0.5 * n.lz);
         if (i < nx && j < ny) f.Vz[c] = ebg * zv;
     } else {
         if (i < nx) f.Vy[c] = ebg * ((double)j * n.dy - 0.5 * n.ly);

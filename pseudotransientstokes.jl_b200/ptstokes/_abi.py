@@ -119,6 +119,11 @@ SIGNATURES = {
     "pts_init_inclusion": ([_P, _D, _D, _D, _D], ctypes.c_int),
     "pts_init_inclusions": ([_P, ctypes.POINTER(PtsInclusion), _I32, _D, _D], ctypes.c_int),
     "pts_smooth": ([_P, _I32, _D], ctypes.c_int),
+    # z-slab decomposition (ptstokes.multi)
+    "pts_set_decomposition": ([_P, _I32, _I32], ctypes.c_int),
+    "pts_get_plane_device": ([_P, _I32, _I32, _DP, _I64], ctypes.c_int),
+    "pts_set_plane_device": ([_P, _I32, _I32, _DP, _I64], ctypes.c_int),
+    "pts_check_partials": ([_P, ctypes.POINTER(_D)], ctypes.c_int),
     "pts_compute_maxloc": ([_P], ctypes.c_int),
     "pts_compute_iter_params": ([_P], ctypes.c_int),
     "pts_set_damping": ([_P] + [ctypes.c_double] * 4, ctypes.c_int),
