@@ -222,6 +222,28 @@ function top_vz(logμ::Array{Float64,3}, fwd::Ctx, adj::Ctx, Vwall)
     return Vz[2:end-1, 2:end-1, end-1]
 end
 
+# ---- z-slab decomposition (the ImplicitGlobalGrid part of Stokes3D_ve_multixpu.jl) ----
+# The caller owns the transport (MPI from Julia): these move planes and reduce nothing.
+
+"Make `ctx` the z-slab [zoff, zoff+nz) of a global grid of nz_g cells (before the set-up)."
+set_decomposition!(ctx::Ctx, zoff::Integer, nz_g::Integer) =
+    check(ctx, ccall((:pts_set_decomposition, libpts), Cint, (Ptr{Cvoid}, Int32, Int32), ctx.ptr, zoff, nz_g))
+
+"z-plane k (0-based) of a field to/from a CuArray's device memory (`pointer(A)` as UInt)."
+get_plane_device!(ctx::Ctx, f::Symbol, k::Integer, devptr::UInt, n::Integer) =
+    check(ctx, ccall((:pts_get_plane_device, libpts), Cint, (Ptr{Cvoid}, Int32, Int32, UInt, Int64),
+                     ctx.ptr, field_id(f), k, devptr, n))
+set_plane_device!(ctx::Ctx, f::Symbol, k::Integer, devptr::UInt, n::Integer) =
+    check(ctx, ccall((:pts_set_plane_device, libpts), Cint, (Ptr{Cvoid}, Int32, Int32, UInt, Int64),
+                     ctx.ptr, field_id(f), k, devptr, n))
+
+"{Σ Rx², Σ Ry², Σ Rz², Σ ∇V², min Vx, max Vx, min Pt, max Pt} of this slab, for MPI.Allreduce."
+function check_partials(ctx::Ctx)
+    out = zeros(Float64, 8)
+    check(ctx, ccall((:pts_check_partials, libpts), Cint, (Ptr{Cvoid}, Ptr{Float64}), ctx.ptr, out))
+    return out
+end
+
 # Reverse rules for top_vz (and its visco-elastic time-loop twin top_vz_ve) are the
 # ChainRulesCore.rrule methods of PTStokesB200ChainRules.jl, next to this file.
 

@@ -7,8 +7,9 @@
   the oracle after a few PT iterations (NaN where the oracle has NaN).
 * A full-size case: 3D VE (Stokes3D_ve_perf.jl kernels) at 255^3, three iterations, bit for
   bit against the oracle.
-* The largest size of the benchmark, 511^3, through a property that needs no oracle: the
-  single-pass kernels and the two-kernel path give the same fields bit for bit.
+* The benchmark's size, 511^3: the set-up and three PT iterations of the Stokes3D_ve_perf.jl
+  problem bit for bit against the oracle (the z-marching kernels, the default), and the
+  single-pass kernels against the two-kernel path.
 """
 import numpy as np
 import pytest
@@ -71,6 +72,18 @@ def test_full_size_255_bit_exact(gpu_lib):
     g.iterate(3)
     g.sync()
     _equal(o, g, F3)
+    g.close()
+
+
+def test_full_size_511_bit_exact(gpu_lib):
+    o, g = _pair(gpu_lib, "3d_ve_perf", (511, 511, 511))
+    o.assign_tau()
+    g.assign_tau()
+    for _ in range(3):
+        o.iteration()
+    g.iterate(3)
+    g.sync()
+    _equal(o, g, ["Mus", "Must"] + F3)
     g.close()
 
 
