@@ -125,7 +125,9 @@ enum pts_field {
     PTS_F_COUNT
 };
 
-/* Result of one convergence check (Stokes3D_ve_perf.jl:210-218). */
+/* Result of one convergence check (Stokes3D_ve_perf.jl:210-218). The norms are
+ * ‖R‖/(Pmax-Pmin)*L/√len and ‖∇V‖/(Vmax-Vmin)*L/√len with L = lx for every norm, as the
+ * scripts do, unless pts_set_norm_scales says otherwise. */
 typedef struct pts_check {
     double err;                                       /* max of the four norms      */
     double norm_Rx, norm_Ry, norm_Rz, norm_divV;      /* norm_Rz = 0 in 2D          */
@@ -206,6 +208,10 @@ PTS_API int pts_set_plane_device(pts_ctx* ctx, int32_t id, int32_t k, const doub
 /* The local pieces of the check, to be reduced over ranks (norm_g, minimum_g, maximum_g,
  * :243-248): {Σ Rx², Σ Ry², Σ Rz², Σ ∇V², min Vx, max Vx, min Pt, max Pt}; synchronous. */
 PTS_API int pts_check_partials(pts_ctx* ctx, double out[8]);
+/* The lengths L of norm_Rx, norm_Ry, norm_Rz and norm_∇V (default lx for all four). The
+ * aspect-ratio script scales norm_Rx by lx and norm_Ry, norm_∇V by ly
+ * (scripts/Stokes2D_ve_param.jl:175-177). */
+PTS_API int pts_set_norm_scales(pts_ctx* ctx, double sRx, double sRy, double sRz, double sdiv);
 /* smooth!(Mus2, Mus, fact) nsweeps times with the Mus/Mus2 swap (Stokes3D_ve_perf.jl:173-177). */
 PTS_API int pts_smooth(pts_ctx* ctx, int32_t nsweeps, double fact);
 /* Musτ .= Mus; compute_maxloc!(Musτ, Mus); bc_x!/bc_y!/bc_z!(Musτ) (Stokes3D_ve_perf.jl:178-182). */

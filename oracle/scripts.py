@@ -289,6 +289,61 @@ class VE2D(_Case2D):
         return self.norm_err(("Rx", "Ry"), "divV")
 
 
+class VE2DParam(VE2D):
+    """scripts/Stokes2D_ve_param.jl, the aspect-ratio study (2D Maxwell VE, role kernels):
+    ly = 10, lx = nsub*ly, nx = nsub*(ny+1)-1 (:99-107), nsub inclusions of radius 1 along x
+    (:138-141), min_lxy = fact*min(lx,ly) in the iteration parameters (:110, :150), CFL
+    0.87/sqrt(2), eps = 1e-6, iterMax = 100nx, nout = nx (:103-109), and norm_Rx scaled by lx,
+    norm_Ry and norm_∇V by ly (:175-177)."""
+
+    defaults = dict(nt=5, eps=1e-6, CFL=0.87 / math.sqrt(2), Re=5 * PI, r=1.0, nsub=1, fact=1.0, ly=10.0)
+
+    def __init__(self, ny, nsub=1, fact=1.0, **kw):
+        ly = kw.pop("ly", 10.0)
+        nx = nsub * (ny + 1) - 1
+        super().__init__(nx, ny, None, ly=ly, lx=nsub * ly, nsub=nsub, fact=fact, **kw)
+        self.iterMax = 100 * nx
+        self.nout = nx
+
+    def setup(self):
+        super().setup()  # allocations, the script's Vx/Vy; Mus replaced below
+        nx, ny, dx, dy, ly = self.nx, self.ny, self.dx, self.dy, self.ly
+        ix = np.arange(1, nx + 1, dtype=np.float64)
+        iy = np.arange(1, ny + 1, dtype=np.float64)
+        Mus = self.mus0 * np.ones((nx, ny), order="F")
+        for isub in range(1, self.nsub + 1):
+            X = (ix - 1) * dx + 0.5 * dx - 0.5 * ly - (isub - 1) * ly
+            Y = (iy - 1) * dy + 0.5 * dy - 0.5 * ly
+            Rad2 = X[:, None] ** 2 + Y[None, :] ** 2
+            Mus[Rad2 < 1.0] = self.musi
+        for k in ("Pt", "divV", "txx", "tyy", "txy", "txx_o", "tyy_o", "txy_o"):
+            self.f[k][...] = 0.0
+        self.init_viscosity(Mus)
+        return self
+
+    def iter_params(self):
+        min_lxy = self.fact * min(self.lx, self.ly)
+        self.L.ora_iter_params_ve(self.A("dtRho"), self.A("Gdt"), self.A("Must"), self.Vpdt, self.G, self.dt,
+                                  self.Re, self.r, min_lxy)
+
+    def check(self):
+        A = self.A
+        self.L.ora2ve_compute_Res(A("Rx"), A("Ry"), A("Pt"), A("txx"), A("tyy"), A("txy"), self.dx, self.dy)
+        _, vmin, vmax = stats(self.f["Vx"])
+        _, pmin, pmax = stats(self.f["Pt"])
+        norms = []
+        for n, L in (("Rx", self.lx), ("Ry", self.ly)):
+            sq, _, _ = stats(self.f[n])
+            norms.append(math.sqrt(sq) / (pmax - pmin) * L / math.sqrt(self.f[n].size))
+        sq, _, _ = stats(self.f["divV"])
+        norms.append(math.sqrt(sq) / (vmax - vmin) * self.ly / math.sqrt(self.f["divV"].size))
+        return max(norms), norms
+
+    def output_line(self):
+        """The script's result line (`println(io, "$(nx) $(ny) $(nsub) $(fact) $(ittot) $(nt) $(err)")`)."""
+        return self.nx, self.ny, self.nsub, self.fact, self.ittot, self.nt
+
+
 class VE2DPerf(VE2D):
     """scripts/Stokes2D_ve_perf.jl (2D VE, fused explicit-index kernels)."""
 

@@ -523,6 +523,7 @@ int pts_create(const pts_desc* d, pts_ctx** out) {
     n.Vpdt = (d3 ? std::min(std::min(n.dx, n.dy), n.dz) : std::min(n.dx, n.dy)) * d->CFL;
     n.max_l = d->max_l > 0 ? d->max_l : (d3 ? std::max(std::max(d->lx, d->ly), d->lz) : std::max(d->lx, d->ly));
     n.adjoint = d->adjoint ? 1 : 0;
+    for (double& v : n.nsc) v = d->lx;  // norm_R* = ‖R‖/(Pmax-Pmin)*lx/√len (Stokes3D_ve_perf.jl:212-216)
     if (d3) set_damping(c, 4.0, 3.0, 1.0, 5.0);  // Stokes3D0_multixpu.jl:105-108
     else set_damping(c, 4.0, 2.0, 1.0, 3.0);     // Stokes2D_ve0.jl:95-98
     int rc = PTS_OK;
@@ -793,6 +794,19 @@ int pts_check_partials(pts_ctx* c, double out[8]) {
     const CheckResult& r = *c->h_result;
     const double v[8] = {r.sRx, r.sRy, r.sRz, r.sdiv, r.vmin, r.vmax, r.pmin, r.pmax};
     for (int q = 0; q < 8; ++q) out[q] = v[q];
+    return PTS_OK;
+}
+
+int pts_set_norm_scales(pts_ctx* c, double sRx, double sRy, double sRz, double sdiv) {
+    int rc = enter(c);
+    if (rc) return rc;
+    if (!(sRx > 0) || !(sRy > 0) || !(sRz > 0) || !(sdiv > 0)) return fail(c, PTS_E_INVAL, "scales must be > 0");
+    c->n.nsc[0] = sRx;
+    c->n.nsc[1] = sRy;
+    c->n.nsc[2] = sRz;
+    c->n.nsc[3] = sdiv;
+    CK(cudaStreamSynchronize(c->stream));
+    drop_graph(c);  // the captured check holds the previous scales
     return PTS_OK;
 }
 

@@ -64,6 +64,7 @@ struct Num {
     double lx, ly, lz;
     int adjoint;  // 3D_V: iterate the transposed (adjoint) system, ghosts folded (pts_abi.cu)
     int zoff;     // z-slab decomposition: global index of this context's first z-plane (ICs)
+    double nsc[4];  // lengths that scale norm_Rx, norm_Ry, norm_Rz, norm_∇V in the check
     // damped variants (Stokes2D_ve0.jl:95-105, Stokes3D0_multixpu.jl:105-120): Vdmp, β_n,
     // Vsc, Ptsc and the derived dampX = 1-Vdmp/nx (Y, Z alike), min_dxy2 = min(dx,dy[,dz])^2,
     // max_nxy = max(nx,ny[,nz])

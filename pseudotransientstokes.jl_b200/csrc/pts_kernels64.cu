@@ -819,7 +819,7 @@ __global__ void __launch_bounds__(256) k2_check(Geom g, Fields64 f, Num n, doubl
 
 // Finaliser: fixed-order sum of the block partials, then the norms of the check
 // (Stokes3D_ve_perf.jl:213-218): norm_R = norm(R)/(Pmax-Pmin)*lx/sqrt(length(R)).
-__global__ void k_check_finalize(const double* partials, int nblocks, double lx, double lenRx, double lenRy,
+__global__ void k_check_finalize(const double* partials, int nblocks, double4 sc, double lenRx, double lenRy,
                                  double lenRz, double lenDiv, int ndim, CheckResult* out) {
     __shared__ double sm[256][kCheckSlots];
     const int t = threadIdx.x;
@@ -843,10 +843,10 @@ __global__ void k_check_finalize(const double* partials, int nblocks, double lx,
     if (t == 0) {
         const double dP = sm[0][7] - sm[0][6], dV = sm[0][5] - sm[0][4];
         CheckResult c;
-        c.nRx = sqrt(sm[0][0]) / dP * lx / sqrt(lenRx);
-        c.nRy = sqrt(sm[0][1]) / dP * lx / sqrt(lenRy);
-        c.nRz = (ndim == 3) ? sqrt(sm[0][2]) / dP * lx / sqrt(lenRz) : 0.0;
-        c.ndiv = sqrt(sm[0][3]) / dV * lx / sqrt(lenDiv);
+        c.nRx = sqrt(sm[0][0]) / dP * sc.x / sqrt(lenRx);
+        c.nRy = sqrt(sm[0][1]) / dP * sc.y / sqrt(lenRy);
+        c.nRz = (ndim == 3) ? sqrt(sm[0][2]) / dP * sc.z / sqrt(lenRz) : 0.0;
+        c.ndiv = sqrt(sm[0][3]) / dV * sc.w / sqrt(lenDiv);
         c.vmin = sm[0][4]; c.vmax = sm[0][5]; c.pmin = sm[0][6]; c.pmax = sm[0][7];
         c.sRx = sm[0][0]; c.sRy = sm[0][1]; c.sRz = sm[0][2]; c.sdiv = sm[0][3];
         const bool bad = isnan(c.nRx) || isnan(c.nRy) || isnan(c.nRz) || isnan(c.ndiv);
@@ -1815,7 +1815,7 @@ cudaError_t launch_check(int v, const Geom& g, const Fields64& f, const Num& n, 
     const double lenRy = d3 ? (nx - 2) * (ny - 1) * (nz - 2) : (nx - 2) * (ny - 1);
     const double lenRz = d3 ? (nx - 2) * (ny - 2) * (nz - 1) : 1.0;
     const double lenDiv = nx * ny * nz;
-    k_check_finalize<<<1, 256, 0, s>>>(partials, nb, n.lx, lenRx, lenRy, lenRz, lenDiv, d3 ? 3 : 2, result);
+    k_check_finalize<<<1, 256, 0, s>>>(partials, nb, make_double4(n.nsc[0], n.nsc[1], n.nsc[2], n.nsc[3]), lenRx, lenRy, lenRz, lenDiv, d3 ? 3 : 2, result);
     return cudaGetLastError();
 }
 
@@ -1870,7 +1870,7 @@ cudaError_t launch_sources(int v, const Geom& g, const Fields64& f, const Mixed3
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     const double nx = g.nx, ny = g.ny, nz = g.nz;
-    k_check_finalize<<<1, 256, 0, s>>>(partials, nb, n.lx, (nx - 1) * (ny - 2) * (nz - 2), (nx - 2) * (ny - 1) * (nz - 2),
+    k_check_finalize<<<1, 256, 0, s>>>(partials, nb, make_double4(n.nsc[0], n.nsc[1], n.nsc[2], n.nsc[3]), (nx - 1) * (ny - 2) * (nz - 2), (nx - 2) * (ny - 1) * (nz - 2),
                                        (nx - 2) * (ny - 2) * (nz - 1), nx * ny * nz, 3, result);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     k3_srcw<<<grid_faces(g, true), blk(), 0, s>>>(g, f, m, n);

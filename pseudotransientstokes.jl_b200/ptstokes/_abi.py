@@ -124,6 +124,7 @@ SIGNATURES = {
     "pts_get_plane_device": ([_P, _I32, _I32, _DP, _I64], ctypes.c_int),
     "pts_set_plane_device": ([_P, _I32, _I32, _DP, _I64], ctypes.c_int),
     "pts_check_partials": ([_P, ctypes.POINTER(_D)], ctypes.c_int),
+    "pts_set_norm_scales": ([_P, _D, _D, _D, _D], ctypes.c_int),
     "pts_compute_maxloc": ([_P], ctypes.c_int),
     "pts_compute_iter_params": ([_P], ctypes.c_int),
     "pts_set_damping": ([_P] + [ctypes.c_double] * 4, ctypes.c_int),

@@ -11,6 +11,8 @@ scripts' NX/NY/NZ environment variables (``haskey(ENV, "NX") ? parse(Int, ENV["N
     Stokes3D_ve         scripts/stokes_3D/Stokes3D_ve_multixpu.jl (one rank)
     Stokes3D_ve_perf    scripts/stokes_3D/Stokes3D_ve_perf.jl
     Stokes3D_v          3D viscous (no reference script)
+    Stokes2D_ve_param   scripts/Stokes2D_ve_param.jl (aspect-ratio study); aspect_ratio_sweep is
+                        scripts/runme_Stokes2D_aspect_ratio.jl's loop over its parameters
     Stokes2D0           scripts/previous_damp/Stokes2D0.jl    (damped scheme)
     Stokes2D_ve0        scripts/previous_damp/Stokes2D_ve0.jl (damped scheme)
     Stokes3D0           scripts/stokes_3D/previous_damp/Stokes3D0_multixpu.jl (one rank, damped scheme)
@@ -102,6 +104,107 @@ def Stokes3D0(nx=None, ny=None, nz=None, return_solver=False, verbose=False, **k
     damped scheme; NX, NY, NZ default 63)."""
     return _script("3d_v_damp", nx or _env("NX", 63), ny or _env("NY", 63), nz or _env("NZ", 63), return_solver,
                    verbose, **kw)
+
+
+def ve_param_solver(ny, nsub=1, fact=1.0, ly=10.0, lib=None, **kw):
+    """The context of scripts/Stokes2D_ve_param.jl: ly = 10, lx = nsub*ly, nx = nsub*(ny+1)-1
+    (:99-107); CFL 0.87/sqrt(2), eps = 1e-6, iterMax = 100nx, nout = nx (:103-109);
+    min_lxy = fact*min(lx,ly) as the length of the iteration parameters (:110, :150); norm_Rx
+    scaled by lx, norm_Ry and norm_∇V by ly (:175-177). Set up as the script does: pure-shear
+    velocities, nsub inclusions of radius 1 centred at (isub-1)*ly + ly/2 along x (built on the
+    host as the script builds it, :138-141), 10 smooth! sweeps, maxloc, iteration parameters."""
+    import math
+
+    import numpy as np
+
+    lx = nsub * ly
+    nx = nsub * (ny + 1) - 1
+    p = dict(lx=lx, ly=ly, CFL=0.87 / math.sqrt(2), eps=1e-6, iter_max=100 * nx, nout=nx, nt=5,
+             max_l=fact * min(lx, ly))
+    p.update(kw)
+    s = Solver("2d_ve", nx, ny, lib=lib, **p)
+    s._ck(s.lib.pts_set_norm_scales(s.ctx, lx, ly, 1.0, ly))
+    dx, dy = lx / nx, ly / ny
+    ix = np.arange(1, nx + 1, dtype=np.float64)
+    iy = np.arange(1, ny + 1, dtype=np.float64)
+    mus = np.ones((nx, ny), order="F")
+    for isub in range(1, nsub + 1):
+        X = (ix - 1) * dx + 0.5 * dx - 0.5 * ly - (isub - 1) * ly
+        Y = (iy - 1) * dy + 0.5 * dy - 0.5 * ly
+        mus[(X[:, None] ** 2 + Y[None, :] ** 2) < 1.0] = 1e-3
+    s.init_inclusion(1.0, 1.0, 0.0, 1.0)  # pure shear, every other field zero
+    s.set("Mus", mus)
+    s.smooth(10, 1.0)
+    s.compute_maxloc()
+    s.compute_iter_params()
+    s.nsub, s.fact = nsub, fact
+    return s
+
+
+def Stokes2D_ve_param(ny=None, nsub=None, fact=None, return_solver=False, verbose=False, **kw):
+    """scripts/Stokes2D_ve_param.jl:87-212: 5 Maxwell steps of the aspect-ratio problem (RESOL,
+    NSUB, FACT from the environment as the script reads them). Returns (xc, yc, Pt) and, with
+    return_solver, the solver and its outcome, including the script's output line
+    ``nx ny nsub fact ittot nt err``."""
+    ny = ny or _env("RESOL", 255)
+    nsub = nsub or _env("NSUB", 1)
+    fact = fact if fact is not None else float(os.environ.get("FACT", "1.0"))
+    s = ve_param_solver(ny, nsub, fact, **kw)
+    t0 = time.perf_counter()
+    res = s.run()
+    res["wall_s"] = time.perf_counter() - t0
+    res["line"] = f"{s.nx} {s.ny} {nsub} {fact} {res['ittot']} {len(res['iters'])} {res['last']['err']}"
+    if verbose:
+        print(res["line"])
+    out = (*s.centres(), s.get("Pt"))
+    if return_solver:
+        return out, s, res
+    s.close()
+    return out
+
+
+def aspect_ratio_sweep(facts=(1.0, 0.9, 0.8, 0.7, 0.6, 0.5, 0.4, 0.3, 0.2, 0.1), nsubs=(1, 2, 4, 8),
+                       resols=(127, 255, 511, 1023, 2047), in_flight=4, lib=None):
+    """scripts/runme_Stokes2D_aspect_ratio.jl: Stokes2D_ve_param for the Cartesian product of
+    FACT x NSUB x RESOL (the reference starts one Julia process per instance). Here up to
+    `in_flight` contexts iterate at once, one host thread each (the C calls release the GIL),
+    on their own streams. Returns one result per instance, in the reference's loop order, with
+    the script's output line."""
+    import itertools
+    import threading
+
+    jobs = list(itertools.product(facts, nsubs, resols))
+    out = [None] * len(jobs)
+    nxt = [0]
+    lock = threading.Lock()
+    errors = []
+
+    def worker():
+        while True:
+            with lock:
+                q = nxt[0]
+                nxt[0] += 1
+            if q >= len(jobs) or errors:
+                return
+            fact, nsub, ny = jobs[q]
+            try:
+                s = ve_param_solver(ny, nsub, fact, lib=lib)
+                res = s.run()
+                res["line"] = f"{s.nx} {s.ny} {nsub} {fact} {res['ittot']} {len(res['iters'])} {res['last']['err']}"
+                res.update(fact=fact, nsub=nsub, ny=ny, nx=s.nx)
+                s.close()
+                out[q] = res
+            except Exception as e:  # re-raised below
+                errors.append(e)
+
+    threads = [threading.Thread(target=worker) for _ in range(max(1, in_flight))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    if errors:
+        raise errors[0]
+    return out
 
 
 # Effective memory traffic per PT iteration, in bytes, by the reference's own

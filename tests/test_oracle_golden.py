@@ -68,3 +68,20 @@ def test_oracle_reproduces_the_published_2d_ve_iteration_counts():
         o = S.make("2d_ve", nx, ny)
         o.run()
         assert len(o.iters) == nt and sum(o.iters) == ittot, (nx, o.iters, ittot)
+
+
+def test_oracle_reproduces_the_published_aspect_ratio_counts():
+    """scripts/Stokes2D_ve_param.jl, as runme_Stokes2D_aspect_ratio.jl sweeps it:
+    output/out_Stokes2D_ve_aspect_ratio_param.txt lists `nx ny nsub fact ittot nt err` per
+    instance; the oracle takes exactly as many iterations (all ten facts of the 127^2 grid, two
+    of the 255x127 grid with two inclusions) and ends at the same error."""
+    from oracle import scripts as S
+    d = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_output_lines.json")))
+    rows = [r.split() for r in d["out_Stokes2D_ve_aspect_ratio_param.txt"]]
+    picked = [r for r in rows if r[:3] == ["127", "127", "1"]]
+    picked += [r for r in rows if r[:3] == ["255", "127", "2"] and r[3] in ("0.5", "0.4")]
+    assert len(picked) == 12
+    for nx, ny, nsub, fact, ittot, nt, err in picked:
+        o = S.VE2DParam(int(ny), nsub=int(nsub), fact=float(fact)).setup().run()
+        assert o.nx == int(nx) and len(o.iters) == int(nt) and o.ittot == int(ittot), (nx, nsub, fact, o.iters)
+        assert abs(o.err_hist[-1][2] - float(err)) <= 1e-9 * float(err), (nx, nsub, fact, o.err_hist[-1][2], err)
