@@ -244,6 +244,11 @@ function check_partials(ctx::Ctx)
     return out
 end
 
+"Lengths scaling norm_Rx, norm_Ry, norm_Rz, norm_∇V (Stokes2D_ve_param.jl:175-177: lx, ly, -, ly)."
+set_norm_scales!(ctx::Ctx, sRx, sRy, sRz, sdiv) =
+    check(ctx, ccall((:pts_set_norm_scales, libpts), Cint, (Ptr{Cvoid}, Float64, Float64, Float64, Float64),
+                     ctx.ptr, sRx, sRy, sRz, sdiv))
+
 # Reverse rules for top_vz (and its visco-elastic time-loop twin top_vz_ve) are the
 # ChainRulesCore.rrule methods of PTStokesB200ChainRules.jl, next to this file.
 
