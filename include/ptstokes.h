@@ -94,7 +94,12 @@ typedef struct pts_desc {
     int32_t stencil_kz;     /* z-marching kernels: z-planes per thread block (0 = default 32) */
     int32_t stencil_vtile;  /* z-marching compute_V! + bc: tile configuration
                              * 0 .. pts_stencil_vtiles(precision)-1 (0 = default) */
-    int32_t reserved[1];
+    int32_t mixed_sweep;    /* MIXED with stencil 0: 0 = compute_V! + bc of one FP32 sweep and
+                             * compute_Pt_τ! of the next in one z-marching pass (27 arrays per
+                             * sweep instead of 37; a second set of the ten corrections is
+                             * allocated), with its default tile; 1 = two kernels per sweep;
+                             * 2 + q = the one-pass kernel with tile configuration
+                             * q < pts_mixed_sweep_tiles(). Same arithmetic either way. */
 } pts_desc;
 
 /* Fields, by the reference's names. Extents are the reference's (pts_field_shape). */
@@ -212,6 +217,10 @@ PTS_API int pts_check_partials(pts_ctx* ctx, double out[8]);
  * aspect-ratio script scales norm_Rx by lx and norm_Ry, norm_∇V by ly
  * (scripts/Stokes2D_ve_param.jl:175-177). */
 PTS_API int pts_set_norm_scales(pts_ctx* ctx, double sRx, double sRy, double sRz, double sdiv);
+/* The form of the FP32 sweeps of a MIXED context (pts_desc.mixed_sweep), and the number of
+ * tile configurations of the one-pass form. */
+PTS_API int pts_set_mixed_sweep(pts_ctx* ctx, int32_t mixed_sweep);
+PTS_API int pts_mixed_sweep_tiles(void);
 /* smooth!(Mus2, Mus, fact) nsweeps times with the Mus/Mus2 swap (Stokes3D_ve_perf.jl:173-177). */
 PTS_API int pts_smooth(pts_ctx* ctx, int32_t nsweeps, double fact);
 /* Musτ .= Mus; compute_maxloc!(Musτ, Mus); bc_x!/bc_y!/bc_z!(Musτ) (Stokes3D_ve_perf.jl:178-182). */

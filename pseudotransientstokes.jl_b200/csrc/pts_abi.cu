@@ -38,6 +38,9 @@ struct pts_ctx {
     bool zs = false;         // compute_Pt_τ! by the z-marching TMA-staged kernel
     bool mixed = false;      // FP32 inner sweeps + FP64 defect correction
     Mixed32 m{};
+    Mixed32 m2{};            // second set of the ten FP32 corrections (one-pass sweeps)
+    bool fused32 = false;    // one-pass FP32 sweeps (compute_V! + bc, then compute_Pt_τ!)
+    int ftile = 0;           // its tile configuration
     std::vector<float*> owned32;
     int parity = 0;  // number of buffer swaps mod 2
     std::vector<double*> owned;  // every device allocation
@@ -299,6 +302,41 @@ int V_bc(pts_ctx* c, bool update) {
     return PTS_OK;
 }
 
+// The ten FP32 corrections of the current and the second buffer set trade places.
+void swap_m(pts_ctx* c) {
+    float** a[10] = {&c->m.dPt, &c->m.dVx, &c->m.dVy, &c->m.dVz, &c->m.dtxx,
+                     &c->m.dtyy, &c->m.dtzz, &c->m.dtxy, &c->m.dtxz, &c->m.dtyz};
+    float** b[10] = {&c->m2.dPt, &c->m2.dVx, &c->m2.dVy, &c->m2.dVz, &c->m2.dtxx,
+                     &c->m2.dtyy, &c->m2.dtzz, &c->m2.dtxy, &c->m2.dtxz, &c->m2.dtyz};
+    for (int q = 0; q < 10; ++q) std::swap(*a[q], *b[q]);
+}
+
+// The second buffer set of the one-pass FP32 sweeps (allocated once, zeroed).
+int alloc_m2(pts_ctx* c) {
+    if (c->m2.dPt) return PTS_OK;
+    float** p[10] = {&c->m2.dPt, &c->m2.dVx, &c->m2.dVy, &c->m2.dVz, &c->m2.dtxx,
+                     &c->m2.dtyy, &c->m2.dtzz, &c->m2.dtxy, &c->m2.dtxz, &c->m2.dtyz};
+    for (float** q : p) {
+        void* d = nullptr;
+        if (cudaMalloc(&d, (size_t)c->g.n * sizeof(float)) != cudaSuccess ||
+            cudaMemsetAsync(d, 0, (size_t)c->g.n * sizeof(float), c->stream) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(c, PTS_E_NOMEM, "allocation of the second FP32 correction set failed");
+        }
+        *q = (float*)d;
+        c->owned32.push_back(*q);
+    }
+    // the stress points the sweeps never update hold -w in both sets (k3_srcw); fill the new
+    // set from the current one
+    float* src[6] = {c->m.dtxx, c->m.dtyy, c->m.dtzz, c->m.dtxy, c->m.dtxz, c->m.dtyz};
+    float* dst[6] = {c->m2.dtxx, c->m2.dtyy, c->m2.dtzz, c->m2.dtxy, c->m2.dtxz, c->m2.dtyz};
+    for (int q = 0; q < 6; ++q) {
+        CK(cudaMemcpyAsync(dst[q], src[q], (size_t)c->g.n * sizeof(float), cudaMemcpyDeviceToDevice, c->stream));
+        c->m.u2[q] = dst[q];
+    }
+    return PTS_OK;
+}
+
 // One PT iteration with the two-kernel path: compute_Pt_τ! then compute_V! + bc.
 int iteration(pts_ctx* c, bool store_divV) {
     int rc = Pt_tau(c, store_divV);
@@ -314,6 +352,26 @@ int iteration(pts_ctx* c, bool store_divV) {
 // role variants.
 int enqueue_block(pts_ctx* c, int64_t m, bool store_last) {
     if (m <= 0) return PTS_OK;
+    if (c->mixed && c->fused32) {
+        // compute_Pt_τ! of sweep 1 and compute_V! + bc of sweep m in place; in between, one
+        // pass per pair (V of sweep q, Pt/τ of q+1) from one buffer set into the other. An
+        // even number of passes leaves the current set where it was (the graph of a block
+        // is the same for every block); an odd count gives one pair to the two kernels.
+        CK(launch_corr_A32_zs(c->v, c->d.stencil_tile, c->g, c->m, c->n, c->d.stencil_kz, c->d_kerr, c->stream));
+        int64_t passes = m - 1;
+        if (passes & 1) {
+            CK(launch_corr_B32_zs(c->v, c->d.stencil_vtile, c->g, c->m, c->n, c->d.stencil_kz, c->d_kerr, c->stream));
+            CK(launch_corr_A32_zs(c->v, c->d.stencil_tile, c->g, c->m, c->n, c->d.stencil_kz, c->d_kerr, c->stream));
+            --passes;
+        }
+        for (int64_t q = 0; q < passes; ++q) {
+            CK(launch_corr_BA32_zs(c->v, c->ftile, c->g, c->m, c->m2, c->n, c->d.stencil_kz, c->d_kerr, c->stream));
+            swap_m(c);
+        }
+        CK(launch_corr_B32_zs(c->v, c->d.stencil_vtile, c->g, c->m, c->n, c->d.stencil_kz, c->d_kerr, c->stream));
+        CK(launch_fold(c->g, c->f, c->m, c->stream));
+        return PTS_OK;
+    }
     if (c->mixed) {
         // m FP32 sweeps on the correction, then the FP64 fold X += δ (δ = 0 again). The
         // sources must already describe the current X (mixed_prepare or a previous check).
@@ -436,10 +494,30 @@ int pts_set_stencil(pts_ctx* c, int32_t stencil, int32_t tile, int32_t kz, int32
     c->d.stencil_kz = kz;
     c->d.stencil_vtile = vtile;
     c->zs = (c->v == VE3D || c->v == VE3D_PERF || c->v == V3D) && !c->fused && stencil == 0;
+    c->fused32 = c->mixed && c->zs && c->d.mixed_sweep != 1;
+    if (c->fused32 && (rc = alloc_m2(c)) != PTS_OK) return rc;
     CK(cudaStreamSynchronize(c->stream));
     drop_graph(c);  // the captured check blocks hold the previous kernels
     return PTS_OK;
 }
+
+int pts_set_mixed_sweep(pts_ctx* c, int32_t mixed_sweep) {
+    int rc = enter(c);
+    if (rc) return rc;
+    if (!c->mixed) return fail(c, PTS_E_STATE, "pts_set_mixed_sweep needs a MIXED context");
+    if (mixed_sweep < 0 || mixed_sweep >= 2 + zfused32_num_configs())
+        return fail(c, PTS_E_INVAL, "mixed_sweep out of range (0, 1, 2 + pts_mixed_sweep_tiles())");
+    CK(cudaStreamSynchronize(c->stream));
+    c->d.mixed_sweep = mixed_sweep;
+    c->fused32 = c->zs && mixed_sweep != 1;
+    c->ftile = mixed_sweep >= 2 ? mixed_sweep - 2 : 0;
+    if (c->fused32 && (rc = alloc_m2(c)) != PTS_OK) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    drop_graph(c);
+    return PTS_OK;
+}
+
+int pts_mixed_sweep_tiles(void) { return zfused32_num_configs(); }
 
 int pts_stencil_tiles(int32_t precision) {
     return precision == PTS_MIXED ? zstage32_num_configs() : zstage_num_configs();
@@ -484,6 +562,8 @@ int pts_create(const pts_desc* d, pts_ctx** out) {
     if (d->stencil_vtile < 0 ||
         d->stencil_vtile >= (d->precision == PTS_MIXED ? zvbc32_num_configs() : zvbc_num_configs()))
         return fail(nullptr, PTS_E_INVAL, "stencil_vtile out of range (pts_stencil_vtiles)");
+    if (d->mixed_sweep < 0 || d->mixed_sweep >= 2 + zfused32_num_configs())
+        return fail(nullptr, PTS_E_INVAL, "mixed_sweep out of range (0, 1, 2 + pts_mixed_sweep_tiles())");
     if (d->adjoint && ((d->variant != PTS_3D_V && d->variant != PTS_3D_VE_PERF) || d->precision != PTS_FP64 ||
                        d->single_pass))
         return fail(nullptr, PTS_E_INVAL,
@@ -601,6 +681,9 @@ int pts_create(const pts_desc* d, pts_ctx** out) {
         }
         c->m.GM = (float2*)q;
         c->owned32.push_back((float*)q);
+        c->fused32 = c->zs && d->mixed_sweep != 1;
+        c->ftile = d->mixed_sweep >= 2 ? d->mixed_sweep - 2 : 0;
+        if (c->fused32 && (rc = alloc_m2(c)) != PTS_OK) return bail(rc);
     }
     if (c->fused) {
         for (int q = 0; q < 10; ++q)

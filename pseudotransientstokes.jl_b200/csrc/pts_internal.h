@@ -151,6 +151,7 @@ struct Mixed32 {
     float *aP, *atxx, *atyy, *atzz, *atxy, *atxz, *atyz, *aVx, *aVy, *aVz;
     float2* GM;    // Gdτ and Mus interleaved: one 8-byte load gives both at a point
     float* dtRho;
+    float* u2[6];  // the stress corrections of the second buffer set (one-pass sweeps), or null
 };
 // FP32 inner sweep (pts_kernels32.cu): δ-form compute_Pt_τ! and compute_V! + bc.
 cudaError_t launch_corr_A32(int variant, const Geom& g, const Mixed32& m, const Num& n, cudaStream_t s);
@@ -169,6 +170,13 @@ cudaError_t launch_corr_B32_zs(int variant, int tile, const Geom& g, const Mixed
                                cudaStream_t s);
 int zvbc_num_configs();
 int zvbc32_num_configs();
+// compute_V! + bc of one FP32 sweep and compute_Pt_τ! of the next in one z-marching pass,
+// from the corrections in `m` into the other buffer set `out` (its ten δ arrays); the same
+// arithmetic as launch_corr_B32_zs followed by launch_corr_A32_zs. `tile` <
+// zfused32_num_configs(), `kz` planes per block (0: 64).
+cudaError_t launch_corr_BA32_zs(int variant, int tile, const Geom& g, const Mixed32& m, const Mixed32& out,
+                                const Num& n, int kz, int* err, cudaStream_t s);
+int zfused32_num_configs();
 bool zstage32_tile_info(int tile, int* ty, int* ring);
 // FP64 outer step (pts_kernels64.cu): fold X += δ and clear δ; residual sources of X
 // (aP = ∇·V, aτ = constitutive residual, aV = momentum residual R) with the check

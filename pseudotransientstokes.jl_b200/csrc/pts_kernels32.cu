@@ -359,6 +359,360 @@ Num32 num32(const Num& n) {
     return Num32{(float)n._dx, (float)n._dy, (float)n._dz, (float)n.r, (float)n.gdt, n.gdt == 1.0 ? 1 : 0};
 }
 
+// ---- compute_V! + bc of one sweep and compute_Pt_τ! of the next in one z-marching pass ----
+//
+// The two δ-form kernels above exchange u and δPt through memory every sweep: the stress
+// kernel writes them and the velocity kernel reads them back (and δV the other way). This
+// kernel does the velocity update of sweep q and the stress/pressure update of sweep q+1
+// in one pass, so per pair it reads δV, u, δPt, the sources and the coefficients once and
+// writes δV, u, δPt once (27 arrays of 4 B instead of 37). The updates are the same
+// expressions as k3_corrB / the FP32 zvbc instantiation and k3_corrA_zs, in the same order.
+//
+// Inputs come from one set of buffers (`m`) and the results go to the other (`o`): a CTA
+// computes velocities on a halo of its tile that neighbouring CTAs own, so the update
+// cannot be in place. A CTA owns a 32 x TY column of cells and marches through a chunk of
+// z-planes; stage t of the ring holds plane p = kb-1+t of every input as halo boxes
+// (columns i0-4 .. i0+35, rows j0-2 .. j0+TY+1): δVx δVy δVz u_xx u_yy u_zz u_xy u_xz
+// u_yz δPt dτ_Rho aVx aVy aVz, plus the (Gdτ, Mus) pairs (columns i0-2 .. i0+31, rows
+// j0-1 .. j0+TY-1) and aP (the tile). At step t (newest plane s = kb-1+t):
+//   1. velocities of plane s-1 (δVx, δVy) and of z-face s (δVz) on the extended region
+//      E = columns i0-1 .. i0+32, rows j0-1 .. j0+TY, into shared memory (three rotating
+//      planes); the free-slip copies are values of the interior point they copy (the
+//      tangential index clamped into the interior), the boundary faces keep their value;
+//      the owned part is written to `o`;
+//   2. after a barrier of the consumer warps, u and δPt of cell plane s-1 from those
+//      velocities, into `o`.
+// The z-ghost planes of δVx and δVy are the copies of planes 1 and nz-2: plane nz-2's
+// values are still in shared memory when plane nz-1 is reached; plane 1 comes one step
+// after plane 0, so δPt of plane 0 (the only update of plane 0 that reads δVx, δVy there)
+// is finished one step late, and τxz/τyz of z-face 1 see a zero z-difference, as the copy
+// makes them. Waits are bounded; a warp whose wait gives up keeps taking the barriers with
+// the others and skips its work.
+namespace zf32 {
+using namespace tma;
+constexpr int TX = 32;
+constexpr int XP = 4;            // halo boxes start 4 floats (16 bytes) left of the tile
+constexpr int HW = TX + 2 * XP;  // 40 columns
+constexpr int NB = 14;           // halo-box arrays
+enum { B_VX, B_VY, B_VZ, B_XX, B_YY, B_ZZ, B_XY, B_XZ, B_YZ, B_PT, B_RHO, B_AX, B_AY, B_AZ };
+constexpr int GW = TX + 2;  // (Gdτ, Mus) pair box: columns i0-2 .. i0+31
+constexpr int EW = TX + 2;  // extended region: columns i0-1 .. i0+TX
+
+struct alignas(64) Maps {
+    CUtensorMap h[NB];
+    CUtensorMap gm;
+    CUtensorMap ap;
+};
+
+// The other buffer set of the ten iterated corrections.
+struct Out {
+    float *dPt, *dVx, *dVy, *dVz;
+    float* u[6];  // xx yy zz xy xz yz
+};
+
+template <int TY>
+struct Cfg {
+    static constexpr int HH = TY + 4;
+    static constexpr int HBOX = HW * HH * 4;
+    static constexpr int HS = (HBOX + 127) / 128 * 128 / 4;  // floats between halo boxes
+    static constexpr int GH = TY + 1;
+    static constexpr int GBOX = GW * GH * 8;
+    static constexpr int GSTRIDE = (GBOX + 127) / 128 * 128;
+    static constexpr int PBOX = TX * TY * 4;
+    static constexpr int PSTRIDE = (PBOX + 127) / 128 * 128;
+    static constexpr int SLOT = NB * HS * 4 + GSTRIDE + PSTRIDE;
+    static constexpr int EH = TY + 2;
+    static constexpr int EN = EW * EH;
+    static constexpr int VBUF = 3 * 3 * EN * 4;  // δVx, δVy, δVz of three rotating planes
+    static constexpr uint32_t TXB = NB * HBOX + GBOX + PBOX;
+};
+
+template <int TY, int R>
+__device__ __forceinline__ void issue_f(const Maps& maps, unsigned char* smem, uint64_t* full, int t, int i0, int j0,
+                                        int kb) {
+    using C = Cfg<TY>;
+    const int slot = t % R, p = kb - 1 + t;
+    unsigned char* base = smem + (size_t)slot * C::SLOT;
+    mbar_expect_tx(&full[slot], C::TXB);
+#pragma unroll
+    for (int q = 0; q < NB; ++q) tma_load3(base + q * C::HS * 4, &maps.h[q], i0 - XP, j0 - 2, p, &full[slot]);
+    tma_load3(base + NB * C::HS * 4, &maps.gm, i0 - 2, j0 - 1, p, &full[slot]);
+    tma_load3(base + NB * C::HS * 4 + C::GSTRIDE, &maps.ap, i0, j0, p, &full[slot]);
+}
+
+__device__ __forceinline__ void consumer_sync(int nthreads) {
+    asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory");
+}
+
+template <bool EL, int TY, int R, int MINB>
+__global__ void __launch_bounds__(32 * (TY + 1), MINB)
+    k3_corrBA_zs(const __grid_constant__ Maps maps, Geom g, Out o, Num32 n, int kz, int* err) {
+    using C = Cfg<TY>;
+    constexpr int HS = C::HS, EN = C::EN, NT = 32 * TY;
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+    float* sv = (float*)(smem + (size_t)R * C::SLOT);
+    uint64_t* full = (uint64_t*)(smem + (size_t)R * C::SLOT + C::VBUF);
+    uint64_t* empty = full + R;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
+    const int kb = blockIdx.z * kz;
+    const int ke = min(kb + kz, g.nz);
+    const int nst = ke - kb + 2;  // planes kb-1 .. ke
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < R; ++q) {
+            mbar_init(&full[q], 1);
+            mbar_init(&empty[q], TY);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (warp == TY) {  // producer warp: lane 0 keeps the ring R-1 stages ahead
+        if (lane != 0) return;
+        for (int q = 0; q < NB; ++q) prefetch_map(&maps.h[q]);
+        prefetch_map(&maps.gm);
+        prefetch_map(&maps.ap);
+        int issued = 0;
+        for (int t = 0; t < nst; ++t) {
+            if (t >= R && !mbar_wait(&empty[t % R], (t / R - 1) & 1)) {
+                atomicExch(err, 1);
+                break;
+            }
+            issue_f<TY, R>(maps, smem, full, t, i0, j0, kb);
+            issued = t + 1;
+        }
+        // wait (bounded) for the copies nobody will consume, so none is in flight at exit
+        for (int t = (issued > R ? issued - R : 0); t < issued; ++t)
+            if (!mbar_wait(&full[t % R], (t / R) & 1)) {
+                atomicExch(err, 1);
+                break;
+            }
+        return;
+    }
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const idx_t sz = (idx_t)g.pxy;
+    // own cell of the stress/pressure update
+    const int i = i0 + lane, j = j0 + warp;
+    const bool in = i < nx && j < ny;
+    const bool jI = j >= 1 && j <= ny - 2, iI = i >= 1 && i <= nx - 2;
+    const bool cx = in && jI, cy = in && iI, czz = in && iI && jI;
+    const bool cxy = in && i >= 1 && j >= 1, cxz = in && i >= 1 && jI, cyz = in && iI && j >= 1;
+    const int e0 = (warp + 1) * EW + (lane + 1);     // own cell in the extended region
+    const int h0 = (warp + 2) * HW + (lane + XP);    // own cell in a halo box
+    const int g0 = (warp + 1) * GW + (lane + 2);     // own cell in the pair box
+    const int p0 = warp * TX + lane;                 // own cell in the aP box
+    float vx_m = 0.0f, vy_m = 0.0f;                  // δVx, δVy of plane k-1 at the own cell
+    float2 g_m = make_float2(0.0f, 0.0f), gx_m = g_m, gy_m = g_m;  // pairs of plane k-1: c, c-x, c-y
+    float pt0 = 0.0f, gc0 = 0.0f, ap0 = 0.0f, dvz0 = 0.0f;        // δPt of plane 0, finished at plane 1
+    bool ok = true;
+    for (int t = 0; t < nst; ++t) {
+        const int slot = t % R;
+        if (ok && !mbar_wait(&full[slot], (t / R) & 1)) {
+            atomicExch(err, 1);
+            ok = false;
+        }
+        if (t == 0) continue;  // plane kb-1 only arrives
+        const int s = kb - 1 + t, kv = s - 1;
+        const float* Hc = (const float*)(smem + (size_t)slot * C::SLOT);                // plane s
+        const float* Hp = (const float*)(smem + (size_t)((t + R - 1) % R) * C::SLOT);   // plane s-1
+        float* vxn = sv + (t % 3) * 3 * EN;  // δVx, δVy of plane s-1 and δVz of face s
+        float* vyn = vxn + EN;
+        float* vzn = vyn + EN;
+        const float* vxo = sv + ((t + 2) % 3) * 3 * EN;  // the step before: plane s-2, face s-1
+        const float* vzo = vxo + 2 * EN;
+        const bool own_v = kv >= kb && kv < ke, own_f = s >= kb && s < ke;
+        const bool zlo = kv == 0, zhi = kv == nz - 1;
+        // ---- 1. velocities on the extended region
+        if (ok) {
+            for (int e = threadIdx.x; e < EN; e += NT) {
+                const int ex = e % EW, ey = e / EW;
+                const int x = i0 - 1 + ex, y = j0 - 1 + ey;
+                const bool owned = ex >= 1 && ex <= TX && ey >= 1 && ey <= TY;
+                float vx = 0.0f, vy = 0.0f, vz = 0.0f;
+                // δVx of plane kv: x-faces 0 and nx keep their value; rows 0 and ny-1 and the
+                // z-planes 0 and nz-1 are copies
+                if (kv >= 0 && kv < nz && x >= 0 && x <= nx && y >= 0 && y <= ny - 1) {
+                    if (zhi) {
+                        vx = vxo[e];
+                    } else if (!zlo) {
+                        const int h = (min(max(y, 1), ny - 2) - j0 + 2) * HW + (x - i0 + XP);
+                        float v = Hp[B_VX * HS + h];
+                        if (x >= 1 && x <= nx - 1) {
+                            float Rx = ((n._dx * (Hp[B_XX * HS + h] - Hp[B_XX * HS + h - 1]) +
+                                         n._dy * (Hp[B_XY * HS + h + HW] - Hp[B_XY * HS + h])) +
+                                        n._dz * (Hc[B_XZ * HS + h] - Hp[B_XZ * HS + h])) -
+                                       n._dx * (Hp[B_PT * HS + h] - Hp[B_PT * HS + h - 1]);
+                            Rx = Rx + Hp[B_AX * HS + h];
+                            v = v + Rx * ((Hp[B_RHO * HS + h - 1] + Hp[B_RHO * HS + h]) * 0.5f);
+                        }
+                        vx = v;
+                    }
+                    if (owned && own_v && !zlo) {
+                        o.dVx[gidx32(g, x, y, kv)] = vx;
+                        if (kv == 1) o.dVx[gidx32(g, x, y, 0)] = vx;  // the copy into z-plane 0
+                    }
+                }
+                // δVy of plane kv: y-faces 0 and ny keep their value; columns 0 and nx-1 and
+                // the z-planes 0 and nz-1 are copies
+                if (kv >= 0 && kv < nz && x >= 0 && x <= nx - 1 && y >= 0 && y <= ny) {
+                    if (zhi) {
+                        vy = vxo[EN + e];
+                    } else if (!zlo) {
+                        const int h = (y - j0 + 2) * HW + (min(max(x, 1), nx - 2) - i0 + XP);
+                        float v = Hp[B_VY * HS + h];
+                        if (y >= 1 && y <= ny - 1) {
+                            float Ry = ((n._dy * (Hp[B_YY * HS + h] - Hp[B_YY * HS + h - HW]) +
+                                         n._dx * (Hp[B_XY * HS + h + 1] - Hp[B_XY * HS + h])) +
+                                        n._dz * (Hc[B_YZ * HS + h] - Hp[B_YZ * HS + h])) -
+                                       n._dy * (Hp[B_PT * HS + h] - Hp[B_PT * HS + h - HW]);
+                            Ry = Ry + Hp[B_AY * HS + h];
+                            v = v + Ry * ((Hp[B_RHO * HS + h - HW] + Hp[B_RHO * HS + h]) * 0.5f);
+                        }
+                        vy = v;
+                    }
+                    if (owned && own_v && !zlo) {
+                        o.dVy[gidx32(g, x, y, kv)] = vy;
+                        if (kv == 1) o.dVy[gidx32(g, x, y, 0)] = vy;
+                    }
+                }
+                // δVz of z-face s: faces 0 and nz keep their value; columns 0, nx-1 and rows
+                // 0, ny-1 are copies
+                if (s >= 0 && s <= nz && x >= 0 && x <= nx - 1 && y >= 0 && y <= ny - 1) {
+                    const int h = (min(max(y, 1), ny - 2) - j0 + 2) * HW + (min(max(x, 1), nx - 2) - i0 + XP);
+                    float v = Hc[B_VZ * HS + h];
+                    if (s >= 1 && s <= nz - 1) {
+                        float Rz = ((n._dz * (Hc[B_ZZ * HS + h] - Hp[B_ZZ * HS + h]) +
+                                     n._dx * (Hc[B_XZ * HS + h + 1] - Hc[B_XZ * HS + h])) +
+                                    n._dy * (Hc[B_YZ * HS + h + HW] - Hc[B_YZ * HS + h])) -
+                                   n._dz * (Hc[B_PT * HS + h] - Hp[B_PT * HS + h]);
+                        Rz = Rz + Hc[B_AZ * HS + h];
+                        v = v + Rz * ((Hp[B_RHO * HS + h] + Hc[B_RHO * HS + h]) * 0.5f);
+                    }
+                    vz = v;
+                    if (owned && own_f) o.dVz[gidx32(g, x, y, s)] = vz;
+                }
+                vxn[e] = vx;
+                vyn[e] = vy;
+                vzn[e] = vz;
+            }
+        }
+        consumer_sync(NT);
+        // ---- 2. u and δPt of cell plane k = s-1
+        const int k = kv;
+        if (ok && k >= kb && k < ke && in) {
+            const float2* GM = (const float2*)(Hp + NB * HS);
+            const float* AP = (const float*)((const unsigned char*)(Hp + NB * HS) + C::GSTRIDE);
+            const idx_t c = gidx32(g, i, j, k);
+            const float2 gm = GM[g0], gmx = GM[g0 - 1], gmy = GM[g0 - GW];
+            const float Gc = gm.x, Mc = gm.y;
+            const float vx = vxn[e0], vy = vyn[e0];
+            const float dvx = vxn[e0 + 1] - vx;
+            const float dvy = vyn[e0 + EW] - vy;
+            const float dvz = vzn[e0] - vzo[e0];
+            if (k == 0) {  // δVx, δVy of plane 0 are the copies of plane 1: finished next step
+                pt0 = Hp[B_PT * HS + h0];
+                gc0 = Gc;
+                ap0 = AP[p0];
+                dvz0 = dvz;
+            } else {
+                o.dPt[c] = Hp[B_PT * HS + h0] - n.r * Gc * (AP[p0] + ((n._dx * dvx + n._dy * dvy) + n._dz * dvz));
+                if (k == 1 && kb == 0)
+                    o.dPt[c - sz] = pt0 - n.r * gc0 * (ap0 + ((n._dx * dvx + n._dy * dvy) + n._dz * dvz0));
+            }
+            const bool kI = k >= 1 && k <= nz - 2, k1 = k >= 1;
+            if (k == 1 && kb == 0) vx_m = vx, vy_m = vy;  // the z-plane 0 copies
+            const float Dn = (1.0f + __fdividef(Gc, Mc)) + (EL ? gr32(Gc, n) : 0.0f);
+            const float G2 = 2.0f * Gc;
+            const float rDn = __fdividef(1.0f, Dn);
+            if (cx && kI) o.u[0][c] = (Hp[B_XX * HS + h0] + G2 * (n._dx * dvx)) * rDn;
+            if (cy && kI) o.u[1][c] = (Hp[B_YY * HS + h0] + G2 * (n._dy * dvy)) * rDn;
+            if (czz) o.u[2][c] = (Hp[B_ZZ * HS + h0] + G2 * (n._dz * dvz)) * rDn;
+            if (cxy && kI) {
+                const float2 a = GM[g0 - GW - 1];
+                const float ag = (((a.x + gmy.x) + gmx.x) + Gc) * 0.25f;
+                const float am = (((a.y + gmy.y) + gmx.y) + Mc) * 0.25f;
+                const float sh = 0.5f * (n._dy * (vx - vxn[e0 - EW]) + n._dx * (vy - vyn[e0 - 1]));
+                o.u[3][c] = __fdividef(Hp[B_XY * HS + h0] + (2.0f * ag) * sh,
+                                       (1.0f + __fdividef(ag, am)) + (EL ? gr32(ag, n) : 0.0f));
+            }
+            if (cxz && k1) {
+                const float ag = (((gx_m.x + g_m.x) + gmx.x) + Gc) * 0.25f;
+                const float am = (((gx_m.y + g_m.y) + gmx.y) + Mc) * 0.25f;
+                const float sh = 0.5f * (n._dz * (vx - vx_m) + n._dx * (vzo[e0] - vzo[e0 - 1]));
+                o.u[4][c] = __fdividef(Hp[B_XZ * HS + h0] + (2.0f * ag) * sh,
+                                       (1.0f + __fdividef(ag, am)) + (EL ? gr32(ag, n) : 0.0f));
+            }
+            if (cyz && k1) {
+                const float ag = (((gy_m.x + g_m.x) + gmy.x) + Gc) * 0.25f;
+                const float am = (((gy_m.y + g_m.y) + gmy.y) + Mc) * 0.25f;
+                const float sh = 0.5f * (n._dz * (vy - vy_m) + n._dy * (vzo[e0] - vzo[e0 - EW]));
+                o.u[5][c] = __fdividef(Hp[B_YZ * HS + h0] + (2.0f * ag) * sh,
+                                       (1.0f + __fdividef(ag, am)) + (EL ? gr32(ag, n) : 0.0f));
+            }
+        }
+        // this plane becomes the -z neighbour of the next
+        if (ok) {
+            const float2* GM = (const float2*)(Hp + NB * HS);
+            vx_m = vxn[e0];
+            vy_m = vyn[e0];
+            g_m = GM[g0];
+            gx_m = GM[g0 - 1];
+            gy_m = GM[g0 - GW];
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[(t + R - 1) % R]);  // stage t-1 is no longer read
+    }
+}
+
+// Tile configurations (TY, R, blocks per SM). Shared memory per block: 8x3 104 KB,
+// 4x3 67 KB, 4x4 87 KB.
+struct FTile {
+    int ty, r, minb;
+};
+constexpr FTile kFTiles[] = {{8, 3, 2}, {4, 3, 3}, {4, 4, 2}};
+constexpr int kNumFTiles = (int)(sizeof(kFTiles) / sizeof(kFTiles[0]));
+
+template <bool EL, int Q>
+cudaError_t launch_f(const Geom& g, const Mixed32& m, const Out& o, const Num32& n, int kz, int* err, cudaStream_t s) {
+    constexpr FTile f = kFTiles[Q];
+    using C = Cfg<f.ty>;
+    Maps maps;
+    memset(&maps, 0, sizeof(maps));
+    const void* hsrc[NB] = {m.dVx, m.dVy, m.dVz, m.dtxx, m.dtyy, m.dtzz, m.dtxy,
+                            m.dtxz, m.dtyz, m.dPt, m.dtRho, m.aVx, m.aVy, m.aVz};
+    for (int q = 0; q < NB; ++q)
+        if (!encode_field(&maps.h[q], hsrc[q], g, 4, HW, C::HH)) return cudaErrorInvalidValue;
+    if (!encode_field(&maps.gm, m.GM, g, 8, GW, C::GH)) return cudaErrorInvalidValue;
+    if (!encode_field(&maps.ap, m.aP, g, 4, TX, f.ty)) return cudaErrorInvalidValue;
+    const size_t smem = 128 + (size_t)f.r * C::SLOT + C::VBUF + 2 * f.r * sizeof(uint64_t);
+    static bool attr[64] = {};  // per device: the opt-in to more than 48 KB of shared memory
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!attr[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(k3_corrBA_zs<EL, f.ty, f.r, f.minb>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr[dev] = true;
+    }
+    if (kz <= 0) kz = 64;
+    if (kz < 2) kz = 2;  // plane 0's δPt is finished at plane 1 by the same block
+    const dim3 grid((g.nx + TX - 1) / TX, (g.ny + f.ty - 1) / f.ty, (g.nz + kz - 1) / kz);
+    k3_corrBA_zs<EL, f.ty, f.r, f.minb><<<grid, 32 * (f.ty + 1), smem, s>>>(maps, g, o, n, kz, err);
+    return cudaGetLastError();
+}
+
+template <bool EL>
+cudaError_t launch_f_form(int tile, const Geom& g, const Mixed32& m, const Out& o, const Num32& n, int kz, int* err,
+                          cudaStream_t s) {
+    switch (tile) {
+        case 0: return launch_f<EL, 0>(g, m, o, n, kz, err, s);
+        case 1: return launch_f<EL, 1>(g, m, o, n, kz, err, s);
+        case 2: return launch_f<EL, 2>(g, m, o, n, kz, err, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+}  // namespace zf32
+
 }  // namespace
 
 cudaError_t launch_corr_A32(int v, const Geom& g, const Mixed32& m, const Num& n, cudaStream_t s) {
@@ -422,6 +776,18 @@ cudaError_t launch_corr_B32_zs(int v, int tile, const Geom& g, const Mixed32& m,
 }
 
 int zvbc32_num_configs() { return zvbc32::kNumVTiles; }
+
+cudaError_t launch_corr_BA32_zs(int v, int tile, const Geom& g, const Mixed32& m, const Mixed32& out, const Num& n,
+                                int kz, int* err, cudaStream_t s) {
+    zf32::Out o{out.dPt, out.dVx, out.dVy, out.dVz, {out.dtxx, out.dtyy, out.dtzz, out.dtxy, out.dtxz, out.dtyz}};
+    for (float* p : {o.dPt, o.dVx, o.dVy, o.dVz, o.u[0], o.u[1], o.u[2], o.u[3], o.u[4], o.u[5]})
+        if (!p) return cudaErrorInvalidValue;
+    if (v == VE3D_PERF) return zf32::launch_f_form<true>(tile, g, m, o, num32(n), kz, err, s);
+    if (v == V3D) return zf32::launch_f_form<false>(tile, g, m, o, num32(n), kz, err, s);
+    return cudaErrorInvalidValue;
+}
+
+int zfused32_num_configs() { return zf32::kNumFTiles; }
 
 cudaError_t launch_corr_B32(int v, const Geom& g, const Mixed32& m, const Num& n, cudaStream_t s) {
     if (v != VE3D_PERF && v != V3D) return cudaErrorInvalidValue;

@@ -1514,12 +1514,14 @@ __global__ void __launch_bounds__(256) k3_srcw(Geom g, Fields64 f, Mixed32 m, Nu
     if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 1)
         m.aVz[c] = (float)(f.Rz[c] + ((n._dz * (W(m.atzz, c) - W(m.atzz, c - sz)) + n._dx * (W(m.atxz, c + sx) - W(m.atxz, c))) +
                                       n._dy * (W(m.atyz, c + sy) - W(m.atyz, c))));
-    m.dtxx[c] = -m.atxx[c];
-    m.dtyy[c] = -m.atyy[c];
-    m.dtzz[c] = -m.atzz[c];
-    m.dtxy[c] = -m.atxy[c];
-    m.dtxz[c] = -m.atxz[c];
-    m.dtyz[c] = -m.atyz[c];
+    const float* W6[6] = {m.atxx, m.atyy, m.atzz, m.atxy, m.atxz, m.atyz};
+    float* U6[6] = {m.dtxx, m.dtyy, m.dtzz, m.dtxy, m.dtxz, m.dtyz};
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        const float u = -W6[q][c];
+        U6[q][c] = u;
+        if (m.u2[q]) m.u2[q][c] = u;  // the points the one-pass sweeps never update stay -w in both sets
+    }
 }
 
 __global__ void k_coef32(int64_t n, const double* Gdt, const double* Mus, const double* dtRho, float2* GM32,

@@ -30,7 +30,7 @@ struct Desc
     max_l::Float64; eps::Float64; iter_max::Float64
     mixed_inner::Int32; single_pass::Int32; adjoint::Int32
     stencil::Int32; stencil_tile::Int32; stencil_kz::Int32; stencil_vtile::Int32
-    reserved::NTuple{1,Int32}
+    mixed_sweep::Int32
 end
 
 struct Check
@@ -61,9 +61,9 @@ A device context for one problem (the scripts' `Stokes2D_()`/`Stokes3D_()` state
 """
 function Ctx(variant::Variant, nx, ny, nz=1; lx=10.0, ly=10.0, lz=10.0, G=1.0, dt=1.0, r=1.0, Re, CFL,
              nout=200, ε=1e-8, iterMax=2e5, max_l=0.0, precision=0, single_pass=0, adjoint=0, stencil=0,
-             stencil_tile=0, stencil_kz=0, stencil_vtile=0)
+             stencil_tile=0, stencil_kz=0, stencil_vtile=0, mixed_sweep=0)
     d = Desc(Int32(variant), Int32(precision), nx, ny, nz, nout, lx, ly, lz, G, dt, r, Re, CFL, max_l, ε, iterMax,
-             0, single_pass, adjoint, stencil, stencil_tile, stencil_kz, stencil_vtile, ntuple(_ -> Int32(0), 1))
+             0, single_pass, adjoint, stencil, stencil_tile, stencil_kz, stencil_vtile, mixed_sweep)
     out = Ref{Ptr{Cvoid}}(C_NULL)
     check(nothing, ccall((:pts_create, libpts), Cint, (Ref{Desc}, Ref{Ptr{Cvoid}}), d, out))
     ctx = Ctx(out[])

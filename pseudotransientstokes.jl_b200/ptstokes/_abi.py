@@ -54,7 +54,7 @@ class PtsDesc(ctypes.Structure):
         ("max_l", ctypes.c_double), ("eps", ctypes.c_double), ("iter_max", ctypes.c_double),
         ("mixed_inner", ctypes.c_int32), ("single_pass", ctypes.c_int32), ("adjoint", ctypes.c_int32),
         ("stencil", ctypes.c_int32), ("stencil_tile", ctypes.c_int32), ("stencil_kz", ctypes.c_int32),
-        ("stencil_vtile", ctypes.c_int32), ("reserved", ctypes.c_int32 * 1),
+        ("stencil_vtile", ctypes.c_int32), ("mixed_sweep", ctypes.c_int32),
     ]
 
 
@@ -125,6 +125,8 @@ SIGNATURES = {
     "pts_set_plane_device": ([_P, _I32, _I32, _DP, _I64], ctypes.c_int),
     "pts_check_partials": ([_P, ctypes.POINTER(_D)], ctypes.c_int),
     "pts_set_norm_scales": ([_P, _D, _D, _D, _D], ctypes.c_int),
+    "pts_set_mixed_sweep": ([_P, ctypes.c_int32], ctypes.c_int),
+    "pts_mixed_sweep_tiles": ([], ctypes.c_int),
     "pts_compute_maxloc": ([_P], ctypes.c_int),
     "pts_compute_iter_params": ([_P], ctypes.c_int),
     "pts_set_damping": ([_P] + [ctypes.c_double] * 4, ctypes.c_int),

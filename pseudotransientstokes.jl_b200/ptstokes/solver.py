@@ -62,7 +62,7 @@ class Solver:
         self.variant = variant
         self.ndim = 3 if variant.startswith("3d") else 2
         p = dict(lx=10.0, ly=10.0, lz=10.0, xi=1.0, mus0=1.0, G=1.0, max_l=0.0, mixed_inner=0, single_pass=0,
-                 adjoint=0, stencil=0, stencil_tile=0, stencil_kz=0, stencil_vtile=0)
+                 adjoint=0, stencil=0, stencil_tile=0, stencil_kz=0, stencil_vtile=0, mixed_sweep=0)
         p.update(VARIANT_DEFAULTS[variant])
         p.update(kw)
         self.p = p
@@ -84,6 +84,7 @@ class Solver:
         d.stencil_tile = int(p["stencil_tile"])
         d.stencil_kz = int(p["stencil_kz"])
         d.stencil_vtile = int(p["stencil_vtile"])
+        d.mixed_sweep = int(p["mixed_sweep"])
         self.desc = d
         ctx = ctypes.c_void_p()
         check(self.lib, None, self.lib.pts_create(ctypes.byref(d), ctypes.byref(ctx)))
