@@ -94,12 +94,12 @@ typedef struct pts_desc {
     int32_t stencil_kz;     /* z-marching kernels: z-planes per thread block (0 = default 32) */
     int32_t stencil_vtile;  /* z-marching compute_V! + bc: tile configuration
                              * 0 .. pts_stencil_vtiles(precision)-1 (0 = default) */
-    int32_t mixed_sweep;    /* MIXED with stencil 0: 0 = compute_V! + bc of one FP32 sweep and
-                             * compute_Pt_τ! of the next in one z-marching pass (27 arrays per
+    int32_t mixed_sweep;    /* MIXED with stencil 0: 0 = two z-marching kernels per FP32 sweep
+                             * (default, the faster on a B200); 1 + q = compute_V! + bc of one
+                             * sweep and compute_Pt_τ! of the next in one z-marching pass with
+                             * tile configuration q < pts_mixed_sweep_tiles() (27 arrays per
                              * sweep instead of 37; a second set of the ten corrections is
-                             * allocated), with its default tile; 1 = two kernels per sweep;
-                             * 2 + q = the one-pass kernel with tile configuration
-                             * q < pts_mixed_sweep_tiles(). Same arithmetic either way. */
+                             * allocated). The same FP32 expressions either way. */
 } pts_desc;
 
 /* Fields, by the reference's names. Extents are the reference's (pts_field_shape). */

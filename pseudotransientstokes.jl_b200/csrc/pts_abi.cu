@@ -494,7 +494,7 @@ int pts_set_stencil(pts_ctx* c, int32_t stencil, int32_t tile, int32_t kz, int32
     c->d.stencil_kz = kz;
     c->d.stencil_vtile = vtile;
     c->zs = (c->v == VE3D || c->v == VE3D_PERF || c->v == V3D) && !c->fused && stencil == 0;
-    c->fused32 = c->mixed && c->zs && c->d.mixed_sweep != 1;
+    c->fused32 = c->mixed && c->zs && c->d.mixed_sweep >= 1;
     if (c->fused32 && (rc = alloc_m2(c)) != PTS_OK) return rc;
     CK(cudaStreamSynchronize(c->stream));
     drop_graph(c);  // the captured check blocks hold the previous kernels
@@ -505,12 +505,12 @@ int pts_set_mixed_sweep(pts_ctx* c, int32_t mixed_sweep) {
     int rc = enter(c);
     if (rc) return rc;
     if (!c->mixed) return fail(c, PTS_E_STATE, "pts_set_mixed_sweep needs a MIXED context");
-    if (mixed_sweep < 0 || mixed_sweep >= 2 + zfused32_num_configs())
-        return fail(c, PTS_E_INVAL, "mixed_sweep out of range (0, 1, 2 + pts_mixed_sweep_tiles())");
+    if (mixed_sweep < 0 || mixed_sweep >= 1 + zfused32_num_configs())
+        return fail(c, PTS_E_INVAL, "mixed_sweep out of range (0, 1 + tile < 1 + pts_mixed_sweep_tiles())");
     CK(cudaStreamSynchronize(c->stream));
     c->d.mixed_sweep = mixed_sweep;
-    c->fused32 = c->zs && mixed_sweep != 1;
-    c->ftile = mixed_sweep >= 2 ? mixed_sweep - 2 : 0;
+    c->fused32 = c->zs && mixed_sweep >= 1;
+    c->ftile = mixed_sweep >= 1 ? mixed_sweep - 1 : 0;
     if (c->fused32 && (rc = alloc_m2(c)) != PTS_OK) return rc;
     CK(cudaStreamSynchronize(c->stream));
     drop_graph(c);
@@ -562,8 +562,8 @@ int pts_create(const pts_desc* d, pts_ctx** out) {
     if (d->stencil_vtile < 0 ||
         d->stencil_vtile >= (d->precision == PTS_MIXED ? zvbc32_num_configs() : zvbc_num_configs()))
         return fail(nullptr, PTS_E_INVAL, "stencil_vtile out of range (pts_stencil_vtiles)");
-    if (d->mixed_sweep < 0 || d->mixed_sweep >= 2 + zfused32_num_configs())
-        return fail(nullptr, PTS_E_INVAL, "mixed_sweep out of range (0, 1, 2 + pts_mixed_sweep_tiles())");
+    if (d->mixed_sweep < 0 || d->mixed_sweep >= 1 + zfused32_num_configs())
+        return fail(nullptr, PTS_E_INVAL, "mixed_sweep out of range (0, 1 + tile < 1 + pts_mixed_sweep_tiles())");
     if (d->adjoint && ((d->variant != PTS_3D_V && d->variant != PTS_3D_VE_PERF) || d->precision != PTS_FP64 ||
                        d->single_pass))
         return fail(nullptr, PTS_E_INVAL,
@@ -681,8 +681,8 @@ int pts_create(const pts_desc* d, pts_ctx** out) {
         }
         c->m.GM = (float2*)q;
         c->owned32.push_back((float*)q);
-        c->fused32 = c->zs && d->mixed_sweep != 1;
-        c->ftile = d->mixed_sweep >= 2 ? d->mixed_sweep - 2 : 0;
+        c->fused32 = c->zs && d->mixed_sweep >= 1;
+        c->ftile = d->mixed_sweep >= 1 ? d->mixed_sweep - 1 : 0;
         if (c->fused32 && (rc = alloc_m2(c)) != PTS_OK) return bail(rc);
     }
     if (c->fused) {
