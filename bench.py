@@ -263,7 +263,8 @@ def run_ours(args, ws, rank, local, pg):
     nout = args.iters_per_step
     variant = args.variant
     s = ptstokes.Solver(variant, n, n, n, nout=nout, eps=1e-300, iter_max=nout - 1,
-                        single_pass=args.single_pass, precision=args.precision, stencil=args.stencil)
+                        single_pass=args.single_pass, precision=args.precision, stencil=args.stencil,
+                        stencil_tile=args.stencil_tile)
     s.setup_inclusion()
     s.assign_tau()
     stream = torch.cuda.ExternalStream(s.stream_handle())
@@ -359,7 +360,8 @@ def run_ours(args, ws, rank, local, pg):
         # GIL): the copies and set-up of one overlap the PT iterations of another
         nctx = max(1, min(args.e2e_contexts, args.steps))
         ctxs = [s] + [ptstokes.Solver(variant, n, n, n, nout=nout, eps=1e-300, iter_max=nout - 1,
-                                      single_pass=args.single_pass, precision=args.precision, stencil=args.stencil)
+                                      single_pass=args.single_pass, precision=args.precision, stencil=args.stencil,
+                        stencil_tile=args.stencil_tile)
                       for _ in range(nctx - 1)]
         outs = [torch.empty(n * n * n, dtype=torch.float64, pin_memory=True).numpy().reshape((n, n, n), order="F")
                 for _ in ctxs]
@@ -470,7 +472,8 @@ def run_2d(args, ws, rank, local, pg):
 
     torch.cuda.set_device(local)
     n, nout = args.n2, args.iters_per_step
-    s = ptstokes.Solver("2d_ve_perf", n, n, nout=nout, eps=1e-300, iter_max=nout - 1)
+    s = ptstokes.Solver("2d_ve_perf", n, n, nout=nout, eps=1e-300, iter_max=nout - 1, stencil=args.stencil,
+                        stencil_tile=args.stencil_tile)
     s.setup_inclusion()
     s.assign_tau()
     stream = torch.cuda.ExternalStream(s.stream_handle())
@@ -521,7 +524,8 @@ def run_2d(args, ws, rank, local, pg):
             "reference_published": {"value": 932.8, "unit": "GB/s", "hardware": "A100 SXM4",
                                     "source": "output/out_Stokes2D_ve_perf_ampere.txt:45 (8191^2)"},
             "roofline": {"bound": "hbm", "achieved": round(bytes_A / (ms_A / 1e3) / 1e9, 1), "peak": peak, "unit": "GB/s",
-                         "frac": round(bytes_A / (ms_A / 1e3) / 1e9 / peak, 4), "traffic": None, "kernel": "k2_Pt_tau",
+                         "frac": round(bytes_A / (ms_A / 1e3) / 1e9 / peak, 4), "traffic": None,
+                         "kernel": "k2_Pt_tau_ys" if args.stencil == 0 else "k2_Pt_tau",
                          "peak_kind": peak_kind, "kernel_ms": round(ms_A, 4), "algorithmic_bytes": bytes_A,
                          "kernel_ms_from": "mean over the timed region's launches",
                          "check_ms_per_block": round(ms_check, 4),
@@ -905,6 +909,7 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--stencil", type=int, default=0, choices=[0, 1],
                     help="0: z-marching TMA-staged kernels, 1: one thread per point")
+    ap.add_argument("--stencil-tile", type=int, default=0, help="tile configuration of the TMA-staged compute_Pt_τ!")
     ap.add_argument("--ttt-n", type=int, default=511, help="grid of the time-to-tolerance comparison (0: skip)")
     ap.add_argument("--ttt-n2", type=int, default=255, help="a second, smaller time-to-tolerance grid (0: skip)")
     ap.add_argument("--incl-default-n", type=int, default=255,

@@ -90,7 +90,10 @@ typedef struct pts_desc {
                              * thread per cell or face, operands read directly. Same arithmetic
                              * (FP64: same bits). */
     int32_t stencil_tile;   /* z-marching kernel: tile configuration 0 .. pts_stencil_tiles(precision)-1
-                             * (0 = default; see pts_stencil_tile_info) */
+                             * (0 = default; see pts_stencil_tile_info); 2D contexts: the y-marching
+                             * compute_Pt_τ!, 0 .. pts_stencil_tiles_2d()-1 */
+    /* 2D (PTS_2D_V, PTS_2D_VE, PTS_2D_VE_PERF): stencil 0 also selects a y-marching
+     * compute_Pt_τ! with TMA-staged tiles (stencil_kz = rows per block, 0 = 128); same bits. */
     int32_t stencil_kz;     /* z-marching kernels: z-planes per thread block (0 = default 32) */
     int32_t stencil_vtile;  /* z-marching compute_V! + bc: tile configuration
                              * 0 .. pts_stencil_vtiles(precision)-1 (0 = default) */
@@ -221,6 +224,8 @@ PTS_API int pts_set_norm_scales(pts_ctx* ctx, double sRx, double sRy, double sRz
  * tile configurations of the one-pass form. */
 PTS_API int pts_set_mixed_sweep(pts_ctx* ctx, int32_t mixed_sweep);
 PTS_API int pts_mixed_sweep_tiles(void);
+/* Tile configurations of the 2D y-marching compute_Pt_τ! (pts_desc.stencil_tile of 2D contexts). */
+PTS_API int pts_stencil_tiles_2d(void);
 /* smooth!(Mus2, Mus, fact) nsweeps times with the Mus/Mus2 swap (Stokes3D_ve_perf.jl:173-177). */
 PTS_API int pts_smooth(pts_ctx* ctx, int32_t nsweeps, double fact);
 /* Musτ .= Mus; compute_maxloc!(Musτ, Mus); bc_x!/bc_y!/bc_z!(Musτ) (Stokes3D_ve_perf.jl:178-182). */

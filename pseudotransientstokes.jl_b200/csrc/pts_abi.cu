@@ -36,6 +36,7 @@ struct pts_ctx {
     Fields64 alt{};  // second buffers of the ten iterated fields (single-pass 3D path)
     bool fused = false;
     bool zs = false;         // compute_Pt_τ! by the z-marching TMA-staged kernel
+    bool ys = false;         // 2D: compute_Pt_τ! by the y-marching TMA-staged kernel
     bool mixed = false;      // FP32 inner sweeps + FP64 defect correction
     Mixed32 m{};
     Mixed32 m2{};            // second set of the ten FP32 corrections (one-pass sweeps)
@@ -284,7 +285,10 @@ int copy3d(pts_ctx* c, int id, const double* src_dense, double* dst_dense, int64
 // compute_Pt_τ! (both roles) on the context's fields: the z-marching TMA-staged kernel
 // unless the context asked for the one-thread-per-cell form (same bits either way).
 int Pt_tau(pts_ctx* c, bool store_divV) {
-    if (c->zs)
+    if (c->ys)
+        CK(launch_Pt_tau_ys(c->v, c->d.stencil_tile, c->g, c->f, c->n, c->d.stencil_kz, store_divV && !c->perf,
+                            c->d_kerr, c->stream));
+    else if (c->zs)
         CK(launch_Pt_tau_zs(c->v, c->d.stencil_tile, c->g, c->f, c->n, c->d.stencil_kz, store_divV && !c->perf,
                             c->d_kerr, c->stream));
     else
@@ -300,6 +304,12 @@ int V_bc(pts_ctx* c, bool update) {
     else
         CK(launch_V_bc(c->v, c->g, c->f, c->n, update, c->stream));
     return PTS_OK;
+}
+
+// Tile configurations of the TMA-staged compute_Pt_τ! of a context: 3D FP64, 3D FP32
+// sweeps, 2D.
+int tile_count(bool d3, bool mixed) {
+    return mixed ? zstage32_num_configs() : (d3 ? zstage_num_configs() : ystage_num_configs());
 }
 
 // The ten FP32 corrections of the current and the second buffer set trade places.
@@ -484,8 +494,8 @@ int pts_set_stencil(pts_ctx* c, int32_t stencil, int32_t tile, int32_t kz, int32
     int rc = enter(c);
     if (rc) return rc;
     if (stencil != 0 && stencil != 1) return fail(c, PTS_E_INVAL, "stencil must be 0 or 1");
-    if (tile < 0 || tile >= (c->mixed ? zstage32_num_configs() : zstage_num_configs()))
-        return fail(c, PTS_E_INVAL, "stencil_tile out of range (pts_stencil_tiles)");
+    if (tile < 0 || tile >= tile_count(c->d3, c->mixed))
+        return fail(c, PTS_E_INVAL, "stencil_tile out of range (pts_stencil_tiles, pts_stencil_tiles_2d)");
     if (vtile < 0 || vtile >= (c->mixed ? zvbc32_num_configs() : zvbc_num_configs()))
         return fail(c, PTS_E_INVAL, "stencil_vtile out of range (pts_stencil_vtiles)");
     if (kz < 0) return fail(c, PTS_E_INVAL, "stencil_kz must be >= 0");
@@ -494,6 +504,7 @@ int pts_set_stencil(pts_ctx* c, int32_t stencil, int32_t tile, int32_t kz, int32
     c->d.stencil_kz = kz;
     c->d.stencil_vtile = vtile;
     c->zs = (c->v == VE3D || c->v == VE3D_PERF || c->v == V3D) && !c->fused && stencil == 0;
+    c->ys = (c->v == V2D || c->v == VE2D || c->v == VE2D_PERF) && stencil == 0;
     c->fused32 = c->mixed && c->zs && c->d.mixed_sweep >= 1;
     if (c->fused32 && (rc = alloc_m2(c)) != PTS_OK) return rc;
     CK(cudaStreamSynchronize(c->stream));
@@ -518,6 +529,8 @@ int pts_set_mixed_sweep(pts_ctx* c, int32_t mixed_sweep) {
 }
 
 int pts_mixed_sweep_tiles(void) { return zfused32_num_configs(); }
+
+int pts_stencil_tiles_2d(void) { return ystage_num_configs(); }
 
 int pts_stencil_tiles(int32_t precision) {
     return precision == PTS_MIXED ? zstage32_num_configs() : zstage_num_configs();
@@ -555,9 +568,8 @@ int pts_create(const pts_desc* d, pts_ctx** out) {
         return fail(nullptr, PTS_E_INVAL, "mixed_inner: the FP64 correction runs with every check, so it must be 0 or nout");
     if (!(d->lx > 0) || !(d->ly > 0) || (d3 && !(d->lz > 0))) return fail(nullptr, PTS_E_INVAL, "domain extents must be > 0");
     if (d->stencil != 0 && d->stencil != 1) return fail(nullptr, PTS_E_INVAL, "stencil must be 0 or 1");
-    if (d->stencil_tile < 0 ||
-        d->stencil_tile >= (d->precision == PTS_MIXED ? zstage32_num_configs() : zstage_num_configs()))
-        return fail(nullptr, PTS_E_INVAL, "stencil_tile out of range (pts_stencil_tiles)");
+    if (d->stencil_tile < 0 || d->stencil_tile >= tile_count(d3, d->precision == PTS_MIXED))
+        return fail(nullptr, PTS_E_INVAL, "stencil_tile out of range (pts_stencil_tiles, pts_stencil_tiles_2d)");
     if (d->stencil_kz < 0) return fail(nullptr, PTS_E_INVAL, "stencil_kz must be >= 0");
     if (d->stencil_vtile < 0 ||
         d->stencil_vtile >= (d->precision == PTS_MIXED ? zvbc32_num_configs() : zvbc_num_configs()))
@@ -657,6 +669,7 @@ int pts_create(const pts_desc* d, pts_ctx** out) {
     c->fused = variant_fused(c->v) && d->single_pass != 0 && !c->mixed;
     // z-marching TMA-staged compute_Pt_τ!: the FP64 two-kernel path, and the FP32 sweeps
     c->zs = (c->v == VE3D || c->v == VE3D_PERF || c->v == V3D) && !c->fused && d->stencil == 0;
+    c->ys = (c->v == V2D || c->v == VE2D || c->v == VE2D_PERF) && d->stencil == 0;
     if (c->mixed) {
         float** p32[] = {&c->m.dPt, &c->m.dVx, &c->m.dVy, &c->m.dVz, &c->m.dtxx, &c->m.dtyy, &c->m.dtzz, &c->m.dtxy,
                          &c->m.dtxz, &c->m.dtyz, &c->m.aP, &c->m.atxx, &c->m.atyy, &c->m.atzz, &c->m.atxy,

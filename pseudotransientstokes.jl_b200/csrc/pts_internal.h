@@ -177,6 +177,11 @@ int zvbc32_num_configs();
 cudaError_t launch_corr_BA32_zs(int variant, int tile, const Geom& g, const Mixed32& m, const Mixed32& out,
                                 const Num& n, int kz, int* err, cudaStream_t s);
 int zfused32_num_configs();
+// compute_Pt_τ! (2D: V2D, VE2D, VE2D_PERF) as a y-marching kernel with TMA-staged tiles; the
+// same bits as launch_Pt_tau. `tile` < ystage_num_configs(), `ky` rows per block (0: 128).
+cudaError_t launch_Pt_tau_ys(int variant, int tile, const Geom& g, const Fields64& f, const Num& n, int ky,
+                             bool store_divV, int* err, cudaStream_t s);
+int ystage_num_configs();
 bool zstage32_tile_info(int tile, int* ty, int* ring);
 // FP64 outer step (pts_kernels64.cu): fold X += δ and clear δ; residual sources of X
 // (aP = ∇·V, aτ = constitutive residual, aV = momentum residual R) with the check

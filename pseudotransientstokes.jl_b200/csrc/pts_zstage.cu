@@ -375,6 +375,226 @@ cudaError_t launch_V_bc_zs(int variant, int tile, const Geom& g, const Fields64&
     }
 }
 
+// ---- compute_Pt_τ! (2D) as a y-marching kernel with TMA-staged tiles ----
+//
+// Reference: compute_Pt_τ! of scripts/Stokes2D_ve_perf.jl:34-53 and the role pairs
+// compute_P! + compute_τ! of Stokes2D_ve.jl:35-50 and Stokes2D.jl:33-44, evaluated exactly
+// as the one-thread-per-cell kernel (pt_tau_2d in pts_kernels64.cu) evaluates them,
+// operand for operand, so the result is the same bits. A CTA owns a 32-column strip and a
+// chunk of `ky` rows, which it walks in tiles of TY rows: one consumer warp per row, one
+// cell per lane. Per tile one producer warp issues one 3D tensor copy per input array into
+// a ring of R shared-memory slots:
+//   halo group, box (TX+4) x (TY+2) at (i0-2, j0-1): Vx, Vy, Gdτ, Mus
+//   point group, box TX x TY at (i0, j0):            Pt, τxx, τyy, τxy [, τxx_o, τyy_o, τxy_o]
+// (the halo box starts two columns left of the tile, the 16-byte rule for the x offset).
+// Every cell writes only its own Pt and τ: the update is in place. Waits are bounded.
+namespace ys2 {
+using namespace expr;
+using namespace tma;
+constexpr int TX = 32;
+constexpr int HW = TX + 4;
+constexpr int NH = 4;
+
+struct alignas(64) Maps {
+    CUtensorMap h[NH];  // Vx Vy Gdτ Mus
+    CUtensorMap p[7];   // Pt τxx τyy τxy [τxx_o τyy_o τxy_o]
+};
+
+template <int TY, bool EL>
+struct Cfg {
+    static constexpr int HH = TY + 2;
+    static constexpr int HBOX = HW * HH * 8;
+    static constexpr int HSTRIDE = (HBOX + 127) / 128 * 128;
+    static constexpr int NP = EL ? 7 : 4;
+    static constexpr int PBOX = TX * TY * 8;
+    static constexpr int SLOT = NH * HSTRIDE + NP * PBOX;
+};
+
+template <bool EL, int TY, int R>
+__device__ __forceinline__ void issue_y(const Maps& maps, unsigned char* smem, uint64_t* full, int t, int i0, int jb) {
+    using C = Cfg<TY, EL>;
+    const int slot = t % R, j0 = jb + t * TY;
+    unsigned char* base = smem + (size_t)slot * C::SLOT;
+    mbar_expect_tx(&full[slot], NH * C::HBOX + C::NP * C::PBOX);
+#pragma unroll
+    for (int q = 0; q < NH; ++q) tma_load3(base + q * C::HSTRIDE, &maps.h[q], i0 - 2, j0 - 1, 0, &full[slot]);
+#pragma unroll
+    for (int q = 0; q < C::NP; ++q) tma_load3(base + NH * C::HSTRIDE + q * C::PBOX, &maps.p[q], i0, j0, 0, &full[slot]);
+}
+
+template <int VAR, int TY, int R, int MINB>
+__global__ void __launch_bounds__(32 * (TY + 1), MINB)
+    k2_Pt_tau_ys(const __grid_constant__ Maps maps, Geom g, Fields64 f, Num n, int ky, int store_divV, int* err) {
+    constexpr bool EL = VAR != V2D, PERF = VAR == VE2D_PERF;
+    using C = Cfg<TY, EL>;
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+    uint64_t* full = (uint64_t*)(smem + (size_t)R * C::SLOT);
+    uint64_t* empty = full + R;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i0 = blockIdx.x * TX, jb = blockIdx.y * ky;
+    const int je = min(jb + ky, g.ny);
+    const int nst = (je - jb + TY - 1) / TY;
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < R; ++q) {
+            mbar_init(&full[q], 1);
+            mbar_init(&empty[q], TY);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (warp == TY) {  // producer warp
+        if (lane != 0) return;
+        for (int q = 0; q < NH; ++q) prefetch_map(&maps.h[q]);
+        for (int q = 0; q < C::NP; ++q) prefetch_map(&maps.p[q]);
+        int issued = 0;
+        for (int t = 0; t < nst; ++t) {
+            if (t >= R && !mbar_wait(&empty[t % R], (t / R - 1) & 1)) {
+                atomicExch(err, 1);
+                break;
+            }
+            issue_y<EL, TY, R>(maps, smem, full, t, i0, jb);
+            issued = t + 1;
+        }
+        for (int t = (issued > R ? issued - R : 0); t < issued; ++t)
+            if (!mbar_wait(&full[t % R], (t / R) & 1)) {
+                atomicExch(err, 1);
+                break;
+            }
+        return;
+    }
+    const int nx = g.nx, ny = g.ny;
+    const int i = i0 + lane;
+    const int hc = (warp + 1) * HW + (lane + 2);
+    const int pc = warp * TX + lane;
+    constexpr int PS = TX * TY;
+    constexpr int HS = C::HSTRIDE / 8;
+    for (int t = 0; t < nst; ++t) {
+        const int slot = t % R;
+        if (!mbar_wait(&full[slot], (t / R) & 1)) {
+            atomicExch(err, 1);
+            return;
+        }
+        const int j = jb + t * TY + warp;
+        if (i < nx && j < je) {
+            const double* H = (const double*)(smem + (size_t)slot * C::SLOT);
+            const double* hVx = H;
+            const double* hVy = H + HS;
+            const double* hG = H + 2 * HS;
+            const double* hM = H + 3 * HS;
+            const double* P = H + NH * HS;
+            const idx_t c = gidx32(g, i, j, 0);
+            const double vx = hVx[hc], vy = hVy[hc];
+            const double dvx = hVx[hc + 1] - vx;
+            const double dvy = hVy[hc + HW] - vy;
+            const double Gc = hG[hc];
+            if (VAR == VE2D_PERF) {
+                f.Pt[c] = P[pc] - n.r * Gc * (n._dx * dvx + n._dy * dvy);
+            } else {
+                const double dv = dvx / n.dx + dvy / n.dy;
+                if (store_divV) f.divV[c] = dv;
+                f.Pt[c] = P[pc] - n.r * Gc * dv;
+            }
+            const double Mc = hM[hc];
+            if (VAR == V2D) {
+                const double den = Gc / Mc + 1.0;
+                f.txx[c] = (P[PS + pc] + ((2.0 * Gc) * dvx) / n.dx) / den;
+                f.tyy[c] = (P[2 * PS + pc] + ((2.0 * Gc) * dvy) / n.dy) / den;
+            } else {
+                const double Gr = gr_of(Gc, n.gdt);
+                const double ex = PERF ? n._dx * dvx : dvx / n.dx;
+                const double ey = PERF ? n._dy * dvy : dvy / n.dy;
+                const double den = (1.0 + Gc / Mc) + Gr;
+                f.txx[c] = ((P[PS + pc] + P[4 * PS + pc] * Gr) + (2.0 * Gc) * ex) / den;
+                f.tyy[c] = ((P[2 * PS + pc] + P[5 * PS + pc] * Gr) + (2.0 * Gc) * ey) / den;
+            }
+            // τxy on the vertex (x-face i, y-face j): i in [1,nx-1], j in [1,ny-1]
+            if (i >= 1 && j >= 1) {
+                const double ag = (((hG[hc - HW - 1] + hG[hc - HW]) + hG[hc - 1]) + Gc) * 0.25;
+                const double am = (((hM[hc - HW - 1] + hM[hc - HW]) + hM[hc - 1]) + Mc) * 0.25;
+                const double d1 = vx - hVx[hc - HW];  // @d_yi(Vx)
+                const double d2 = vy - hVy[hc - 1];   // @d_xi(Vy)
+                if (VAR == V2D) {
+                    f.txy[c] = (P[3 * PS + pc] + (2.0 * ag) * (0.5 * (d1 / n.dy + d2 / n.dx))) / (ag / am + 1.0);
+                } else if (VAR == VE2D) {
+                    const double Gr = gr_of(ag, n.gdt);
+                    f.txy[c] = ((P[3 * PS + pc] + P[6 * PS + pc] * Gr) + (2.0 * ag) * (0.5 * (d1 / n.dy + d2 / n.dx))) /
+                               ((1.0 + ag / am) + Gr);
+                } else {
+                    const double Gr = gr_of(ag, n.gdt);
+                    f.txy[c] = ((P[3 * PS + pc] + P[6 * PS + pc] * Gr) + ((2.0 * ag) * 0.5) * (n._dy * d1 + n._dx * d2)) /
+                               ((1.0 + ag / am) + Gr);
+                }
+            }
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[slot]);
+    }
+}
+
+// Tile configurations (TY, R, blocks per SM); shared memory for the visco-elastic form:
+// 32x8 with 2 slots 52 KB, 32x4 with 3 slots 42 KB, 32x8 with 3 slots 78 KB, 32x16 2 slots 97 KB.
+struct YTile {
+    int ty, r, minb;
+};
+constexpr YTile kYTiles[] = {{8, 2, 3}, {4, 3, 4}, {8, 3, 2}, {16, 2, 1}};
+constexpr int kNumYTiles = (int)(sizeof(kYTiles) / sizeof(kYTiles[0]));
+
+template <int VAR, int Q>
+cudaError_t launch_y(const Geom& g, const Fields64& f, const Num& n, int ky, bool sd, int* err, cudaStream_t s) {
+    constexpr YTile y = kYTiles[Q];
+    constexpr bool EL = VAR != V2D;
+    using C = Cfg<y.ty, EL>;
+    Maps maps;
+    memset(&maps, 0, sizeof(maps));
+    const double* hsrc[NH] = {f.Vx, f.Vy, f.Gdt, f.Mus};
+    for (int q = 0; q < NH; ++q)
+        if (!encode_field(&maps.h[q], hsrc[q], g, 8, HW, C::HH)) return cudaErrorInvalidValue;
+    const double* psrc[7] = {f.Pt, f.txx, f.tyy, f.txy, f.txx_o, f.tyy_o, f.txy_o};
+    for (int q = 0; q < C::NP; ++q)
+        if (!encode_field(&maps.p[q], psrc[q], g, 8, TX, y.ty)) return cudaErrorInvalidValue;
+    const size_t smem = 128 + (size_t)y.r * C::SLOT + 2 * y.r * sizeof(uint64_t);
+    static bool attr[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!attr[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(k2_Pt_tau_ys<VAR, y.ty, y.r, y.minb>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr[dev] = true;
+    }
+    if (ky <= 0) ky = 128;
+    ky = (ky + y.ty - 1) / y.ty * y.ty;  // whole tiles per chunk
+    const dim3 grid((g.nx + TX - 1) / TX, (g.ny + ky - 1) / ky, 1);
+    k2_Pt_tau_ys<VAR, y.ty, y.r, y.minb><<<grid, 32 * (y.ty + 1), smem, s>>>(maps, g, f, n, ky, sd ? 1 : 0, err);
+    return cudaGetLastError();
+}
+
+template <int VAR>
+cudaError_t launch_y_form(int tile, const Geom& g, const Fields64& f, const Num& n, int ky, bool sd, int* err,
+                          cudaStream_t s) {
+    switch (tile) {
+        case 0: return launch_y<VAR, 0>(g, f, n, ky, sd, err, s);
+        case 1: return launch_y<VAR, 1>(g, f, n, ky, sd, err, s);
+        case 2: return launch_y<VAR, 2>(g, f, n, ky, sd, err, s);
+        case 3: return launch_y<VAR, 3>(g, f, n, ky, sd, err, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+}  // namespace ys2
+
+int ystage_num_configs() { return ys2::kNumYTiles; }
+
+cudaError_t launch_Pt_tau_ys(int variant, int tile, const Geom& g, const Fields64& f, const Num& n, int ky,
+                             bool store_divV, int* err, cudaStream_t s) {
+    switch (variant) {
+        case V2D: return ys2::launch_y_form<V2D>(tile, g, f, n, ky, store_divV, err, s);
+        case VE2D: return ys2::launch_y_form<VE2D>(tile, g, f, n, ky, store_divV, err, s);
+        case VE2D_PERF: return ys2::launch_y_form<VE2D_PERF>(tile, g, f, n, ky, false, err, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
 cudaError_t launch_Pt_tau_zs(int variant, int cfg, const Geom& g, const Fields64& f, const Num& n, int kz,
                              bool store_divV, int* err, cudaStream_t s) {
     if (kz <= 0) kz = 32;

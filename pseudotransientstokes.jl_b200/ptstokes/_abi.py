@@ -127,6 +127,7 @@ SIGNATURES = {
     "pts_set_norm_scales": ([_P, _D, _D, _D, _D], ctypes.c_int),
     "pts_set_mixed_sweep": ([_P, ctypes.c_int32], ctypes.c_int),
     "pts_mixed_sweep_tiles": ([], ctypes.c_int),
+    "pts_stencil_tiles_2d": ([], ctypes.c_int),
     "pts_compute_maxloc": ([_P], ctypes.c_int),
     "pts_compute_iter_params": ([_P], ctypes.c_int),
     "pts_set_damping": ([_P] + [ctypes.c_double] * 4, ctypes.c_int),

@@ -93,3 +93,42 @@ def test_fp32_sweep_forms_agree(gpu_lib, variant):
             scale = max(float(np.abs(ref[k]).max()), 1e-300)
             # same FP32 arithmetic up to the compiler's multiply-add contraction
             assert float(np.abs(got[k] - ref[k]).max()) <= 1e-5 * scale, (tile, k)
+
+
+ITERATED2 = ("Pt", "Vx", "Vy", "txx", "tyy", "txy")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("variant", ["2d_ve_perf", "2d_ve", "2d_v"])
+@pytest.mark.parametrize("dims", [(47, 39), (33, 70), (65, 9), (3, 3)])
+def test_2d_y_marching_tiles_are_bit_exact(gpu_lib, variant, dims):
+    """The 2D y-marching compute_Pt_τ! (stencil 0) against the one-thread-per-cell kernel
+    (stencil 1): every tile configuration and several rows-per-block chunk lengths, on grids
+    whose strips, chunks and halos fall off every edge."""
+    import ctypes
+
+    import ptstokes
+    from ptstokes._abi import PtsCheck
+
+    def run2(**kw):
+        s = ptstokes.Solver(variant, *dims, lib=gpu_lib, nout=9, eps=1e-300, iter_max=10 ** 9, **kw)
+        s.setup_inclusion()
+        if variant != "2d_v":
+            s.assign_tau()
+        s.iterate(9)
+        if variant != "2d_v":
+            s.assign_tau()
+        s.iterate(9)
+        c = PtsCheck()
+        rc = gpu_lib.pts_compute_res(s.ctx, ctypes.byref(c))
+        out = {k: s.get(k) for k in ITERATED2}
+        s.close()
+        return out, (rc, bytes(c))
+
+    ref, cref = run2(stencil=1)
+    for tile in range(gpu_lib.pts_stencil_tiles_2d()):
+        for ky in (0, 5, 16):
+            got, c = run2(stencil=0, stencil_tile=tile, stencil_kz=ky)
+            for k in ITERATED2:
+                assert same_bits(got[k], ref[k]), (tile, ky, k)
+            assert c == cref
