@@ -501,6 +501,14 @@ def run_2d(args, ws, rank, local, pg):
     ms_A, ms_B, ms_check = block_kernel_means(blocks, nout)
     peak, peak_kind = hbm_peak()
     bytes_A = 15 * n * n * 8  # Vx Vy Gdτ Mus Pt τ(3) τ_o(3) read, Pt τ(3) written
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "dram_traffic_per_cell.txt")  # from the committed ncu capture
+    if args.stencil == 0 and os.path.exists(tp):
+        try:
+            tj = json.load(open(tp)).get("k2_Pt_tau_ys")
+            traffic = tj["bytes_per_cell"] * n * n if tj else None
+        except Exception:
+            traffic = None
     s.close()
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -524,7 +532,7 @@ def run_2d(args, ws, rank, local, pg):
             "reference_published": {"value": 932.8, "unit": "GB/s", "hardware": "A100 SXM4",
                                     "source": "output/out_Stokes2D_ve_perf_ampere.txt:45 (8191^2)"},
             "roofline": {"bound": "hbm", "achieved": round(bytes_A / (ms_A / 1e3) / 1e9, 1), "peak": peak, "unit": "GB/s",
-                         "frac": round(bytes_A / (ms_A / 1e3) / 1e9 / peak, 4), "traffic": None,
+                         "frac": round(bytes_A / (ms_A / 1e3) / 1e9 / peak, 4), "traffic": traffic,
                          "kernel": "k2_Pt_tau_ys" if args.stencil == 0 else "k2_Pt_tau",
                          "peak_kind": peak_kind, "kernel_ms": round(ms_A, 4), "algorithmic_bytes": bytes_A,
                          "kernel_ms_from": "mean over the timed region's launches",
