@@ -248,6 +248,9 @@ PTS_API int pts_compute_V(pts_ctx* ctx);         /* compute_V! (Stokes3D_ve_mult
 PTS_API int pts_apply_bc(pts_ctx* ctx);          /* the bc_x!/bc_y!/bc_z! calls on V (…_perf.jl:202-207) */
 PTS_API int pts_compute_Pt_tau(pts_ctx* ctx);    /* compute_Pt_τ! (Stokes3D_ve_perf.jl:69-78)           */
 PTS_API int pts_compute_V_bc(pts_ctx* ctx);      /* compute_V! + bc (Stokes3D_ve_perf.jl:83-88,202-207)  */
+/* MIXED: one half of an FP32 sweep on the current corrections, asynchronous, no fold:
+ * which = 0 the δ-form compute_Pt_τ!, 1 the δ-form compute_V! + bc (for timing them). */
+PTS_API int pts_sweep32_kernel(pts_ctx* ctx, int32_t which);
 /* compute_Res! + the norms of the check (Stokes3D_ve_perf.jl:209-219). Synchronous. */
 PTS_API int pts_compute_res(pts_ctx* ctx, pts_check* out);
 

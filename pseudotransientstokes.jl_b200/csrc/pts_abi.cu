@@ -1012,6 +1012,26 @@ int pts_compute_V_bc(pts_ctx* c) {
     return V_bc(c, true);
 }
 
+int pts_sweep32_kernel(pts_ctx* c, int32_t which) {
+    int rc = enter(c);
+    if (rc) return rc;
+    if (!c->mixed) return fail(c, PTS_E_STATE, "pts_sweep32_kernel needs a MIXED context");
+    if (which == 0) {
+        if (c->zs)
+            CK(launch_corr_A32_zs(c->v, c->d.stencil_tile, c->g, c->m, c->n, c->d.stencil_kz, c->d_kerr, c->stream));
+        else
+            CK(launch_corr_A32(c->v, c->g, c->m, c->n, c->stream));
+    } else if (which == 1) {
+        if (c->zs)
+            CK(launch_corr_B32_zs(c->v, c->d.stencil_vtile, c->g, c->m, c->n, c->d.stencil_kz, c->d_kerr, c->stream));
+        else
+            CK(launch_corr_B32(c->v, c->g, c->m, c->n, c->stream));
+    } else {
+        return fail(c, PTS_E_INVAL, "which must be 0 (compute_Pt_τ!) or 1 (compute_V! + bc)");
+    }
+    return PTS_OK;
+}
+
 int pts_compute_res(pts_ctx* c, pts_check* out) {
     int rc = enter(c);
     if (rc) return rc;
