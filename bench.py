@@ -306,13 +306,18 @@ def run_ours(args, ws, rank, local, pg):
     # the dominant kernel compute_Pt_τ! (25 arrays/launch) and compute_V!+bc (14): their mean
     # durations over the timed region (per_kernel), else timed alternating right after it, in
     # the state the timed steps left, each launch bracketed by CUDA events on the context's stream
+    mixed = args.precision == "mixed"
+
     def time_pair(reps=20):
+        # the mixed path's FP32 sweep kernels on its corrections, else the FP64 kernels
+        fa = (lambda: s._ck(s.lib.pts_sweep32_kernel(s.ctx, 0))) if mixed else s.compute_Pt_tau
+        fb = (lambda: s._ck(s.lib.pts_sweep32_kernel(s.ctx, 1))) if mixed else s.compute_V_bc
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * reps + 1)]
         ev[0].record(stream)
         for q in range(reps):
-            s.compute_Pt_tau()
+            fa()
             ev[2 * q + 1].record(stream)
-            s.compute_V_bc()
+            fb()
             ev[2 * q + 2].record(stream)
         ev[-1].synchronize()
         ta = sum(ev[2 * q].elapsed_time(ev[2 * q + 1]) for q in range(reps)) / reps
@@ -324,13 +329,16 @@ def run_ours(args, ws, rank, local, pg):
     else:
         (ms_A, ms_B), ms_check = time_pair(), None
     peak, peak_kind = hbm_peak()
-    bytes_A = 25 * n ** 3 * 8
+    # algorithmic bytes: FP64 compute_Pt_τ! 25 arrays x 8 B, compute_V! + bc 14 x 8 B; the
+    # FP32 sweep's δ-form kernels 20 x 4 B and 17 x 4 B
+    bytes_A = (20 * 4 if mixed else 25 * 8) * n ** 3
+    bytes_B = (17 * 4 if mixed else 14 * 8) * n ** 3
     achieved = bytes_A / (ms_A / 1e3) / 1e9
     traffic = None
     tp = os.path.join(ROOT, "profiles", "dram_traffic_per_cell.txt")  # from the committed ncu capture
     if os.path.exists(tp):
         try:
-            tj = json.load(open(tp)).get("k3_Pt_tau_zs" if args.stencil == 0 else "k3_Pt_tau")
+            tj = None if mixed else json.load(open(tp)).get("k3_Pt_tau_zs" if args.stencil == 0 else "k3_Pt_tau")
             if tj:
                 traffic = tj["bytes_per_cell"] * n ** 3
         except Exception:
@@ -449,13 +457,15 @@ def run_ours(args, ws, rank, local, pg):
                        "parallelism": f"replicas x{ws}", "l2": "inputs larger than L2 (1.07 GB per field)"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
-                         "kernel": "k3_Pt_tau_zs" if args.stencil == 0 else "k3_Pt_tau",
+                         "kernel": ("k3_corrA_zs" if mixed else "k3_Pt_tau_zs") if args.stencil == 0 else
+                                   ("k3_corrA" if mixed else "k3_Pt_tau"),
                          "peak_kind": peak_kind, "kernel_ms": round(ms_A, 4), "algorithmic_bytes": bytes_A,
                          "kernel_ms_from": "mean over the timed region's launches" if per_kernel else
                                            "20 alternating launches after the timed region",
                          "check_ms_per_block": None if ms_check is None else round(ms_check, 4),
-                         "other_kernel": {"name": "k3_V_bc_zs" if args.stencil == 0 else "k3_V_bc", "ms": round(ms_B, 4),
-                                          "achieved": round(14 * n ** 3 * 8 / (ms_B / 1e3) / 1e9, 1)}},
+                         "other_kernel": {"name": ("k3_V_bc_zs<float>" if mixed else "k3_V_bc_zs") if args.stencil == 0
+                                          else ("k3_corrB" if mixed else "k3_V_bc"), "ms": round(ms_B, 4),
+                                          "achieved": round(bytes_B / (ms_B / 1e3) / 1e9, 1)}},
             "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clocks,
             "time_to_tol": ttt, "time_to_tol_small": ttt2, "inclusions_20": incl,
         }

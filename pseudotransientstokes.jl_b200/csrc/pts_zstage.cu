@@ -95,18 +95,13 @@ __device__ __forceinline__ void drain(uint64_t* full, int from, int issued, int*
         }
 }
 
-// compute_Pt_τ! over a 32 x TY tile and planes [kb, ke): TY/RW consumer warps of RW tile
-// rows each, and either one extra producer warp (PW) or thread 0 issuing the copies between
-// its own steps (a warp's registers saved). R = slots in the shared-memory ring; MINB =
-// blocks per SM the register allocation must allow. With RW = 2 a warp updates two rows per
-// plane: the per-plane waits, barrier arrivals and loop control are shared by twice the
-// cells, and each row's arithmetic is independent of the other's (more instruction-level
-// parallelism per warp, at more registers per thread).
-template <bool EL, bool PERF, int TY, int R, bool PW, int MINB, int RW>
-__global__ void __launch_bounds__(32 * (TY / RW + (PW ? 1 : 0)), MINB)
+// compute_Pt_τ! over a 32 x TY tile and planes [kb, ke): TY consumer warps, and either one
+// extra producer warp (PW) or thread 0 issuing the copies between its own steps (a warp's
+// registers saved). R = slots in the shared-memory ring; MINB = blocks per SM the register
+// allocation must allow.
+template <bool EL, bool PERF, int TY, int R, bool PW, int MINB>
+__global__ void __launch_bounds__(32 * (TY + (PW ? 1 : 0)), MINB)
     k3_Pt_tau_zs(const __grid_constant__ Maps maps, Geom g, Fields64 f, Num n, int kz, int store_divV, int* err) {
-    static_assert(TY % RW == 0, "rows per warp must divide the tile height");
-    constexpr int NW = TY / RW;  // consumer warps
     using C = Cfg<TY, EL>;
     extern __shared__ unsigned char smem_raw[];
     unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
@@ -122,13 +117,13 @@ __global__ void __launch_bounds__(32 * (TY / RW + (PW ? 1 : 0)), MINB)
     if (threadIdx.x == 0) {
         for (int s = 0; s < R; ++s) {
             mbar_init(&full[s], 1);
-            mbar_init(&empty[s], NW);
+            mbar_init(&empty[s], TY);
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
 
-    if (PW && warp == NW) {
+    if (PW && warp == TY) {
         // ---------------- producer warp: one lane issues every copy, R stages ahead
         if (lane != 0) return;
         for (int q = 0; q < NH; ++q) prefetch_map(&maps.h[q]);
@@ -156,30 +151,26 @@ __global__ void __launch_bounds__(32 * (TY / RW + (PW ? 1 : 0)), MINB)
         for (; issued < R - 1 && issued < nst; ++issued) issue_stage<EL, TY, R>(maps, smem, full, issued, i0, j0, kb);
     }
 
-    // ---------------- consumers: rows warp*RW .. warp*RW+RW-1 of the tile, lane = column
-    const int i = i0 + lane;
+    // ---------------- consumers: warp = tile row, lane = tile column
+    const int i = i0 + lane, j = j0 + warp;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const bool in = i < nx && j < ny;
+    // tangential conditions of each stress point that do not depend on k
+    const bool jI = j >= 1 && j <= ny - 2, iI = i >= 1 && i <= nx - 2;
+    const bool cx = in && jI, cy = in && iI, czz = in && iI && jI;                   // τxx, τyy, τzz
+    const bool cxy = in && i >= 1 && j >= 1, cxz = in && i >= 1 && jI, cyz = in && iI && j >= 1;
     const double gdt = n.gdt;
-    const bool iI = i >= 1 && i <= nx - 2;
-    constexpr int PS = C::PBOX / 8;
-    bool in[RW], cx[RW], cy[RW], czz[RW], cxy[RW], cxz[RW], cyz[RW];
-    int hc[RW], pc[RW];
-    idx_t c[RW];
-    // registers carried from the previous plane (the -z neighbours), per row
-    double vx_m[RW], vy_m[RW], g_m[RW], gx_m[RW], gy_m[RW], m_m[RW], mx_m[RW], my_m[RW];  // plane k-1
-    double vz_c[RW], vz_x[RW], vz_y[RW];  // Vz at plane k: c, c-sx, c-sy
-#pragma unroll
-    for (int r = 0; r < RW; ++r) {
-        const int row = warp * RW + r, j = j0 + row;
-        in[r] = i < nx && j < ny;
-        // tangential conditions of each stress point that do not depend on k
-        const bool jI = j >= 1 && j <= ny - 2;
-        cx[r] = in[r] && jI, cy[r] = in[r] && iI, czz[r] = in[r] && iI && jI;  // τxx, τyy, τzz
-        cxy[r] = in[r] && i >= 1 && j >= 1, cxz[r] = in[r] && i >= 1 && jI, cyz[r] = in[r] && iI && j >= 1;
-        hc[r] = (row + 1) * C::HW + (lane + 2);  // halo-box offset of this cell
-        pc[r] = row * TX + lane;
-        c[r] = gidx32(g, i, j, kb);
-    }
+
+    // halo-box offsets (elements) of this cell and its -x / -y neighbours
+    const int hc = (warp + 1) * C::HW + (lane + 2);
+    const int hxm = hc - 1, hym = hc - C::HW, hxp = hc + 1, hyp = hc + C::HW, hxym = hc - C::HW - 1;
+    const int pc = warp * TX + lane;
+
+    // registers carried from the previous plane (the -z neighbours)
+    double vx_m, vy_m, g_m, gx_m, gy_m, m_m, mx_m, my_m;  // plane k-1
+    double vz_c, vz_x, vz_y;                               // Vz at plane k: c, c-sx, c-sy
+
+    idx_t c = gidx32(g, i, j, kb);
     const idx_t sz = (idx_t)g.pxy;
     int t = 0;
     for (; t < nst; ++t) {
@@ -202,70 +193,64 @@ __global__ void __launch_bounds__(32 * (TY / RW + (PW ? 1 : 0)), MINB)
         const double* hG = H + 2 * (C::HSTRIDE / 8);
         const double* hM = H + 3 * (C::HSTRIDE / 8);
         const double* hVz = H + 4 * (C::HSTRIDE / 8);  // Vz of plane s+1
-        const double* P = H + NH * (C::HSTRIDE / 8);
-        const double* Po = P + 7 * PS;  // τ_o
-        const int k = kb + t - 1;
-        const bool kI = k >= 1 && k <= nz - 2, k1 = k >= 1;
-#pragma unroll
-        for (int r = 0; r < RW; ++r) {
-            const int h = hc[r], hxm = h - 1, hym = h - C::HW, hxp = h + 1, hyp = h + C::HW, hxym = h - C::HW - 1;
-            const int q = pc[r];
-            const double vx = hVx[h], vy = hVy[h], Gc = hG[h], Mc = hM[h];
-            const double Gx = hG[hxm], Gy = hG[hym], Mx = hM[hxm], My = hM[hym];
-            const double vzn = hVz[h], vznx = hVz[hxm], vzny = hVz[hym];
-            if (t > 0 && in[r]) {
-                const idx_t cc = c[r];
-                const double dvx = hVx[hxp] - vx;
-                const double dvy = hVy[hyp] - vy;
-                const double dvz = vzn - vz_c[r];
-                if (PERF) {
-                    f.Pt[cc] = P[q] - n.r * Gc * ((n._dx * dvx + n._dy * dvy) + n._dz * dvz);
-                } else {
-                    const double dv = (dvx / n.dx + dvy / n.dy) + dvz / n.dz;
-                    if (store_divV) f.divV[cc] = dv;
-                    f.Pt[cc] = P[q] - n.r * Gc * dv;
-                }
-                if ((cx[r] && kI) || (cy[r] && kI) || czz[r]) {
-                    const double Gr = EL ? gr_of(Gc, gdt) : 0.0;
-                    const double den = EL ? ((1.0 + Gc / Mc) + Gr) : (1.0 + Gc / Mc);
-                    if (cx[r] && kI)
-                        f.txx[cc] = tau_n_den<EL, PERF>(P[1 * PS + q], EL ? Po[0 * PS + q] : 0.0, Gc, Gr, den, n.dx,
-                                                        n._dx, dvx);
-                    if (cy[r] && kI)
-                        f.tyy[cc] = tau_n_den<EL, PERF>(P[2 * PS + q], EL ? Po[1 * PS + q] : 0.0, Gc, Gr, den, n.dy,
-                                                        n._dy, dvy);
-                    if (czz[r])
-                        f.tzz[cc] = tau_n_den<EL, PERF>(P[3 * PS + q], EL ? Po[2 * PS + q] : 0.0, Gc, Gr, den, n.dz,
-                                                        n._dz, dvz);
-                }
-                // τxy on edge (x-face i, y-face j, cell k): i in [1,nx-1], j in [1,ny-1], k in [1,nz-2]
-                if (cxy[r] && kI) {
-                    const double ag = (((hG[hxym] + Gy) + Gx) + Gc) * 0.25;
-                    const double am = (((hM[hxym] + My) + Mx) + Mc) * 0.25;
-                    f.txy[cc] = tau_s<EL, PERF>(P[4 * PS + q], EL ? Po[3 * PS + q] : 0.0, ag, am, gdt, n.dy, n._dy,
-                                                vx - hVx[hym], n.dx, n._dx, vy - hVy[hxm]);
-                }
-                // τxz on edge (x-face i, cell j, z-face k): i in [1,nx-1], j in [1,ny-2], k in [1,nz-1]
-                if (cxz[r] && k1) {
-                    const double ag = (((gx_m[r] + g_m[r]) + Gx) + Gc) * 0.25;
-                    const double am = (((mx_m[r] + m_m[r]) + Mx) + Mc) * 0.25;
-                    f.txz[cc] = tau_s<EL, PERF>(P[5 * PS + q], EL ? Po[4 * PS + q] : 0.0, ag, am, gdt, n.dz, n._dz,
-                                                vx - vx_m[r], n.dx, n._dx, vz_c[r] - vz_x[r]);
-                }
-                // τyz on edge (cell i, y-face j, z-face k): i in [1,nx-2], j in [1,ny-1], k in [1,nz-1]
-                if (cyz[r] && k1) {
-                    const double ag = (((gy_m[r] + g_m[r]) + Gy) + Gc) * 0.25;
-                    const double am = (((my_m[r] + m_m[r]) + My) + Mc) * 0.25;
-                    f.tyz[cc] = tau_s<EL, PERF>(P[6 * PS + q], EL ? Po[5 * PS + q] : 0.0, ag, am, gdt, n.dz, n._dz,
-                                                vy - vy_m[r], n.dy, n._dy, vz_c[r] - vz_y[r]);
-                }
-                c[r] = cc + sz;
+        const double vx = hVx[hc], vy = hVy[hc], Gc = hG[hc], Mc = hM[hc];
+        const double Gx = hG[hxm], Gy = hG[hym], Mx = hM[hxm], My = hM[hym];
+        const double vzn = hVz[hc], vznx = hVz[hxm], vzny = hVz[hym];
+        if (t > 0 && in) {
+            const int k = kb + t - 1;
+            const double* P = H + NH * (C::HSTRIDE / 8);
+            const double dvx = hVx[hxp] - vx;
+            const double dvy = hVy[hyp] - vy;
+            const double dvz = vzn - vz_c;
+            if (PERF) {
+                f.Pt[c] = P[pc] - n.r * Gc * ((n._dx * dvx + n._dy * dvy) + n._dz * dvz);
+            } else {
+                const double dv = (dvx / n.dx + dvy / n.dy) + dvz / n.dz;
+                if (store_divV) f.divV[c] = dv;
+                f.Pt[c] = P[pc] - n.r * Gc * dv;
             }
-            // this plane becomes the -z neighbour of the next
-            vx_m[r] = vx, vy_m[r] = vy, g_m[r] = Gc, gx_m[r] = Gx, gy_m[r] = Gy, m_m[r] = Mc, mx_m[r] = Mx,
-            my_m[r] = My;
-            vz_c[r] = vzn, vz_x[r] = vznx, vz_y[r] = vzny;
+            const bool kI = k >= 1 && k <= nz - 2, k1 = k >= 1;
+            const double* Po = P + 7 * (C::PBOX / 8);  // τ_o
+            constexpr int PS = C::PBOX / 8;
+            if ((cx && kI) || (cy && kI) || czz) {
+                const double Gr = EL ? gr_of(Gc, gdt) : 0.0;
+                const double den = EL ? ((1.0 + Gc / Mc) + Gr) : (1.0 + Gc / Mc);
+                if (cx && kI)
+                    f.txx[c] = tau_n_den<EL, PERF>(P[1 * PS + pc], EL ? Po[0 * PS + pc] : 0.0, Gc, Gr, den, n.dx,
+                                                   n._dx, dvx);
+                if (cy && kI)
+                    f.tyy[c] = tau_n_den<EL, PERF>(P[2 * PS + pc], EL ? Po[1 * PS + pc] : 0.0, Gc, Gr, den, n.dy,
+                                                   n._dy, dvy);
+                if (czz)
+                    f.tzz[c] = tau_n_den<EL, PERF>(P[3 * PS + pc], EL ? Po[2 * PS + pc] : 0.0, Gc, Gr, den, n.dz,
+                                                   n._dz, dvz);
+            }
+            // τxy on edge (x-face i, y-face j, cell k): i in [1,nx-1], j in [1,ny-1], k in [1,nz-2]
+            if (cxy && kI) {
+                const double ag = (((hG[hxym] + Gy) + Gx) + Gc) * 0.25;
+                const double am = (((hM[hxym] + My) + Mx) + Mc) * 0.25;
+                f.txy[c] = tau_s<EL, PERF>(P[4 * PS + pc], EL ? Po[3 * PS + pc] : 0.0, ag, am, gdt, n.dy, n._dy,
+                                           vx - hVx[hym], n.dx, n._dx, vy - hVy[hxm]);
+            }
+            // τxz on edge (x-face i, cell j, z-face k): i in [1,nx-1], j in [1,ny-2], k in [1,nz-1]
+            if (cxz && k1) {
+                const double ag = (((gx_m + g_m) + Gx) + Gc) * 0.25;
+                const double am = (((mx_m + m_m) + Mx) + Mc) * 0.25;
+                f.txz[c] = tau_s<EL, PERF>(P[5 * PS + pc], EL ? Po[4 * PS + pc] : 0.0, ag, am, gdt, n.dz, n._dz,
+                                           vx - vx_m, n.dx, n._dx, vz_c - vz_x);
+            }
+            // τyz on edge (cell i, y-face j, z-face k): i in [1,nx-2], j in [1,ny-1], k in [1,nz-1]
+            if (cyz && k1) {
+                const double ag = (((gy_m + g_m) + Gy) + Gc) * 0.25;
+                const double am = (((my_m + m_m) + My) + Mc) * 0.25;
+                f.tyz[c] = tau_s<EL, PERF>(P[6 * PS + pc], EL ? Po[5 * PS + pc] : 0.0, ag, am, gdt, n.dz, n._dz,
+                                           vy - vy_m, n.dy, n._dy, vz_c - vz_y);
+            }
+            c += sz;
         }
+        // this plane becomes the -z neighbour of the next
+        vx_m = vx, vy_m = vy, g_m = Gc, gx_m = Gx, gy_m = Gy, m_m = Mc, mx_m = Mx, my_m = My;
+        vz_c = vzn, vz_x = vznx, vz_y = vzny;
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[slot]);
     }
@@ -274,7 +259,7 @@ __global__ void __launch_bounds__(32 * (TY / RW + (PW ? 1 : 0)), MINB)
 
 // ---- host side ----
 
-template <bool EL, bool PERF, int TY, int R, bool PW, int MINB, int RW>
+template <bool EL, bool PERF, int TY, int R, bool PW, int MINB>
 cudaError_t launch_cfg(const Geom& g, const Fields64& f, const Num& n, int kz, bool store_divV, int* err,
                        cudaStream_t s) {
     using C = Cfg<TY, EL>;
@@ -292,14 +277,14 @@ cudaError_t launch_cfg(const Geom& g, const Fields64& f, const Num& n, int kz, b
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
     if (!attr[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(k3_Pt_tau_zs<EL, PERF, TY, R, PW, MINB, RW>,
+        cudaError_t e = cudaFuncSetAttribute(k3_Pt_tau_zs<EL, PERF, TY, R, PW, MINB>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         attr[dev] = true;
     }
     const dim3 grid((g.nx + TX - 1) / TX, (g.ny + TY - 1) / TY, (g.nz + kz - 1) / kz);
-    k3_Pt_tau_zs<EL, PERF, TY, R, PW, MINB, RW>
-        <<<grid, 32 * (TY / RW + (PW ? 1 : 0)), smem, s>>>(maps, g, f, n, kz, store_divV ? 1 : 0, err);
+    k3_Pt_tau_zs<EL, PERF, TY, R, PW, MINB>
+        <<<grid, 32 * (TY + (PW ? 1 : 0)), smem, s>>>(maps, g, f, n, kz, store_divV ? 1 : 0, err);
     return cudaGetLastError();
 }
 
@@ -308,16 +293,15 @@ cudaError_t launch_cfg(const Geom& g, const Fields64& f, const Num& n, int kz, b
 // slots 45 KB (4 blocks/SM by registers), 32x8 83 KB (2), 32x6 63 KB (3). The first is the
 // fastest measured at 511^3 on a B200 (5.01 ms; without the producer warp 5.07, 32x8 5.12).
 struct TileCfg {
-    int ty, r, pw, minb, rw;
+    int ty, r, pw, minb;
 };
-constexpr TileCfg kTiles[] = {{4, 2, 1, 4, 1}, {4, 2, 0, 5, 1}, {8, 2, 1, 2, 1}, {6, 2, 1, 3, 1},
-                              {8, 2, 0, 2, 1}, {4, 2, 1, 4, 2}, {8, 2, 1, 2, 2}, {4, 2, 0, 5, 2}};
+constexpr TileCfg kTiles[] = {{4, 2, 1, 4}, {4, 2, 0, 5}, {8, 2, 1, 2}, {6, 2, 1, 3}, {8, 2, 0, 2}};
 constexpr int kNumTiles = (int)(sizeof(kTiles) / sizeof(kTiles[0]));
 
 template <bool EL, bool PERF, int Q>
 cudaError_t launch_q(const Geom& g, const Fields64& f, const Num& n, int kz, bool sd, int* err, cudaStream_t s) {
     constexpr TileCfg c = kTiles[Q];
-    return launch_cfg<EL, PERF, c.ty, c.r, c.pw != 0, c.minb, c.rw>(g, f, n, kz, sd, err, s);
+    return launch_cfg<EL, PERF, c.ty, c.r, c.pw != 0, c.minb>(g, f, n, kz, sd, err, s);
 }
 
 template <bool EL, bool PERF>
@@ -329,9 +313,6 @@ cudaError_t launch_form(int cfg, const Geom& g, const Fields64& f, const Num& n,
         case 2: return launch_q<EL, PERF, 2>(g, f, n, kz, sd, err, s);
         case 3: return launch_q<EL, PERF, 3>(g, f, n, kz, sd, err, s);
         case 4: return launch_q<EL, PERF, 4>(g, f, n, kz, sd, err, s);
-        case 5: return launch_q<EL, PERF, 5>(g, f, n, kz, sd, err, s);
-        case 6: return launch_q<EL, PERF, 6>(g, f, n, kz, sd, err, s);
-        case 7: return launch_q<EL, PERF, 7>(g, f, n, kz, sd, err, s);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -67,3 +67,23 @@ def test_mixed_is_rejected_where_not_implemented(gpu_lib):
 
     with pytest.raises(ptstokes.PtsError):
         ptstokes.Solver("2d_ve", 31, 31, precision="mixed", lib=gpu_lib)
+
+
+def test_sweep32_kernel_entry(gpu_lib):
+    """pts_sweep32_kernel runs one half of an FP32 sweep on a MIXED context's corrections
+    (for timing); it refuses other contexts and unknown halves."""
+    import ptstokes
+    from ptstokes import _abi
+
+    m = ptstokes.Solver("3d_ve_perf", 23, 19, 17, precision="mixed", lib=gpu_lib)
+    m.setup_inclusion()
+    m.assign_tau()
+    m.iterate(4)
+    assert gpu_lib.pts_sweep32_kernel(m.ctx, 0) == _abi.PTS_OK
+    assert gpu_lib.pts_sweep32_kernel(m.ctx, 1) == _abi.PTS_OK
+    assert gpu_lib.pts_sweep32_kernel(m.ctx, 2) == _abi.PTS_E_INVAL
+    m.sync()
+    m.close()
+    p = ptstokes.Solver("3d_ve_perf", 11, 9, 7, lib=gpu_lib)
+    assert gpu_lib.pts_sweep32_kernel(p.ctx, 0) == _abi.PTS_E_STATE
+    p.close()
