@@ -221,33 +221,16 @@ def run_reference(args, ws, rank, pg):
 
 
 # ------------------------------------------------------------------------------ GPU arm
-def kernel_events_block(s, nout, stream):
-    """One check block launched kernel by kernel: nout x (compute_Pt_τ!, compute_V! + bc), a
-    CUDA event recorded on the context's stream before the block and after every kernel, then
-    the check (compute_Res! + norms, read back: synchronises). Returns the events; the check's
-    time is the gap between the last event and the next block's first."""
-    import torch
-
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * nout + 2)]
-    ev[0].record(stream)
-    for q in range(nout):
-        s.compute_Pt_tau()
-        ev[2 * q + 1].record(stream)
-        s.compute_V_bc()
-        ev[2 * q + 2].record(stream)
-    s.compute_res()
-    ev[-1].record(stream)
-    return ev
-
-
 def block_kernel_means(blocks, nout):
-    """Mean duration (ms) of the first kernel, the second kernel and the check over the blocks
-    of kernel_events_block."""
+    """Mean duration (ms) of the first kernel, the second kernel and the rest of a block (the
+    check; in mixed precision the FP64 fold and the sources/check) over check blocks whose
+    per-kernel times (pts_kernel_times: compute_Pt_τ!, compute_V! + bc, ..., the rest) were
+    read after each block."""
     a = b = c = 0.0
-    for ev in blocks:
-        a += sum(ev[2 * q].elapsed_time(ev[2 * q + 1]) for q in range(nout))
-        b += sum(ev[2 * q + 1].elapsed_time(ev[2 * q + 2]) for q in range(nout))
-        c += ev[2 * nout].elapsed_time(ev[2 * nout + 1])
+    for t in blocks:
+        a += sum(t[2 * q] for q in range(nout))
+        b += sum(t[2 * q + 1] for q in range(nout))
+        c += sum(t[2 * nout:])
     k = max(len(blocks), 1)
     return a / (k * nout), b / (k * nout), c / k
 
@@ -268,17 +251,18 @@ def run_ours(args, ws, rank, local, pg):
     s.setup_inclusion()
     s.assign_tau()
     stream = torch.cuda.ExternalStream(s.stream_handle())
-    # FP64 two-kernel path: the timed steps launch the iteration's two kernels directly with a
-    # CUDA event after each, so the roofline's per-kernel durations come from the timed region
-    # itself; other paths run one graph launch per step (nout PT iterations + check).
-    per_kernel = args.precision == "fp64" and not args.single_pass
+    # A step is one graph launch: nout PT iterations + check. On the FP64 two-kernel path the
+    # graph also records a CUDA event after each kernel (pts_set_kernel_timing), read back
+    # after each step, so the roofline's per-kernel durations come from the timed region.
+    per_kernel = not args.single_pass
     blocks = []
+    if per_kernel:
+        s.set_kernel_timing(True)
 
     def step():
+        s.solve()
         if per_kernel:
-            blocks.append(kernel_events_block(s, nout, stream))
-        else:
-            s.solve()
+            blocks.append(s.kernel_times())
 
     for _ in range(args.warmup):
         step()
@@ -431,7 +415,10 @@ def run_ours(args, ws, rank, local, pg):
                          f"{args.cpu_iters} PT iterations, {dt:.1f} s",
                "time_to_tol_2d_127": small_2d_case()}
 
-    launches = args.steps * (2 * nout + 2) if args.precision == "fp64" else args.steps * (2 * nout + 3)
+    # per step: 2 kernels per iteration and the check (k3_check, k_check_finalize); mixed:
+    # the sweeps' 2 per iteration, the fold, the sources/check (3) and, in pts_solve's
+    # preparation, the FP32 coefficient copy and the sources again (4)
+    launches = args.steps * (2 * nout + 2) if args.precision == "fp64" else args.steps * (2 * nout + 8)
     s.close()
     ttt = ttt2 = incl = None
     if args.ttt_n > 0:
@@ -451,9 +438,8 @@ def run_ours(args, ws, rank, local, pg):
             "config": {"workload": f"3D VE Stokes (Stokes3D_ve_perf.jl kernels), {args.precision.upper()}, {n}^3, "
                                    "box 10^3",
                        "nx": n, "ny": n, "nz": n, "iters_per_step": nout, "t_it_ms": round(t_it * 1e3, 4),
-                       "path": ("2 kernels per PT iteration launched directly, a CUDA event after each; "
-                                "check + readback per block") if per_kernel else
-                               "CUDA graph per check block",
+                       "path": "CUDA graph per check block (2 kernels per PT iteration" +
+                               (", a CUDA event-record node after each)" if per_kernel else ")"),
                        "parallelism": f"replicas x{ws}", "l2": "inputs larger than L2 (1.07 GB per field)"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
@@ -487,11 +473,11 @@ def run_2d(args, ws, rank, local, pg):
     s.setup_inclusion()
     s.assign_tau()
     stream = torch.cuda.ExternalStream(s.stream_handle())
+    s.set_kernel_timing(True)  # a CUDA event after each kernel of the check block's graph
     blocks = []
     for _ in range(args.warmup):
-        blocks.append(kernel_events_block(s, nout, stream))
+        s.solve()
     s.sync()
-    blocks.clear()
     barrier(pg)
     clk = ClockSampler(local)
     clk.start()
@@ -499,7 +485,8 @@ def run_2d(args, ws, rank, local, pg):
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):
-        blocks.append(kernel_events_block(s, nout, stream))
+        s.solve()
+        blocks.append(s.kernel_times())
     e1.record(stream)
     e1.synchronize()
     barrier(pg)
@@ -536,8 +523,8 @@ def run_2d(args, ws, rank, local, pg):
             "config": {"workload": f"2D VE Stokes (Stokes2D_ve_perf.jl kernels), FP64, {n}^2, box 10^2", "nx": n,
                        "ny": n, "iters_per_step": nout, "t_it_ms": round(t_it * 1e3, 5),
                        "A_eff": "18 arrays x 8 B per cell (Stokes2D_ve_perf.jl:173)",
-                       "path": "2 kernels per PT iteration launched directly, a CUDA event after each; check + "
-                               "readback per block",
+                       "path": "CUDA graph per check block (2 kernels per PT iteration, a CUDA event-record "
+                               "node after each)",
                        "l2": f"inputs larger than L2 ({n * n * 8 / 1e6:.0f} MB per field)"},
             "reference_published": {"value": 932.8, "unit": "GB/s", "hardware": "A100 SXM4",
                                     "source": "output/out_Stokes2D_ve_perf_ampere.txt:45 (8191^2)"},

@@ -251,6 +251,13 @@ PTS_API int pts_compute_V_bc(pts_ctx* ctx);      /* compute_V! + bc (Stokes3D_ve
 /* MIXED: one half of an FP32 sweep on the current corrections, asynchronous, no fold:
  * which = 0 the δ-form compute_Pt_τ!, 1 the δ-form compute_V! + bc (for timing them). */
 PTS_API int pts_sweep32_kernel(pts_ctx* ctx, int32_t which);
+/* Per-kernel timing (on = 1): every block of PT iterations records a CUDA event before its
+ * first kernel and after each kernel it launches (the check's too), inside the check
+ * block's graph as event-record nodes. pts_kernel_times gives the elapsed ms between
+ * consecutive events of the last block enqueued, in launch order (FP64 two-kernel path:
+ * compute_Pt_τ!, compute_V! + bc, ..., the check); synchronous. */
+PTS_API int pts_set_kernel_timing(pts_ctx* ctx, int32_t on);
+PTS_API int pts_kernel_times(pts_ctx* ctx, float* ms, int64_t cap, int64_t* count);
 /* compute_Res! + the norms of the check (Stokes3D_ve_perf.jl:209-219). Synchronous. */
 PTS_API int pts_compute_res(pts_ctx* ctx, pts_check* out);
 

@@ -51,6 +51,9 @@ struct pts_ctx {
     CheckResult* h_result = nullptr;  // pinned
     cudaGraphExec_t chunk[2] = {nullptr, nullptr};  // nout iterations + check, per starting parity
     int* d_kerr = nullptr;  // set by a kernel whose bounded wait timed out
+    bool timing = false;             // a CUDA event after each kernel of a block (pts_set_kernel_timing)
+    std::vector<cudaEvent_t> tev;    // those events, in launch order
+    int tev_n = 0;                   // events the last enqueued block records
     pts_inclusion* d_incl = nullptr;  // inclusion list of pts_init_inclusions
     int incl_cap = 0;
     std::string err;
@@ -306,6 +309,25 @@ int V_bc(pts_ctx* c, bool update) {
     return PTS_OK;
 }
 
+// With kernel timing on, the next event of the block being enqueued: recorded on the
+// context's stream, or, during graph capture, as an event-record node of the graph.
+int mark(pts_ctx* c) {
+    if (!c->timing) return PTS_OK;
+    if (c->tev_n >= (int)c->tev.size()) {
+        cudaEvent_t e = nullptr;
+        CK(cudaEventCreate(&e));
+        c->tev.push_back(e);
+    }
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(c->stream, &st));
+    if (st == cudaStreamCaptureStatusActive)
+        CK(cudaEventRecordWithFlags(c->tev[c->tev_n], c->stream, cudaEventRecordExternal));
+    else
+        CK(cudaEventRecord(c->tev[c->tev_n], c->stream));
+    ++c->tev_n;
+    return PTS_OK;
+}
+
 // Tile configurations of the TMA-staged compute_Pt_τ! of a context: 3D FP64, 3D FP32
 // sweeps, 2D.
 int tile_count(bool d3, bool mixed) {
@@ -350,9 +372,9 @@ int alloc_m2(pts_ctx* c) {
 // One PT iteration with the two-kernel path: compute_Pt_τ! then compute_V! + bc.
 int iteration(pts_ctx* c, bool store_divV) {
     int rc = Pt_tau(c, store_divV);
-    if (rc) return rc;
+    if (rc || (rc = mark(c))) return rc;
     rc = V_bc(c, true);
-    if (rc) return rc;
+    if (rc || (rc = mark(c))) return rc;
     return PTS_OK;
 }
 
@@ -362,6 +384,8 @@ int iteration(pts_ctx* c, bool store_divV) {
 // role variants.
 int enqueue_block(pts_ctx* c, int64_t m, bool store_last) {
     if (m <= 0) return PTS_OK;
+    c->tev_n = 0;
+    if (int rc = mark(c)) return rc;
     if (c->mixed && c->fused32) {
         // compute_Pt_τ! of sweep 1 and compute_V! + bc of sweep m in place; in between, one
         // pass per pair (V of sweep q, Pt/τ of q+1) from one buffer set into the other. An
@@ -390,13 +414,16 @@ int enqueue_block(pts_ctx* c, int64_t m, bool store_last) {
                 CK(launch_corr_A32_zs(c->v, c->d.stencil_tile, c->g, c->m, c->n, c->d.stencil_kz, c->d_kerr, c->stream));
             else
                 CK(launch_corr_A32(c->v, c->g, c->m, c->n, c->stream));
+            if (int rc = mark(c)) return rc;
             if (c->zs)
                 CK(launch_corr_B32_zs(c->v, c->d.stencil_vtile, c->g, c->m, c->n, c->d.stencil_kz, c->d_kerr,
                                       c->stream));
             else
                 CK(launch_corr_B32(c->v, c->g, c->m, c->n, c->stream));
+            if (int rc = mark(c)) return rc;
         }
         CK(launch_fold(c->g, c->f, c->m, c->stream));
+        if (int rc = mark(c)) return rc;
         return PTS_OK;
     }
     if (!c->fused) {
@@ -425,7 +452,7 @@ int enqueue_check(pts_ctx* c) {
     else
         CK(launch_check(c->v, c->g, c->f, c->n, c->partials, c->partials_cap, c->d_result, c->stream));
     CK(cudaMemcpyAsync(c->h_result, c->d_result, sizeof(CheckResult), cudaMemcpyDeviceToHost, c->stream));
-    return PTS_OK;
+    return mark(c);
 }
 
 // Mixed precision: FP32 copies of the coefficients and the sources of the current iterate
@@ -529,6 +556,27 @@ int pts_set_mixed_sweep(pts_ctx* c, int32_t mixed_sweep) {
 }
 
 int pts_mixed_sweep_tiles(void) { return zfused32_num_configs(); }
+
+int pts_set_kernel_timing(pts_ctx* c, int32_t on) {
+    int rc = enter(c);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    c->timing = on != 0;
+    c->tev_n = 0;
+    drop_graph(c);  // the next check block is captured with (or without) its events
+    return PTS_OK;
+}
+
+int pts_kernel_times(pts_ctx* c, float* ms, int64_t cap, int64_t* count) {
+    int rc = enter(c);
+    if (rc) return rc;
+    if (!count || (cap > 0 && !ms)) return fail(c, PTS_E_INVAL, "null argument");
+    CK(cudaStreamSynchronize(c->stream));
+    const int64_t n = c->timing && c->tev_n > 1 ? c->tev_n - 1 : 0;
+    for (int64_t q = 0; q < n && q < cap; ++q) CK(cudaEventElapsedTime(&ms[q], c->tev[q], c->tev[q + 1]));
+    *count = n;
+    return PTS_OK;
+}
 
 int pts_stencil_tiles_2d(void) { return ystage_num_configs(); }
 
@@ -732,6 +780,7 @@ int pts_destroy(pts_ctx* c) {
     if (c->d_kerr) cudaFree(c->d_kerr);
     if (c->d_incl) cudaFree(c->d_incl);
     if (c->h_result) cudaFreeHost(c->h_result);
+    for (cudaEvent_t e : c->tev) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return PTS_OK;

@@ -463,7 +463,7 @@ __global__ void __launch_bounds__(32 * (TY + 1), MINB)
             }
         return;
     }
-    const int nx = g.nx, ny = g.ny;
+    const int nx = g.nx;
     const int i = i0 + lane;
     const int hc = (warp + 1) * HW + (lane + 2);
     const int pc = warp * TX + lane;

@@ -140,6 +140,9 @@ SIGNATURES = {
     "pts_compute_Pt_tau": ([_P], ctypes.c_int),
     "pts_compute_V_bc": ([_P], ctypes.c_int),
     "pts_sweep32_kernel": ([_P, ctypes.c_int32], ctypes.c_int),
+    "pts_set_kernel_timing": ([_P, ctypes.c_int32], ctypes.c_int),
+    "pts_kernel_times": ([_P, ctypes.POINTER(ctypes.c_float), ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)],
+                         ctypes.c_int),
     "pts_compute_res": ([_P, ctypes.POINTER(PtsCheck)], ctypes.c_int),
     "pts_iterate": ([_P, _I64], ctypes.c_int),
     "pts_solve": ([_P, ctypes.POINTER(PtsSolveInfo)], ctypes.c_int),

@@ -207,6 +207,17 @@ class Solver:
     def compute_V_bc(self):
         self._ck(self.lib.pts_compute_V_bc(self.ctx))
 
+    def set_kernel_timing(self, on=True):
+        """A CUDA event after each kernel of every block of PT iterations (graph blocks too)."""
+        self._ck(self.lib.pts_set_kernel_timing(self.ctx, 1 if on else 0))
+
+    def kernel_times(self, cap=1 << 16):
+        """Elapsed ms between the events of the last block, in launch order (synchronous)."""
+        buf = (ctypes.c_float * cap)()
+        cnt = ctypes.c_int64()
+        self._ck(self.lib.pts_kernel_times(self.ctx, buf, cap, ctypes.byref(cnt)))
+        return list(buf[: min(cnt.value, cap)])
+
     def compute_res(self):
         c = PtsCheck()
         self._ck(self.lib.pts_compute_res(self.ctx, ctypes.byref(c)))
