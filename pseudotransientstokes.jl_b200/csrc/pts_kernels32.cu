@@ -29,11 +29,11 @@ namespace pts {
 namespace {
 
 struct Num32 {
-    float _dx, _dy, _dz, r, gdt;
-    int gdt_one;
+    float _dx, _dy, _dz, r;
+    float igdt;  // 1/(G*dt): Gr = Gdτ/(G*dt) as one multiply (exact when G*dt = 1, as in the scripts)
 };
 
-__device__ __forceinline__ float gr32(float g, const Num32& n) { return n.gdt_one ? g : __fdividef(g, n.gdt); }
+__device__ __forceinline__ float gr32(float g, const Num32& n) { return g * n.igdt; }
 
 // δ-form compute_Pt_τ! (stresses as u = δτ - w), one thread per cell (arrays it only reads go through the read-only
 // data path).
@@ -356,7 +356,7 @@ __global__ void __launch_bounds__(256) k3_corrB(Geom g, Mixed32 m, Num32 n) {
 }
 
 Num32 num32(const Num& n) {
-    return Num32{(float)n._dx, (float)n._dy, (float)n._dz, (float)n.r, (float)n.gdt, n.gdt == 1.0 ? 1 : 0};
+    return Num32{(float)n._dx, (float)n._dy, (float)n._dz, (float)n.r, (float)(1.0 / n.gdt)};
 }
 
 // ---- compute_V! + bc of one sweep and compute_Pt_τ! of the next in one z-marching pass ----
