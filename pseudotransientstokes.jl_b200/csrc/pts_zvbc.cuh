@@ -155,13 +155,18 @@ __global__ void __launch_bounds__(32 * (TY + (PW ? 1 : 0)), MINB)
     const bool fx = in && j >= 1 && j <= ny - 2, ux = fx && i >= 1 && i <= nx - 1;
     const bool fy = in && i >= 1 && i <= nx - 2, uy = fy && j >= 1 && j <= ny - 1;
     const bool fz = in && i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2;
+    // faces whose free-slip copies do not depend on the plane: Vx next to a y-boundary, Vy next
+    // to an x-boundary, every Vz with a copy (the others copy only on the planes next to a
+    // z-boundary)
+    const bool ex = j == 1 || j == ny - 2, ey = i == 1 || i == nx - 2, ez = ex || ey;
     const int hc = (warp + 1) * C::HW + (lane + C::XP);
     const int pc = warp * TX + lane;
     constexpr int PS = TX * TY;
     const idx_t sx = 1, sy = g.px, sz = (idx_t)g.pxy;
+    idx_t c = gidx32(g, i, j, kb) - sz;  // this column at plane s = kb-1+t (advanced per step)
     T txz_m = T(0), tyz_m = T(0), tzz_m = T(0), pt_m = T(0), dr_m = T(0);  // plane s at the face, from stage s-1
     int t = 0;
-    for (; t < nst; ++t) {
+    for (; t < nst; ++t, c += sz) {
         const int slot = t % R, s = kb - 1 + t;
         if (prod && issued < nst) {
             if (issued >= R && !mbar_wait(&empty[issued % R], (issued / R - 1) & 1)) {
@@ -188,8 +193,7 @@ __global__ void __launch_bounds__(32 * (TY + (PW ? 1 : 0)), MINB)
         const T txz_p = hxz[hc], tyz_p = hyz[hc];
         const T tzz_p = P[3 * PS + pc], pt_p = P[4 * PS + pc], dr_p = P[5 * PS + pc];
         if (t > 0 && in) {
-            const idx_t c = gidx32(g, i, j, s);
-            const bool kI = s >= 1 && s <= nz - 2;
+            const bool kI = s >= 1 && s <= nz - 2, zedge = s == 1 || s == nz - 2;
             // Vx of plane s (Stokes3D_ve_perf.jl:84, @inn: i in [1,nx-1], j in [1,ny-2], k in [1,nz-2])
             if (fx && kI) {
                 T v = P[pc];
@@ -202,7 +206,7 @@ __global__ void __launch_bounds__(32 * (TY + (PW ? 1 : 0)), MINB)
                     v = v + Rx * ((hR[hc - 1] + hR[hc]) * n.half);
                     a.Vx[c] = v;
                 }
-                copies(a.Vx, c, v, j, 1, ny - 2, sy, s, 1, nz - 2, sz);
+                if (ex || zedge) copies(a.Vx, c, v, j, 1, ny - 2, sy, s, 1, nz - 2, sz);
             }
             // Vy of plane s (i in [1,nx-2], j in [1,ny-1], k in [1,nz-2])
             if (fy && kI) {
@@ -216,14 +220,14 @@ __global__ void __launch_bounds__(32 * (TY + (PW ? 1 : 0)), MINB)
                     v = v + Ry * ((hR[hc - C::HW] + hR[hc]) * n.half);
                     a.Vy[c] = v;
                 }
-                copies(a.Vy, c, v, i, 1, nx - 2, sx, s, 1, nz - 2, sz);
+                if (ey || zedge) copies(a.Vy, c, v, i, 1, nx - 2, sx, s, 1, nz - 2, sz);
             }
         }
         // Vz of z-face s+1 (i in [1,nx-2], j in [1,ny-2], k in [1,nz-1]); the first chunk also
         // makes the copies of z-face 0
         if (fz && (t > 0 || kb == 0)) {
             const int kf = s + 1;
-            const idx_t c = gidx32(g, i, j, kf);
+            const idx_t cz = c + sz;
             T v = P[2 * PS + pc];
             if (kf >= 1 && kf <= nz - 1) {
                 T Rz = ((dsv<T, PERF>(tzz_p - tzz_m, n.dz, n._dz) +
@@ -232,9 +236,9 @@ __global__ void __launch_bounds__(32 * (TY + (PW ? 1 : 0)), MINB)
                        dsv<T, PERF>(pt_p - pt_m, n.dz, n._dz);
                 if (SRC) Rz = Rz + P[8 * PS + pc];
                 v = v + Rz * ((dr_m + dr_p) * n.half);
-                a.Vz[c] = v;
+                a.Vz[cz] = v;
             }
-            copies(a.Vz, c, v, i, 1, nx - 2, sx, j, 1, ny - 2, sy);
+            if (ez) copies(a.Vz, cz, v, i, 1, nx - 2, sx, j, 1, ny - 2, sy);
         }
         txz_m = txz_p, tyz_m = tyz_p, tzz_m = tzz_p, pt_m = pt_p, dr_m = dr_p;
         __syncwarp();
