@@ -244,6 +244,23 @@ function check_partials(ctx::Ctx)
     return out
 end
 
+"MIXED contexts: 0 = two kernels per FP32 sweep (default), 1 + tile = the one-pass sweep."
+set_mixed_sweep!(ctx::Ctx, mixed_sweep::Integer) =
+    check(ctx, ccall((:pts_set_mixed_sweep, libpts), Cint, (Ptr{Cvoid}, Int32), ctx.ptr, mixed_sweep))
+
+"A CUDA event after each kernel of every block of PT iterations (inside the check-block graphs)."
+set_kernel_timing!(ctx::Ctx, on::Bool) =
+    check(ctx, ccall((:pts_set_kernel_timing, libpts), Cint, (Ptr{Cvoid}, Int32), ctx.ptr, on ? 1 : 0))
+
+"Per-kernel times (ms) of the last block, in launch order."
+function kernel_times(ctx::Ctx; cap::Integer=1 << 16)
+    ms = zeros(Float32, cap)
+    n = Ref{Int64}(0)
+    check(ctx, ccall((:pts_kernel_times, libpts), Cint, (Ptr{Cvoid}, Ptr{Float32}, Int64, Ref{Int64}),
+                     ctx.ptr, ms, cap, n))
+    return ms[1:min(n[], cap)]
+end
+
 "Lengths scaling norm_Rx, norm_Ry, norm_Rz, norm_∇V (Stokes2D_ve_param.jl:175-177: lx, ly, -, ly)."
 set_norm_scales!(ctx::Ctx, sRx, sRy, sRz, sdiv) =
     check(ctx, ccall((:pts_set_norm_scales, libpts), Cint, (Ptr{Cvoid}, Float64, Float64, Float64, Float64),
