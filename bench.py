@@ -579,6 +579,16 @@ def run_batch(args, ws, rank, local):
         "algorithmic_GBs": round(14 * 8 * cell_it / sec / 1e9, 1),
         "algorithmic_convention": "8 arrays read (Vx Vy Pt txx tyy txy Mus rhog) + 6 written, 8 B each",
     }
+    # roofline of the one launch: the operands of its two phases per cell-iteration (compute_P!
+    # + compute_τ! reads 7 arrays and writes 4, compute_V! + bc reads 7 and writes 2: 20 x 8 B),
+    # against the measured copy peak; DRAM traffic per cell-iteration from the committed capture
+    peak, peak_kind = hbm_peak()
+    alg = 20 * 8 * cell_it
+    line["roofline"] = {"bound": "hbm", "achieved": round(alg / sec / 1e9, 1), "peak": peak, "unit": "GB/s",
+                        "frac": round(alg / sec / 1e9 / peak, 4), "traffic": round(167.3 * cell_it),
+                        "traffic_from": "profiles/k2_batch_sweep_64inst.md (167.3 B per cell-iteration)",
+                        "kernel": "k2_batch", "peak_kind": peak_kind, "kernel_ms": round(sec * 1e3, 3),
+                        "algorithmic_bytes": alg}
     b.close()
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -247,7 +247,8 @@ class Solver:
         d.stencil, d.stencil_tile, d.stencil_kz, d.stencil_vtile = int(stencil), int(tile), int(kz), int(vtile)
 
     def tune_stencil(self, iters=20, kzs=(16, 32, 64), use_cache=True):
-        """Time every z-marching tile configuration x planes-per-block in `kzs` on this problem
+        """Time every z-marching (2D: y-marching) tile configuration x planes-per-block (2D: rows
+        per block) in `kzs` on this problem
         (`iters` PT iterations each, CUDA events on the context's stream), keep the fastest,
         and cache the choice per (variant, precision, grid) in ~/.cache/ptstokes/stencil.json.
         The iterations advance the fields; results do not depend on the configuration."""
@@ -282,11 +283,14 @@ class Solver:
             b.synchronize()
             return a.elapsed_time(b) / iters
 
-        # compute_Pt_τ! tiles x z-chunks with the default compute_V! tile, then the V tiles
-        ms = {f"{t}:{kz}:0": timed(t, kz, 0) for t in range(self.lib.pts_stencil_tiles(self.desc.precision))
-              for kz in kzs}
+        # compute_Pt_τ! tiles x z-chunks (2D: rows per block) with the default compute_V! tile,
+        # then the V tiles (3D only: 2D compute_V! has one form)
+        ntiles = (self.lib.pts_stencil_tiles(self.desc.precision) if self.ndim == 3
+                  else self.lib.pts_stencil_tiles_2d())
+        ms = {f"{t}:{kz}:0": timed(t, kz, 0) for t in range(ntiles) for kz in kzs}
         tile, kz, _ = map(int, min(ms, key=ms.get).split(":"))
-        for v in range(1, self.lib.pts_stencil_vtiles(self.desc.precision)):
+        nv = self.lib.pts_stencil_vtiles(self.desc.precision) if self.ndim == 3 else 1
+        for v in range(1, nv):
             ms[f"{tile}:{kz}:{v}"] = timed(tile, kz, v)
         tile, kz, vtile = map(int, min(ms, key=ms.get).split(":"))
         self.set_stencil(0, tile, kz, vtile)

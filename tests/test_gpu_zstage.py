@@ -132,3 +132,20 @@ def test_2d_y_marching_tiles_are_bit_exact(gpu_lib, variant, dims):
             for k in ITERATED2:
                 assert same_bits(got[k], ref[k]), (tile, ky, k)
             assert c == cref
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("variant,dims", [("3d_ve_perf", (37, 29, 23)), ("2d_ve_perf", (65, 47))])
+def test_tune_stencil_picks_a_valid_configuration(gpu_lib, variant, dims):
+    import ptstokes
+
+    s = ptstokes.Solver(variant, *dims, lib=gpu_lib, nout=20, eps=1e-300, iter_max=19)
+    s.setup_inclusion()
+    s.assign_tau()
+    e = s.tune_stencil(iters=3, kzs=(8, 0), use_cache=False)
+    ntiles = gpu_lib.pts_stencil_tiles(0) if variant.startswith("3d") else gpu_lib.pts_stencil_tiles_2d()
+    assert 0 <= e["tile"] < ntiles and e["kz"] in (8, 0)
+    assert len(e["ms_per_iteration"]) >= ntiles * 2
+    r = s.solve()
+    assert r["iters"] == 20 and np.isfinite(r["last"]["err"])
+    s.close()
