@@ -247,7 +247,7 @@ def run_ours(args, ws, rank, local, pg):
     variant = args.variant
     s = ptstokes.Solver(variant, n, n, n, nout=nout, eps=1e-300, iter_max=nout - 1,
                         single_pass=args.single_pass, precision=args.precision, stencil=args.stencil,
-                        stencil_tile=args.stencil_tile)
+                        stencil_tile=args.stencil_tile, stencil_vtile=args.stencil_vtile, stencil_kz=args.stencil_kz)
     s.setup_inclusion()
     s.assign_tau()
     stream = torch.cuda.ExternalStream(s.stream_handle())
@@ -353,7 +353,7 @@ def run_ours(args, ws, rank, local, pg):
         nctx = max(1, min(args.e2e_contexts, args.steps))
         ctxs = [s] + [ptstokes.Solver(variant, n, n, n, nout=nout, eps=1e-300, iter_max=nout - 1,
                                       single_pass=args.single_pass, precision=args.precision, stencil=args.stencil,
-                        stencil_tile=args.stencil_tile)
+                        stencil_tile=args.stencil_tile, stencil_vtile=args.stencil_vtile, stencil_kz=args.stencil_kz)
                       for _ in range(nctx - 1)]
         outs = [torch.empty(n * n * n, dtype=torch.float64, pin_memory=True).numpy().reshape((n, n, n), order="F")
                 for _ in ctxs]
@@ -469,7 +469,7 @@ def run_2d(args, ws, rank, local, pg):
     torch.cuda.set_device(local)
     n, nout = args.n2, args.iters_per_step
     s = ptstokes.Solver("2d_ve_perf", n, n, nout=nout, eps=1e-300, iter_max=nout - 1, stencil=args.stencil,
-                        stencil_tile=args.stencil_tile)
+                        stencil_tile=args.stencil_tile, stencil_kz=args.stencil_kz)
     s.setup_inclusion()
     s.assign_tau()
     stream = torch.cuda.ExternalStream(s.stream_handle())
@@ -925,6 +925,8 @@ def main():
     ap.add_argument("--stencil", type=int, default=0, choices=[0, 1],
                     help="0: z-marching TMA-staged kernels, 1: one thread per point")
     ap.add_argument("--stencil-tile", type=int, default=0, help="tile configuration of the TMA-staged compute_Pt_τ!")
+    ap.add_argument("--stencil-vtile", type=int, default=0, help="tile configuration of the TMA-staged compute_V!")
+    ap.add_argument("--stencil-kz", type=int, default=0, help="z-planes (2D: rows) per block of the TMA-staged kernels")
     ap.add_argument("--ttt-n", type=int, default=511, help="grid of the time-to-tolerance comparison (0: skip)")
     ap.add_argument("--ttt-n2", type=int, default=255, help="a second, smaller time-to-tolerance grid (0: skip)")
     ap.add_argument("--incl-default-n", type=int, default=255,
