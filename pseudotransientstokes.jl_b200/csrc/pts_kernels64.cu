@@ -1205,6 +1205,10 @@ constexpr int kListSmem = 1024;  // active lists up to this many instances are w
 #ifndef PTS_SWEEP_THREADS_PER_SM
 #define PTS_SWEEP_THREADS_PER_SM 1024
 #endif
+// tiles ahead of the one being computed whose first lines are requested into L2
+#ifndef PTS_SWEEP_PREFETCH
+#define PTS_SWEEP_PREFETCH 1
+#endif
 template <int TX, int TY>
 __global__ void __launch_bounds__(TX* TY, PTS_SWEEP_THREADS_PER_SM / (TX * TY)) k2_batch(const BInst* __restrict__ inst, int ntiles, int ninst, SweepF F,
                                                    BState st, int nout, int64_t iter_last, double eps) {
@@ -1259,7 +1263,10 @@ __global__ void __launch_bounds__(TX* TY, PTS_SWEEP_THREADS_PER_SM / (TX * TY)) 
                 P = sweep_params(inst[b], iter_last);
             }
             const int q = v - f0;
-            if (v + 1 < v1 && v + 1 < f1) pre(P, ((q + 1) % P.ntx) * TX + tx, ((q + 1) / P.ntx) * TY + ty);
+#pragma unroll
+            for (int d = 1; d <= PTS_SWEEP_PREFETCH; ++d)
+                if (v + d < v1 && v + d < f1 && (d == PTS_SWEEP_PREFETCH || v == v0))
+                    pre(P, ((q + d) % P.ntx) * TX + tx, ((q + d) / P.ntx) * TY + ty);
             body(P, b, P.tile0 + q, (q % P.ntx) * TX + tx, (q / P.ntx) * TY + ty);
         }
     };
