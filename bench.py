@@ -358,13 +358,15 @@ def run_ours(args, ws, rank, local, pg):
         outs = [torch.empty(n * n * n, dtype=torch.float64, pin_memory=True).numpy().reshape((n, n, n), order="F")
                 for _ in ctxs]
 
-        def e2e_step(c, out):
+        def e2e_step(c, out, before_solve=None):
             for name, a in host.items():
                 c._ck(c.lib.pts_set_field(c.ctx, ptstokes._abi.FIELD_ID[name], a.ctypes.data, a.size))
             c.smooth(10, 1.0)
             c.compute_maxloc()
             c.compute_iter_params()
             c.assign_tau()
+            if before_solve:
+                before_solve()
             c.solve()
             c._ck(c.lib.pts_get_field(c.ctx, ptstokes._abi.FIELD_ID["Pt"], out.ctypes.data, out.size))
 
@@ -379,15 +381,24 @@ def run_ours(args, ws, rank, local, pg):
         a.record(stream)
         a.synchronize()
         failures = []
+        # staggered start: context q begins its first step once context q-1 has launched its
+        # first solve, so one context's copies and set-up run while another iterates (started
+        # together, the contexts would copy at the same time and iterate at the same time)
+        solving = [threading.Event() for _ in ctxs]
 
-        def worker(c, o, k):
+        def worker(q, c, o, k):
             try:
-                for _ in range(k):
-                    e2e_step(c, o)
+                if q > 0 and not solving[q - 1].wait(timeout=600):
+                    raise RuntimeError("the previous context did not start")
+                for step in range(k):
+                    e2e_step(c, o, solving[q].set if step == 0 else None)
             except Exception as exc:  # re-raised below: a failed step must not yield a number
                 failures.append(exc)
+            finally:
+                solving[q].set()
 
-        threads = [threading.Thread(target=worker, args=(c, o, k)) for c, o, k in zip(ctxs, outs, share)]
+        threads = [threading.Thread(target=worker, args=(q, c, o, k))
+                   for q, (c, o, k) in enumerate(zip(ctxs, outs, share))]
         for t in threads:
             t.start()
         for t in threads:
@@ -405,7 +416,8 @@ def run_ours(args, ws, rank, local, pg):
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "ms_per_step": round(t_e2e / args.steps, 3), "contexts": nctx,
                "includes": "per step: pinned H2D of Mus,Vx,Vy,Vz; set-up kernels; nout PT iterations + check; "
-                           "D2H of Pt; with several contexts the copies of one overlap the iterations of another"}
+                           "D2H of Pt; with several contexts, started staggered, the copies of one overlap the "
+                           "iterations of another"}
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
