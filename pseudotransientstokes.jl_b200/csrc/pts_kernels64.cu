@@ -1050,14 +1050,14 @@ __device__ __forceinline__ SweepF sweep_at(const SweepF& F, int64_t off) {
 // What a tile of the sweep needs of its instance, loaded into registers when a block's walk
 // enters the instance.
 struct SweepP {
-    int nx, ny, px, ntx, tile0;
+    int nx, ny, px, py, ntx, tile0;
     int64_t off, cap;
     double dx, dy, r, G, R;  // G = Gdτ, R = dτ_Rho (uniform per instance)
 };
 
 __device__ __forceinline__ SweepP sweep_params(const BInst& I, int64_t iter_last) {
     SweepP P;
-    P.nx = I.g.nx; P.ny = I.g.ny; P.px = I.g.px; P.ntx = I.ntx; P.tile0 = I.tile0;
+    P.nx = I.g.nx; P.ny = I.g.ny; P.px = I.g.px; P.py = I.g.py; P.ntx = I.ntx; P.tile0 = I.tile0;
     P.off = I.off;
     P.cap = I.iter_last < iter_last ? I.iter_last : iter_last;
     P.dx = I.n.dx; P.dy = I.n.dy; P.r = I.n.r; P.G = I.Gd; P.R = I.dR;
@@ -1069,6 +1069,34 @@ __device__ __forceinline__ SweepP sweep_params(const BInst& I, int64_t iter_last
 // @av(Gdτ) is formed from it in the reference's order and no Gdτ array is read. Every load
 // is issued before the first store (the fields are distinct arrays), so a point costs one
 // round trip to memory rather than one per store.
+// The arithmetic of the sweep's compute_P! + compute_τ! at one point, on operand values
+// (shared by the direct and the staged walks, so both give the same bits).
+struct SweepA {
+    double dv, pt, txx, tyy, txy;
+};
+__device__ __forceinline__ SweepA pt_tau_core(const SweepP& P, bool edge, double vx0, double vx1, double vy0, double vy1,
+                                              double pt, double Mc, double sxx, double syy, double m11, double m01,
+                                              double m10, double vxs, double vys, double sxy) {
+    SweepA o;
+    const double G = P.G;
+    const double dvx = vx1 - vx0, dvy = vy1 - vy0;
+    o.dv = dvx / P.dx + dvy / P.dy;
+    const double mu = 1.0 / (1.0 / G + 1.0 / Mc);  // @μ_veτ
+    o.pt = pt - P.r * G * o.dv;
+    o.txx = 2.0 * mu * (dvx / P.dx + sxx / G / 2.0);
+    o.tyy = 2.0 * mu * (dvy / P.dy + syy / G / 2.0);
+    o.txy = 0.0;
+    if (edge) {
+        const double ag = (((G + G) + G) + G) * 0.25;
+        const double am = (((m11 + m01) + m10) + Mc) * 0.25;
+        const double mua = 1.0 / (1.0 / ag + 1.0 / am);  // @μ_veτ_av
+        const double d1 = vx0 - vxs;                       // @d_yi(Vx)
+        const double d2 = vy0 - vys;                       // @d_xi(Vy)
+        o.txy = 2.0 * mua * (0.5 * (d1 / P.dy + d2 / P.dx) + sxy / ag / 2.0);
+    }
+    return o;
+}
+
 __device__ __forceinline__ void pt_tau_sweep(const SweepF& f, const SweepP& P, int i, int j, bool store_divV) {
     if (i >= P.nx || j >= P.ny) return;
     const idx_t sx = 1, sy = P.px;
@@ -1085,39 +1113,62 @@ __device__ __forceinline__ void pt_tau_sweep(const SweepF& f, const SweepP& P, i
         vys = f.Vy[c - sx];
         sxy = f.txy[c];
     }
-    const double G = P.G;
-    const double dvx = vx1 - vx0, dvy = vy1 - vy0;
-    const double dv = dvx / P.dx + dvy / P.dy;
-    const double mu = 1.0 / (1.0 / G + 1.0 / Mc);  // @μ_veτ
-    if (store_divV) f.divV[c] = dv;
-    f.Pt[c] = pt - P.r * G * dv;
-    f.txx[c] = 2.0 * mu * (dvx / P.dx + sxx / G / 2.0);
-    f.tyy[c] = 2.0 * mu * (dvy / P.dy + syy / G / 2.0);
-    if (edge) {
-        const double ag = (((G + G) + G) + G) * 0.25;
-        const double am = (((m11 + m01) + m10) + Mc) * 0.25;
-        const double mua = 1.0 / (1.0 / ag + 1.0 / am);  // @μ_veτ_av
-        const double d1 = vx0 - vxs;                       // @d_yi(Vx)
-        const double d2 = vy0 - vys;                       // @d_xi(Vy)
-        f.txy[c] = 2.0 * mua * (0.5 * (d1 / P.dy + d2 / P.dx) + sxy / ag / 2.0);
-    }
+    const SweepA o = pt_tau_core(P, edge, vx0, vx1, vy0, vy1, pt, Mc, sxx, syy, m11, m01, m10, vxs, vys, sxy);
+    if (store_divV) f.divV[c] = o.dv;
+    f.Pt[c] = o.pt;
+    f.txx[c] = o.txx;
+    f.tyy[c] = o.tyy;
+    if (edge) f.txy[c] = o.txy;
 }
 
 // Rx, Ry of compute_dV! (Stokes2D_param.jl:58-59), Ry with the buoyancy term -@av_yi(ρg)
+__device__ __forceinline__ double res_x_core(const SweepP& P, double xx, double xx_m, double xy_p, double xy, double pt,
+                                             double pt_m) {
+    return ((xx - xx_m) / P.dx + (xy_p - xy) / P.dy) - (pt - pt_m) / P.dx;
+}
+__device__ __forceinline__ double res_y_core(const SweepP& P, double yy, double yy_m, double xy_p, double xy, double pt,
+                                             double pt_m, double rg_m, double rg) {
+    const double R = ((yy - yy_m) / P.dy + (xy_p - xy) / P.dx) - (pt - pt_m) / P.dy;
+    return R - (rg_m + rg) * 0.5;
+}
 __device__ __forceinline__ double res_sweep_x(const SweepF& f, const SweepP& P, idx_t c, idx_t sy) {
-    return ((f.txx[c] - f.txx[c - 1]) / P.dx + (f.txy[c + sy] - f.txy[c]) / P.dy) - (f.Pt[c] - f.Pt[c - 1]) / P.dx;
+    return res_x_core(P, f.txx[c], f.txx[c - 1], f.txy[c + sy], f.txy[c], f.Pt[c], f.Pt[c - 1]);
 }
 __device__ __forceinline__ double res_sweep_y(const SweepF& f, const SweepP& P, idx_t c, idx_t sy) {
-    const double R = ((f.tyy[c] - f.tyy[c - sy]) / P.dy + (f.txy[c + 1] - f.txy[c]) / P.dx) - (f.Pt[c] - f.Pt[c - sy]) / P.dy;
-    return R - (f.rhog[c - sy] + f.rhog[c]) * 0.5;
+    return res_y_core(P, f.tyy[c], f.tyy[c - sy], f.txy[c + 1], f.txy[c], f.Pt[c], f.Pt[c - sy], f.rhog[c - sy],
+                      f.rhog[c]);
 }
 
 // compute_dV! + compute_V! + bc_y!(Vx), bc_x!(Vy) of the sweep script (Stokes2D_param.jl:57-81,
 // 198-200) with the uniform dτ_Rho R: @av_xi(dτ_Rho) = (R + R)*0.5. Loads first, as above.
+// The update and the free-slip copies of one face point, from its operands (shared by the
+// direct and the staged walks).
+__device__ __forceinline__ void v_bc_apply(const SweepF& f, const SweepP& P, int i, int j, idx_t c, bool fx, bool ux,
+                                           bool fy, bool uy, double vx, double vy, double Rx, double Ry) {
+    const idx_t sx = 1, sy = P.px;
+    const double aR = (P.R + P.R) * 0.5;
+    if (fx) {
+        if (ux) {
+            vx = vx + Rx * aR;
+            f.Vx[c] = vx;
+        }
+        if (j == 1) f.Vx[c - sy] = vx;
+        if (j == P.ny - 2) f.Vx[c + sy] = vx;
+    }
+    if (fy) {
+        if (uy) {
+            vy = vy + Ry * aR;
+            f.Vy[c] = vy;
+        }
+        if (i == 1) f.Vy[c - sx] = vy;
+        if (i == P.nx - 2) f.Vy[c + sx] = vy;
+    }
+}
+
 __device__ __forceinline__ void v_bc_sweep(const SweepF& f, const SweepP& P, int i, int j) {
     const int nx = P.nx, ny = P.ny;
     if (i > nx || j > ny) return;
-    const idx_t sx = 1, sy = P.px;
+    const idx_t sy = P.px;
     const idx_t c = i + sy * j;
     const bool fx = (j >= 1 && j <= ny - 2), ux = fx && (i >= 1 && i <= nx - 1);
     const bool fy = (i >= 1 && i <= nx - 2), uy = fy && (j >= 1 && j <= ny - 1);
@@ -1126,23 +1177,7 @@ __device__ __forceinline__ void v_bc_sweep(const SweepF& f, const SweepP& P, int
     if (fy) vy = f.Vy[c];
     if (ux) Rx = res_sweep_x(f, P, c, sy);
     if (uy) Ry = res_sweep_y(f, P, c, sy);
-    const double aR = (P.R + P.R) * 0.5;
-    if (fx) {
-        if (ux) {
-            vx = vx + Rx * aR;
-            f.Vx[c] = vx;
-        }
-        if (j == 1) f.Vx[c - sy] = vx;
-        if (j == ny - 2) f.Vx[c + sy] = vx;
-    }
-    if (fy) {
-        if (uy) {
-            vy = vy + Ry * aR;
-            f.Vy[c] = vy;
-        }
-        if (i == 1) f.Vy[c - sx] = vy;
-        if (i == nx - 2) f.Vy[c + sx] = vy;
-    }
+    v_bc_apply(f, P, i, j, c, fx, ux, fy, uy, vx, vy, Rx, Ry);
 }
 
 // Active list of the sweep (built by block 0): act[0] = K instances still iterating,
@@ -1209,6 +1244,17 @@ constexpr int kListSmem = 1024;  // active lists up to this many instances are w
 #ifndef PTS_SWEEP_PREFETCH
 #define PTS_SWEEP_PREFETCH 1
 #endif
+// 1: the PT phases walk tiles whose operands are staged in shared memory (cp.async, double
+// buffer); 0: every point loads its operands from global memory
+#ifndef PTS_SWEEP_STAGED
+#define PTS_SWEEP_STAGED 0
+#endif
+// doubles of one staging buffer: the larger of the two phases' operand sets
+__host__ __device__ constexpr int sweep_stage_doubles(int tx, int ty) {
+    return 3 * (tx + 2) * (ty + 2) + 4 * tx * ty > 5 * (tx + 2) * (ty + 2) + 2 * tx * ty
+               ? 3 * (tx + 2) * (ty + 2) + 4 * tx * ty
+               : 5 * (tx + 2) * (ty + 2) + 2 * tx * ty;
+}
 template <int TX, int TY>
 __global__ void __launch_bounds__(TX* TY, PTS_SWEEP_THREADS_PER_SM / (TX * TY)) k2_batch(const BInst* __restrict__ inst, int ntiles, int ninst, SweepF F,
                                                    BState st, int nout, int64_t iter_last, double eps) {
@@ -1270,6 +1316,92 @@ __global__ void __launch_bounds__(TX* TY, PTS_SWEEP_THREADS_PER_SM / (TX * TY)) 
             body(P, b, P.tile0 + q, (q % P.ntx) * TX + tx, (q / P.ntx) * TY + ty);
         }
     };
+#if PTS_SWEEP_STAGED
+    // Staged walk: the operands of a tile, with a one-point halo, are copied into shared memory
+    // by cp.async (zero where the halo leaves the instance's arrays), double-buffered, so the
+    // copies of tile v+1 are in flight while tile v computes.
+    constexpr int HX = TX + 2, H = HX * (TY + 2), PT = TX * TY;
+    constexpr int SD = sweep_stage_doubles(TX, TY);
+    extern __shared__ double sbuf[];
+    auto cp8 = [](double* dst, const double* src, bool ok) {
+        const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(ok ? 8 : 0) : "memory");
+    };
+    // rows j0-1 .. j0+TY, columns i0-1 .. i0+TX of A
+    auto stage_halo = [&](double* dst, const double* A, const SweepP& P, int i0, int j0) {
+        for (int e = tid; e < H; e += PT) {
+            const int x = i0 - 1 + e % HX, y = j0 - 1 + e / HX;
+            const bool ok = x >= 0 && x < P.px && y >= 0 && y < P.py;
+            cp8(dst + e, ok ? A + (x + (idx_t)P.px * y) : A, ok);
+        }
+    };
+    // the tile's own points of A (one per thread)
+    auto stage_pt = [&](double* dst, const double* A, const SweepP& P, int i0, int j0) {
+        const int x = i0 + tx, y = j0 + ty;
+        const bool ok = x < P.px && y < P.py;
+        cp8(dst + tid, ok ? A + (x + (idx_t)P.px * y) : A, ok);
+    };
+    auto walk_staged = [&](auto&& load, auto&& body) {
+        const int chunk = (T + (int)gridDim.x - 1) / (int)gridDim.x;
+        const int v0 = (int)blockIdx.x * chunk, v1 = min(T, v0 + chunk);
+        if (v0 >= v1) return;
+        int lo = 0, hi = K - 1;  // last k with first_at(k) <= v0
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (first_at(mid) <= v0) lo = mid;
+            else hi = mid - 1;
+        }
+        // cursor of the tile computed (c*) and of the tile staged next (n*)
+        int ck = lo, cf0 = first_at(ck), cf1 = first_at(ck + 1);
+        SweepP cP = sweep_params(inst[id_at(ck)], iter_last);
+        int nk = ck, nf0 = cf0, nf1 = cf1;
+        SweepP nP = cP;
+        load(cP, ((v0 - cf0) % cP.ntx) * TX, ((v0 - cf0) / cP.ntx) * TY, sbuf);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        for (int v = v0; v < v1; ++v) {
+            if (v >= cf1) {
+                do { ++ck; cf0 = cf1; cf1 = first_at(ck + 1); } while (v >= cf1);
+                cP = sweep_params(inst[id_at(ck)], iter_last);
+            }
+            const int w = v + 1;
+            if (w < v1) {
+                if (w >= nf1) {
+                    do { ++nk; nf0 = nf1; nf1 = first_at(nk + 1); } while (w >= nf1);
+                    nP = sweep_params(inst[id_at(nk)], iter_last);
+                }
+                load(nP, ((w - nf0) % nP.ntx) * TX, ((w - nf0) / nP.ntx) * TY, sbuf + (w & 1) * SD);
+            }
+            asm volatile("cp.async.commit_group;" ::: "memory");
+            asm volatile("cp.async.wait_group 1;" ::: "memory");  // tile v has landed
+            __syncthreads();
+            body(cP, ((v - cf0) % cP.ntx) * TX, ((v - cf0) / cP.ntx) * TY, (const double*)(sbuf + (v & 1) * SD));
+            __syncthreads();  // buffer v&1 is refilled for tile v+2
+        }
+    };
+    // compute_P! + compute_τ!: halos Vx Vy Mus, points Pt τxx τyy τxy
+    auto loadA = [&](const SweepP& P, int i0, int j0, double* S) {
+        const SweepF f = sweep_at(F, P.off);
+        stage_halo(S, f.Vx, P, i0, j0);
+        stage_halo(S + H, f.Vy, P, i0, j0);
+        stage_halo(S + 2 * H, f.Mus, P, i0, j0);
+        stage_pt(S + 3 * H, f.Pt, P, i0, j0);
+        stage_pt(S + 3 * H + PT, f.txx, P, i0, j0);
+        stage_pt(S + 3 * H + 2 * PT, f.tyy, P, i0, j0);
+        stage_pt(S + 3 * H + 3 * PT, f.txy, P, i0, j0);
+    };
+    // compute_dV! + compute_V! + bc: halos τxx τyy τxy Pt ρg, points Vx Vy
+    auto loadB = [&](const SweepP& P, int i0, int j0, double* S) {
+        const SweepF f = sweep_at(F, P.off);
+        stage_halo(S, f.txx, P, i0, j0);
+        stage_halo(S + H, f.tyy, P, i0, j0);
+        stage_halo(S + 2 * H, f.txy, P, i0, j0);
+        stage_halo(S + 3 * H, f.Pt, P, i0, j0);
+        stage_halo(S + 4 * H, f.rhog, P, i0, j0);
+        stage_pt(S + 5 * H, f.Vx, P, i0, j0);
+        stage_pt(S + 5 * H + PT, f.Vy, P, i0, j0);
+    };
+    const int hs = (ty + 1) * HX + (tx + 1);  // this thread's point in a halo box
+#endif
     // L2 prefetches of the lines a point's stencil reads first, at an address clamped into the
     // instance's own padded arrays (always a valid address)
     auto pf = [](const double* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); };
@@ -1297,6 +1429,48 @@ __global__ void __launch_bounds__(TX* TY, PTS_SWEEP_THREADS_PER_SM / (TX * TY)) 
     for (;;) {
         if (*(volatile int*)st.nactive == 0 || iter > iter_last) break;
         const bool chk = ((iter + 1) % nout == 0);
+#if PTS_SWEEP_STAGED
+        walk_staged(loadA, [&](const SweepP& P, int i0, int j0, const double* S) {
+            const int i = i0 + tx, j = j0 + ty;
+            if (iter > P.cap || i >= P.nx || j >= P.ny) return;
+            const double *hVx = S, *hVy = S + H, *hM = S + 2 * H, *pP = S + 3 * H;
+            const bool edge = (i >= 1 && j >= 1);
+            double m11 = 0.0, m01 = 0.0, m10 = 0.0, vxs = 0.0, vys = 0.0, sxy = 0.0;
+            if (edge) {
+                m11 = hM[hs - HX - 1];
+                m01 = hM[hs - HX];
+                m10 = hM[hs - 1];
+                vxs = hVx[hs - HX];
+                vys = hVy[hs - 1];
+                sxy = pP[3 * PT + tid];
+            }
+            const SweepA o = pt_tau_core(P, edge, hVx[hs], hVx[hs + 1], hVy[hs], hVy[hs + HX], pP[tid], hM[hs],
+                                         pP[PT + tid], pP[2 * PT + tid], m11, m01, m10, vxs, vys, sxy);
+            const SweepF f = sweep_at(F, P.off);
+            const idx_t c = i + (idx_t)P.px * j;
+            if (chk) f.divV[c] = o.dv;
+            f.Pt[c] = o.pt;
+            f.txx[c] = o.txx;
+            f.tyy[c] = o.tyy;
+            if (edge) f.txy[c] = o.txy;
+        });
+        grid.sync();
+        walk_staged(loadB, [&](const SweepP& P, int i0, int j0, const double* S) {
+            const int i = i0 + tx, j = j0 + ty, nx = P.nx, ny = P.ny;
+            if (iter > P.cap || i > nx || j > ny) return;
+            const double *hxx = S, *hyy = S + H, *hxy = S + 2 * H, *hP = S + 3 * H, *hR = S + 4 * H;
+            const double* pV = S + 5 * H;
+            const bool fx = (j >= 1 && j <= ny - 2), ux = fx && (i >= 1 && i <= nx - 1);
+            const bool fy = (i >= 1 && i <= nx - 2), uy = fy && (j >= 1 && j <= ny - 1);
+            double vx = 0.0, vy = 0.0, Rx = 0.0, Ry = 0.0;
+            if (fx) vx = pV[tid];
+            if (fy) vy = pV[PT + tid];
+            if (ux) Rx = res_x_core(P, hxx[hs], hxx[hs - 1], hxy[hs + HX], hxy[hs], hP[hs], hP[hs - 1]);
+            if (uy)
+                Ry = res_y_core(P, hyy[hs], hyy[hs - HX], hxy[hs + 1], hxy[hs], hP[hs], hP[hs - HX], hR[hs - HX], hR[hs]);
+            v_bc_apply(sweep_at(F, P.off), P, i, j, i + (idx_t)P.px * j, fx, ux, fy, uy, vx, vy, Rx, Ry);
+        });
+#else
         walk([&](const SweepP& P, int, int, int i, int j) {
             if (iter <= P.cap) pt_tau_sweep(sweep_at(F, P.off), P, i, j, chk);
         }, preA);
@@ -1304,6 +1478,7 @@ __global__ void __launch_bounds__(TX* TY, PTS_SWEEP_THREADS_PER_SM / (TX * TY)) 
         walk([&](const SweepP& P, int, int, int i, int j) {
             if (iter <= P.cap) v_bc_sweep(sweep_at(F, P.off), P, i, j);
         }, preB);
+#endif
         // an instance doing its last allowed iteration leaves the active count here
         for (int b = blockIdx.x * TX * TY + tid; b < ninst; b += gridDim.x * TX * TY) {
             const int64_t cap = inst[b].iter_last < iter_last ? inst[b].iter_last : iter_last;
@@ -1345,7 +1520,11 @@ __global__ void __launch_bounds__(TX* TY, PTS_SWEEP_THREADS_PER_SM / (TX * TY)) 
         }, no_pre);
         grid.sync();
         // per-instance finalisation: one block per instance, fixed-order reduction
+#if PTS_SWEEP_STAGED
+        double (*red)[kCheckSlots] = reinterpret_cast<double (*)[kCheckSlots]>(sbuf);  // the staging buffers are idle here
+#else
         __shared__ double red[TX * TY][kCheckSlots];
+#endif
         for (int b = blockIdx.x; b < ninst; b += gridDim.x) {
             const BInst& I = inst[b];
             const int64_t cap = I.iter_last < iter_last ? I.iter_last : iter_last;
@@ -1839,7 +2018,13 @@ static cudaError_t launch_batch_t(const BInst* d_inst, int ntiles, int ninst, co
                                   int nout, int64_t iter_last, double eps, cudaStream_t s) {
     SweepF F{F64.Pt, F64.Vx, F64.Vy, F64.txx, F64.tyy, F64.txy, F64.Mus, F64.divV, F64.Rx, F64.Ry, F64.rhog};
     int per_sm = 0, dev = 0, nsm = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k2_batch<TX, TY>, TX * TY, 0);
+    const size_t dyn = PTS_SWEEP_STAGED ? 2 * sizeof(double) * (size_t)sweep_stage_doubles(TX, TY) : 0;
+    cudaError_t e = cudaSuccess;
+    if (dyn > 48 * 1024 &&
+        (e = cudaFuncSetAttribute(k2_batch<TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn)) !=
+            cudaSuccess)
+        return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k2_batch<TX, TY>, TX * TY, dyn);
     if (e != cudaSuccess) return e;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
@@ -1849,7 +2034,7 @@ static cudaError_t launch_batch_t(const BInst* d_inst, int ntiles, int ninst, co
     if (grid < 1) return cudaErrorInvalidConfiguration;
     void* args[] = {(void*)&d_inst, (void*)&ntiles,    (void*)&ninst, (void*)&F,
                     (void*)&st,     (void*)&nout,      (void*)&iter_last, (void*)&eps};
-    return cudaLaunchCooperativeKernel((const void*)k2_batch<TX, TY>, dim3(grid), dim3(TX, TY), args, 0, s);
+    return cudaLaunchCooperativeKernel((const void*)k2_batch<TX, TY>, dim3(grid), dim3(TX, TY), args, dyn, s);
 }
 
 cudaError_t launch_batch(int tile, const BInst* d_inst, int ntiles, int ninst,
