@@ -1356,7 +1356,7 @@ __global__ void __launch_bounds__(TX* TY, PTS_SWEEP_THREADS_PER_SM / (TX * TY)) 
         SweepP cP = sweep_params(inst[id_at(ck)], iter_last);
         int nk = ck, nf0 = cf0, nf1 = cf1;
         SweepP nP = cP;
-        load(cP, ((v0 - cf0) % cP.ntx) * TX, ((v0 - cf0) / cP.ntx) * TY, sbuf);
+        load(cP, ((v0 - cf0) % cP.ntx) * TX, ((v0 - cf0) / cP.ntx) * TY, sbuf + (v0 & 1) * SD);
         asm volatile("cp.async.commit_group;" ::: "memory");
         for (int v = v0; v < v1; ++v) {
             if (v >= cf1) {
