@@ -2020,7 +2020,8 @@ static cudaError_t launch_batch_t(const BInst* d_inst, int ntiles, int ninst, co
     int per_sm = 0, dev = 0, nsm = 0;
     const size_t dyn = PTS_SWEEP_STAGED ? 2 * sizeof(double) * (size_t)sweep_stage_doubles(TX, TY) : 0;
     cudaError_t e = cudaSuccess;
-    if (dyn > 48 * 1024 &&
+    // the opt-in above the default 48 KB of static plus dynamic shared memory per block
+    if (dyn > 0 &&
         (e = cudaFuncSetAttribute(k2_batch<TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn)) !=
             cudaSuccess)
         return e;
