@@ -1244,17 +1244,7 @@ constexpr int kListSmem = 1024;  // active lists up to this many instances are w
 #ifndef PTS_SWEEP_PREFETCH
 #define PTS_SWEEP_PREFETCH 1
 #endif
-// 1: the PT phases walk tiles whose operands are staged in shared memory (cp.async, double
-// buffer); 0: every point loads its operands from global memory
-#ifndef PTS_SWEEP_STAGED
-#define PTS_SWEEP_STAGED 0
-#endif
-// doubles of one staging buffer: the larger of the two phases' operand sets
-__host__ __device__ constexpr int sweep_stage_doubles(int tx, int ty) {
-    return 3 * (tx + 2) * (ty + 2) + 4 * tx * ty > 5 * (tx + 2) * (ty + 2) + 2 * tx * ty
-               ? 3 * (tx + 2) * (ty + 2) + 4 * tx * ty
-               : 5 * (tx + 2) * (ty + 2) + 2 * tx * ty;
-}
+
 template <int TX, int TY>
 __global__ void __launch_bounds__(TX* TY, PTS_SWEEP_THREADS_PER_SM / (TX * TY)) k2_batch(const BInst* __restrict__ inst, int ntiles, int ninst, SweepF F,
                                                    BState st, int nout, int64_t iter_last, double eps) {
@@ -1316,92 +1306,6 @@ __global__ void __launch_bounds__(TX* TY, PTS_SWEEP_THREADS_PER_SM / (TX * TY)) 
             body(P, b, P.tile0 + q, (q % P.ntx) * TX + tx, (q / P.ntx) * TY + ty);
         }
     };
-#if PTS_SWEEP_STAGED
-    // Staged walk: the operands of a tile, with a one-point halo, are copied into shared memory
-    // by cp.async (zero where the halo leaves the instance's arrays), double-buffered, so the
-    // copies of tile v+1 are in flight while tile v computes.
-    constexpr int HX = TX + 2, H = HX * (TY + 2), PT = TX * TY;
-    constexpr int SD = sweep_stage_doubles(TX, TY);
-    extern __shared__ double sbuf[];
-    auto cp8 = [](double* dst, const double* src, bool ok) {
-        const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(ok ? 8 : 0) : "memory");
-    };
-    // rows j0-1 .. j0+TY, columns i0-1 .. i0+TX of A
-    auto stage_halo = [&](double* dst, const double* A, const SweepP& P, int i0, int j0) {
-        for (int e = tid; e < H; e += PT) {
-            const int x = i0 - 1 + e % HX, y = j0 - 1 + e / HX;
-            const bool ok = x >= 0 && x < P.px && y >= 0 && y < P.py;
-            cp8(dst + e, ok ? A + (x + (idx_t)P.px * y) : A, ok);
-        }
-    };
-    // the tile's own points of A (one per thread)
-    auto stage_pt = [&](double* dst, const double* A, const SweepP& P, int i0, int j0) {
-        const int x = i0 + tx, y = j0 + ty;
-        const bool ok = x < P.px && y < P.py;
-        cp8(dst + tid, ok ? A + (x + (idx_t)P.px * y) : A, ok);
-    };
-    auto walk_staged = [&](auto&& load, auto&& body) {
-        const int chunk = (T + (int)gridDim.x - 1) / (int)gridDim.x;
-        const int v0 = (int)blockIdx.x * chunk, v1 = min(T, v0 + chunk);
-        if (v0 >= v1) return;
-        int lo = 0, hi = K - 1;  // last k with first_at(k) <= v0
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (first_at(mid) <= v0) lo = mid;
-            else hi = mid - 1;
-        }
-        // cursor of the tile computed (c*) and of the tile staged next (n*)
-        int ck = lo, cf0 = first_at(ck), cf1 = first_at(ck + 1);
-        SweepP cP = sweep_params(inst[id_at(ck)], iter_last);
-        int nk = ck, nf0 = cf0, nf1 = cf1;
-        SweepP nP = cP;
-        load(cP, ((v0 - cf0) % cP.ntx) * TX, ((v0 - cf0) / cP.ntx) * TY, sbuf + (v0 & 1) * SD);
-        asm volatile("cp.async.commit_group;" ::: "memory");
-        for (int v = v0; v < v1; ++v) {
-            if (v >= cf1) {
-                do { ++ck; cf0 = cf1; cf1 = first_at(ck + 1); } while (v >= cf1);
-                cP = sweep_params(inst[id_at(ck)], iter_last);
-            }
-            const int w = v + 1;
-            if (w < v1) {
-                if (w >= nf1) {
-                    do { ++nk; nf0 = nf1; nf1 = first_at(nk + 1); } while (w >= nf1);
-                    nP = sweep_params(inst[id_at(nk)], iter_last);
-                }
-                load(nP, ((w - nf0) % nP.ntx) * TX, ((w - nf0) / nP.ntx) * TY, sbuf + (w & 1) * SD);
-            }
-            asm volatile("cp.async.commit_group;" ::: "memory");
-            asm volatile("cp.async.wait_group 1;" ::: "memory");  // tile v has landed
-            __syncthreads();
-            body(cP, ((v - cf0) % cP.ntx) * TX, ((v - cf0) / cP.ntx) * TY, (const double*)(sbuf + (v & 1) * SD));
-            __syncthreads();  // buffer v&1 is refilled for tile v+2
-        }
-    };
-    // compute_P! + compute_τ!: halos Vx Vy Mus, points Pt τxx τyy τxy
-    auto loadA = [&](const SweepP& P, int i0, int j0, double* S) {
-        const SweepF f = sweep_at(F, P.off);
-        stage_halo(S, f.Vx, P, i0, j0);
-        stage_halo(S + H, f.Vy, P, i0, j0);
-        stage_halo(S + 2 * H, f.Mus, P, i0, j0);
-        stage_pt(S + 3 * H, f.Pt, P, i0, j0);
-        stage_pt(S + 3 * H + PT, f.txx, P, i0, j0);
-        stage_pt(S + 3 * H + 2 * PT, f.tyy, P, i0, j0);
-        stage_pt(S + 3 * H + 3 * PT, f.txy, P, i0, j0);
-    };
-    // compute_dV! + compute_V! + bc: halos τxx τyy τxy Pt ρg, points Vx Vy
-    auto loadB = [&](const SweepP& P, int i0, int j0, double* S) {
-        const SweepF f = sweep_at(F, P.off);
-        stage_halo(S, f.txx, P, i0, j0);
-        stage_halo(S + H, f.tyy, P, i0, j0);
-        stage_halo(S + 2 * H, f.txy, P, i0, j0);
-        stage_halo(S + 3 * H, f.Pt, P, i0, j0);
-        stage_halo(S + 4 * H, f.rhog, P, i0, j0);
-        stage_pt(S + 5 * H, f.Vx, P, i0, j0);
-        stage_pt(S + 5 * H + PT, f.Vy, P, i0, j0);
-    };
-    const int hs = (ty + 1) * HX + (tx + 1);  // this thread's point in a halo box
-#endif
     // L2 prefetches of the lines a point's stencil reads first, at an address clamped into the
     // instance's own padded arrays (always a valid address)
     auto pf = [](const double* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); };
@@ -1429,48 +1333,6 @@ __global__ void __launch_bounds__(TX* TY, PTS_SWEEP_THREADS_PER_SM / (TX * TY)) 
     for (;;) {
         if (*(volatile int*)st.nactive == 0 || iter > iter_last) break;
         const bool chk = ((iter + 1) % nout == 0);
-#if PTS_SWEEP_STAGED
-        walk_staged(loadA, [&](const SweepP& P, int i0, int j0, const double* S) {
-            const int i = i0 + tx, j = j0 + ty;
-            if (iter > P.cap || i >= P.nx || j >= P.ny) return;
-            const double *hVx = S, *hVy = S + H, *hM = S + 2 * H, *pP = S + 3 * H;
-            const bool edge = (i >= 1 && j >= 1);
-            double m11 = 0.0, m01 = 0.0, m10 = 0.0, vxs = 0.0, vys = 0.0, sxy = 0.0;
-            if (edge) {
-                m11 = hM[hs - HX - 1];
-                m01 = hM[hs - HX];
-                m10 = hM[hs - 1];
-                vxs = hVx[hs - HX];
-                vys = hVy[hs - 1];
-                sxy = pP[3 * PT + tid];
-            }
-            const SweepA o = pt_tau_core(P, edge, hVx[hs], hVx[hs + 1], hVy[hs], hVy[hs + HX], pP[tid], hM[hs],
-                                         pP[PT + tid], pP[2 * PT + tid], m11, m01, m10, vxs, vys, sxy);
-            const SweepF f = sweep_at(F, P.off);
-            const idx_t c = i + (idx_t)P.px * j;
-            if (chk) f.divV[c] = o.dv;
-            f.Pt[c] = o.pt;
-            f.txx[c] = o.txx;
-            f.tyy[c] = o.tyy;
-            if (edge) f.txy[c] = o.txy;
-        });
-        grid.sync();
-        walk_staged(loadB, [&](const SweepP& P, int i0, int j0, const double* S) {
-            const int i = i0 + tx, j = j0 + ty, nx = P.nx, ny = P.ny;
-            if (iter > P.cap || i > nx || j > ny) return;
-            const double *hxx = S, *hyy = S + H, *hxy = S + 2 * H, *hP = S + 3 * H, *hR = S + 4 * H;
-            const double* pV = S + 5 * H;
-            const bool fx = (j >= 1 && j <= ny - 2), ux = fx && (i >= 1 && i <= nx - 1);
-            const bool fy = (i >= 1 && i <= nx - 2), uy = fy && (j >= 1 && j <= ny - 1);
-            double vx = 0.0, vy = 0.0, Rx = 0.0, Ry = 0.0;
-            if (fx) vx = pV[tid];
-            if (fy) vy = pV[PT + tid];
-            if (ux) Rx = res_x_core(P, hxx[hs], hxx[hs - 1], hxy[hs + HX], hxy[hs], hP[hs], hP[hs - 1]);
-            if (uy)
-                Ry = res_y_core(P, hyy[hs], hyy[hs - HX], hxy[hs + 1], hxy[hs], hP[hs], hP[hs - HX], hR[hs - HX], hR[hs]);
-            v_bc_apply(sweep_at(F, P.off), P, i, j, i + (idx_t)P.px * j, fx, ux, fy, uy, vx, vy, Rx, Ry);
-        });
-#else
         walk([&](const SweepP& P, int, int, int i, int j) {
             if (iter <= P.cap) pt_tau_sweep(sweep_at(F, P.off), P, i, j, chk);
         }, preA);
@@ -1478,7 +1340,6 @@ __global__ void __launch_bounds__(TX* TY, PTS_SWEEP_THREADS_PER_SM / (TX * TY)) 
         walk([&](const SweepP& P, int, int, int i, int j) {
             if (iter <= P.cap) v_bc_sweep(sweep_at(F, P.off), P, i, j);
         }, preB);
-#endif
         // an instance doing its last allowed iteration leaves the active count here
         for (int b = blockIdx.x * TX * TY + tid; b < ninst; b += gridDim.x * TX * TY) {
             const int64_t cap = inst[b].iter_last < iter_last ? inst[b].iter_last : iter_last;
@@ -1520,11 +1381,7 @@ __global__ void __launch_bounds__(TX* TY, PTS_SWEEP_THREADS_PER_SM / (TX * TY)) 
         }, no_pre);
         grid.sync();
         // per-instance finalisation: one block per instance, fixed-order reduction
-#if PTS_SWEEP_STAGED
-        double (*red)[kCheckSlots] = reinterpret_cast<double (*)[kCheckSlots]>(sbuf);  // the staging buffers are idle here
-#else
         __shared__ double red[TX * TY][kCheckSlots];
-#endif
         for (int b = blockIdx.x; b < ninst; b += gridDim.x) {
             const BInst& I = inst[b];
             const int64_t cap = I.iter_last < iter_last ? I.iter_last : iter_last;
@@ -2018,14 +1875,7 @@ static cudaError_t launch_batch_t(const BInst* d_inst, int ntiles, int ninst, co
                                   int nout, int64_t iter_last, double eps, cudaStream_t s) {
     SweepF F{F64.Pt, F64.Vx, F64.Vy, F64.txx, F64.tyy, F64.txy, F64.Mus, F64.divV, F64.Rx, F64.Ry, F64.rhog};
     int per_sm = 0, dev = 0, nsm = 0;
-    const size_t dyn = PTS_SWEEP_STAGED ? 2 * sizeof(double) * (size_t)sweep_stage_doubles(TX, TY) : 0;
-    cudaError_t e = cudaSuccess;
-    // the opt-in above the default 48 KB of static plus dynamic shared memory per block
-    if (dyn > 0 &&
-        (e = cudaFuncSetAttribute(k2_batch<TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn)) !=
-            cudaSuccess)
-        return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k2_batch<TX, TY>, TX * TY, dyn);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k2_batch<TX, TY>, TX * TY, 0);
     if (e != cudaSuccess) return e;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
@@ -2035,7 +1885,7 @@ static cudaError_t launch_batch_t(const BInst* d_inst, int ntiles, int ninst, co
     if (grid < 1) return cudaErrorInvalidConfiguration;
     void* args[] = {(void*)&d_inst, (void*)&ntiles,    (void*)&ninst, (void*)&F,
                     (void*)&st,     (void*)&nout,      (void*)&iter_last, (void*)&eps};
-    return cudaLaunchCooperativeKernel((const void*)k2_batch<TX, TY>, dim3(grid), dim3(TX, TY), args, dyn, s);
+    return cudaLaunchCooperativeKernel((const void*)k2_batch<TX, TY>, dim3(grid), dim3(TX, TY), args, 0, s);
 }
 
 cudaError_t launch_batch(int tile, const BInst* d_inst, int ntiles, int ninst,
