@@ -1815,8 +1815,12 @@ cudaError_t launch_add_dV(int v, const Geom& g, const Fields64& f, cudaStream_t 
     return cudaGetLastError();
 }
 
+// z-blocks of the 3D check/sources passes (each thread walks nz/PTS_CHECK_GZ planes)
+#ifndef PTS_CHECK_GZ
+#define PTS_CHECK_GZ 32
+#endif
 static dim3 check_grid(int v, const Geom& g) {
-    if (variant_is3d(v)) return dim3((g.nx + 1 + 31) / 32, (g.ny + 7) / 8, g.nz < 32 ? g.nz : 32);
+    if (variant_is3d(v)) return dim3((g.nx + 1 + 31) / 32, (g.ny + 7) / 8, g.nz < PTS_CHECK_GZ ? g.nz : PTS_CHECK_GZ);
     return dim3((g.nx + 1 + 31) / 32, (g.ny + 7) / 8, 1);
 }
 
