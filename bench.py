@@ -606,6 +606,72 @@ def run_batch(args, ws, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_batch_ve(args, ws, rank, local):
+    """The visco-elastic aspect-ratio sweep: Stokes2D_ve_param.jl for every FACT x NSUB of
+    runme_Stokes2D_aspect_ratio.jl at RESOL = `--ve-ny` (5 Maxwell steps each, eps = 1e-6,
+    nout = nx, iterMax = 100nx), all instances in one persistent launch; beside it the same
+    instances as separate contexts (`--ve-contexts` in flight on their own streams). Work =
+    Σ instances cells x PT iterations; iteration totals checked against the published rows of
+    output/out_Stokes2D_ve_aspect_ratio_param.txt (a committed fixture)."""
+    import time
+
+    import torch
+
+    from ptstokes.batch import TILE_SHAPES, BatchVE, aspect_ratio_instances
+    from ptstokes.scripts import aspect_ratio_sweep
+
+    torch.cuda.set_device(local)
+    nsubs = tuple(args.ve_nsub)
+    inst = aspect_ratio_instances(nsubs=nsubs, resols=(args.ve_ny,))
+    b = BatchVE(inst, tile=args.ve_tile)
+    b.setup()
+    st = torch.cuda.ExternalStream(b.stream_handle())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    res = b.solve()
+    e1.record(st)
+    e1.synchronize()
+    sec = e0.elapsed_time(e1) / 1e3
+    cell_it = sum(d["nx"] * d["ny"] * it for d, it in zip(b.instances, res["ittot"]))
+    golden = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden", "reference_output_lines.json")
+    rows = json.load(open(golden))["out_Stokes2D_ve_aspect_ratio_param.txt"]
+    pub = {tuple(r.split()[:4]): int(r.split()[4]) for r in rows}
+    keyed = [tuple(ln.split()[:4]) for ln in res["lines"]]
+    have = [q for q, k in enumerate(keyed) if k in pub]
+    match = [q for q in have if res["ittot"][q] == pub[keyed[q]]]
+    line = {
+        "metric": "batched 2D VE aspect-ratio sweep (Stokes2D_ve_param.jl x FACT x NSUB), one persistent launch: "
+                  "cell-iterations/s",
+        "value": round(cell_it / sec, 1), "unit": "cell-iterations/s", "n_gpus": ws, "higher_is_better": True,
+        "scaling": "weak", "dtype": "f64", "data": "the reference's own sweep problem (no random input)",
+        "config": {"workload": f"{len(inst)} instances: RESOL {args.ve_ny}, NSUB {list(nsubs)}, FACT 1.0..0.1, "
+                               f"5 Maxwell steps each, eps 1e-6", "instances": len(inst),
+                   "total_cells": sum(d["nx"] * d["ny"] for d in b.instances), "tile": TILE_SHAPES[b.tile],
+                   "graph": res["used_graph"]},
+        "seconds": round(sec, 3), "ittot": {"min": min(res["ittot"]), "max": max(res["ittot"])},
+        "converged_last_step": sum(res["converged"]),
+        "published_rows_matched": f"{len(match)} of {len(have)} (iteration totals equal)",
+    }
+    peak, peak_kind = hbm_peak()
+    alg = 24 * 8 * cell_it  # phase A reads 11 arrays and writes 4, phase B reads 7 and writes 2
+    line["roofline"] = {"bound": "hbm", "achieved": round(alg / sec / 1e9, 1), "peak": peak, "unit": "GB/s",
+                        "frac": round(alg / sec / 1e9 / peak, 4), "traffic": None, "kernel": "k2_batch_ve",
+                        "peak_kind": peak_kind, "kernel_ms": round(sec * 1e3, 3), "algorithmic_bytes": alg}
+    b.close()
+    if args.ve_contexts > 0:
+        t0 = time.perf_counter()
+        out = aspect_ratio_sweep(facts=tuple(sorted({d["fact"] for d in inst}, reverse=True)), nsubs=nsubs,
+                                 resols=(args.ve_ny,), in_flight=args.ve_contexts)
+        sec_ctx = time.perf_counter() - t0
+        by_key = {(r["fact"], r["nsub"], r["ny"]): r["ittot"] for r in out}
+        same = all(by_key[(d["fact"], d["nsub"], d["ny"])] == t for d, t in zip(b.instances, res["ittot"]))
+        line["contexts"] = {"seconds": round(sec_ctx, 3), "in_flight": args.ve_contexts,
+                            "same_iteration_totals": same, "speedup_of_one_launch": round(sec_ctx / sec, 2)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_adjoint(args, ws, rank, local):
     """Adjoint gradient of the 3D viscous solve at `--adj-n`³: viscosity = matrix 1 plus 20
     seeded spherical inclusions (radii U[0.3,0.8], log10 μ U[-L,L], L = `--log10-range`),
@@ -946,6 +1012,13 @@ def main():
     ap.add_argument("--ttt-nt", type=int, default=5, help="physical steps of the time-to-tolerance comparison")
     ap.add_argument("--batch", action="store_true", help="run the batched 2D sweep instead")
     ap.add_argument("--batch-n", type=int, default=256)
+    ap.add_argument("--batch-ve", action="store_true",
+                    help="run the batched visco-elastic aspect-ratio sweep (Stokes2D_ve_param.jl) instead")
+    ap.add_argument("--ve-ny", type=int, default=127, help="RESOL of the aspect-ratio sweep")
+    ap.add_argument("--ve-nsub", type=int, nargs="*", default=[1, 2, 4], help="NSUB values of the aspect-ratio sweep")
+    ap.add_argument("--ve-tile", type=int, default=1, help="tile shape of the aspect-ratio sweep (0..3)")
+    ap.add_argument("--ve-contexts", type=int, default=4,
+                    help="contexts in flight for the per-instance comparison run (0: skip)")
     ap.add_argument("--adjoint", action="store_true", help="run the adjoint-gradient configuration instead")
     ap.add_argument("--adj-n", type=int, default=255)
     ap.add_argument("--adj-ve-steps", type=int, default=5, help="visco-elastic adjoint steps (0: skip)")
@@ -973,6 +1046,8 @@ def main():
             run_reference(args, ws, rank, pg)
         elif args.batch:
             run_batch(args, ws, rank, local)
+        elif args.batch_ve:
+            run_batch_ve(args, ws, rank, local)
         elif args.adjoint:
             run_adjoint(args, ws, rank, local)
         elif args.inclusions:

@@ -353,6 +353,37 @@ PTS_API int pts_batch_solve(pts_batch* b, int64_t iter_limit, int64_t* iters, do
 PTS_API int pts_batch_get_field(pts_batch* b, int32_t instance, int32_t field, double* host, int64_t n);
 PTS_API int pts_batch_stream(pts_batch* b, void** stream);
 
+/* ---- batched 2D visco-elastic aspect-ratio sweep: all instances in one persistent launch ----
+ * Replaces scripts/runme_Stokes2D_aspect_ratio.jl:1-24, which runs one Julia process of
+ * scripts/Stokes2D_ve_param.jl per (FACT, NSUB, RESOL). Each instance is that script:
+ * ly = ly, lx = nsub*ly, nx = nsub*(ny+1)-1, ny = RESOL (:99-107), matrix viscosity 1 and
+ * nsub inclusions of radius 1 and viscosity musi (:133-141), G = dt = 1, pure shear 1,
+ * 10 smooth! sweeps, local-max iteration parameters with min_lxy = fact*min(lx,ly)
+ * (:110, :142-150), and nt physical steps, each `assign_τ!; while err > ε && iter <= iterMax`
+ * with a check every nout iterations, norm_Rx scaled by lx and norm_Ry, norm_∇V by ly
+ * (:152-186). The descriptor gives eps, r, Re, CFL and the tile shape; nout <= 0 gives
+ * each instance the script's nout = nx, iter_max <= 0 its iterMax = 100nx. The rest of the
+ * batch API applies: pts_batch_setup builds the ICs of every instance, pts_batch_solve runs
+ * every instance's nt steps (iters receives each instance's ittot, converged is 1 when its
+ * last step reached eps; an instance whose check gives NaN is frozen, as the script stops
+ * there, and the call returns PTS_E_NAN), pts_batch_get_field reads Pt Vx Vy τxx τyy τxy
+ * τxx_o τyy_o τxy_o Mus Musτ Gdτ dτ_Rho ∇V Rx Ry. */
+typedef struct pts_batch_ve_instance {
+    int32_t ny;      /* RESOL: cells in y (>= 3) */
+    int32_t nsub;    /* NSUB: subdomains along x, one inclusion each (>= 1) */
+    int32_t nt;      /* physical steps (1..64; the script: 5) */
+    int32_t reserved;
+    double fact;     /* FACT: min_lxy = fact*min(lx,ly) */
+    double ly;       /* box height (the script: 10) */
+    double musi;     /* inclusion viscosity (the script: 1e-3) */
+} pts_batch_ve_instance;
+PTS_API int pts_batch_create_ve(const pts_batch_desc* desc, const pts_batch_ve_instance* inst, int32_t n,
+                                pts_batch** out);
+/* PT iterations of each finished step of one instance (Stokes2D_ve_param.jl:186, the iter
+ * added to ittot): up to max_steps values into iters, the number of finished steps into
+ * nsteps. Visco-elastic sweeps only. */
+PTS_API int pts_batch_steps(pts_batch* b, int32_t instance, int64_t* iters, int32_t max_steps, int32_t* nsteps);
+
 /* ---- convergence check without any allocation ----
  * This entry point has no counterpart in the reference. It is for callers that cannot
  * allocate device memory: programs whose device memory all belongs to another allocator

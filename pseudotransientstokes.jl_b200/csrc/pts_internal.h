@@ -202,6 +202,10 @@ struct BInst {
     double lenRx, lenRy, lenDiv, ly;
     double Gd, dR;     // the instance's uniform Gdτ and dτ_Rho (Musτ .= μs0)
     int64_t iter_last; // its PT loop runs while iter <= iter_last (iterMax)
+    // visco-elastic sweep only: the norm_Rx scale lx, the instance's check cadence and its
+    // number of physical steps
+    double lx;
+    int nout, nt;
 };
 struct BState {
     int* converged;   // per instance: 1 its PT loop has ended on the tolerance, 2 frozen on NaN
@@ -212,6 +216,18 @@ struct BState {
     int* act;         // active list rebuilt at each check: K, T, first tile[K+1], instance[K] (2n+3 ints)
     int* nan_flag;
 };
+// Per-instance state of the batched visco-elastic sweep (k2_batch_ve). The instance's
+// status lives in BState::converged: 0 iterating, 1 finished with its last step converged,
+// 2 frozen on NaN, 3 finished with its last step stopped by iterMax. BState::iters holds
+// its total PT iterations (ittot).
+constexpr int kBatchMaxSteps = 64;
+struct BStateVE {
+    int64_t* start;       // global iteration count at which the current step began
+    int* steps;           // physical steps finished
+    int64_t* step_iters;  // PT iterations of each finished step, kBatchMaxSteps per instance
+    int* assign;          // 1: a step has just ended and the next begins (τ_o ← τ pending)
+    int64_t* next_event;  // [0]: next global iteration count at which an instance checks or ends a step
+};
 constexpr int kBatchTileShapes = 4;
 inline void batch_tile_dims(int tile, int* tx, int* ty) {
     static const int d[kBatchTileShapes][2] = {{32, 4}, {32, 8}, {64, 4}, {32, 16}};
@@ -220,6 +236,12 @@ inline void batch_tile_dims(int tile, int* tx, int* ty) {
 }
 cudaError_t launch_batch(int tile, const BInst* d_inst, int ntiles, int ninst,
                          const Fields64& F, const BState& st, int nout, int64_t iter_last, double eps, cudaStream_t s);
+cudaError_t launch_batch_ve(int tile, const BInst* d_inst, int ntiles, int ninst, const Fields64& F,
+                            const BState& st, const BStateVE& sv, int64_t iter_cap, double eps, cudaStream_t s);
+// Mus of one instance of the visco-elastic aspect-ratio sweep: musi in nsub circles of
+// radius 1 centred at ((isub-1)*ly + ly/2, ly/2), mus0 elsewhere
+cudaError_t launch_init_ve_param(const Geom& g, const Fields64& f, const Num& n, int nsub, double mus0, double musi,
+                                 cudaStream_t s);
 // ICs of one sweep instance: Mus/ρg = inclusion (radius2) ? (musi, rhogi) : (1, 0), pure shear ebg
 cudaError_t launch_init_sweep(const Geom& g, const Fields64& f, const Num& n, double musi, double radius2,
                               double rhogi, double ebg, cudaStream_t s);

@@ -12,6 +12,7 @@
 #include <cooperative_groups.h>
 
 #include <cfloat>
+#include <climits>
 #include <cmath>
 #include <cstdlib>
 
@@ -1049,10 +1050,16 @@ __device__ __forceinline__ SweepF sweep_at(const SweepF& F, int64_t off) {
 
 // What a tile of the sweep needs of its instance, loaded into registers when a block's walk
 // enters the instance.
+// The subexpressions that depend on the instance only (1/Gdτ, @av(Gdτ), 1/@av(Gdτ),
+// @av_xi(dτ_Rho)) are formed here once, with the reference's operations, so every point
+// uses the same bits it would compute itself.
 struct SweepP {
     int nx, ny, px, py, ntx, tile0;
     int64_t off, cap;
-    double dx, dy, r, G, R;  // G = Gdτ, R = dτ_Rho (uniform per instance)
+    double dx, dy, r, G;  // G = Gdτ (uniform per instance)
+    double invG;          // 1.0/Gdτ
+    double ag, invag;     // @av(Gdτ) = (((G+G)+G)+G)*0.25 and 1.0/@av(Gdτ)
+    double aR;            // @av_xi(dτ_Rho) = @av_yi(dτ_Rho) = (R+R)*0.5, R = dτ_Rho
 };
 
 __device__ __forceinline__ SweepP sweep_params(const BInst& I, int64_t iter_last) {
@@ -1060,7 +1067,11 @@ __device__ __forceinline__ SweepP sweep_params(const BInst& I, int64_t iter_last
     P.nx = I.g.nx; P.ny = I.g.ny; P.px = I.g.px; P.py = I.g.py; P.ntx = I.ntx; P.tile0 = I.tile0;
     P.off = I.off;
     P.cap = I.iter_last < iter_last ? I.iter_last : iter_last;
-    P.dx = I.n.dx; P.dy = I.n.dy; P.r = I.n.r; P.G = I.Gd; P.R = I.dR;
+    P.dx = I.n.dx; P.dy = I.n.dy; P.r = I.n.r; P.G = I.Gd;
+    P.invG = 1.0 / P.G;
+    P.ag = (((P.G + P.G) + P.G) + P.G) * 0.25;
+    P.invag = 1.0 / P.ag;
+    P.aR = (I.dR + I.dR) * 0.5;
     return P;
 }
 
@@ -1081,18 +1092,18 @@ __device__ __forceinline__ SweepA pt_tau_core(const SweepP& P, bool edge, double
     const double G = P.G;
     const double dvx = vx1 - vx0, dvy = vy1 - vy0;
     o.dv = dvx / P.dx + dvy / P.dy;
-    const double mu = 1.0 / (1.0 / G + 1.0 / Mc);  // @μ_veτ
+    // x/2.0 is written x*0.5: both are the correctly rounded x/2, the same bits for every x
+    const double mu = 1.0 / (P.invG + 1.0 / Mc);  // @μ_veτ
     o.pt = pt - P.r * G * o.dv;
-    o.txx = 2.0 * mu * (dvx / P.dx + sxx / G / 2.0);
-    o.tyy = 2.0 * mu * (dvy / P.dy + syy / G / 2.0);
+    o.txx = 2.0 * mu * (dvx / P.dx + (sxx / G) * 0.5);
+    o.tyy = 2.0 * mu * (dvy / P.dy + (syy / G) * 0.5);
     o.txy = 0.0;
     if (edge) {
-        const double ag = (((G + G) + G) + G) * 0.25;
         const double am = (((m11 + m01) + m10) + Mc) * 0.25;
-        const double mua = 1.0 / (1.0 / ag + 1.0 / am);  // @μ_veτ_av
-        const double d1 = vx0 - vxs;                       // @d_yi(Vx)
-        const double d2 = vy0 - vys;                       // @d_xi(Vy)
-        o.txy = 2.0 * mua * (0.5 * (d1 / P.dy + d2 / P.dx) + sxy / ag / 2.0);
+        const double mua = 1.0 / (P.invag + 1.0 / am);  // @μ_veτ_av
+        const double d1 = vx0 - vxs;                      // @d_yi(Vx)
+        const double d2 = vy0 - vys;                      // @d_xi(Vy)
+        o.txy = 2.0 * mua * (0.5 * (d1 / P.dy + d2 / P.dx) + (sxy / P.ag) * 0.5);
     }
     return o;
 }
@@ -1146,7 +1157,7 @@ __device__ __forceinline__ double res_sweep_y(const SweepF& f, const SweepP& P, 
 __device__ __forceinline__ void v_bc_apply(const SweepF& f, const SweepP& P, int i, int j, idx_t c, bool fx, bool ux,
                                            bool fy, bool uy, double vx, double vy, double Rx, double Ry) {
     const idx_t sx = 1, sy = P.px;
-    const double aR = (P.R + P.R) * 0.5;
+    const double aR = P.aR;
     if (fx) {
         if (ux) {
             vx = vx + Rx * aR;
@@ -1292,18 +1303,33 @@ __global__ void __launch_bounds__(TX* TY, PTS_SWEEP_THREADS_PER_SM / (TX * TY)) 
         }
         int k = lo, b = id_at(k), f0 = first_at(k), f1 = first_at(k + 1);
         SweepP P = sweep_params(inst[b], iter_last);
+        // tile coordinates (qx, qy) of q = v - f0, advanced by one tile per step: integer
+        // divisions only where the walk enters an instance or a prefetch wraps a tile row
+        int qx = (v0 - f0) % P.ntx, qy = (v0 - f0) / P.ntx;
         for (int v = v0; v < v1; ++v) {
             if (v >= f1) {
                 do { ++k; f0 = f1; f1 = first_at(k + 1); } while (v >= f1);
                 b = id_at(k);
                 P = sweep_params(inst[b], iter_last);
+                qx = (v - f0) % P.ntx;
+                qy = (v - f0) / P.ntx;
             }
             const int q = v - f0;
 #pragma unroll
             for (int d = 1; d <= PTS_SWEEP_PREFETCH; ++d)
-                if (v + d < v1 && v + d < f1 && (d == PTS_SWEEP_PREFETCH || v == v0))
-                    pre(P, ((q + d) % P.ntx) * TX + tx, ((q + d) / P.ntx) * TY + ty);
-            body(P, b, P.tile0 + q, (q % P.ntx) * TX + tx, (q / P.ntx) * TY + ty);
+                if (v + d < v1 && v + d < f1 && (d == PTS_SWEEP_PREFETCH || v == v0)) {
+                    int nx_ = qx + d, ny_ = qy;
+                    if (nx_ >= P.ntx) {
+                        nx_ = (q + d) % P.ntx;
+                        ny_ = (q + d) / P.ntx;
+                    }
+                    pre(P, nx_ * TX + tx, ny_ * TY + ty);
+                }
+            body(P, b, P.tile0 + q, qx * TX + tx, qy * TY + ty);
+            if (++qx == P.ntx) {
+                qx = 0;
+                ++qy;
+            }
         }
     };
     // L2 prefetches of the lines a point's stencil reads first, at an address clamped into the
@@ -1430,6 +1456,316 @@ __global__ void __launch_bounds__(TX* TY, PTS_SWEEP_THREADS_PER_SM / (TX * TY)) 
     for (int b = blockIdx.x * TX * TY + tid; b < ninst; b += gridDim.x * TX * TY) {
         const int64_t cap = inst[b].iter_last < iter_last ? inst[b].iter_last : iter_last;
         if (!st.converged[b]) st.iters[b] = iter < cap + 1 ? iter : cap + 1;
+    }
+}
+
+// ------------------------------------------------------------------ batched 2D visco-elastic sweep
+//
+// scripts/Stokes2D_ve_param.jl (the aspect-ratio study) for many instances at once, as its
+// driver scripts/runme_Stokes2D_aspect_ratio.jl sweeps FACT x NSUB x RESOL with one Julia
+// process per instance. Each instance keeps the script's own numerics: the role kernels
+// compute_P!, compute_τ!, compute_dV! + compute_V! + bc (the per-point functions of the 2D
+// visco-elastic contexts, pt_tau_2d<VE2D> and v_bc_2d<VE2D>, so every instance computes
+// the bits a context would), local-max iteration parameters, a check every nout of its own
+// iterations with norm_Rx scaled by lx and norm_Ry, norm_∇V by ly (:170-177), and nt
+// physical steps, each starting with assign_τ! and ending when err <= ε or after iterMax
+// (:152-186).
+
+// Mus of an instance (:133-141): μs0, and μsi where
+//   ((ix-1)*dx + 0.5*dx - 0.5*ly - (isub-1)*ly)^2 + ((iy-1)*dy + 0.5*dy - 0.5*ly)^2 < 1
+// for some isub in 1..nsub, in the script's operation order.
+__global__ void k2_init_ve_param(Geom g, Fields64 f, Num n, int nsub, double mus0, double musi) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= g.nx || j >= g.ny) return;
+    const double Y = ((double)j * n.dy + 0.5 * n.dy) - 0.5 * n.ly;
+    double mu = mus0;
+    for (int s = 1; s <= nsub; ++s) {
+        const double X = (((double)i * n.dx + 0.5 * n.dx) - 0.5 * n.ly) - (double)(s - 1) * n.ly;
+        if (X * X + Y * Y < 1.0) mu = musi;
+    }
+    f.Mus[gidx32(g, i, j, 0)] = mu;
+}
+
+// The fields of one instance: every arena advanced to the instance's first element.
+__device__ __forceinline__ Fields64 ve_at(const Fields64& F, int64_t off) {
+    Fields64 f = F;
+    f.Pt = F.Pt + off; f.Vx = F.Vx + off; f.Vy = F.Vy + off;
+    f.txx = F.txx + off; f.tyy = F.tyy + off; f.txy = F.txy + off;
+    f.txx_o = F.txx_o + off; f.tyy_o = F.tyy_o + off; f.txy_o = F.txy_o + off;
+    f.Mus = F.Mus + off; f.Gdt = F.Gdt + off; f.dtRho = F.dtRho + off;
+    f.divV = F.divV + off; f.Rx = F.Rx + off; f.Ry = F.Ry + off;
+    return f;
+}
+
+// Block 0: the list of instances still iterating (as build_active_list) and the next global
+// iteration count at which one of them checks (a multiple of its nout within its step) or
+// ends its step (iterMax + 1 iterations); clears the pending assign_τ! flags.
+__device__ void build_list_ve(const BInst* __restrict__ inst, int ninst, const BState& st, const BStateVE& sv,
+                              int64_t iter, int* s_cnt, long long* s_min) {
+    const int nt = blockDim.x * blockDim.y, tid = threadIdx.x + blockDim.x * threadIdx.y;
+    const int per = (ninst + nt - 1) / nt, b0 = tid * per, b1 = min(ninst, b0 + per);
+    int k = 0, t = 0;
+    long long ev = LLONG_MAX;
+    for (int b = b0; b < b1; ++b) {
+        sv.assign[b] = 0;
+        if (*(volatile const int*)&st.converged[b] != 0) continue;
+        ++k;
+        t += inst[b].ntx * inst[b].nty;
+        const int64_t s0 = *(volatile const int64_t*)&sv.start[b], it = iter - s0, nout = inst[b].nout;
+        const int64_t nc = s0 + (it / nout + 1) * nout, ne = s0 + inst[b].iter_last + 1;
+        ev = min(ev, (long long)(nc < ne ? nc : ne));
+    }
+    s_cnt[2 * tid] = k;
+    s_cnt[2 * tid + 1] = t;
+    for (int o = 16; o > 0; o >>= 1) ev = min(ev, __shfl_down_sync(kFull, ev, o));
+    if ((tid & 31) == 0) s_min[tid >> 5] = ev;
+    __syncthreads();
+    if (tid == 0) {
+        int K = 0, T = 0;
+        for (int u = 0; u < nt; ++u) {
+            const int dk = s_cnt[2 * u], dt = s_cnt[2 * u + 1];
+            s_cnt[2 * u] = K;
+            s_cnt[2 * u + 1] = T;
+            K += dk;
+            T += dt;
+        }
+        st.act[0] = K;
+        st.act[1] = T;
+        st.act[2 + K] = T;
+        long long m = LLONG_MAX;
+        for (int w = 0; w < (nt + 31) / 32; ++w) m = min(m, s_min[w]);
+        *(volatile long long*)sv.next_event = m;
+    }
+    __syncthreads();
+    k = s_cnt[2 * tid];
+    t = s_cnt[2 * tid + 1];
+    for (int b = b0; b < b1; ++b)
+        if (*(volatile const int*)&st.converged[b] == 0) {
+            st.act[2 + k] = t;
+            st.act[3 + ninst + k] = b;
+            ++k;
+            t += inst[b].ntx * inst[b].nty;
+        }
+    __syncthreads();
+}
+
+// All instances in one cooperative launch, in lockstep on a global iteration count. Per PT
+// iteration: compute_P! + compute_τ!, grid barrier, compute_dV! + compute_V! + bc, grid
+// barrier. At an event (some instance has done a multiple of its nout iterations in its
+// current step, or iterMax + 1 of them): the check of those instances from per-tile
+// partials, per-instance step bookkeeping, assign_τ! (τ_o ← τ) for the instances that begin
+// a new step, a rebuilt list of the instances still iterating and the next event. ∇V is
+// stored on event iterations only: the check is its only reader, and an instance's last
+// iteration is always an event.
+template <int TX, int TY>
+__global__ void __launch_bounds__(TX* TY, PTS_SWEEP_THREADS_PER_SM / (TX * TY))
+    k2_batch_ve(const BInst* __restrict__ inst, int ninst, Fields64 F, BState st, BStateVE sv, int64_t iter_cap,
+                double eps) {
+    cooperative_groups::grid_group grid = cooperative_groups::this_grid();
+    constexpr int NT = TX * TY;
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + TX * ty;
+    __shared__ int s_first[kListSmem + 1];
+    __shared__ int s_id[kListSmem];
+    __shared__ int s_cnt[2 * NT];
+    __shared__ int s_KT[2];
+    __shared__ long long s_min[NT / 32];
+    __shared__ double red[NT][kCheckSlots];
+    const int* g_first = st.act + 2;
+    const int* g_id = st.act + 3 + ninst;
+    int K = 0, T = 0;
+    bool in_smem = false;
+    auto load_list = [&]() {
+        if (tid == 0) {
+            s_KT[0] = *(volatile int*)&st.act[0];
+            s_KT[1] = *(volatile int*)&st.act[1];
+        }
+        __syncthreads();
+        K = s_KT[0];
+        T = s_KT[1];
+        in_smem = K <= kListSmem;
+        if (in_smem) {
+            for (int u = tid; u <= K; u += NT) s_first[u] = ((volatile const int*)g_first)[u];
+            for (int u = tid; u < K; u += NT) s_id[u] = ((volatile const int*)g_id)[u];
+        }
+        __syncthreads();
+    };
+    auto first_at = [&](int k) { return in_smem ? s_first[k] : ((volatile const int*)g_first)[k]; };
+    auto id_at = [&](int k) { return in_smem ? s_id[k] : ((volatile const int*)g_id)[k]; };
+    // enter(b) when the walk enters instance b, then body(b, t, i, j) for every point of this
+    // block's chunk of the active tiles (t: the tile's index in the flattened tile list)
+    auto walk = [&](auto&& enter, auto&& body) {
+        const int chunk = (T + (int)gridDim.x - 1) / (int)gridDim.x;
+        const int v0 = (int)blockIdx.x * chunk, v1 = min(T, v0 + chunk);
+        if (v0 >= v1) return;
+        int lo = 0, hi = K - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (first_at(mid) <= v0) lo = mid;
+            else hi = mid - 1;
+        }
+        int k = lo, b = id_at(k), f0 = first_at(k), f1 = first_at(k + 1);
+        int ntx = inst[b].ntx, tile0 = inst[b].tile0;
+        int qx = (v0 - f0) % ntx, qy = (v0 - f0) / ntx;
+        enter(b);
+        for (int v = v0; v < v1; ++v) {
+            if (v >= f1) {
+                do { ++k; f0 = f1; f1 = first_at(k + 1); } while (v >= f1);
+                b = id_at(k);
+                ntx = inst[b].ntx;
+                tile0 = inst[b].tile0;
+                qx = (v - f0) % ntx;
+                qy = (v - f0) / ntx;
+                enter(b);
+            }
+            body(b, tile0 + (v - f0), qx * TX + tx, qy * TY + ty);
+            if (++qx == ntx) {
+                qx = 0;
+                ++qy;
+            }
+        }
+    };
+    // what the stencils need of the instance the walk is in
+    Geom gI{};
+    Num nI{};
+    int64_t offI = 0;
+    bool chkI = false, asgI = false;  // the instance checks at this event / begins a new step
+    int64_t iter = 0;                 // PT iterations done, counted globally
+    auto enter = [&](int b) {
+        const BInst& I = inst[b];
+        gI = I.g;
+        nI.dx = I.n.dx; nI.dy = I.n.dy; nI._dx = I.n._dx; nI._dy = I.n._dy;
+        nI.r = I.n.r; nI.gdt = I.n.gdt;
+        offI = I.off;
+        chkI = ((iter - *(volatile const int64_t*)&sv.start[b]) % I.nout) == 0;
+        asgI = *(volatile const int*)&sv.assign[b] != 0;
+    };
+
+    if (blockIdx.x == 0) {
+        for (int b = tid; b < ninst; b += NT) st.err[b] = 2.0 * eps;  // err = 2ε of every step
+        __syncthreads();
+        build_list_ve(inst, ninst, st, sv, 0, s_cnt, s_min);
+    }
+    grid.sync();
+    load_list();
+    for (;;) {
+        if (*(volatile int*)st.nactive == 0 || iter >= iter_cap) break;
+        const int64_t ev = *(volatile long long*)sv.next_event;
+        const int sdv = (iter + 1 == ev) ? 1 : 0;
+        walk(enter, [&](int, int, int i, int j) {
+            pt_tau_2d<VE2D>(gI, ve_at(F, offI), nI, i, j, ROLE_P | ROLE_TAU, sdv);
+        });
+        grid.sync();
+        walk(enter, [&](int, int, int i, int j) { v_bc_2d<VE2D>(gI, ve_at(F, offI), nI, i, j, 1); });
+        grid.sync();
+        ++iter;
+        if (iter != ev) continue;
+        // per-tile partials of the check (compute_Res! + the reductions of :170-177) of the
+        // instances with a multiple of nout iterations in their current step
+        walk(enter, [&](int, int t, int i, int j) {
+            if (!chkI) return;  // uniform over the block (one tile)
+            const int nx = gI.nx, ny = gI.ny;
+            const Fields64 f = ve_at(F, offI);
+            Acc a;
+            acc_init(a);
+            if (i <= nx && j < ny) {
+                const idx_t sy = gI.px, c = i + sy * j;
+                const double vx = f.Vx[c];
+                a.vmin = vx;
+                a.vmax = vx;
+                if (i < nx) {
+                    a.pmin = a.pmax = f.Pt[c];
+                    const double dv = f.divV[c];
+                    a.s[3] = dv * dv;
+                }
+                if (i >= 1 && i <= nx - 1 && j >= 1 && j <= ny - 2) {
+                    const double R = res2_x<false>(f, nI, c, 1, sy);
+                    f.Rx[c] = R;
+                    a.s[0] = R * R;
+                }
+                if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 1) {
+                    const double R = res2_y<false>(f, nI, c, 1, sy);
+                    f.Ry[c] = R;
+                    a.s[1] = R * R;
+                }
+            }
+            acc_block_store_to(a, st.partials + (int64_t)t * kCheckSlots);
+        });
+        grid.sync();
+        // per instance (one block each): norms, then the step's end (err <= ε, or iterMax + 1
+        // iterations done) with the next step's start or the instance's end
+        for (int b = blockIdx.x; b < ninst; b += gridDim.x) {
+            if (st.converged[b] != 0) continue;
+            const BInst& I = inst[b];
+            const int64_t it = iter - sv.start[b];
+            const bool chk = (it % I.nout) == 0, endmax = it == I.iter_last + 1;
+            if (!chk && !endmax) continue;
+            if (chk) {
+                const int nt = I.ntx * I.nty;
+                double r[kCheckSlots] = {0.0, 0.0, 0.0, 0.0, DBL_MAX, -DBL_MAX, DBL_MAX, -DBL_MAX};
+                for (int u = tid; u < nt; u += NT) {
+                    const double* p = st.partials + (int64_t)(I.tile0 + u) * kCheckSlots;
+                    for (int w = 0; w < 4; ++w) r[w] += p[w];
+                    r[4] = fmin(r[4], p[4]); r[5] = fmax(r[5], p[5]);
+                    r[6] = fmin(r[6], p[6]); r[7] = fmax(r[7], p[7]);
+                }
+                for (int w = 0; w < kCheckSlots; ++w) red[tid][w] = r[w];
+                __syncthreads();
+                for (int s = NT / 2; s > 0; s >>= 1) {
+                    if (tid < s) {
+                        for (int w = 0; w < 4; ++w) red[tid][w] += red[tid + s][w];
+                        red[tid][4] = fmin(red[tid][4], red[tid + s][4]); red[tid][5] = fmax(red[tid][5], red[tid + s][5]);
+                        red[tid][6] = fmin(red[tid][6], red[tid + s][6]); red[tid][7] = fmax(red[tid][7], red[tid + s][7]);
+                    }
+                    __syncthreads();
+                }
+            }
+            if (tid == 0) {
+                double err = st.err[b];
+                if (chk) {
+                    const double dP = red[0][7] - red[0][6], dV = red[0][5] - red[0][4];
+                    const double nRx = sqrt(red[0][0]) / dP * I.lx / sqrt(I.lenRx);
+                    const double nRy = sqrt(red[0][1]) / dP * I.ly / sqrt(I.lenRy);
+                    const double nDv = sqrt(red[0][3]) / dV * I.ly / sqrt(I.lenDiv);
+                    const bool bad = isnan(nRx) || isnan(nRy) || isnan(nDv);
+                    err = bad ? NAN : fmax(fmax(nRx, nRy), fmax(0.0, nDv));
+                    st.err[b] = err;
+                }
+                if (isnan(err)) {  // the script stops with error("NaN"): this instance freezes
+                    st.converged[b] = 2;
+                    atomicExch(st.nan_flag, 1);
+                    atomicSub(st.nactive, 1);
+                } else if (endmax || !(err > eps)) {
+                    const int s = sv.steps[b];
+                    if (s < kBatchMaxSteps) sv.step_iters[(int64_t)b * kBatchMaxSteps + s] = it;
+                    st.iters[b] += it;  // ittot += iter
+                    sv.steps[b] = s + 1;
+                    if (s + 1 >= I.nt) {
+                        st.converged[b] = !(err > eps) ? 1 : 3;
+                        atomicSub(st.nactive, 1);
+                    } else {  // next step: err = 2ε; iter = 0; assign_τ!
+                        st.err[b] = 2.0 * eps;
+                        sv.start[b] = iter;
+                        sv.assign[b] = 1;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        grid.sync();
+        // assign_τ! (τ_o ← τ) of the instances that begin a new step
+        walk(enter, [&](int, int, int i, int j) {
+            if (!asgI || i > gI.nx || j > gI.ny) return;
+            const Fields64 f = ve_at(F, offI);
+            const idx_t c = i + (idx_t)gI.px * j;
+            f.txx_o[c] = f.txx[c];
+            f.tyy_o[c] = f.tyy[c];
+            f.txy_o[c] = f.txy[c];
+        });
+        grid.sync();
+        if (blockIdx.x == 0) build_list_ve(inst, ninst, st, sv, iter, s_cnt, s_min);
+        grid.sync();
+        load_list();
     }
 }
 
@@ -1901,6 +2237,40 @@ cudaError_t launch_batch(int tile, const BInst* d_inst, int ntiles, int ninst,
         case 3: return launch_batch_t<32, 16>(d_inst, ntiles, ninst, F, st, nout, iter_last, eps, s);
         default: return cudaErrorInvalidValue;
     }
+}
+
+template <int TX, int TY>
+static cudaError_t launch_batch_ve_t(const BInst* d_inst, int ntiles, int ninst, const Fields64& F, BState st,
+                                     BStateVE sv, int64_t iter_cap, double eps, cudaStream_t s) {
+    int per_sm = 0, dev = 0, nsm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k2_batch_ve<TX, TY>, TX * TY, 0);
+    if (e != cudaSuccess) return e;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    int grid = per_sm * nsm;  // every block co-resident, as grid.sync() requires
+    const int want = ntiles > ninst ? ntiles : ninst;
+    if (grid > want) grid = want;
+    if (grid < 1) return cudaErrorInvalidConfiguration;
+    Fields64 Fv = F;
+    void* args[] = {(void*)&d_inst, (void*)&ninst, (void*)&Fv, (void*)&st, (void*)&sv, (void*)&iter_cap, (void*)&eps};
+    return cudaLaunchCooperativeKernel((const void*)k2_batch_ve<TX, TY>, dim3(grid), dim3(TX, TY), args, 0, s);
+}
+
+cudaError_t launch_batch_ve(int tile, const BInst* d_inst, int ntiles, int ninst, const Fields64& F,
+                            const BState& st, const BStateVE& sv, int64_t iter_cap, double eps, cudaStream_t s) {
+    switch (tile) {
+        case 0: return launch_batch_ve_t<32, 4>(d_inst, ntiles, ninst, F, st, sv, iter_cap, eps, s);
+        case 1: return launch_batch_ve_t<32, 8>(d_inst, ntiles, ninst, F, st, sv, iter_cap, eps, s);
+        case 2: return launch_batch_ve_t<64, 4>(d_inst, ntiles, ninst, F, st, sv, iter_cap, eps, s);
+        case 3: return launch_batch_ve_t<32, 16>(d_inst, ntiles, ninst, F, st, sv, iter_cap, eps, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_init_ve_param(const Geom& g, const Fields64& f, const Num& n, int nsub, double mus0, double musi,
+                                 cudaStream_t s) {
+    k2_init_ve_param<<<grid_cells(g), blk(), 0, s>>>(g, f, n, nsub, mus0, musi);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_fold(const Geom& g, const Fields64& f, const Mixed32& m, cudaStream_t s) {

@@ -193,6 +193,42 @@ function solve!(b::Batch; iter_limit=-1)
     return iters, err, conv .== 1
 end
 
+# ---- the visco-elastic aspect-ratio sweep in one launch (pts_batch_create_ve) ----
+# runme_Stokes2D_aspect_ratio.jl starts one Julia process of Stokes2D_ve_param.jl per
+# (FACT, NSUB, RESOL); here every instance runs its nt Maxwell steps in one persistent launch.
+
+struct BatchVEInstance
+    ny::Int32; nsub::Int32; nt::Int32; reserved::Int32
+    fact::Float64; ly::Float64; μsi::Float64
+end
+BatchVEInstance(ny, nsub, fact; nt=5, ly=10.0, μsi=1e-3) = BatchVEInstance(ny, nsub, nt, 0, fact, ly, μsi)
+
+"""
+    BatchVE(instances; ε=1e-6, tile=1, r=1.0, Re=5π, CFL=0.87/sqrt(2), nout=0, iterMax=0.0)
+
+The aspect-ratio sweep; `nout <= 0` and `iterMax <= 0` give each instance the script's
+nout = nx and iterMax = 100nx. `setup!` and `solve!` as for `Batch` (solve! returns each
+instance's ittot); `steps(b, q)` the iterations of each Maxwell step of instance q.
+"""
+function BatchVE(inst::Vector{BatchVEInstance}; ε=1e-6, tile=1, r=1.0, Re=5π, CFL=0.87/sqrt(2), nout=0, iterMax=0.0)
+    d = BatchDesc(nout, tile, ε, iterMax, r, Re, CFL, ntuple(_ -> Int32(0), 4))
+    out = Ref{Ptr{Cvoid}}(C_NULL)
+    rc = ccall((:pts_batch_create_ve, libpts), Cint, (Ref{BatchDesc}, Ptr{BatchVEInstance}, Int32, Ref{Ptr{Cvoid}}),
+               d, inst, length(inst), out)
+    rc == 0 || error("pts_batch_create_ve: ", unsafe_string(ccall((:pts_last_error, libpts), Cstring, (Ptr{Cvoid},), C_NULL)))
+    b = Batch(out[], length(inst))
+    finalizer(x -> ccall((:pts_batch_destroy, libpts), Cint, (Ptr{Cvoid},), x.ptr), b)
+    return b
+end
+
+"Iterations of each finished Maxwell step of instance q (1-based)."
+function steps(b::Batch, q::Integer)
+    buf = zeros(Int64, 64); k = Ref{Int32}(0)
+    batch_check(b, ccall((:pts_batch_steps, libpts), Cint, (Ptr{Cvoid}, Int32, Ptr{Int64}, Int32, Ref{Int32}),
+                         b.ptr, q - 1, buf, 64, k))
+    return buf[1:min(k[], 64)]
+end
+
 # ---- adjoint of the 3D viscous solve (pts_apply_operator, pts_gradient_logmu) ----
 
 "One application of the operator (or of its transpose on an adjoint context)."

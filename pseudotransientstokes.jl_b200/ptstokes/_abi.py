@@ -82,6 +82,12 @@ class PtsBatchInstance(ctypes.Structure):
                 ("ebg", ctypes.c_double)]
 
 
+class PtsBatchVEInstance(ctypes.Structure):
+    _fields_ = [("ny", ctypes.c_int32), ("nsub", ctypes.c_int32), ("nt", ctypes.c_int32),
+                ("reserved", ctypes.c_int32), ("fact", ctypes.c_double), ("ly", ctypes.c_double),
+                ("musi", ctypes.c_double)]
+
+
 class PtsBatchDesc(ctypes.Structure):
     _fields_ = [("nout", ctypes.c_int32), ("tile", ctypes.c_int32), ("eps", ctypes.c_double),
                 ("iter_max", ctypes.c_double), ("r", ctypes.c_double), ("Re", ctypes.c_double),
@@ -164,6 +170,10 @@ SIGNATURES = {
                          ctypes.POINTER(_I32)], ctypes.c_int),
     "pts_batch_get_field": ([_P, _I32, _I32, _DP, _I64], ctypes.c_int),
     "pts_batch_stream": ([_P, ctypes.POINTER(_P)], ctypes.c_int),
+    # batched 2D visco-elastic aspect-ratio sweep
+    "pts_batch_create_ve": ([ctypes.POINTER(PtsBatchDesc), ctypes.POINTER(PtsBatchVEInstance), _I32,
+                             ctypes.POINTER(_P)], ctypes.c_int),
+    "pts_batch_steps": ([_P, _I32, ctypes.POINTER(_I64), _I32, ctypes.POINTER(_I32)], ctypes.c_int),
 }
 
 _lib = None

@@ -16,7 +16,7 @@ import time
 import numpy as np
 
 from . import _abi
-from ._abi import FIELD_ID, PtsBatchDesc, PtsBatchInstance
+from ._abi import FIELD_ID, PtsBatchDesc, PtsBatchInstance, PtsBatchVEInstance
 
 TILE_SHAPES = [(32, 4), (32, 8), (64, 4), (32, 16)]
 
@@ -115,6 +115,78 @@ class Batch:
         out = np.empty(self.shape(q, name), dtype=np.float64, order="F")
         self._ck(self.lib.pts_batch_get_field(self.h, q, FIELD_ID[name], out.ctypes.data, out.size))
         return out
+
+
+ASPECT_RATIO_FACTS = (1.0, 0.9, 0.8, 0.7, 0.6, 0.5, 0.4, 0.3, 0.2, 0.1)
+
+
+def aspect_ratio_instances(facts=ASPECT_RATIO_FACTS, nsubs=(1, 2, 4, 8), resols=(127, 255, 511, 1023, 2047), nt=5,
+                           ly=10.0, musi=1e-3):
+    """The instances of scripts/runme_Stokes2D_aspect_ratio.jl: FACT x NSUB x RESOL in its
+    loop order (Iterators.product: FACT fastest, RESOL slowest), each one run of
+    Stokes2D_ve_param.jl."""
+    return [dict(ny=ny, nsub=nsub, fact=fact, nt=nt, ly=ly, musi=musi)
+            for ny in resols for nsub in nsubs for fact in facts]
+
+
+class BatchVE(Batch):
+    """The visco-elastic aspect-ratio sweep (scripts/Stokes2D_ve_param.jl per instance) in
+    one persistent launch (``pts_batch_create_ve``): every instance's nt Maxwell steps,
+    with its own check cadence nout = nx and iterMax = 100nx unless `nout` / `iter_max` are
+    positive, tolerance eps = 1e-6, CFL 0.87/sqrt(2) (:103-109)."""
+
+    def __init__(self, instances, tile=1, eps=1e-6, CFL=0.87 / math.sqrt(2), Re=5 * math.pi, r=1.0, nout=0,
+                 iter_max=0, lib=None):
+        self.lib = lib or _abi.load()
+        self.instances = []
+        for d in instances:
+            d = dict(d)
+            d.setdefault("nt", 5)
+            d.setdefault("ly", 10.0)
+            d.setdefault("musi", 1e-3)
+            d["nx"] = d["nsub"] * (d["ny"] + 1) - 1
+            self.instances.append(d)
+        n = len(self.instances)
+        arr = (PtsBatchVEInstance * n)()
+        for q, d in enumerate(self.instances):
+            arr[q] = PtsBatchVEInstance(d["ny"], d["nsub"], d["nt"], 0, d["fact"], d["ly"], d["musi"])
+        desc = PtsBatchDesc()
+        desc.nout, desc.tile, desc.eps, desc.iter_max = int(nout), tile, eps, float(iter_max)
+        desc.r, desc.Re, desc.CFL = r, Re, CFL
+        self.desc = desc
+        h = ctypes.c_void_p()
+        rc = self.lib.pts_batch_create_ve(ctypes.byref(desc), arr, n, ctypes.byref(h))
+        if rc != 0:
+            raise _abi.PtsError(rc, (self.lib.pts_last_error(None) or b"").decode())
+        self.h = h
+        self.n = n
+        self.tile = tile
+
+    def steps(self, q):
+        """PT iterations of each finished Maxwell step of instance q."""
+        buf = (ctypes.c_int64 * 64)()
+        k = ctypes.c_int32()
+        self._ck(self.lib.pts_batch_steps(self.h, q, buf, 64, ctypes.byref(k)))
+        return list(buf[: min(k.value, 64)])
+
+    def solve(self, iter_limit=-1, raise_on_nan=True):
+        """Run every instance's steps. Result: ittot, err (of each instance's last check),
+        converged (its last step reached eps), steps (iterations per step), and the script's
+        output line ``nx ny nsub fact ittot nt err`` per instance."""
+        from .output import jl
+
+        res = super().solve(iter_limit=iter_limit, raise_on_nan=raise_on_nan)
+        res["ittot"] = res.pop("iters")
+        res["steps"] = [self.steps(q) for q in range(self.n)]
+        res["lines"] = [f"{d['nx']} {d['ny']} {d['nsub']} {jl(d['fact'])} {t} {d['nt']} {jl(e)}"
+                        for d, t, e in zip(self.instances, res["ittot"], res["err"])]
+        return res
+
+    def shape(self, q, name):
+        if name == "txy_o":
+            nx, ny = self.instances[q]["nx"], self.instances[q]["ny"]
+            return (nx - 1, ny - 1)
+        return super().shape(q, name)
 
 
 def _cache_path():
