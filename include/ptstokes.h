@@ -213,6 +213,15 @@ PTS_API int pts_set_decomposition(pts_ctx* ctx, int32_t zoff, int32_t nz_global)
  * device buffer of extent(1)*extent(2) doubles; synchronous. */
 PTS_API int pts_get_plane_device(pts_ctx* ctx, int32_t id, int32_t k, double* dev, int64_t n);
 PTS_API int pts_set_plane_device(pts_ctx* ctx, int32_t id, int32_t k, const double* dev, int64_t n);
+/* compute_V! + bc (pts_compute_V_bc) on the face planes k in [k0, k1) only (0 <= k0 <= k1 <=
+ * nz+1), enqueued on `stream` (NULL: the context's stream); asynchronous. The boundary and
+ * inner regions of @hide_communication b_width (Stokes3D_ve_multixpu.jl:136,230-239): after
+ * pts_compute_Pt_tau, the planes next to the slab ends are updated first so their halo
+ * exchange overlaps the inner planes' update on another stream. A face update reads V only
+ * at its own point and writes bc copies only next to the first and last interior planes, so
+ * disjoint ranges may run concurrently. FP64 3D_VE, 3D_VE_PERF, 3D_V contexts without
+ * momentum sources or adjoint mode. */
+PTS_API int pts_compute_V_bc_planes(pts_ctx* ctx, int32_t k0, int32_t k1, void* stream);
 /* The local pieces of the check, to be reduced over ranks (norm_g, minimum_g, maximum_g,
  * :243-248): {Σ Rx², Σ Ry², Σ Rz², Σ ∇V², min Vx, max Vx, min Pt, max Pt}; synchronous. */
 PTS_API int pts_check_partials(pts_ctx* ctx, double out[8]);

@@ -901,6 +901,18 @@ int pts_set_decomposition(pts_ctx* c, int32_t zoff, int32_t nz_global) {
     return PTS_OK;
 }
 
+int pts_compute_V_bc_planes(pts_ctx* c, int32_t k0, int32_t k1, void* stream) {
+    int rc = enter(c);
+    if (rc) return rc;
+    if (!c->d3 || variant_damped(c->v) || c->mixed || c->f.Fx || c->n.adjoint)
+        return fail(c, PTS_E_STATE,
+                    "pts_compute_V_bc_planes needs an FP64 3D_VE, 3D_VE_PERF or 3D_V context without sources or adjoint mode");
+    if (k0 < 0 || k1 > c->g.nz + 1 || k0 > k1)
+        return fail(c, PTS_E_INVAL, "face planes [k0, k1) must lie in [0, nz+1]");
+    CK(launch_V_bc_planes(c->v, c->g, c->f, c->n, k0, k1, stream ? (cudaStream_t)stream : c->stream));
+    return PTS_OK;
+}
+
 // One z-plane k of a 3D field (the reference's extents) to or from a dense device buffer.
 int plane_copy(pts_ctx* c, int32_t id, int32_t k, double* dev, int64_t n, bool to_field) {
     int rc = enter(c);

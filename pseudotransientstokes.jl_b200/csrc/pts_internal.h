@@ -102,6 +102,9 @@ cudaError_t launch_Pt_tau(int variant, const Geom& g, const Fields64& f, const N
                           cudaStream_t s);
 cudaError_t launch_V_bc(int variant, const Geom& g, const Fields64& f, const Num& n, bool apply_update,
                         cudaStream_t s);
+// compute_V! + bc on the face planes [k0, k1) only (3D_VE, 3D_VE_PERF, 3D_V; no sources, not adjoint)
+cudaError_t launch_V_bc_planes(int variant, const Geom& g, const Fields64& f, const Num& n, int k0, int k1,
+                               cudaStream_t s);
 cudaError_t launch_dV(int variant, const Geom& g, const Fields64& f, const Num& n, cudaStream_t s);
 cudaError_t launch_add_dV(int variant, const Geom& g, const Fields64& f, cudaStream_t s);
 cudaError_t launch_check(int variant, const Geom& g, const Fields64& f, const Num& n, double* partials,

@@ -179,10 +179,8 @@ __device__ __forceinline__ void bc_copies(double* A, idx_t c, double v, int a, i
 // (adjoint mode, explicit-index form only) the residual is the folded one and the ghosts
 // are not written (they stay zero).
 template <bool PERF, bool SRC = false, bool ADJ = false>
-__global__ void __launch_bounds__(256) k3_V_bc(Geom g, Fields64 f, Num n, int update) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int k = blockIdx.z;
+__device__ __forceinline__ void v_bc3_point(const Geom& g, const Fields64& f, const Num& n, int i, int j, int k,
+                                            int update) {
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     if (i > nx || j > ny) return;
     const idx_t c = gidx32(g, i, j, k);
@@ -220,6 +218,22 @@ __global__ void __launch_bounds__(256) k3_V_bc(Geom g, Fields64 f, Num n, int up
         }
         if (!ADJ) bc_copies(f.Vz, c, v, i, 1, nx - 2, sx, j, 1, ny - 2, sy);
     }
+}
+
+template <bool PERF, bool SRC = false, bool ADJ = false>
+__global__ void __launch_bounds__(256) k3_V_bc(Geom g, Fields64 f, Num n, int update) {
+    v_bc3_point<PERF, SRC, ADJ>(g, f, n, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y * blockDim.y + threadIdx.y,
+                                blockIdx.z, update);
+}
+
+// The same update on the face planes k0 .. k0 + gridDim.z - 1 only: the boundary and inner
+// regions of @hide_communication (Stokes3D_ve_multixpu.jl:230-239). A face update reads V
+// only at its own point and writes bc copies only next to the domain's first and last
+// interior planes, so disjoint plane ranges may run concurrently, in any order.
+template <bool PERF>
+__global__ void __launch_bounds__(256) k3_V_bc_planes(Geom g, Fields64 f, Num n, int k0) {
+    v_bc3_point<PERF>(g, f, n, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y * blockDim.y + threadIdx.y,
+                      k0 + (int)blockIdx.z, 1);
 }
 
 // compute_dV! alone (Stokes3D_ve_multixpu.jl:79-84): dV = R*@av_xi(dτ_Rho) at interior faces
@@ -2119,6 +2133,21 @@ cudaError_t launch_V_bc(int v, const Geom& g, const Fields64& f, const Num& n, b
         case VE2D_PERF: k2_V_bc<VE2D_PERF><<<grid_faces(g, false), blk(), 0, s>>>(g, f, n, u); break;
         case V2D_DAMP:
         case VE2D_DAMP: k2d_V_bc<<<grid_faces(g, false), blk(), 0, s>>>(g, f, n, u); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_V_bc_planes(int v, const Geom& g, const Fields64& f, const Num& n, int k0, int k1,
+                               cudaStream_t s) {
+    if (k0 < 0 || k1 > g.nz + 1 || k0 > k1) return cudaErrorInvalidValue;
+    if (k1 == k0) return cudaSuccess;
+    dim3 gr = grid_faces(g, true);
+    gr.z = (unsigned)(k1 - k0);
+    switch (v) {
+        case VE3D: k3_V_bc_planes<false><<<gr, blk(), 0, s>>>(g, f, n, k0); break;
+        case VE3D_PERF:
+        case V3D: k3_V_bc_planes<true><<<gr, blk(), 0, s>>>(g, f, n, k0); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

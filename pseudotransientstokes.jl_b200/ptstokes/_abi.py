@@ -158,6 +158,7 @@ SIGNATURES = {
     "pts_gradient_logmu": ([_P, _P], ctypes.c_int),
     "pts_gradient_logmu_add": ([_P, _P], ctypes.c_int),
     # residual check on caller-owned device arrays; allocates nothing
+    "pts_compute_V_bc_planes": ([_P, _I32, _I32, _P], ctypes.c_int),
     "pts_check_noalloc": ([ctypes.POINTER(PtsDesc), ctypes.POINTER(_P), _P, _P], ctypes.c_int),
     # batched 2D sweep
     "pts_batch_create": ([ctypes.POINTER(PtsBatchDesc), ctypes.POINTER(PtsBatchInstance), _I32, ctypes.POINTER(_P)],

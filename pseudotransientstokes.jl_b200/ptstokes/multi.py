@@ -21,6 +21,7 @@ are the first ol planes of rank r+1, and with a halo of one plane: rank r's last
 rank r+1's plane ol-1, and rank r+1's first plane takes rank r's plane n-ol (0-based, n the
 field's local z-extent).
 """
+import ctypes
 import math
 
 import numpy as np
@@ -129,6 +130,42 @@ def global_check(partials, slabs, nx, ny, lx, dist, group=None, device="cpu"):
     return err, norms
 
 
+B_WIDTH_Z = 4  # the z component of b_width = (8, 4, 4) (Stokes3D_ve_multixpu.jl:136)
+
+
+def _overlap_begin(s, side, bz):
+    """One PT iteration of context `s` as @hide_communication b_width (Stokes3D_ve_multixpu.jl:
+    230-239): compute_P! + compute_τ!, then compute_V! + bc on the bz face planes at each end of
+    the slab on the context's stream and on the inner planes on the stream `side` (after
+    compute_τ!). The halo planes that update_halo! reads and writes lie in the end regions, so
+    the exchange can start once the context's stream is done while the inner planes are still
+    being updated. Returns (context stream, event of the inner update) for _overlap_end."""
+    import torch
+
+    cs = torch.cuda.ExternalStream(s.stream_handle())
+    s.compute_Pt_tau()
+    nf = s.nz + 1  # face planes of Vz, the z-extent of the update
+    lib, ctx = s.lib, s.ctx
+    if nf > 2 * bz:
+        ready = torch.cuda.Event()
+        ready.record(cs)
+        side.wait_event(ready)
+        s._ck(lib.pts_compute_V_bc_planes(ctx, bz, nf - bz, ctypes.c_void_p(side.cuda_stream)))
+        s._ck(lib.pts_compute_V_bc_planes(ctx, 0, bz, None))
+        s._ck(lib.pts_compute_V_bc_planes(ctx, nf - bz, nf, None))
+        done = torch.cuda.Event()
+        done.record(side)
+        return cs, done
+    s._ck(lib.pts_compute_V_bc_planes(ctx, 0, nf, None))
+    return cs, None
+
+
+def _overlap_end(cs, done):
+    """The context's stream waits for the inner planes' update before its next work."""
+    if done is not None:
+        cs.wait_event(done)
+
+
 class _DevicePlanes:
     """get_plane/set_plane of a GPU context's fields through dense device buffers."""
 
@@ -163,8 +200,12 @@ class SlabSolver:
     initial conditions use the global z coordinate, with halo exchanges and a reduced check.
     ``dist`` is torch.distributed with an initialised process group (NCCL for GPUs)."""
 
-    def __init__(self, variant, nx, ny, nz_global, dist, group=None, lib=None, **kw):
+    def __init__(self, variant, nx, ny, nz_global, dist, group=None, lib=None, overlap=False, b_width=B_WIDTH_Z,
+                 **kw):
+        """With `overlap`, each iteration hides its halo exchange behind the update of the inner
+        planes, as @hide_communication b_width does (b_width: face planes at each slab end)."""
         self.dist, self.group = dist, group
+        self.overlap, self.b_width = overlap, int(b_width)
         size = dist.get_world_size(group) if dist is not None else 1
         rank = dist.get_rank(group) if dist is not None else 0
         self.slabs = Slabs(nz_global, size, rank)
@@ -173,6 +214,10 @@ class SlabSolver:
         self.s._ck(self.s.lib.pts_set_decomposition(self.s.ctx, self.slabs.zoff, nz_global))
         self.planes = _DevicePlanes(self.s)
         self.lx = self.s.p["lx"]
+        if overlap:
+            import torch
+
+            self.side = torch.cuda.Stream()
 
     def close(self):
         self.s.close()
@@ -197,7 +242,13 @@ class SlabSolver:
         self.s.assign_tau()
 
     def iteration(self):
-        """compute_P!, compute_τ!, compute_dV!, compute_V! + bc, then update_halo!(Vx, Vy, Vz)."""
+        """compute_P!, compute_τ!, compute_dV!, compute_V! + bc, then update_halo!(Vx, Vy, Vz);
+        with overlap, the exchange runs while the inner planes are updated."""
+        if self.overlap:
+            cs, done = _overlap_begin(self.s, self.side, self.b_width)
+            self.halo("Vx", "Vy", "Vz")
+            _overlap_end(cs, done)
+            return
         self.s.iterate(1)
         self.halo("Vx", "Vy", "Vz")
 
@@ -243,9 +294,12 @@ class SlabGroup:
     (``exchange_local``) and the check reduced on the host. The same numerics as P ranks of
     ``SlabSolver``; for several GPUs in one process, or to run a decomposition on one GPU."""
 
-    def __init__(self, variant, nx, ny, nz_global, nslabs, devices=None, lib=None, **kw):
+    def __init__(self, variant, nx, ny, nz_global, nslabs, devices=None, lib=None, overlap=False, b_width=B_WIDTH_Z,
+                 **kw):
         import torch
 
+        self.overlap, self.b_width = overlap, int(b_width)
+        self.sides = []
         self.slabs = [Slabs(nz_global, nslabs, r) for r in range(nslabs)]
         self.nx, self.ny = nx, ny
         self.solvers, self.planes = [], []
@@ -256,6 +310,8 @@ class SlabGroup:
             s._ck(s.lib.pts_set_decomposition(s.ctx, sl.zoff, nz_global))
             self.solvers.append(s)
             self.planes.append(_DevicePlanes(s))
+            if overlap:
+                self.sides.append(torch.cuda.Stream())
         self.lx = self.solvers[0].p["lx"]
 
     def close(self):
@@ -286,6 +342,12 @@ class SlabGroup:
             s.assign_tau()
 
     def iteration(self):
+        if self.overlap:
+            pend = [_overlap_begin(s, side, self.b_width) for s, side in zip(self.solvers, self.sides)]
+            self.halo("Vx", "Vy", "Vz")
+            for cs, done in pend:
+                _overlap_end(cs, done)
+            return
         for s in self.solvers:
             s.iterate(1)
         self.halo("Vx", "Vy", "Vz")
