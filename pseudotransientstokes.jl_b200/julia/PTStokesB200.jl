@@ -273,6 +273,18 @@ set_plane_device!(ctx::Ctx, f::Symbol, k::Integer, devptr::UInt, n::Integer) =
     check(ctx, ccall((:pts_set_plane_device, libpts), Cint, (Ptr{Cvoid}, Int32, Int32, UInt, Int64),
                      ctx.ptr, field_id(f), k, devptr, n))
 
+"""
+    compute_V_bc_planes!(ctx, k0, k1, stream=C_NULL)
+
+compute_V! + bc on the face planes [k0, k1) only, on `stream` (a CuStream's handle; C_NULL: the
+context's stream). `@hide_communication b_width` is: the end regions [0, b) and [nz+1-b, nz+1)
+on the context's stream, the inner region on another stream, then update_halo! of the
+end planes while the inner region runs.
+"""
+compute_V_bc_planes!(ctx::Ctx, k0::Integer, k1::Integer, stream::Ptr{Cvoid}=C_NULL) =
+    check(ctx, ccall((:pts_compute_V_bc_planes, libpts), Cint, (Ptr{Cvoid}, Int32, Int32, Ptr{Cvoid}),
+                     ctx.ptr, k0, k1, stream))
+
 "{Σ Rx², Σ Ry², Σ Rz², Σ ∇V², min Vx, max Vx, min Pt, max Pt} of this slab, for MPI.Allreduce."
 function check_partials(ctx::Ctx)
     out = zeros(Float64, 8)
