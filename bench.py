@@ -617,14 +617,15 @@ def run_batch_ve(args, ws, rank, local):
 
     import torch
 
-    from ptstokes.batch import TILE_SHAPES, BatchVE, aspect_ratio_instances
+    from ptstokes.batch import TILE_SHAPES, BatchVE, aspect_ratio_instances, autotune
     from ptstokes.scripts import aspect_ratio_sweep
 
     torch.cuda.set_device(local)
     nsubs = tuple(args.ve_nsub)
     inst = aspect_ratio_instances(nsubs=nsubs, resols=(args.ve_ny,))
-    b = BatchVE(inst, tile=args.ve_tile)
+    b = BatchVE(inst, tile=max(args.ve_tile, 0))
     b.setup()
+    tune = autotune(b) if args.ve_tile < 0 else {}
     st = torch.cuda.ExternalStream(b.stream_handle())
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -648,7 +649,7 @@ def run_batch_ve(args, ws, rank, local):
         "config": {"workload": f"{len(inst)} instances: RESOL {args.ve_ny}, NSUB {list(nsubs)}, FACT 1.0..0.1, "
                                f"5 Maxwell steps each, eps 1e-6", "instances": len(inst),
                    "total_cells": sum(d["nx"] * d["ny"] for d in b.instances), "tile": TILE_SHAPES[b.tile],
-                   "graph": res["used_graph"]},
+                   "autotune_ms": tune.get("ms"), "graph": res["used_graph"]},
         "seconds": round(sec, 3), "ittot": {"min": min(res["ittot"]), "max": max(res["ittot"])},
         "converged_last_step": sum(res["converged"]),
         "published_rows_matched": f"{len(match)} of {len(have)} (iteration totals equal)",
@@ -1016,7 +1017,8 @@ def main():
                     help="run the batched visco-elastic aspect-ratio sweep (Stokes2D_ve_param.jl) instead")
     ap.add_argument("--ve-ny", type=int, default=127, help="RESOL of the aspect-ratio sweep")
     ap.add_argument("--ve-nsub", type=int, nargs="*", default=[1, 2, 4], help="NSUB values of the aspect-ratio sweep")
-    ap.add_argument("--ve-tile", type=int, default=1, help="tile shape of the aspect-ratio sweep (0..3)")
+    ap.add_argument("--ve-tile", type=int, default=-1,
+                    help="tile shape of the aspect-ratio sweep (0..3; -1: the autotuner's choice)")
     ap.add_argument("--ve-contexts", type=int, default=4,
                     help="contexts in flight for the per-instance comparison run (0: skip)")
     ap.add_argument("--adjoint", action="store_true", help="run the adjoint-gradient configuration instead")

@@ -197,12 +197,14 @@ def _cache_path():
 def _batch_key(batch):
     cells = sum(d["nx"] * d["ny"] for d in batch.instances)
     classes = sorted({d["nx"] for d in batch.instances})
-    return f"2d|fp64|n={batch.n}|cells~{2 ** int(math.log2(max(cells, 1)))}|nx={','.join(map(str, classes))}"
+    form = "ve" if isinstance(batch, BatchVE) else "v"
+    return (f"2d|{form}|fp64|n={batch.n}|cells~{2 ** int(math.log2(max(cells, 1)))}|"
+            f"nx={','.join(map(str, classes))}")
 
 
 def autotune(batch, iters=None, use_cache=True):
-    """Time each tile shape on `batch` for a short run (from its set-up state) and keep the
-    fastest; the choice is cached per (dimension, precision, batch size class)."""
+    """Time each tile shape on `batch` (a Batch or a BatchVE) for a short run from its set-up
+    state and keep the fastest; the choice is cached per (form, precision, batch size class)."""
     import torch
 
     key = _batch_key(batch)
@@ -216,7 +218,9 @@ def autotune(batch, iters=None, use_cache=True):
     if use_cache and key in cache:
         batch.set_tile(cache[key]["tile"])
         return cache[key]
-    iters = iters or 2 * batch.desc.nout - 1
+    if not iters:  # two checks of the instances (a visco-elastic sweep checks every nx iterations)
+        nout = batch.desc.nout if batch.desc.nout > 0 else min(d["nx"] for d in batch.instances)
+        iters = 2 * nout - 1
     stream = torch.cuda.ExternalStream(batch.stream_handle())
     timings = {}
     for t in range(len(TILE_SHAPES)):

@@ -99,3 +99,24 @@ def test_batch_ve_published_totals_in_one_launch(gpu_lib):
         assert got[:6] == [nx, ny, nsub, fact, ittot, nt], (got, ittot)
         assert abs(float(got[6]) - float(err)) <= 1e-9 * float(err)
     b.close()
+
+
+def test_autotune_picks_a_tile_for_the_ve_sweep(gpu_lib, tmp_path, monkeypatch):
+    """The autotuner times the four tile shapes on a visco-elastic batch (two checks of its
+    smallest instance), caches the choice under a key of its own, and the sweep run on the
+    chosen tile still equals the oracle."""
+    from ptstokes.batch import TILE_SHAPES, BatchVE, _batch_key, autotune
+    from oracle import scripts as S
+
+    monkeypatch.setenv("XDG_CACHE_HOME", str(tmp_path))
+    b = BatchVE(CASES[:2], lib=gpu_lib)
+    b.setup()
+    entry = autotune(b)
+    assert entry["iters"] == 2 * 31 - 1 and len(entry["ms"]) == len(TILE_SHAPES)
+    assert b.tile == entry["tile"] and _batch_key(b).startswith("2d|ve|")
+    assert autotune(b)["tile"] == entry["tile"]  # from the cache
+    res = b.solve()
+    for q, d in enumerate(CASES[:2]):
+        o = S.VE2DParam(d["ny"], nsub=d["nsub"], fact=d["fact"]).setup().run()
+        _compare(b, res, q, o)
+    b.close()
