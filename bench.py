@@ -1006,10 +1006,13 @@ def main():
     ap.add_argument("--stencil-tile", type=int, default=0, help="tile configuration of the TMA-staged compute_Pt_τ!")
     ap.add_argument("--stencil-vtile", type=int, default=0, help="tile configuration of the TMA-staged compute_V!")
     ap.add_argument("--stencil-kz", type=int, default=0, help="z-planes (2D: rows) per block of the TMA-staged kernels")
-    ap.add_argument("--ttt-n", type=int, default=511, help="grid of the time-to-tolerance comparison (0: skip)")
-    ap.add_argument("--ttt-n2", type=int, default=255, help="a second, smaller time-to-tolerance grid (0: skip)")
-    ap.add_argument("--incl-default-n", type=int, default=255,
-                    help="grid of the 20-inclusion mixed-vs-FP64 block of the default line (0: skip)")
+    ap.add_argument("--ttt-n", type=int, default=None,
+                    help="grid of the time-to-tolerance comparison (0: skip; default 511 on one GPU, skipped on more)")
+    ap.add_argument("--ttt-n2", type=int, default=None,
+                    help="a second, smaller time-to-tolerance grid (0: skip; default 255 on one GPU, skipped on more)")
+    ap.add_argument("--incl-default-n", type=int, default=None,
+                    help="grid of the 20-inclusion mixed-vs-FP64 block of the default line "
+                         "(0: skip; default 255 on one GPU, skipped on more)")
     ap.add_argument("--ttt-nt", type=int, default=5, help="physical steps of the time-to-tolerance comparison")
     ap.add_argument("--batch", action="store_true", help="run the batched 2D sweep instead")
     ap.add_argument("--batch-n", type=int, default=256)
@@ -1043,6 +1046,14 @@ def main():
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     ws, rank, local, pg = dist_setup()
+    # the time-to-tolerance and 20-inclusion blocks take minutes per replica: they belong to
+    # the one-GPU line; a replica run measures the throughput alone unless asked for them
+    if args.ttt_n is None:
+        args.ttt_n = 511 if ws == 1 else 0
+    if args.ttt_n2 is None:
+        args.ttt_n2 = 255 if ws == 1 else 0
+    if args.incl_default_n is None:
+        args.incl_default_n = 255 if ws == 1 else 0
     try:
         if args.impl == "reference":
             run_reference(args, ws, rank, pg)

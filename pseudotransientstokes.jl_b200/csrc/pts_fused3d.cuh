@@ -90,7 +90,7 @@ struct Cfg {
     static constexpr size_t smem_bytes = kBar + kStage + kSV;
 };
 
-// ---- bulk-copy / mbarrier primitives (sm_90+; no cluster multicast) ----
+// ---- bulk-copy / mbarrier primitives (sm_90+; each copy lands in the issuing CTA alone) ----
 __device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(saddr(b)), "r"(count) : "memory");

@@ -29,7 +29,8 @@
 //
 // Waits are bounded (2 s of %globaltimer): a wait that gives up sets the context's error
 // flag, the producer still waits (bounded) for every copy it issued, and the kernel ends.
-// No copy uses cluster multicast; every tensor map covers this GPU's own fields.
+// Every copy lands in the issuing CTA's shared memory alone; every tensor map covers this
+// GPU's own fields.
 #include <cstring>
 
 #include "pts_expr64.cuh"
