@@ -986,6 +986,19 @@ def field_errors(got, ref):
     return out
 
 
+def resolve_block_defaults(args, ws):
+    """The time-to-tolerance (511^3, 255^3) and 20-inclusion (255^3) blocks take minutes per
+    replica: they belong to the one-GPU line, and a replica run (ws > 1) measures the
+    throughput alone unless a grid is given for them."""
+    if args.ttt_n is None:
+        args.ttt_n = 511 if ws == 1 else 0
+    if args.ttt_n2 is None:
+        args.ttt_n2 = 255 if ws == 1 else 0
+    if args.incl_default_n is None:
+        args.incl_default_n = 255 if ws == 1 else 0
+    return args
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1046,14 +1059,7 @@ def main():
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     ws, rank, local, pg = dist_setup()
-    # the time-to-tolerance and 20-inclusion blocks take minutes per replica: they belong to
-    # the one-GPU line; a replica run measures the throughput alone unless asked for them
-    if args.ttt_n is None:
-        args.ttt_n = 511 if ws == 1 else 0
-    if args.ttt_n2 is None:
-        args.ttt_n2 = 255 if ws == 1 else 0
-    if args.incl_default_n is None:
-        args.incl_default_n = 255 if ws == 1 else 0
+    resolve_block_defaults(args, ws)
     try:
         if args.impl == "reference":
             run_reference(args, ws, rank, pg)

@@ -62,3 +62,24 @@ def test_reference_arm_under_torchrun_prints_once():
     assert len(lines) == 1
     line = json.loads(lines[0])
     assert line["impl"] == "reference" and line["n_gpus"] == 2 and line["value"] > 0
+
+
+def test_replica_runs_skip_the_time_to_tolerance_blocks():
+    """The minutes-long time-to-tolerance and 20-inclusion blocks run on the one-GPU line;
+    under torchrun with several ranks they are skipped unless a grid is asked for."""
+    import argparse
+
+    sys.path.insert(0, ROOT)
+    import bench
+
+    def ns(**kw):
+        base = dict(ttt_n=None, ttt_n2=None, incl_default_n=None)
+        base.update(kw)
+        return argparse.Namespace(**base)
+
+    one = bench.resolve_block_defaults(ns(), 1)
+    assert (one.ttt_n, one.ttt_n2, one.incl_default_n) == (511, 255, 255)
+    many = bench.resolve_block_defaults(ns(), 4)
+    assert (many.ttt_n, many.ttt_n2, many.incl_default_n) == (0, 0, 0)
+    asked = bench.resolve_block_defaults(ns(ttt_n=255, ttt_n2=0), 2)
+    assert (asked.ttt_n, asked.ttt_n2, asked.incl_default_n) == (255, 0, 0)
