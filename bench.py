@@ -194,6 +194,22 @@ def small_2d_case():
     return out
 
 
+DATA_3D = "synthetic (the reference's own inclusion problem: spherical inclusion r=1 mu=1e-3, pure shear, G=1, dt=1)"
+
+
+def workload_config(n, precision):
+    """The `config` of the default line: the workload alone, the same for both arms (the
+    reference arm times bounded samples of it; its cpu_baseline.sample says how many PT
+    iterations a step holds)."""
+    px = (n + 1 + 15) // 16 * 16  # the padded x-extent of every field (128-byte rows)
+    field_gb = px * (n + 1) * (n + 1) * 8 / 1e9
+    return {"workload": f"3D VE Stokes (Stokes3D_ve_perf.jl kernels), {precision.upper()}, {n}^3, box 10^3, "
+                        "spherical inclusion r=1 mu=1e-3",
+            "nx": n, "ny": n, "nz": n,
+            "l2": f"inputs larger than L2 ({field_gb:.2f} GB per field)" if field_gb > 0.126 else
+                  f"inputs of {field_gb:.3f} GB per field: not larger than L2"}
+
+
 def run_reference(args, ws, rank, pg):
     if rank != 0:
         return
@@ -208,9 +224,8 @@ def run_reference(args, ws, rank, pg):
     line = {
         "impl": "reference", "metric": METRIC, "value": round(val, 3), "unit": "GB/s", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (the reference's own inclusion problem)",
-        "config": {"workload": "3D VE Stokes (Stokes3D_ve_perf.jl), FP64, 511^3 box 10^3, inclusion r=1 mu=1e-3",
-                   "cpu_grid": n},
+        "vs_baseline": None, "dtype": "f64", "data": DATA_3D,
+        "config": workload_config(args.n, "fp64"),
         "cpu_baseline": {"value": round(val, 3), "unit": "GB/s", "cores": thr, "kind": "port",
                          "sample": sample},
         "e2e": {"value": round(val, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -445,14 +460,12 @@ def run_ours(args, ws, rank, local, pg):
             "warmup": args.warmup, "ms_per_step": round(t_ms / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if args.precision == "fp64" else "f32 sweeps, f64 correction",
-            "data": "synthetic (the reference's own inclusion problem: spherical inclusion r=1 mu=1e-3, pure shear, "
-            "G=1, dt=1)",
-            "config": {"workload": f"3D VE Stokes (Stokes3D_ve_perf.jl kernels), {args.precision.upper()}, {n}^3, "
-                                   "box 10^3",
-                       "nx": n, "ny": n, "nz": n, "iters_per_step": nout, "t_it_ms": round(t_it * 1e3, 4),
-                       "path": "CUDA graph per check block (2 kernels per PT iteration" +
-                               (", a CUDA event-record node after each)" if per_kernel else ")"),
-                       "parallelism": f"replicas x{ws}", "l2": "inputs larger than L2 (1.07 GB per field)"},
+            "data": DATA_3D,
+            "config": workload_config(n, args.precision),
+            "run": {"iters_per_step": nout, "t_it_ms": round(t_it * 1e3, 4),
+                    "path": "CUDA graph per check block (2 kernels per PT iteration" +
+                            (", a CUDA event-record node after each)" if per_kernel else ")"),
+                    "parallelism": f"replicas x{ws}"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
                          "kernel": ("k3_corrA_zs" if mixed else "k3_Pt_tau_zs") if args.stencil == 0 else
