@@ -34,11 +34,64 @@ def _flag(name):
     return os.environ.get(name, "false").strip().lower() in ("true", "1")
 
 
-def _script(variant, nx, ny, nz, return_solver, verbose, do_save=None, do_save_viz=None, **kw):
+def length_error(s, chk):
+    """The error measure the 2D scripts keep commented out beside their check
+    (Stokes2D_ve0.jl:166, Stokes2D0.jl:145, Stokes2D.jl:142): max of ||Rx||/length(Rx),
+    ||Ry||/length(Ry), ||∇V||/length(∇V). It is recovered from a check `chk` of context `s`
+    (pts_compute_res: norm_R = ||R|| / (Pmax-Pmin) * lx / sqrt(length(R)), norm_∇V likewise
+    with Vmax-Vmin and the context's default norm scale lx)."""
+    import math
+
+    nx, ny, lx = s.nx, s.ny, s.p["lx"]
+    lens = ((nx - 1) * (ny - 2), (nx - 2) * (ny - 1), nx * ny)
+    dP, dV = chk["Pmax"] - chk["Pmin"], chk["Vmax"] - chk["Vmin"]
+    norms = [chk["norm_Rx"] * dP * math.sqrt(lens[0]) / lx / lens[0],
+             chk["norm_Ry"] * dP * math.sqrt(lens[1]) / lx / lens[1],
+             chk["norm_divV"] * dV * math.sqrt(lens[2]) / lx / lens[2]]
+    if any(math.isnan(v) for v in norms):
+        return float("nan"), norms
+    return max(norms), norms
+
+
+def run_length_error(s, nt=None):
+    """The scripts' time loop with the check's commented-out error measure (`length_error`),
+    driven from the host through the context's own calls: per physical step `assign_τ!`,
+    then `while err > ε && iter <= iterMax` in blocks of PT iterations that end on the
+    multiples of nout, where the check runs (Stokes2D_ve0.jl:147-175). The damped rates
+    carry over between steps, as in the script. With it, `Stokes2D_ve0` takes the
+    iteration totals of the reference's output/out_Stokes2D_ve0.txt."""
+    import math
+
+    p = s.p
+    nt = p["nt"] if nt is None else nt
+    eps, nout, iter_max = p["eps"], int(p["nout"]), math.floor(float(p["iter_max"]))
+    iters, err = [], 2 * eps
+    for _ in range(nt):
+        err, it = 2 * eps, 0
+        if s.variant != "2d_v_damp":
+            s.assign_tau()
+        while err > eps and it <= iter_max:
+            k = min(nout - it % nout, iter_max - it + 1)  # up to the next check or past iterMax
+            s.iterate(k)
+            it += k
+            if it % nout == 0:
+                err, _ = length_error(s, s.compute_res())
+                if math.isnan(err):
+                    raise FloatingPointError("NaN")
+        iters.append(it)
+    return dict(ittot=sum(iters), iters=iters, converged=not (err > eps), err=err)
+
+
+def _script(variant, nx, ny, nz, return_solver, verbose, do_save=None, do_save_viz=None, err_form="scaled",
+            **kw):
+    if err_form not in ("scaled", "length"):
+        raise ValueError(f"err_form must be 'scaled' or 'length', not {err_form!r}")
+    if err_form == "length" and variant not in ("2d_ve_damp", "2d_v_damp"):
+        raise ValueError("err_form='length' is the damped 2D scripts' alternative check")
     s = Solver(variant, nx, ny, nz, **kw)
     s.setup_inclusion(musi=kw.get("musi", 1e-3))
     t0 = time.perf_counter()
-    res = s.run()
+    res = s.run() if err_form == "scaled" else run_length_error(s)
     s.sync()
     wall = time.perf_counter() - t0
     res["wall_s"] = wall
@@ -95,7 +148,9 @@ def Stokes2D0(nx=None, ny=None, return_solver=False, verbose=False, **kw):
 
 
 def Stokes2D_ve0(nx=None, ny=None, return_solver=False, verbose=False, **kw):
-    """scripts/previous_damp/Stokes2D_ve0.jl:82-204 (2D Maxwell VE, damped scheme, 5 steps)."""
+    """scripts/previous_damp/Stokes2D_ve0.jl:82-204 (2D Maxwell VE, damped scheme, 5 steps).
+    err_form="length" checks with the script's commented-out measure (:166), the one its
+    published totals (output/out_Stokes2D_ve0.txt) were taken with."""
     return _script("2d_ve_damp", nx or _env("NX", 511), ny or _env("NY", 511), None, return_solver, verbose, **kw)
 
 

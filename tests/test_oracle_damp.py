@@ -1,15 +1,15 @@
 """The damped ("accel. 1") 2D scheme of scripts/previous_damp/Stokes2D0.jl and
 Stokes2D_ve0.jl, restated in the oracle.
 
-The reference holds no fixture for these scripts, and its published iteration totals
-for Stokes2D_ve0 (output/out_Stokes2D_ve0.txt: 2800 iterations at 31^2, 4800 at 63^2)
-are not what the committed script computes: restated line by line it needs 4000 and
-7600 (every other restatement in the oracle reproduces its published totals, so the
-file most likely comes from an earlier version of the script). What pins the
-restatement instead is the fixed point: the damped scheme and the pinned
-Stokes2D.jl / Stokes2D_ve.jl restatements iterate the same discrete Stokes equations
-with different pseudo-time dynamics, so their converged fields must agree to the
-tolerance, step after step.
+The reference holds no fixture for these scripts. Its published iteration totals for
+Stokes2D_ve0 (output/out_Stokes2D_ve0.txt: 2800 at 31^2, 4800 at 63^2, 9000 at 127^2,
+16800 at 255^2) come from the error measure the script keeps commented out beside its
+check (Stokes2D_ve0.jl:166: norm(R)/length(R) for Rx, Ry and ∇V). Restated with that
+measure (err_form "length") the script takes exactly those totals; with its active,
+range-scaled measure (:163-165) it takes 4000 and 7600 at 31^2 and 63^2. Both forms are
+pinned here, and so is the fixed point: the damped scheme and the pinned Stokes2D.jl /
+Stokes2D_ve.jl restatements iterate the same discrete Stokes equations with different
+pseudo-time dynamics, so their converged fields must agree to the tolerance, step after step.
 """
 import numpy as np
 import pytest
@@ -47,11 +47,38 @@ def test_damped_3d_scheme_converges_to_the_3d_viscous_solution():
 
 
 def test_damped_ve_iteration_counts():
-    """Regression values of the restated Stokes2D_ve0.jl (5 steps, nout 200, ε 1e-8)."""
+    """Regression values of the restated Stokes2D_ve0.jl with its active error measure
+    (5 steps, nout 200, ε 1e-8)."""
     from oracle import scripts as S
     c = S.make("2d_ve_damp", 31, 31).run()
     assert c.iters == [800, 800, 800, 800, 800]
     assert all(h[2] <= 1e-8 for h in c.err_hist if h[1] == 800)
+
+
+@pytest.mark.parametrize("n", [31, 63, 127])
+def test_damped_ve_takes_the_published_totals_with_the_scripts_alternative_error(n):
+    """With the error measure of Stokes2D_ve0.jl:166 the restatement takes exactly the
+    iteration totals of the reference's output/out_Stokes2D_ve0.txt (line `nx ny ittot nt`)."""
+    import json
+    import os
+
+    from oracle import scripts as S
+    with open(os.path.join(os.path.dirname(__file__), "golden", "reference_output_lines.json")) as fh:
+        lines = json.load(fh)["out_Stokes2D_ve0.txt"]
+    published = {int(l.split()[0]): (int(l.split()[2]), int(l.split()[3])) for l in lines}
+    c = S.make("2d_ve_damp", n, n, err_form="length").run()
+    assert (c.ittot, len(c.iters)) == published[n]
+    # every step ends at its first check below ε
+    for it, last in enumerate(c.iters, start=1):
+        errs = [h[2] for h in c.err_hist if h[0] == it]
+        assert errs[-1] <= 1e-8 and all(e > 1e-8 for e in errs[:-1])
+
+
+def test_damped_error_form_is_checked():
+    from oracle import scripts as S
+    c = S.make("2d_ve_damp", 31, 31, err_form="sqrt")
+    with pytest.raises(ValueError):
+        c.setup().run(iter_max=200)
 
 
 def test_damped_parameters_matter():
