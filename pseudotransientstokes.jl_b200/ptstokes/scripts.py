@@ -42,6 +42,8 @@ def length_error(s, chk):
     with Vmax-Vmin and the context's default norm scale lx)."""
     import math
 
+    if s.ndim != 2:
+        raise ValueError("length_error restates the 2D scripts' measure")
     nx, ny, lx = s.nx, s.ny, s.p["lx"]
     lens = ((nx - 1) * (ny - 2), (nx - 2) * (ny - 1), nx * ny)
     dP, dV = chk["Pmax"] - chk["Pmin"], chk["Vmax"] - chk["Vmin"]

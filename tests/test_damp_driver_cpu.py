@@ -26,7 +26,7 @@ class OracleContext:
 
         self.o = S.make(variant, n, n)
         self.o.setup()
-        self.variant, self.nx, self.ny = variant, n, n
+        self.variant, self.ndim, self.nx, self.ny = variant, 2, n, n
         d = {"2d_ve_damp": dict(nt=5, nout=200, iter_max=2e5), "2d_v_damp": dict(nt=1, nout=500, iter_max=1e5)}
         self.p = dict(lx=10.0, eps=1e-8, **d[variant])
         self.calls = []
@@ -114,3 +114,12 @@ def test_err_form_is_validated_before_any_context_exists():
         scripts.Stokes2D_ve0(31, 31, err_form="sqrt")
     with pytest.raises(ValueError):
         scripts.Stokes2D_ve(31, 31, err_form="length")
+
+
+def test_length_error_refuses_a_3d_context():
+    from ptstokes.scripts import length_error
+
+    ctx = OracleContext("2d_ve_damp", 31)
+    ctx.ndim = 3
+    with pytest.raises(ValueError):
+        length_error(ctx, {})
