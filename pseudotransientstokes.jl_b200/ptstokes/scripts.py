@@ -67,6 +67,8 @@ def run_length_error(s, nt=None):
     p = s.p
     nt = p["nt"] if nt is None else nt
     eps, nout, iter_max = p["eps"], int(p["nout"]), math.floor(float(p["iter_max"]))
+    if nout < 1:
+        raise ValueError("nout must be >= 1: the check runs every nout PT iterations")
     iters, err = [], 2 * eps
     for _ in range(nt):
         err, it = 2 * eps, 0

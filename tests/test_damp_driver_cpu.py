@@ -123,3 +123,12 @@ def test_length_error_refuses_a_3d_context():
     ctx.ndim = 3
     with pytest.raises(ValueError):
         length_error(ctx, {})
+
+
+def test_host_loop_needs_a_check_cadence():
+    from ptstokes.scripts import run_length_error
+
+    ctx = OracleContext("2d_ve_damp", 31)
+    ctx.p["nout"] = 0
+    with pytest.raises(ValueError):
+        run_length_error(ctx)
