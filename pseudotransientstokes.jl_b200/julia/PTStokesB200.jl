@@ -142,6 +142,47 @@ function run!(ctx::Ctx, nt)
     return per, r[]
 end
 
+"""
+The error measure the 2D scripts keep commented out beside their check (Stokes2D_ve0.jl:166):
+max of norm(R)/length(R) over Rx, Ry and ∇V, recovered from a `compute_Res!` result `c` of an
+nx × ny context whose norms carry the default scale lx.
+"""
+function length_error(c::Check, nx, ny, lx)
+    lens = ((nx - 1) * (ny - 2), (nx - 2) * (ny - 1), nx * ny)
+    dP, dV = c.Pmax - c.Pmin, c.Vmax - c.Vmin
+    n = (c.norm_Rx * dP * sqrt(lens[1]) / lx / lens[1],
+         c.norm_Ry * dP * sqrt(lens[2]) / lx / lens[2],
+         c.norm_∇V * dV * sqrt(lens[3]) / lx / lens[3])
+    return any(isnan, n) ? NaN : maximum(n)
+end
+
+"""
+The damped 2D scripts' time loop checked with `length_error`, the measure the reference's
+output/out_Stokes2D_ve0.txt totals were taken with: per step assign_τ! (visco-elastic only),
+then `while err > ε && iter <= iterMax` in blocks that end on the multiples of nout.
+Returns the per-step iterations.
+"""
+function run_length_error!(ctx::Ctx, nx, ny; nt=5, nout=200, ε=1e-8, iterMax=2e5, lx=10.0, elastic=true)
+    nout >= 1 || throw(ArgumentError("nout must be >= 1"))
+    imax = floor(Int, iterMax)
+    per = Int[]
+    for _ in 1:nt
+        err, iter = 2ε, 0
+        elastic && assign_τ!(ctx)
+        while err > ε && iter <= imax
+            k = min(nout - iter % nout, imax - iter + 1)
+            iterate!(ctx, k)
+            iter += k
+            if iter % nout == 0
+                err = length_error(compute_Res!(ctx), nx, ny, lx)
+                isnan(err) && error("NaN")
+            end
+        end
+        push!(per, iter)
+    end
+    return per
+end
+
 # ---- batched 2D sweeps (pts_batch_*): the runme_Stokes2D_*.jl loops in one launch ----
 
 struct BatchInstance
